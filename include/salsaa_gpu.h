@@ -1,0 +1,203 @@
+/*
+ * salsaa_gpu.h — C ABI of libsalsaa_gpu.so, the B200 (sm_100a) SALSAA prover.
+ *
+ * Two tiers, both plain C (pointers, sizes, integer status codes):
+ *
+ *  1. HEXL-compatible tier.  The twenty symbols that the reference's Rust
+ *     crate binds from libhexl_wrapper.so (src/hexl/bindings.rs:1-74), with
+ *     the signatures of hexl-bindings/hexl_wrapper.cpp.  Buffers are
+ *     caller-owned HOST memory; array operations run on the GPU (one CUDA
+ *     stream and staging buffer per calling thread), scalar ones on the host.
+ *     They are thread-safe, and their tables are built once under a lock
+ *     (the reference's NTTCache, hexl_wrapper.cpp:11-32, is not).
+ *
+ *  2. Device tier.  Subroutine-granularity entry points that keep witnesses,
+ *     commitment-key tables and all intermediate state resident in HBM:
+ *     one call per prover step (src/subroutines/) or per whole proof
+ *     (src/protocol.rs:125-483).  Status 0 = success, negative = error
+ *     (salsaa_last_error() gives the message); no C++ exception crosses the ABI.
+ *
+ * All arithmetic is exact modulo q (q < 2^62; the protocol moduli are 50-bit).
+ * Randomness (CRS, witness, challenges) comes from a counter-based PRF keyed by
+ * the caller's seeds; see DESIGN.md for the stream and the proof byte layout.
+ */
+#ifndef SALSAA_GPU_H
+#define SALSAA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ===================================================================== */
+/* 1. HEXL-compatible tier (hexl-bindings/hexl_wrapper.cpp)               */
+/* ===================================================================== */
+
+/* hexl_wrapper.cpp:34-36 — a*b mod modulus */
+uint64_t multiply_mod(uint64_t a, uint64_t b, uint64_t modulus);
+/* hexl_wrapper.cpp:38-41 — (a+b) mod modulus */
+uint64_t add_mod(uint64_t a, uint64_t b, uint64_t modulus);
+/* hexl_wrapper.cpp:43-45 — (a-b) mod modulus */
+uint64_t sub_mod(uint64_t a, uint64_t b, uint64_t modulus);
+/* hexl_wrapper.cpp:61-63 — a^b mod modulus */
+uint64_t power_mod(uint64_t a, uint64_t b, uint64_t modulus);
+/* hexl_wrapper.cpp:52-54 — a^-1 mod modulus (0 if not invertible) */
+uint64_t inv_mod(uint64_t a, uint64_t modulus);
+/* hexl_wrapper.cpp:47-50 — library-owned table of n roots, psi^i at bit-reversed i */
+const uint64_t* get_roots(size_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:56-59 — library-owned table of n inverse roots, psi^-i at bit-reversed i */
+const uint64_t* get_inv_roots(size_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:65-67 — result = operand1 * operand2 (element-wise) */
+void eltwise_mult_mod(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2, uint64_t n,
+                      uint64_t modulus);
+/* hexl_wrapper.cpp:68-70 — result = operand1 * operand2 + operand3 */
+void eltwise_fma_mod(uint64_t* result, const uint64_t* operand1, uint64_t operand2, const uint64_t* operand3,
+                     uint64_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:188-196 */
+void eltwise_add_mod(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2, size_t n,
+                     uint64_t modulus);
+/* hexl_wrapper.cpp:199-207 */
+void eltwise_sub_mod(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2, size_t n,
+                     uint64_t modulus);
+/* hexl_wrapper.cpp:119-126 — any u64 input reduced mod modulus */
+void eltwise_reduce_mod(uint64_t* result, const uint64_t* operand, size_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:158-186 — same result as eltwise_reduce_mod */
+void eltwise_reduce_mod_naive(uint64_t* result, const uint64_t* operand, size_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:73-94 — negacyclic product in Z_q[X]/(X^n+1) */
+void multiply_poly(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2, uint64_t n,
+                   uint64_t modulus);
+/* hexl_wrapper.cpp:96-117 — kept for link compatibility; computes the
+ * negacyclic product (the reference's body is unused and out of bounds) */
+void polynomial_multiply_cyclotomic_mod(uint64_t* result, const uint64_t* operand1, const uint64_t* operand2,
+                                        size_t phi, uint64_t mod_q);
+/* hexl_wrapper.cpp:213-220 — forward negacyclic NTT in place (bit-reversed output) */
+void ntt_forward_in_place(uint64_t* operand, size_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:222-229 — inverse NTT in place (bit-reversed input, scaled by 1/n) */
+void ntt_inverse_in_place(uint64_t* operand, size_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:231-237 — sum mod modulus */
+uint64_t sum(const uint64_t* operand1, uint64_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:239-260 — same value as sum() */
+uint64_t sum_fast(const uint64_t* operand1, uint64_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:262-268 — sum of squares mod modulus */
+uint64_t sum_sq(const uint64_t* operand1, uint64_t n, uint64_t modulus);
+/* hexl_wrapper.cpp:271-276 — same value as sum_sq() */
+uint64_t sum_sq_fast(const uint64_t* operand1, uint64_t n, uint64_t modulus);
+
+/* ===================================================================== */
+/* 2. Device tier                                                         */
+/* ===================================================================== */
+
+/* Parameter set (src/protocol.rs:22-123). */
+typedef struct salsaa_params {
+  uint64_t d;                /* ring degree N (power of two, 4..512) */
+  uint64_t q;                /* modulus MOD_Q, q = 1 mod d, q < 2^62 */
+  uint64_t module_size;      /* MODULE_SIZE: commitment-key rows */
+  uint64_t wit_len;          /* WIT_LEN: witness width in ring elements (power of two) */
+  uint64_t init_wit_rep;     /* INIT_WIT_REP */
+  uint64_t nof_rounds;       /* NOF_ROUNDS */
+  uint64_t folding;          /* FOLDING_SCHEME: 0 = SNARK, 1 = folding */
+  uint64_t decomp_parts[12]; /* DECOMP_PARTS */
+} salsaa_params;
+
+typedef struct salsaa_ctx salsaa_ctx;       /* parameters + CRS tables on one GPU */
+typedef struct salsaa_prover salsaa_prover; /* workspace + stream for one proof in flight */
+
+/* Phase timings in milliseconds, named as the reference's t_* totals
+ * (src/protocol.rs:474-482). */
+typedef struct salsaa_timing {
+  double commit, norm1, norm2, norm3, split, projection, fold, decomp, total;
+} salsaa_timing;
+
+/* Last error message of the calling thread. */
+const char* salsaa_last_error(void);
+/* Kernel launches this library has issued since it was loaded. */
+uint64_t salsaa_kernel_launches(void);
+/* Fill *out with preset "A0".."C2", "F0".."F2" (src/protocol.rs:28-123). */
+int salsaa_params_preset(const char* name, salsaa_params* out);
+/* Proof length in bytes for a parameter set (0 if the set is invalid). */
+uint64_t salsaa_proof_size(const salsaa_params* p);
+/* Device bytes one in-flight proof needs (workspace), for admission control. */
+uint64_t salsaa_workspace_bytes(const salsaa_params* p);
+
+/* CRS::gen_crs + compute_commitment_keys (src/subroutines/crs.rs:23-72):
+ * samples the module from crs_seed and builds the key tables on `device`. */
+int salsaa_ctx_create(const salsaa_params* p, uint64_t crs_seed, int device, salsaa_ctx** out);
+void salsaa_ctx_destroy(salsaa_ctx* ctx);
+
+/* One proof slot: device workspace sized for the context's parameters and a
+ * private CUDA stream.  Slots of one context may run concurrently. */
+int salsaa_prover_create(salsaa_ctx* ctx, salsaa_prover** out);
+void salsaa_prover_destroy(salsaa_prover* pr);
+/* The slot's CUDA stream (cudaStream_t). */
+void* salsaa_prover_stream(salsaa_prover* pr);
+
+/* protocol() of src/protocol.rs:125-483, asynchronous on the slot's stream.
+ * d_witness: device pointer to init_wit_rep x wit_len x d coefficients, or
+ * NULL to sample the witness from `seed`; d_proof: device buffer of
+ * salsaa_proof_size() bytes.  No host synchronisation inside. */
+int salsaa_prover_enqueue(salsaa_prover* pr, uint64_t seed, const uint64_t* d_witness, uint8_t* d_proof);
+/* Host-buffer variant of salsaa_prover_enqueue, still asynchronous: copies
+ * h_witness (init_wit_rep x wit_len x d words; NULL = sample from seed) to
+ * the slot's workspace, proves, and copies the proof to h_proof, all on the
+ * slot's stream.  For overlap the host buffers should be page-locked. */
+int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof);
+/* 1 while the last enqueued proof runs, 0 when done, negative on error. */
+int salsaa_prover_query(salsaa_prover* pr);
+int salsaa_prover_sync(salsaa_prover* pr);
+/* Per-phase device times of the last completed proof (after sync). */
+int salsaa_prover_timing(salsaa_prover* pr, salsaa_timing* t);
+
+/* Blocking whole proof through host buffers: copies h_witness (or samples
+ * it when NULL) to the GPU, proves, copies the proof to h_proof. */
+int salsaa_prove(salsaa_ctx* ctx, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof,
+                 uint64_t proof_len);
+
+/* ---- subroutine-level entry points (device pointers, cudaStream_t) ---- */
+
+/* Batched negacyclic NTT.  incomplete = 0: `count` polynomials of n
+ * coefficients; incomplete = 1: `count` ring elements of d = 2n in the
+ * reference's IncompleteNTT layout (src/cyclotomic_ring.rs:484-556).
+ * d_in may equal d_out. */
+int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uint64_t count, uint64_t q, int inverse,
+               int incomplete, void* stream);
+
+/* parallel_dot_series_matrix with the commitment-key rows of ctx
+ * (src/arithmetic.rs:459-505): d_w is rows x width x d coefficient form;
+ * d_out receives module_size x rows ring elements (coefficient form). */
+int salsaa_commit(salsaa_ctx* ctx, const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t* d_out,
+                  void* stream);
+
+/* norm_check_1 + sum_check (src/subroutines/fast_norm_check.rs:135-199,282-320)
+ * of each row of d_w (rows x n coefficients, n a power of two >= 4) with the
+ * challenges of (seed, round, rep 0 and 1).  d_claims: rows words;
+ * d_polys: 2 x log2(n) x rows x 3 words (rep-major). */
+int salsaa_sumcheck(const uint64_t* d_w, uint64_t rows, uint64_t n, uint64_t d, uint64_t q, uint64_t seed,
+                    uint64_t round, uint64_t* d_claims, uint64_t* d_polys, void* stream);
+
+/* decompose_matrix_by_chunks (src/arithmetic.rs:1572-1593): d_w rows x width
+ * x d coefficients -> d_out (rows*parts) x width x d; *d_radix = radix. */
+int salsaa_decompose(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q, uint64_t parts,
+                     uint64_t* d_out, uint64_t* d_radix, void* stream);
+
+/* project (src/subroutines/project.rs:50-103) with the challenge of
+ * (seed, round): d_w rows x width x d -> d_out width x d. */
+int salsaa_project(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q, uint64_t seed,
+                   uint64_t round, uint64_t* d_out, void* stream);
+
+/* fold (src/subroutines/fold.rs:22-27): d_w rows x width x d coefficients,
+ * d_c rows ring challenges (coefficients) -> d_out width x d coefficients. */
+int salsaa_fold(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,
+                const uint64_t* d_c, uint64_t* d_out, void* stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

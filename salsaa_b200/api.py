@@ -1,0 +1,224 @@
+"""Host-side mirror of the reference's prover interface over the C ABI.
+
+Function names follow the reference (src/protocol.rs, src/subroutines/*,
+src/arithmetic.rs) so that tests read like its own; the arguments are device
+tensors (torch, int64 storage holding the u64 residues bit-for-bit) or numpy
+uint64 arrays for the host-buffer entry points.  Every call goes to
+libsalsaa_gpu.so; there is no CPU path here.
+"""
+import ctypes
+
+import numpy as np
+
+from . import lib
+from ._abi import SalsaaTiming
+from .params import SalsaaParams
+
+
+class SalsaaError(RuntimeError):
+    pass
+
+
+def _check(rc, what):
+    if rc:
+        msg = lib().salsaa_last_error()
+        raise SalsaaError("%s failed (%d): %s" % (what, rc, msg.decode() if msg else ""))
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise SalsaaError("no CUDA device visible: the SALSAA prover runs on the GPU only")
+    return torch
+
+
+# ---- device buffers ---------------------------------------------------------
+def to_dev(a):
+    """numpy uint64 array -> CUDA int64 tensor with identical bits."""
+    torch = _torch()
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+    return torch.from_numpy(a.view(np.int64)).cuda()
+
+
+def to_host(t):
+    """CUDA int64 tensor -> numpy uint64 array with identical bits."""
+    return t.detach().cpu().contiguous().numpy().view(np.uint64)
+
+
+def dev_empty(shape):
+    torch = _torch()
+    return torch.empty(shape, dtype=torch.int64, device="cuda")
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream():
+    torch = _torch()
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+# ---- parameter sets -----------------------------------------------------------
+def params_preset(name):
+    p = SalsaaParams()
+    _check(lib().salsaa_params_preset(name.encode(), ctypes.byref(p)), "params_preset")
+    return p
+
+
+def proof_size(params):
+    return int(lib().salsaa_proof_size(ctypes.byref(params)))
+
+
+def workspace_bytes(params):
+    return int(lib().salsaa_workspace_bytes(ctypes.byref(params)))
+
+
+# ---- context / prover -----------------------------------------------------------
+class Context:
+    """CRS::gen_crs + compute_commitment_keys on one GPU (src/subroutines/crs.rs:23-72)."""
+
+    def __init__(self, params, crs_seed=0, device=0):
+        self.params = params
+        self.crs_seed = crs_seed
+        self.device = device
+        h = ctypes.c_void_p()
+        _check(lib().salsaa_ctx_create(ctypes.byref(params), crs_seed, device, ctypes.byref(h)), "ctx_create")
+        self.h = h
+        self.proof_bytes = proof_size(params)
+
+    def close(self):
+        if self.h:
+            lib().salsaa_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def prove(self, seed, witness=None):
+        """protocol() through host buffers: returns the proof bytes (numpy uint8)."""
+        out = np.zeros(self.proof_bytes, dtype=np.uint8)
+        wp = None
+        if witness is not None:
+            witness = np.ascontiguousarray(witness, dtype=np.uint64)
+            p = self.params
+            assert witness.size == p.init_wit_rep * p.wit_len * p.d
+            wp = witness.ctypes.data_as(ctypes.c_void_p)
+        _check(lib().salsaa_prove(self.h, seed, wp, out.ctypes.data_as(ctypes.c_void_p), out.size), "prove")
+        return out
+
+    def parallel_dot_series_matrix(self, w):
+        """Commitment-key rows times the witness rows (src/arithmetic.rs:459-505).
+        w: CUDA tensor rows x width x d (coefficients) -> module_size x rows x d."""
+        rows, width, d = w.shape
+        out = dev_empty((self.params.module_size, rows, d))
+        _check(lib().salsaa_commit(self.h, _p(w), rows, width, _p(out), _stream()), "commit")
+        return out
+
+
+class Prover:
+    """One proof slot (device workspace + private stream) of a Context."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        _check(lib().salsaa_prover_create(ctx.h, ctypes.byref(h)), "prover_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().salsaa_prover_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return lib().salsaa_prover_stream(self.h)
+
+    def enqueue(self, seed, d_proof, d_witness=None):
+        _check(lib().salsaa_prover_enqueue(self.h, seed, _p(d_witness), _p(d_proof)), "prover_enqueue")
+
+    def enqueue_host(self, seed, h_proof, h_witness=None):
+        """Asynchronous prove through (preferably page-locked) host buffers."""
+        wp = None if h_witness is None else ctypes.c_void_p(h_witness.ctypes.data)
+        _check(lib().salsaa_prover_enqueue_host(self.h, seed, wp, ctypes.c_void_p(h_proof.ctypes.data)),
+               "prover_enqueue_host")
+
+    def query(self):
+        rc = lib().salsaa_prover_query(self.h)
+        if rc < 0:
+            _check(rc, "prover_query")
+        return rc
+
+    def sync(self):
+        _check(lib().salsaa_prover_sync(self.h), "prover_sync")
+
+    def timing(self):
+        t = SalsaaTiming()
+        _check(lib().salsaa_prover_timing(self.h, ctypes.byref(t)), "prover_timing")
+        return t.as_dict()
+
+
+# ---- subroutine-level entry points -------------------------------------------------
+def ntt(x, n, q, inverse=False, incomplete=False, out=None):
+    """Batched negacyclic NTT of a CUDA tensor whose last axis has n (or d) words."""
+    count = x.numel() // n
+    out = x if out is None else out
+    _check(lib().salsaa_ntt(_p(x), _p(out), n, count, q, int(inverse), int(incomplete), _stream()), "ntt")
+    return out
+
+
+def sum_check(w, d, q, seed, round_):
+    """norm_check_1 + both sum_check repetitions (src/subroutines/fast_norm_check.rs:135-320).
+    w: CUDA tensor rows x n -> (claims[rows], polys[2, log2 n, rows, 3])."""
+    rows = w.shape[0]
+    n = w.numel() // rows
+    nr = n.bit_length() - 1
+    claims = dev_empty((rows,))
+    polys = dev_empty((2, nr, rows, 3))
+    _check(lib().salsaa_sumcheck(_p(w), rows, n, d, q, seed, round_, _p(claims), _p(polys), _stream()), "sumcheck")
+    return claims, polys
+
+
+def decompose_matrix_by_chunks(w, q, parts):
+    """src/arithmetic.rs:1572-1593: rows x width x d -> ((rows*parts) x width x d, radix)."""
+    rows, width, d = w.shape
+    out = dev_empty((rows * parts, width, d))
+    radix = dev_empty((1,))
+    _check(lib().salsaa_decompose(_p(w), rows, width, d, q, parts, _p(out), _p(radix), _stream()), "decompose")
+    return out, radix
+
+
+def project(w, q, seed, round_):
+    """src/subroutines/project.rs:50-103: rows x width x d -> width x d."""
+    rows, width, d = w.shape
+    out = dev_empty((width, d))
+    _check(lib().salsaa_project(_p(w), rows, width, d, q, seed, round_, _p(out), _stream()), "project")
+    return out
+
+
+def fold(w, q, c):
+    """src/subroutines/fold.rs:22-27: rows x width x d with rows ring challenges -> width x d."""
+    rows, width, d = w.shape
+    out = dev_empty((width, d))
+    _check(lib().salsaa_fold(_p(w), rows, width, d, q, _p(c), _p(out), _stream()), "fold")
+    return out
+
+
+# ---- HEXL-compatible tier (host buffers) -------------------------------------------
+def _u64p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+def hexl_call(name, *args):
+    """Call a HEXL-compatible symbol; numpy arrays are passed as uint64*."""
+    conv = [(_u64p(a) if isinstance(a, np.ndarray) else a) for a in args]
+    return getattr(lib(), name)(*conv)

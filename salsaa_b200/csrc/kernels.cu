@@ -1,0 +1,959 @@
+// kernels.cu — the SALSAA prover kernels for sm_100a.
+//
+// Reference algorithms (paths relative to the lattice-arguments/salsaa root):
+//   CRS / commitment keys    src/subroutines/crs.rs:23-72
+//   witness sampling         src/cyclotomic_ring.rs:293-317, src/arithmetic.rs:1160-1175
+//   norm-check sumcheck      src/subroutines/fast_norm_check.rs:135-199,282-441
+//   decomposition            src/arithmetic.rs:1461-1593
+//   projection               src/subroutines/project.rs:26-103
+//   fold                     src/subroutines/fold.rs:22-27,70-75
+//   structured dot products  src/arithmetic.rs:459-536
+#include "kernels.cuh"
+
+namespace salsaa {
+
+namespace {
+
+inline int check_launch(const char* what) {
+  salsaa_count_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, what);
+}
+
+inline unsigned grid_1d(u64 work, unsigned threads, unsigned cap = 148 * 32) {
+  u64 g = (work + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
+
+// Warp + block reduction of a value mod q; result valid in thread 0.
+__device__ __forceinline__ u64 warp_add_mod(u64 v, u64 q) {
+  for (int o = 16; o > 0; o >>= 1) v = add_mod(v, __shfl_down_sync(0xffffffffu, v, o), q);
+  return v;
+}
+__device__ u64 block_add_mod(u64 v, u64 q, u64* sm /* >= 32 words */) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_add_mod(v, q);
+  __syncthreads();
+  if (lane == 0) sm[wid] = v;
+  __syncthreads();
+  v = (threadIdx.x < (unsigned)nw) ? sm[threadIdx.x] : 0;
+  if (wid == 0) v = warp_add_mod(v, q);
+  return v;
+}
+
+// Accumulate a reduced value into a global sum kept mod q.  With q < 2^50
+// and fewer than 2^13 contributions a plain 64-bit add cannot overflow and
+// the consumer reduces at the end; otherwise add modulo q with a CAS loop.
+__device__ __forceinline__ void atomic_add_mod(u64* addr, u64 v, u64 q, bool plain) {
+  if (plain) {
+    atomicAdd((unsigned long long*)addr, (unsigned long long)v);
+    return;
+  }
+  unsigned long long old = *(volatile unsigned long long*)addr, assumed;
+  do {
+    assumed = old;
+    u64 nv = add_mod((u64)assumed % q, v, q);
+    old = atomicCAS((unsigned long long*)addr, assumed, (unsigned long long)nv);
+  } while (old != assumed);
+}
+
+__device__ __forceinline__ u64 nc_challenge(const DevState* ds, u32 round, u32 rep, u64 j, u64 q) {
+  return uni_mod(prf_at(prf_key(ds->seed, domain_id(DOM_NC, round, rep)), j), q);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// CRS: MODULE_SIZE uniform ring elements (CyclotomicRing::random), and the
+// two-level power tables of the commitment-key rows (m, m^2, ..., m^L):
+//   tlo[r][lo] = m^(lo+1) as (even, odd, zeta*odd) planes,  lo < B
+//   thi[r][hi] = m^(hi*B) in slot form,                     hi < L/B
+// so that m^(i+1) = thi[i / B] * tlo[i % B].
+// ---------------------------------------------------------------------------
+__global__ void gen_crs_kernel(u64* m, u32 rows, u32 d, u64 q, u64 crs_seed) {
+  u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (u64)rows * d) return;
+  u32 r = (u32)(t / d), i = (u32)(t % d);
+  m[t] = uni_mod(prf_at(prf_key(crs_seed, domain_id(DOM_CRS, 0, r)), i), q);
+}
+
+int launch_gen_crs(u64* m_coef, u32 rows, u32 d, u64 q, u64 crs_seed, cudaStream_t st) {
+  u64 tot = (u64)rows * d;
+  gen_crs_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(m_coef, rows, d, q, crs_seed);
+  return check_launch("gen_crs");
+}
+
+// (be + X bo)^e in F_q[X]/(X^2 - z).
+__device__ void slot_pow(const ModQ& M, u64 z, u64 be, u64 bo, u64 e, u64& re, u64& ro) {
+  u64 ae = 1 % M.q, ao = 0, xe = be, xo = bo;
+  while (e) {
+    if (e & 1) slot_mul(M, ae, ao, xe, xo, z, ae, ao);
+    e >>= 1;
+    if (e) slot_mul(M, xe, xo, xe, xo, z, xe, xo);
+  }
+  re = ae;
+  ro = ao;
+}
+
+__global__ void ck_tlo_kernel(const u64* ms, u32 rows, u32 n, u32 B, ModQ M, const u64* zeta, u64* tlo) {
+  u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (u64)rows * B * n) return;
+  u32 s = (u32)(t % n);
+  u64 rl = t / n;
+  u32 lo = (u32)(rl % B), r = (u32)(rl / B);
+  const u64* m = ms + (u64)r * 2 * n;
+  u64 e, o;
+  slot_pow(M, zeta[s], m[s], m[n + s], (u64)lo + 1, e, o);
+  u64* dst = tlo + ((u64)r * B + lo) * 3 * n;
+  dst[s] = e;
+  dst[n + s] = o;
+  dst[2 * n + s] = mul_mod(M, zeta[s], o);
+}
+
+__global__ void ck_thi_kernel(const u64* ms, u32 rows, u32 n, u32 B, u32 nhi, ModQ M, const u64* zeta,
+                              u64* thi) {
+  u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (u64)rows * nhi * n) return;
+  u32 s = (u32)(t % n);
+  u64 rh = t / n;
+  u32 hi = (u32)(rh % nhi), r = (u32)(rh / nhi);
+  const u64* m = ms + (u64)r * 2 * n;
+  u64 e, o;
+  slot_pow(M, zeta[s], m[s], m[n + s], (u64)hi * B, e, o);
+  u64* dst = thi + ((u64)r * nhi + hi) * 2 * n;
+  dst[s] = e;
+  dst[n + s] = o;
+}
+
+int launch_ck_tables(const u64* m_slot, u32 rows, const NttDev& T, const ModQ& M, u64 L, u64* tlo, u64* thi,
+                     cudaStream_t st) {
+  const u32 n = T.n;
+  const u32 B = (u32)(L < CK_BLOCK ? L : CK_BLOCK);
+  const u32 nhi = (u32)(L / B);
+  u64 tot = (u64)rows * B * n;
+  ck_tlo_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(m_slot, rows, n, B, M, T.zeta, tlo);
+  int rc = check_launch("ck_tlo");
+  if (rc) return rc;
+  tot = (u64)rows * nhi * n;
+  ck_thi_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(m_slot, rows, n, B, nhi, M, T.zeta, thi);
+  return check_launch("ck_thi");
+}
+
+// ---------------------------------------------------------------------------
+// Witness: random_bounded(2) coefficients (0 w.p. 1/2, +-1 w.p. 1/4 each).
+// ---------------------------------------------------------------------------
+__global__ void gen_witness_kernel(u64* w, u32 rows, u64 per_row, u64 q, const DevState* ds) {
+  const u64 seed = ds->seed;
+  for (u32 k = 0; k < rows; k++) {
+    const u64 key = prf_key(seed, domain_id(DOM_WIT, 0, k));
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < per_row; t += (u64)gridDim.x * blockDim.x) {
+      u64 r = prf_at(key, t);
+      u64 mag = r & 1, neg = (r >> 1) & 1;
+      w[k * per_row + t] = mag ? (neg ? q - 1 : 1) : 0;
+    }
+  }
+}
+
+int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState* ds, cudaStream_t st) {
+  const u64 per_row = width * d;
+  gen_witness_kernel<<<grid_1d(per_row, 256), 256, 0, st>>>(w, rows, per_row, q, ds);
+  return check_launch("gen_witness");
+}
+
+__global__ void fill_kernel(u64* p, u64 n, u64 v) {
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (u64)gridDim.x * blockDim.x) p[t] = v;
+}
+int launch_fill(u64* p, u64 n, u64 v, cudaStream_t st) {
+  if (!n) return 0;
+  fill_kernel<<<grid_1d(n, 256), 256, 0, st>>>(p, n, v);
+  return check_launch("fill");
+}
+
+// ---------------------------------------------------------------------------
+// Norm-check sumcheck (sum_check, src/subroutines/fast_norm_check.rs:135-199)
+// for all witness rows and both amplification repetitions at once.
+//
+// Round j folds v_j (length L) into v_{j+1} = v_j[:L/2] + c_j (v_j[L/2:] -
+// v_j[:L/2]) and the round polynomial is (f0, f1, f2) = (S00, S01 - S00,
+// S11 - 2 S01 + S00) with S00 = sum v0^2, S01 = sum v0 v1, S11 = sum v1^2 over
+// the halves.  Challenges come from the PRF stream, so no host round trip
+// separates the rounds: a kernel that writes v_{j+1} also sums round j+1.
+// sums[((rep * nr + j) * rows + k) * 3 + {0,1,2}] hold S00, S01, S11.
+// ---------------------------------------------------------------------------
+constexpr u32 SC_TAIL = 4096;  // vectors this short finish in one CTA
+
+__global__ void __launch_bounds__(256) sc_first_kernel(RowSet w, u32 rows, u64 nlen, ModQ M,
+                                                       const DevState* ds, u32 round, u64* abuf,
+                                                       u64* sums, u32 nr, bool plain) {
+  __shared__ u64 red[32];
+  const u32 k = blockIdx.y;
+  const u64* x = w.p[k];
+  const u64 q4 = nlen / 4, q = M.q;
+  const u64 c0 = nc_challenge(ds, round, 0, 0, q), c1 = nc_challenge(ds, round, 1, 0, q);
+  u64* o0 = abuf + (0 * (u64)rows + k) * (nlen / 2);
+  u64* o1 = abuf + (1 * (u64)rows + k) * (nlen / 2);
+  u64 s00 = 0, s01 = 0, s11 = 0;
+  u64 t[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < q4; i += (u64)gridDim.x * blockDim.x) {
+    const u64 x0 = x[i], x1 = x[i + q4], x2 = x[i + 2 * q4], x3 = x[i + 3 * q4];
+    s00 = add_mod(s00, add_mod(mul_mod(M, x0, x0), mul_mod(M, x1, x1), q), q);
+    s01 = add_mod(s01, add_mod(mul_mod(M, x0, x2), mul_mod(M, x1, x3), q), q);
+    s11 = add_mod(s11, add_mod(mul_mod(M, x2, x2), mul_mod(M, x3, x3), q), q);
+    const u64 d0 = sub_mod(x2, x0, q), d1 = sub_mod(x3, x1, q);
+#pragma unroll
+    for (int rep = 0; rep < 2; rep++) {
+      const u64 c = rep ? c1 : c0;
+      const u64 a = add_mod(x0, mul_mod(M, c, d0), q), b = add_mod(x1, mul_mod(M, c, d1), q);
+      u64* o = rep ? o1 : o0;
+      o[i] = a;
+      o[i + q4] = b;
+      t[rep][0] = add_mod(t[rep][0], mul_mod(M, a, a), q);
+      t[rep][1] = add_mod(t[rep][1], mul_mod(M, a, b), q);
+      t[rep][2] = add_mod(t[rep][2], mul_mod(M, b, b), q);
+    }
+  }
+  u64 v[9] = {s00, s01, s11, t[0][0], t[0][1], t[0][2], t[1][0], t[1][1], t[1][2]};
+#pragma unroll 1
+  for (int qi = 0; qi < 9; qi++) {
+    u64 r = block_add_mod(v[qi], q, red);
+    if (threadIdx.x == 0) {
+      if (qi < 3) {
+        atomic_add_mod(&sums[((0 * (u64)nr + 0) * rows + k) * 3 + qi], r, q, plain);
+        atomic_add_mod(&sums[((1 * (u64)nr + 0) * rows + k) * 3 + qi], r, q, plain);
+      } else if (nr > 1) {
+        const u32 rep = (qi - 3) / 3, tq = (qi - 3) % 3;
+        atomic_add_mod(&sums[((rep * (u64)nr + 1) * rows + k) * 3 + tq], r, q, plain);
+      }
+    }
+  }
+}
+
+// v_j (length L, per (rep,row) stride sin) -> v_{j+1} (stride sout), sums of round j+1.
+__global__ void __launch_bounds__(256) sc_round_kernel(const u64* in, u64 sin, u64* out, u64 sout, u64 L,
+                                                       u32 rows, ModQ M, const DevState* ds, u32 round,
+                                                       u32 j, u64* sums, u32 nr, bool plain) {
+  __shared__ u64 red[32];
+  const u32 pair = blockIdx.y, rep = pair / rows, k = pair % rows;
+  const u64 q = M.q, q4 = L / 4;
+  const u64* x = in + (u64)pair * sin;
+  u64* y = out + (u64)pair * sout;
+  const u64 c = nc_challenge(ds, round, rep, j, q);
+  u64 a00 = 0, a01 = 0, a11 = 0;
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < q4; i += (u64)gridDim.x * blockDim.x) {
+    const u64 y0 = x[i], y1 = x[i + q4], y2 = x[i + 2 * q4], y3 = x[i + 3 * q4];
+    const u64 a = add_mod(y0, mul_mod(M, c, sub_mod(y2, y0, q)), q);
+    const u64 b = add_mod(y1, mul_mod(M, c, sub_mod(y3, y1, q)), q);
+    y[i] = a;
+    y[i + q4] = b;
+    a00 = add_mod(a00, mul_mod(M, a, a), q);
+    a01 = add_mod(a01, mul_mod(M, a, b), q);
+    a11 = add_mod(a11, mul_mod(M, b, b), q);
+  }
+  u64 v[3] = {a00, a01, a11};
+#pragma unroll 1
+  for (int qi = 0; qi < 3; qi++) {
+    u64 r = block_add_mod(v[qi], q, red);
+    if (threadIdx.x == 0) atomic_add_mod(&sums[((rep * (u64)nr + j + 1) * rows + k) * 3 + qi], r, q, plain);
+  }
+}
+
+// One CTA per (rep,row): finish all rounds from v_j (length L <= SC_TAIL).
+__global__ void __launch_bounds__(1024) sc_tail_kernel(const u64* in, u64 sin, u64 L, u32 rows, ModQ M,
+                                                       const DevState* ds, u32 round, u32 j0, u64* sums,
+                                                       u32 nr, u32 d, u64* cap) {
+  __shared__ u64 v[SC_TAIL];
+  __shared__ u64 red[32];
+  const u32 pair = blockIdx.x, rep = pair / rows, k = pair % rows;
+  const u64 q = M.q;
+  const u64* x = in + (u64)pair * sin;
+  for (u32 i = threadIdx.x; i < L; i += blockDim.x) v[i] = x[i];
+  __syncthreads();
+  u64 cur = L;
+  u32 j = j0;
+  if (cur == d)
+    for (u32 i = threadIdx.x; i < d; i += blockDim.x) cap[(u64)pair * d + i] = v[i];
+  while (cur > 1) {
+    const u64 c = nc_challenge(ds, round, rep, j, q);
+    const u64 h = cur / 2;
+    u64 a[SC_TAIL / 1024 / 2 + 1];
+    u32 cnt = 0;
+    for (u32 i = threadIdx.x; i < h; i += blockDim.x) a[cnt++] = add_mod(v[i], mul_mod(M, c, sub_mod(v[i + h], v[i], q)), q);
+    __syncthreads();
+    cnt = 0;
+    for (u32 i = threadIdx.x; i < h; i += blockDim.x) v[i] = a[cnt++];
+    __syncthreads();
+    cur = h;
+    j++;
+    if (cur == d)
+      for (u32 i = threadIdx.x; i < d; i += blockDim.x) cap[(u64)pair * d + i] = v[i];
+    if (cur >= 2) {
+      const u64 hh = cur / 2;
+      u64 s00 = 0, s01 = 0, s11 = 0;
+      for (u32 i = threadIdx.x; i < hh; i += blockDim.x) {
+        const u64 p0 = v[i], p1 = v[i + hh];
+        s00 = add_mod(s00, mul_mod(M, p0, p0), q);
+        s01 = add_mod(s01, mul_mod(M, p0, p1), q);
+        s11 = add_mod(s11, mul_mod(M, p1, p1), q);
+      }
+      u64 r0 = block_add_mod(s00, q, red);
+      u64 r1 = block_add_mod(s01, q, red);
+      u64 r2 = block_add_mod(s11, q, red);
+      if (threadIdx.x == 0) {
+        u64* s = &sums[((rep * (u64)nr + j) * rows + k) * 3];
+        s[0] = r0;
+        s[1] = r1;
+        s[2] = r2;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Round polynomials and claims from the raw sums, canonical mod q.
+__global__ void sc_finalize_kernel(const u64* sums, u32 rows, u32 nr, u64 q, u64* claims, u64* polys0,
+                                   u64* polys1) {
+  u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2ULL * nr * rows) return;
+  const u32 rep = (u32)(t / ((u64)nr * rows));
+  const u64 jk = t % ((u64)nr * rows);
+  const u64* s = sums + t * 3;
+  const u64 s00 = s[0] % q, s01 = s[1] % q, s11 = s[2] % q;
+  const u64 f0 = s00, f1 = sub_mod(s01, s00, q);
+  const u64 f2 = add_mod(sub_mod(sub_mod(s11, s01, q), s01, q), s00, q);
+  u64* o = (rep ? polys1 : polys0) + jk * 3;
+  o[0] = f0;
+  o[1] = f1;
+  o[2] = f2;
+  if (rep == 0 && jk < rows) claims[jk] = add_mod(s00, s11, q);  // round 0: sum of squares
+}
+
+int launch_sumcheck(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, const DevState* ds, u32 round,
+                    SumcheckBufs B, u64* proof_claims, u64* proof_rep0, u64* proof_rep1, cudaStream_t st) {
+  if (nlen < 4 || (nlen & (nlen - 1)) || rows == 0 || rows > MAX_WROWS)
+    return salsaa_set_error(-2, "sumcheck: bad shape");
+  const u32 nr = 63u - (u32)__builtin_clzll(nlen);
+  const bool plain = M.q < (1ULL << 50);
+  cudaError_t e = cudaMemsetAsync(B.sums, 0, 2ULL * nr * rows * 3 * sizeof(u64), st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sumcheck memset");
+  {
+    dim3 g(grid_1d(nlen / 4, 256, 1024), rows);
+    sc_first_kernel<<<g, 256, 0, st>>>(w, rows, nlen, M, ds, round, B.a, B.sums, nr, plain);
+    int rc = check_launch("sc_first");
+    if (rc) return rc;
+  }
+  // ping-pong: v_1 in a (stride nlen/2), v_2 in b (stride nlen/4), v_3 in a ...
+  u64 L = nlen / 2;
+  u32 j = 1;
+  const u64 sa = nlen / 2, sb = nlen / 4;
+  bool in_a = true;
+  while (L > SC_TAIL) {
+    const u64* in = in_a ? B.a : B.b;
+    u64* out = in_a ? B.b : B.a;
+    dim3 g(grid_1d(L / 4, 256, 1024), 2 * rows);
+    sc_round_kernel<<<g, 256, 0, st>>>(in, in_a ? sa : sb, out, in_a ? sb : sa, L, rows, M, ds, round, j, B.sums,
+                                      nr, plain);
+    int rc = check_launch("sc_round");
+    if (rc) return rc;
+    in_a = !in_a;
+    L /= 2;
+    j++;
+  }
+  sc_tail_kernel<<<2 * rows, 1024, 0, st>>>(in_a ? B.a : B.b, in_a ? sa : sb, L, rows, M, ds, round, j, B.sums,
+                                           nr, d, B.cap);
+  int rc = check_launch("sc_tail");
+  if (rc) return rc;
+  u64 tot = 2ULL * nr * rows;
+  sc_finalize_kernel<<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(B.sums, rows, nr, M.q, proof_claims,
+                                                                    proof_rep0, proof_rep1);
+  return check_launch("sc_finalize");
+}
+
+// ---------------------------------------------------------------------------
+// norm_check_3 (src/subroutines/fast_norm_check.rs:401-441).  The statement
+// row is tensor(cs[0..K]) (x) base with base = conj(tensor(cs[K..nr])), so
+// <row, w_k> = base * (the sumcheck vector after K = nr - log2 d rounds).
+// One CTA per (rep, row) computes base, both NTTs and the product; the
+// repetition's base (slot form) is kept for later commitments.
+// ---------------------------------------------------------------------------
+__device__ void blk_ntt(u64* a, u32 units, const NttDev& T, bool inverse) {
+  const u32 n = T.n, logn = T.logn, half = n >> 1, loghalf = logn - 1;
+  const u32 nbf = units << loghalf;
+  const u64 q = T.q;
+  if (!inverse) {
+    u32 logt = logn;
+    for (u32 m = 1; m < n; m <<= 1) {
+      logt--;
+      const u32 t = 1u << logt;
+      for (u32 b = threadIdx.x; b < nbf; b += blockDim.x) {
+        const u32 u = b >> loghalf, r = b & (half - 1), i = r >> logt, jj = r & (t - 1);
+        const u32 j = (u << logn) + (i << (logt + 1)) + jj;
+        const u64 U = a[j], V = mul_shoup(a[j + t], T.fwd[m + i], T.fwdp[m + i], q);
+        a[j] = add_mod(U, V, q);
+        a[j + t] = sub_mod(U, V, q);
+      }
+      __syncthreads();
+    }
+  } else {
+    u32 logt = 0;
+    for (u32 m = n; m > 1; m >>= 1) {
+      const u32 h = m >> 1, t = 1u << logt;
+      for (u32 b = threadIdx.x; b < nbf; b += blockDim.x) {
+        const u32 u = b >> loghalf, r = b & (half - 1), i = r >> logt, jj = r & (t - 1);
+        const u32 j = (u << logn) + (i << (logt + 1)) + jj;
+        const u64 U = a[j], V = a[j + t];
+        a[j] = add_mod(U, V, q);
+        a[j + t] = mul_shoup(sub_mod(U, V, q), T.inv[h + i], T.invp[h + i], q);
+      }
+      logt++;
+      __syncthreads();
+    }
+    for (u32 t = threadIdx.x; t < units * n; t += blockDim.x) a[t] = mul_shoup(a[t], T.ninv, T.ninvp, q);
+    __syncthreads();
+  }
+}
+
+__global__ void norm3_kernel(const u64* cap, u32 rows, u32 nr, NttDev T, ModQ M, const DevState* ds, u32 round,
+                             u64* rhs0, u64* rhs1, u64* base0, u64* base1) {
+  extern __shared__ u64 sm[];
+  const u32 n = T.n, d = 2 * n, logd = T.logn + 1;
+  const u32 pair = blockIdx.x, rep = pair / rows, k = pair % rows;
+  const u64 q = M.q;
+  const u32 K = nr - logd;
+  u64* ext = sm;          // d
+  u64* bs = sm + d;       // d: base, slot layout after NTT
+  u64* vs = sm + 2 * d;   // d: vector, slot layout after NTT
+  for (u32 i = threadIdx.x; i < d; i += blockDim.x) {
+    u64 v = 1 % q;
+    for (u32 b = 0; b < logd; b++) {
+      const u64 c = nc_challenge(ds, round, rep, K + b, q);
+      const u32 bit = (i >> (logd - 1 - b)) & 1;
+      v = mul_mod(M, v, bit ? c : sub_mod(1 % q, c, q));
+    }
+    ext[i] = v;
+  }
+  __syncthreads();
+  // conjugate, then de-interleave into [even | odd] for the incomplete NTT
+  for (u32 i = threadIdx.x; i < d; i += blockDim.x) {
+    u64 cv = (i == 0) ? ext[0] : (ext[d - i] == 0 ? 0 : q - ext[d - i]);
+    bs[(i & 1) * n + (i >> 1)] = cv;
+    vs[(i & 1) * n + (i >> 1)] = cap[(u64)pair * d + i];
+  }
+  __syncthreads();
+  blk_ntt(bs, 2, T, false);
+  blk_ntt(vs, 2, T, false);
+  if (k == 0) {
+    u64* bo = rep ? base1 : base0;
+    for (u32 i = threadIdx.x; i < d; i += blockDim.x) bo[i] = bs[i];
+  }
+  for (u32 s = threadIdx.x; s < n; s += blockDim.x) {
+    u64 e, o;
+    slot_mul(M, bs[s], bs[n + s], vs[s], vs[n + s], T.zeta[s], e, o);
+    ext[s] = e;
+    ext[n + s] = o;
+  }
+  __syncthreads();
+  blk_ntt(ext, 2, T, true);
+  u64* out = (rep ? rhs1 : rhs0) + (u64)k * d;
+  for (u32 i = threadIdx.x; i < d; i += blockDim.x) out[i] = ext[(i & 1) * n + (i >> 1)];
+}
+
+int launch_norm3(const u64* cap, u32 rows, u32 nr, const NttDev& T, const ModQ& M, const DevState* ds,
+                 u32 round, u64* proof_rep0, u64* proof_rep1, u64* base0, u64* base1, cudaStream_t st) {
+  const u32 d = 2 * T.n;
+  const size_t smem = 3ULL * d * sizeof(u64);
+  norm3_kernel<<<2 * rows, d < 256 ? d : 256, smem, st>>>(cap, rows, nr, T, M, ds, round, proof_rep0, proof_rep1,
+                                                          base0, base1);
+  return check_launch("norm3");
+}
+
+// ---------------------------------------------------------------------------
+// Decomposition (decompose_matrix_by_chunks, src/arithmetic.rs:1572-1593):
+// centre-lift, global bit width of the positive and negative parts, radix
+// 2^ceil(bw/parts), digit_c = ((pos >> c*rlog) & mask) - ((neg >> c*rlog) & mask),
+// output row index = row*parts + c.  The OR and the radix stay on the device.
+// ---------------------------------------------------------------------------
+__global__ void decomp_or_kernel(RowSet in, u32 rows, u64 per_row, u64 q, u64* bw_or) {
+  u64 acc = 0;
+  for (u32 k = 0; k < rows; k++) {
+    const u64* x = in.p[k];
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < per_row; t += (u64)gridDim.x * blockDim.x) {
+      const u64 v = x[t];
+      acc |= (v * 2 > q) ? q - v : v;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc |= __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc) atomicOr((unsigned long long*)bw_or, (unsigned long long)acc);
+}
+
+__device__ __forceinline__ u32 radix_log_of(u64 orv, u32 parts) {
+  const u32 bw = orv ? 64u - (u32)__clzll((long long)orv) : 0u;
+  return (bw + parts - 1) / parts;
+}
+
+__global__ void decomp_digits_kernel(RowSet in, u32 rows, u64 per_row, u64 q, u32 parts, DevState* ds, u32 didx,
+                                     u64* out, u64* proof_radix) {
+  const u32 rlog = radix_log_of(ds->bw_or[didx], parts);
+  const u64 mask = (rlog >= 64) ? ~0ULL : ((1ULL << rlog) - 1);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ds->rlog[didx] = rlog;
+    if (proof_radix) *proof_radix = 1ULL << rlog;
+  }
+  for (u32 k = 0; k < rows; k++) {
+    const u64* x = in.p[k];
+    for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < per_row; t += (u64)gridDim.x * blockDim.x) {
+      const u64 v = x[t];
+      u64 pos = 0, neg = 0;
+      if (v * 2 > q) neg = q - v;
+      else pos = v;
+      for (u32 c = 0; c < parts; c++) {
+        const u32 sh = rlog * c;
+        const u64 pd = (sh >= 64) ? 0 : ((pos >> sh) & mask);
+        const u64 nd = (sh >= 64) ? 0 : ((neg >> sh) & mask);
+        out[((u64)k * parts + c) * per_row + t] = sub_mod(pd, nd, q);
+      }
+    }
+  }
+}
+
+int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds, u64* out,
+                     u64* proof_radix, cudaStream_t st) {
+  if (parts < 1 || didx >= 16) return salsaa_set_error(-2, "decompose: bad arguments");
+  const u64 per_row = width * d;
+  cudaError_t e = cudaMemsetAsync(&ds->bw_or[didx], 0, sizeof(u64), st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "decompose memset");
+  decomp_or_kernel<<<grid_1d(per_row, 256), 256, 0, st>>>(in, rows, per_row, q, &ds->bw_or[didx]);
+  int rc = check_launch("decomp_or");
+  if (rc) return rc;
+  decomp_digits_kernel<<<grid_1d(per_row, 256), 256, 0, st>>>(in, rows, per_row, q, parts, ds, didx, out,
+                                                                proof_radix);
+  return check_launch("decomp_digits");
+}
+
+// ---------------------------------------------------------------------------
+// Projection (src/subroutines/project.rs:26-103).  J is 256 x cw with
+// entries 0 (is_zero), +1 (sign) or -1, drawn from the PRF.  Stored as two
+// bit masks per output row; cj[l] = sum_k J[k][l] feeds batch_projections.
+// ---------------------------------------------------------------------------
+constexpr u32 PROJ_H = 256;
+
+__global__ void proj_tables_kernel(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask) {
+  const u32 words = cw / 32;
+  u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (u64)PROJ_H * words) return;
+  const u32 k = (u32)(t / words), w = (u32)(t % words);
+  const u64 key = prf_key(ds->seed, domain_id(DOM_PROJ, round, 0));
+  u32 pm = 0, nm = 0;
+  for (u32 b = 0; b < 32; b++) {
+    const u64 r = prf_at(key, (u64)k * cw + w * 32 + b);
+    const u32 iz = r & 1, sg = (r >> 1) & 1;
+    if (!iz) {
+      if (sg) pm |= 1u << b;
+      else nm |= 1u << b;
+    }
+  }
+  pos_mask[t] = pm;
+  neg_mask[t] = nm;
+}
+
+__global__ void proj_cj_kernel(u32 cw, const u32* pos_mask, const u32* neg_mask, u64* cj, u64 q) {
+  u32 l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= cw) return;
+  const u32 words = cw / 32;
+  int v = 0;
+  for (u32 k = 0; k < PROJ_H; k++) {
+    v += (pos_mask[(u64)k * words + l / 32] >> (l % 32)) & 1;
+    v -= (neg_mask[(u64)k * words + l / 32] >> (l % 32)) & 1;
+  }
+  cj[l] = v >= 0 ? (u64)v % q : q - ((u64)(-v) % q);
+}
+
+int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, u64* cj, u64 q,
+                       cudaStream_t st) {
+  if (cw % 32) return salsaa_set_error(-2, "project: chunk width must be a multiple of 32");
+  u64 tot = (u64)PROJ_H * (cw / 32);
+  proj_tables_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(ds, round, cw, pos_mask, neg_mask);
+  int rc = check_launch("proj_tables");
+  if (rc) return rc;
+  if (cj) {
+    proj_cj_kernel<<<(cw + 255) / 256, 256, 0, st>>>(cw, pos_mask, neg_mask, cj, q);
+    rc = check_launch("proj_cj");
+  }
+  return rc;
+}
+
+// One CTA per (chunk, tile of KT outputs); one thread per coefficient.
+// With q < 2^52 the +-1 sums (cw terms of value < q, negatives as q - w) fit
+// in 64 bits and are reduced once.
+template <int KT, bool LAZY>
+__global__ void project_kernel(RowSet in, u64 width, u32 d, u64 q, u32 cw, u64 nch, const u32* pos_mask,
+                               const u32* neg_mask, u64* out) {
+  extern __shared__ u32 msk[];  // KT x words (pos), then KT x words (neg)
+  const u32 words = cw / 32;
+  const u64 idx = blockIdx.x;
+  const u32 i = (u32)(idx / nch);
+  const u64 j = idx % nch;
+  const u32 k0 = blockIdx.y * KT;
+  for (u32 t = threadIdx.x; t < KT * words; t += blockDim.x) {
+    const u32 kk = t / words, w = t % words;
+    msk[t] = pos_mask[(u64)(k0 + kk) * words + w];
+    msk[KT * words + t] = neg_mask[(u64)(k0 + kk) * words + w];
+  }
+  __syncthreads();
+  const u32 pos = threadIdx.x;
+  if (pos >= d) return;
+  const u64* chunk = in.p[i] + (j * cw) * d;
+  u64 acc[KT];
+#pragma unroll
+  for (int kk = 0; kk < KT; kk++) acc[kk] = 0;
+  for (u32 w = 0; w < words; w++) {
+    u32 pm[KT], nm[KT];
+#pragma unroll
+    for (int kk = 0; kk < KT; kk++) {
+      pm[kk] = msk[kk * words + w];
+      nm[kk] = msk[KT * words + kk * words + w];
+    }
+    for (u32 b = 0; b < 32; b++) {
+      const u64 x = chunk[(u64)(w * 32 + b) * d + pos];
+      const u64 nx = x ? q - x : 0;
+#pragma unroll
+      for (int kk = 0; kk < KT; kk++) {
+        u64 v = ((pm[kk] >> b) & 1) ? x : 0;
+        v = ((nm[kk] >> b) & 1) ? nx : v;
+        if (LAZY) acc[kk] += v;
+        else acc[kk] = add_mod(acc[kk], v, q);
+      }
+    }
+  }
+#pragma unroll
+  for (int kk = 0; kk < KT; kk++) out[((idx * PROJ_H) + k0 + kk) * d + pos] = LAZY ? acc[kk] % q : acc[kk];
+}
+
+int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_mask, const u32* neg_mask,
+                   u64* out, cudaStream_t st) {
+  const u32 cw = rows * PROJ_H;
+  if (rows == 0 || rows > MAX_WROWS || cw > width || width % cw)
+    return salsaa_set_error(-3, "project: chunk width exceeds witness width");
+  if (d > 1024) return salsaa_set_error(-2, "project: ring degree too large");
+  const u64 nch = width / cw;
+  constexpr int KT = 16;
+  dim3 g((unsigned)(rows * nch), PROJ_H / KT);
+  const size_t smem = 2ULL * KT * (cw / 32) * sizeof(u32);
+  const bool lazy = q < (1ULL << 52) && cw <= 4096;
+  if (lazy) project_kernel<KT, true><<<g, d, smem, st>>>(in, width, d, q, cw, nch, pos_mask, neg_mask, out);
+  else project_kernel<KT, false><<<g, d, smem, st>>>(in, width, d, q, cw, nch, pos_mask, neg_mask, out);
+  return check_launch("project");
+}
+
+// ---------------------------------------------------------------------------
+// Fold (src/subroutines/fold.rs:22-27,70-75): ternary ring challenges
+// (random_biased: q-1, 0, 1 uniformly) and new_w[i] = sum_k w_k[i] * c_k.
+// ---------------------------------------------------------------------------
+__global__ void fold_chal_kernel(const DevState* ds, u32 round, u32 rows, u32 d, u64 q, u64* c) {
+  u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (u64)rows * d) return;
+  const u64 r = prf_at(prf_key(ds->seed, domain_id(DOM_FOLD, round, 0)), t);
+  const u64 v = __umul64hi(r, 3);
+  c[t] = v == 0 ? q - 1 : (v == 1 ? 0 : 1);
+}
+
+int launch_fold_challenge(const DevState* ds, u32 round, u32 rows, u32 d, u64 q, u64* c_coef, cudaStream_t st) {
+  u64 tot = (u64)rows * d;
+  fold_chal_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(ds, round, rows, d, q, c_coef);
+  return check_launch("fold_challenge");
+}
+
+__global__ void fold_kernel(RowSet w, u32 rows, u64 width, u32 n, ModQ M, const u64* zeta, const u64* c,
+                            u64* out) {
+  const u64 tot = width * n;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u64 i = t / n;
+    const u32 s = (u32)(t % n);
+    const u64 z = zeta[s];
+    u64 ae = 0, ao = 0;
+    for (u32 k = 0; k < rows; k++) {
+      const u64* x = w.p[k] + i * 2 * n;
+      u64 e, o;
+      slot_mul(M, x[s], x[n + s], c[(u64)k * 2 * n + s], c[(u64)k * 2 * n + n + s], z, e, o);
+      ae = add_mod(ae, e, M.q);
+      ao = add_mod(ao, o, M.q);
+    }
+    out[i * 2 * n + s] = ae;
+    out[i * 2 * n + n + s] = ao;
+  }
+}
+
+int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot,
+                u64* out_slot, cudaStream_t st) {
+  fold_kernel<<<grid_1d(width * T.n, 256), 256, 0, st>>>(w_slot, rows, width, T.n, M, T.zeta, c_slot, out_slot);
+  return check_launch("fold");
+}
+
+// ---------------------------------------------------------------------------
+// Structured commitment <statement row, witness row> (parallel_dot_series_matrix,
+// src/arithmetic.rs:459-505), all rows in one pass over each witness chunk.
+//
+// Commitment-key rows: value(i) = m^(i+1) = thi[i/B] * tlo[i%B].  A CTA owns a
+// chunk of CH elements inside one B-block; each thread owns one NTT slot and
+// accumulates sum_lo tlo[lo] * w[i] lazily (25-bit limbs, no reduction), then
+// multiplies the reduced sum by thi[hi] and adds it to the global total.
+// ---------------------------------------------------------------------------
+template <int RT, int KT, bool LIMB>
+__global__ void __launch_bounds__(256) ck_commit_kernel(RowSet w, u32 rows, u32 nck, const u64* tlo,
+                                                        const u64* thi, u32 Bt, u32 nhi_t, u32 CH, ModQ M,
+                                                        const u64* zeta, u64* acc, bool plain) {
+  const u32 n = blockDim.x, s = threadIdx.x, d = 2 * n;
+  const u64 i0 = (u64)blockIdx.x * CH;
+  const u32 hi = (u32)(i0 / Bt), lo0 = (u32)(i0 % Bt);
+  const u32 r0 = blockIdx.y * RT, k0 = blockIdx.z * KT;
+  const u64 q = M.q;
+  Acc3 re[RT][KT], im[RT][KT];
+  u64 gre[RT][KT], gim[RT][KT];
+#pragma unroll
+  for (int a = 0; a < RT; a++)
+#pragma unroll
+    for (int b = 0; b < KT; b++) {
+      acc_zero(re[a][b]);
+      acc_zero(im[a][b]);
+      gre[a][b] = gim[a][b] = 0;
+    }
+  const u64* wp[KT];
+#pragma unroll
+  for (int b = 0; b < KT; b++) wp[b] = (k0 + b < rows) ? w.p[k0 + b] : w.p[k0];
+  const u64* tp[RT];
+#pragma unroll
+  for (int a = 0; a < RT; a++) tp[a] = tlo + ((u64)((r0 + a < nck) ? r0 + a : r0) * Bt + lo0) * 3 * n;
+  for (u32 e = 0; e < CH; e++) {
+    const u64 i = i0 + e;
+    u64 we[KT], wo[KT];
+#pragma unroll
+    for (int b = 0; b < KT; b++) {
+      we[b] = wp[b][i * d + s];
+      wo[b] = wp[b][i * d + n + s];
+    }
+#pragma unroll
+    for (int a = 0; a < RT; a++) {
+      const u64* t = tp[a] + (u64)e * 3 * n;
+      const u64 c = t[s], dd = t[n + s], zd = t[2 * n + s];
+      if (LIMB) {
+        u32 c1, c0, d1, d0, z1, z0;
+        split25(c, c1, c0);
+        split25(dd, d1, d0);
+        split25(zd, z1, z0);
+#pragma unroll
+        for (int b = 0; b < KT; b++) {
+          u32 e1, e0, o1, o0;
+          split25(we[b], e1, e0);
+          split25(wo[b], o1, o0);
+          acc_mac(re[a][b], e1, e0, c1, c0);
+          acc_mac(re[a][b], o1, o0, z1, z0);
+          acc_mac(im[a][b], o1, o0, c1, c0);
+          acc_mac(im[a][b], e1, e0, d1, d0);
+        }
+      } else {
+#pragma unroll
+        for (int b = 0; b < KT; b++) {
+          gre[a][b] = add_mod(gre[a][b], add_mod(mul_mod(M, we[b], c), mul_mod(M, wo[b], zd), q), q);
+          gim[a][b] = add_mod(gim[a][b], add_mod(mul_mod(M, wo[b], c), mul_mod(M, we[b], dd), q), q);
+        }
+      }
+    }
+  }
+  const u64 z = zeta[s];
+#pragma unroll
+  for (int a = 0; a < RT; a++) {
+    if (r0 + a >= nck) break;
+    const u64* th = thi + ((u64)(r0 + a) * nhi_t + hi) * d;
+    const u64 he = th[s], ho = th[n + s];
+#pragma unroll
+    for (int b = 0; b < KT; b++) {
+      if (k0 + b >= rows) break;
+      u64 e = LIMB ? acc_reduce(M, re[a][b]) : gre[a][b];
+      u64 o = LIMB ? acc_reduce(M, im[a][b]) : gim[a][b];
+      slot_mul(M, e, o, he, ho, z, e, o);
+      u64* dst = acc + ((u64)(r0 + a) * rows + k0 + b) * d;
+      atomic_add_mod(dst + s, e, q, plain);
+      atomic_add_mod(dst + n + s, o, q, plain);
+    }
+  }
+}
+
+// Scalar-structured rows: value(i) = s_hi[i/Bw] * s_lo[i%Bw]; one thread per
+// coefficient position of the slot-form witness.
+template <int RT, int KT, bool LIMB>
+__global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 nsc, const u64* s_lo,
+                                                        const u64* s_hi, u32 Bw, u32 nhi, u32 CH, ModQ M,
+                                                        u64* acc, bool plain) {
+  const u32 d = blockDim.x, p = threadIdx.x;
+  const u64 i0 = (u64)blockIdx.x * CH;
+  const u32 hi = (u32)(i0 / Bw), lo0 = (u32)(i0 % Bw);
+  const u32 r0 = blockIdx.y * RT, k0 = blockIdx.z * KT;
+  const u64 q = M.q;
+  Acc3 ac[RT][KT];
+  u64 g[RT][KT];
+#pragma unroll
+  for (int a = 0; a < RT; a++)
+#pragma unroll
+    for (int b = 0; b < KT; b++) {
+      acc_zero(ac[a][b]);
+      g[a][b] = 0;
+    }
+  const u64* wp[KT];
+#pragma unroll
+  for (int b = 0; b < KT; b++) wp[b] = (k0 + b < rows) ? w.p[k0 + b] : w.p[k0];
+  const u64* sp[RT];
+#pragma unroll
+  for (int a = 0; a < RT; a++) sp[a] = s_lo + (u64)((r0 + a < nsc) ? r0 + a : r0) * Bw + lo0;
+  for (u32 e = 0; e < CH; e++) {
+    const u64 i = i0 + e;
+    u64 x[KT];
+#pragma unroll
+    for (int b = 0; b < KT; b++) x[b] = wp[b][i * d + p];
+#pragma unroll
+    for (int a = 0; a < RT; a++) {
+      const u64 sv = sp[a][e];
+      if (LIMB) {
+        u32 s1, s0;
+        split25(sv, s1, s0);
+#pragma unroll
+        for (int b = 0; b < KT; b++) {
+          u32 x1, x0;
+          split25(x[b], x1, x0);
+          acc_mac(ac[a][b], x1, x0, s1, s0);
+        }
+      } else {
+#pragma unroll
+        for (int b = 0; b < KT; b++) g[a][b] = add_mod(g[a][b], mul_mod(M, x[b], sv), q);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < RT; a++) {
+    if (r0 + a >= nsc) break;
+    const u64 h = s_hi[(u64)(r0 + a) * nhi + hi];
+#pragma unroll
+    for (int b = 0; b < KT; b++) {
+      if (k0 + b >= rows) break;
+      u64 v = LIMB ? acc_reduce(M, ac[a][b]) : g[a][b];
+      v = mul_mod(M, v, h);
+      atomic_add_mod(acc + ((u64)(r0 + a) * rows + k0 + b) * d + p, v, q, plain);
+    }
+  }
+}
+
+// Per-call scalar tables.  TENSOR: the layer of length 2^j = width uses the
+// last j of the row's K element-index challenges (MSB first):
+// s(i) = prod_t (bit ? c : 1 - c); split at Bw into s_hi (high bits), s_lo.
+__global__ void sc_tables_kernel(const ScalarRowDesc* desc, u32 nsc, u64 width, u32 Bw, u32 nhi, ModQ M,
+                                 const DevState* ds, u64* s_lo, u64* s_hi) {
+  const u32 r = blockIdx.y;
+  const ScalarRowDesc D = desc[r];
+  const u64 q = M.q;
+  const u32 j = 63u - (u32)__clzll((long long)width);
+  const u32 b = 31u - (u32)__clz((int)Bw);
+  for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < Bw + nhi; t += gridDim.x * blockDim.x) {
+    const bool is_lo = t < Bw;
+    const u32 idx = is_lo ? t : t - Bw;
+    u64 v = 1 % q;
+    if (D.type == ROW_TENSOR) {
+      // lo bits: challenges K-b .. K-1 ; hi bits: challenges K-j .. K-b-1
+      const u32 nb = is_lo ? b : j - b;
+      const u32 first = is_lo ? D.K - b : D.K - j;
+      for (u32 u = 0; u < nb; u++) {
+        const u64 c = nc_challenge(ds, D.round, D.rep, first + u, q);
+        const u32 bit = (idx >> (nb - 1 - u)) & 1;
+        v = mul_mod(M, v, bit ? c : sub_mod(1 % q, c, q));
+      }
+    } else if (D.type == ROW_PERIODIC) {
+      v = is_lo ? D.cj[idx % D.cw] : 1 % q;
+    }
+    if (is_lo) s_lo[(u64)r * Bw + idx] = v;
+    else s_hi[(u64)r * nhi + idx] = v;
+  }
+}
+
+__global__ void commit_finalize_kernel(const u64* acc, u32 nck, u32 nsc, u32 rows, u32 n, ModQ M,
+                                       const u64* zeta, const u64* const* bases, u64* out) {
+  const u64 tot = (u64)(nck + nsc) * rows * n;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u32 s = (u32)(t % n);
+    const u64 jk = t / n;
+    const u32 j = (u32)(jk / rows);
+    const u64* a = acc + jk * 2 * n;
+    u64 e = a[s] % M.q, o = a[n + s] % M.q;
+    if (j >= nck && bases) {
+      const u64* bs = bases[j - nck];
+      if (bs) slot_mul(M, e, o, bs[s], bs[n + s], zeta[s], e, o);
+    }
+    out[jk * 2 * n + s] = e;
+    out[jk * 2 * n + n + s] = o;
+  }
+}
+
+template <int RT, int KT>
+static void launch_ck_variant(const CommitArgs& a, u32 n, u32 Bt, u32 nhi_t, u32 CH, const ModQ& M,
+                              const u64* zeta, bool plain, cudaStream_t st) {
+  dim3 g((unsigned)(a.width / CH), (a.nck + RT - 1) / RT, (a.rows + KT - 1) / KT);
+  if (M.q < (1ULL << 50))
+    ck_commit_kernel<RT, KT, true><<<g, n, 0, st>>>(a.w, a.rows, a.nck, a.tlo, a.thi, Bt, nhi_t, CH, M, zeta, a.acc,
+                                                   plain);
+  else
+    ck_commit_kernel<RT, KT, false><<<g, n, 0, st>>>(a.w, a.rows, a.nck, a.tlo, a.thi, Bt, nhi_t, CH, M, zeta,
+                                                    a.acc, plain);
+}
+
+template <int RT, int KT>
+static void launch_sc_variant(const CommitArgs& a, u32 d, u32 Bw, u32 nhi, u32 CH, const ModQ& M, bool plain,
+                              u64* acc_sc, cudaStream_t st) {
+  dim3 g((unsigned)(a.width / CH), (a.nsc + RT - 1) / RT, (a.rows + KT - 1) / KT);
+  if (M.q < (1ULL << 50))
+    sc_commit_kernel<RT, KT, true><<<g, d, 0, st>>>(a.w, a.rows, a.nsc, a.sc_lo, a.sc_hi, Bw, nhi, CH, M, acc_sc,
+                                                   plain);
+  else
+    sc_commit_kernel<RT, KT, false><<<g, d, 0, st>>>(a.w, a.rows, a.nsc, a.sc_lo, a.sc_hi, Bw, nhi, CH, M, acc_sc,
+                                                    plain);
+}
+
+int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st) {
+  const u32 n = T.n, d = 2 * n;
+  if (a.rows == 0 || a.rows > MAX_WROWS || a.width == 0 || (a.width & (a.width - 1)))
+    return salsaa_set_error(-2, "commit: bad witness shape");
+  if (d > 512) return salsaa_set_error(-2, "commit: ring degree above 512");
+  const u32 Bw = (u32)(a.width < CK_BLOCK ? a.width : CK_BLOCK);
+  const u32 nhi = (u32)(a.width / Bw);
+  // chunk: >= 32 elements, at most 4096 chunks, inside one block of either table
+  u64 CH = a.width / 4096;
+  if (CH < 32) CH = 32;
+  if (CH > Bw) CH = Bw;
+  const bool plain = M.q < (1ULL << 50) && (a.width / CH) < (1ULL << 13);
+  cudaError_t e =
+      cudaMemsetAsync(a.acc, 0, (u64)(a.nck + a.nsc) * a.rows * d * sizeof(u64), st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit memset");
+  if (a.nck) {
+    if (Bw > a.ck_bt || a.ck_bt % CH) return salsaa_set_error(-2, "commit: witness wider than the key tables");
+    if (a.rows == 1) launch_ck_variant<8, 1>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);
+    else if (a.rows == 2) launch_ck_variant<4, 2>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);
+    else launch_ck_variant<2, 4>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);
+    int rc = check_launch("ck_commit");
+    if (rc) return rc;
+  }
+  if (a.nsc) {
+    dim3 gt((Bw + nhi + 255) / 256, a.nsc);
+    sc_tables_kernel<<<gt, 256, 0, st>>>(a.sc_desc_dev, a.nsc, a.width, Bw, nhi, M, ds, a.sc_lo, a.sc_hi);
+    int rc = check_launch("sc_tables");
+    if (rc) return rc;
+    u64* acc_sc = a.acc + (u64)a.nck * a.rows * d;
+    if (a.rows == 1) launch_sc_variant<8, 1>(a, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
+    else if (a.rows == 2) launch_sc_variant<4, 2>(a, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
+    else launch_sc_variant<4, 4>(a, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
+    rc = check_launch("sc_commit");
+    if (rc) return rc;
+  }
+  const u64 tot = (u64)(a.nck + a.nsc) * a.rows * n;
+  commit_finalize_kernel<<<grid_1d(tot, 256), 256, 0, st>>>(a.acc, a.nck, a.nsc, a.rows, n, M, T.zeta,
+                                                          a.sc_base_dev, a.out_slot);
+  return check_launch("commit_finalize");
+}
+
+}  // namespace salsaa

@@ -1,0 +1,96 @@
+// kernels.cuh — launchers of the SALSAA prover kernels (sm_100a).
+//
+// Layouts in HBM (u64 words, canonical residues mod q):
+//   coefficient form  row k of a witness: width x d, element-contiguous
+//   slot form         same shape; element = [NTT_n(even coeffs) | NTT_n(odd)]
+// Witness rows are passed as a RowSet of base pointers, so the split step
+// (src/subroutines/split.rs:45-76) is a re-view of the decomposed rows and
+// never copies.
+#pragma once
+#include "common.cuh"
+#include "ntt.cuh"
+
+namespace salsaa {
+
+constexpr int MAX_WROWS = 16;  // witness rows in one call
+constexpr u32 CK_BLOCK = 2048; // two-level split of commitment-key powers
+
+struct RowSet {
+  const u64* p[MAX_WROWS];
+};
+
+// Per-proof device state that data-dependent steps write and later kernels read.
+struct DevState {
+  u64 seed;
+  u64 bw_or[16];   // decomposition: OR of centred magnitudes, per decomposition index
+  u64 rlog[16];    // decomposition: radix log2, per decomposition index
+};
+
+// ---- statement rows -------------------------------------------------------
+enum RowType : int { ROW_CK = 0, ROW_TENSOR = 1, ROW_PERIODIC = 2, ROW_ONES = 3 };
+
+// Scalar-structured row: value(i) = s_hi[i / B'] * s_lo[i % B'] (times a ring
+// base for TENSOR rows).  Tables are produced per commit call.
+struct ScalarRowDesc {
+  int type;
+  u32 round, rep;  // TENSOR: which challenge stream
+  u32 K;           // TENSOR: number of element-index challenges of the row
+  u32 cw;          // PERIODIC: period
+  const u64* cj;   // PERIODIC: cw scalars
+};
+
+// ---- launchers (all asynchronous on `st`; return 0 or a negative code) ----
+int launch_gen_crs(u64* m_coef, u32 rows, u32 d, u64 q, u64 crs_seed, cudaStream_t st);
+int launch_ck_tables(const u64* m_slot, u32 rows, const NttDev& T, const ModQ& M, u64 L, u64* tlo, u64* thi,
+                     cudaStream_t st);
+int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState* ds, cudaStream_t st);
+int launch_fill(u64* p, u64 n, u64 v, cudaStream_t st);
+
+// sumcheck of `rows` witness rows (coefficient form, length nlen each), both
+// amplification repetitions at once; see sumcheck implementation for buffers.
+struct SumcheckBufs {
+  u64* a;     // 2 * rows * nlen/2
+  u64* b;     // 2 * rows * nlen/4
+  u64* sums;  // 2 * nr * rows * 3 (zeroed by the launcher)
+  u64* cap;   // 2 * rows * d: vector after log2(width) rounds
+};
+int launch_sumcheck(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, const DevState* ds, u32 round,
+                    SumcheckBufs B, u64* proof_claims, u64* proof_rep0, u64* proof_rep1, cudaStream_t st);
+// norm_check_3 outputs: rhs (coef, into proof) and each repetition's ring base (slot).
+int launch_norm3(const u64* cap, u32 rows, u32 nr, const NttDev& T, const ModQ& M, const DevState* ds,
+                 u32 round, u64* proof_rep0, u64* proof_rep1, u64* base0, u64* base1, cudaStream_t st);
+
+int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds,
+                     u64* out, u64* proof_radix, cudaStream_t st);
+
+int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, u64* cj, u64 q,
+                       cudaStream_t st);
+int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_mask, const u32* neg_mask,
+                   u64* out, cudaStream_t st);
+
+int launch_fold_challenge(const DevState* ds, u32 round, u32 rows, u32 d, u64 q, u64* c_coef, cudaStream_t st);
+int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot,
+                u64* out_slot, cudaStream_t st);
+
+// <statement rows, witness rows> in slot form.  acc: (nck + nsc) x rows x d
+// scratch; out_slot: results in statement order given by `order`.
+struct CommitArgs {
+  RowSet w;          // slot-form witness rows
+  u32 rows;
+  u64 width;
+  u32 nck;           // commitment-key rows (statement rows 0..nck-1)
+  const u64* tlo;    // nck x ck_bt x 3n
+  const u64* thi;    // nck x ck_nhi x d
+  u32 ck_bt;         // table block: min(L, CK_BLOCK)
+  u32 ck_nhi;        // L / ck_bt
+  u32 nsc;           // scalar rows
+  const ScalarRowDesc* sc_desc_dev;  // nsc descriptors in device memory
+  const u64* const* sc_base_dev;     // nsc ring bases (slot form) or null (= 1)
+  u64* sc_lo;        // scratch nsc x CK_BLOCK
+  u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)
+  u64* acc;          // scratch (nck + nsc) x rows x d
+  u64* out_slot;     // (nck + nsc) x rows x d, statement order = CK rows then scalar rows
+};
+int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st);
+
+}  // namespace salsaa

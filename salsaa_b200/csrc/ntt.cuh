@@ -1,0 +1,47 @@
+// ntt.cuh — batched negacyclic NTT over Z_q[Y]/(Y^n + 1), HEXL conventions:
+// forward output in bit-reversed order, a[i] = A(psi^(2*bitrev(i)+1)) with psi
+// the minimal primitive 2n-th root; inverse takes bit-reversed input and
+// returns natural order scaled by 1/n (hexl-bindings/hexl_wrapper.cpp:213-229).
+//
+// "incomplete" mode transforms ring elements of R_q = Z_q[X]/(X^d+1), d = 2n,
+// between the coefficient layout and the incomplete-NTT ("slot") layout
+// [NTT_n(even coefficients) | NTT_n(odd coefficients)]
+// (src/cyclotomic_ring.rs:484-556).
+#pragma once
+#include "common.cuh"
+
+namespace salsaa {
+
+struct NttDev {
+  u64 q;
+  u32 n, logn;
+  const u64* fwd;   // bit-reversed psi^i
+  const u64* fwdp;  // Shoup companions
+  const u64* inv;   // bit-reversed psi^-i
+  const u64* invp;
+  u64 ninv, ninvp;  // 1/n mod q and its Shoup companion
+  const u64* zeta;  // shift factors NTT_n(Y) (slot order), for ring products
+  const u64* zetap;
+};
+
+// Tables for (n, q) on the current device, built once and kept for the
+// process lifetime (thread-safe).  Returns nullptr when q has no 2n-th root.
+const NttDev* ntt_tables(u32 n, u64 q);
+
+// count units of n (full) or ring elements of 2n (incomplete); in may equal out.
+int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incomplete, bool inverse,
+               cudaStream_t st);
+
+// ---- ring helpers in slot form, used by several kernels ----
+// (a_e + X a_o)(b_e + X b_o) = a_e b_e + zeta a_o b_o + X (a_o b_e + a_e b_o)
+// Inputs are taken by value, so outputs may alias them.
+__device__ __forceinline__ void slot_mul(const ModQ& M, u64 ae, u64 ao, u64 be, u64 bo, u64 z, u64& re,
+                                         u64& ro) {
+  const u64 ee = mul_mod(M, ae, be);
+  const u64 oo = mul_mod(M, mul_mod(M, ao, bo), z);
+  const u64 x = add_mod(mul_mod(M, ao, be), mul_mod(M, ae, bo), M.q);
+  re = add_mod(ee, oo, M.q);
+  ro = x;
+}
+
+}  // namespace salsaa

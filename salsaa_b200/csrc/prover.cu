@@ -1,0 +1,879 @@
+// prover.cu — device-resident SALSAA prover (src/protocol.rs:125-483) and the
+// device tier of the C ABI (include/salsaa_gpu.h).
+//
+// A proof is enqueued on one CUDA stream with no host synchronisation: every
+// challenge comes from the PRF on the device and data-dependent values (the
+// decomposition radix) stay in device memory.  The host only walks the
+// (data-independent) shapes of the protocol to place each prover message at
+// its fixed offset of the proof buffer.
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/salsaa_gpu.h"
+#include "host_math.h"
+#include "kernels.cuh"
+
+using namespace salsaa;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+int salsaa_set_error(int code, const char* msg) {
+  g_err = msg;
+  return code;
+}
+int salsaa_set_cuda_error(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return -1000 - (int)e;
+}
+extern "C" const char* salsaa_last_error(void) { return g_err.c_str(); }
+
+static std::atomic<uint64_t> g_launches{0};
+void salsaa_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+extern "C" uint64_t salsaa_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+#define TRY(x)            \
+  do {                    \
+    int _rc = (x);        \
+    if (_rc) return _rc;  \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// parameters and shapes
+// ---------------------------------------------------------------------------
+static const uint64_t Q0 = 1125899904679937ULL, Q1 = 1125899906840833ULL, Q2 = 1125899906822657ULL;
+
+extern "C" int salsaa_params_preset(const char* name, salsaa_params* out) {
+  struct Pre {
+    const char* name;
+    uint64_t d, q, ms, wl, nr, fold;
+  } pre[] = {
+      {"A0", 128, Q0, 12, 1u << 19, 8, 0},  {"A1", 256, Q1, 7, 1u << 18, 7, 0},  {"A2", 512, Q2, 4, 1u << 17, 6, 0},
+      {"B0", 128, Q0, 12, 1u << 21, 10, 0}, {"B1", 256, Q1, 7, 1u << 20, 9, 0},  {"B2", 512, Q2, 4, 1u << 19, 8, 0},
+      {"C0", 128, Q0, 12, 1u << 23, 12, 0}, {"C1", 256, Q1, 7, 1u << 22, 11, 0}, {"C2", 512, Q2, 4, 1u << 21, 10, 0},
+      {"F0", 128, Q0, 12, 1u << 17, 1, 1},  {"F1", 128, Q0, 13, 1u << 19, 1, 1}, {"F2", 128, Q0, 13, 1u << 21, 1, 1},
+  };
+  if (!name || !out) return salsaa_set_error(-1, "params_preset: null argument");
+  for (const Pre& p : pre)
+    if (!strcmp(p.name, name)) {
+      memset(out, 0, sizeof(*out));
+      out->d = p.d;
+      out->q = p.q;
+      out->module_size = p.ms;
+      out->wit_len = p.wl;
+      out->nof_rounds = p.nr;
+      out->folding = p.fold;
+      out->init_wit_rep = p.fold ? 4 : 1;
+      out->decomp_parts[0] = 1;
+      for (int i = 1; i < 12; i++) out->decomp_parts[i] = 2;
+      return 0;
+    }
+  return salsaa_set_error(-1, "params_preset: unknown name");
+}
+
+static u64 ilog2u(u64 x) { return x ? 63 - (u64)__builtin_clzll(x) : 0; }
+
+// Walk of the protocol's shapes (identical in every proof of a parameter set).
+struct Shapes {
+  bool ok = false;
+  std::string why;
+  u64 proof_words = 0;
+  u64 max_d_rows_width = 0;  // decomposition output / initial witness, rows * width
+  u64 max_nc_rows_width = 0; // norm check rows * width
+  u64 max_fp_width = 0;      // width of projected / folded rows
+  u32 max_rows = 0;          // witness rows in any call
+  u32 max_stmt = 0;          // statement rows
+  u32 nsc_total = 0;         // scalar rows pushed by the whole proof
+};
+
+static Shapes walk(const salsaa_params* p) {
+  Shapes S;
+  if (!p) {
+    S.why = "null params";
+    return S;
+  }
+  const u64 d = p->d, q = p->q;
+  if (d < 4 || d > 512 || (d & (d - 1))) {
+    S.why = "d must be a power of two in [4, 512]";
+    return S;
+  }
+  if (q < 3 || q >= (1ULL << 62) || (q - 1) % d) {
+    S.why = "q must satisfy q < 2^62 and q = 1 mod d";
+    return S;
+  }
+  if (!host::minimal_root(d, q)) {
+    S.why = "q has no primitive d-th root of unity";
+    return S;
+  }
+  const u64 L = p->wit_len;
+  if (L < 2 || (L & (L - 1))) {
+    S.why = "wit_len must be a power of two >= 2";
+    return S;
+  }
+  if (!p->module_size || p->module_size > 64 || !p->init_wit_rep || p->init_wit_rep > MAX_WROWS ||
+      p->nof_rounds > 12) {
+    S.why = "module_size, init_wit_rep or nof_rounds out of range";
+    return S;
+  }
+  u64 w = 8, Sn = p->module_size, K = p->init_wit_rep, width = L;
+  S.max_d_rows_width = K * width;
+  S.max_rows = (u32)K;
+  w += Sn * K * d;
+  for (u64 i = 0; i < p->nof_rounds; i++) {
+    const u64 parts = p->decomp_parts[i < 12 ? i : 11];
+    if (!p->folding && parts > 1) {
+      if (i == 0) {
+        S.why = "decomposition in round 0 is not supported";
+        return S;
+      }
+      w += 1 + Sn * K * parts * d;
+      K *= parts;
+      if (K * width > S.max_d_rows_width) S.max_d_rows_width = K * width;
+    }
+    if (K > MAX_WROWS) {
+      S.why = "too many witness rows";
+      return S;
+    }
+    if (K * width > S.max_nc_rows_width) S.max_nc_rows_width = K * width;
+    if (width * d < 4) {
+      S.why = "witness too short for the sumcheck";
+      return S;
+    }
+    w += K;
+    const u64 nr = ilog2u(width * d);
+    for (int rep = 0; rep < 2; rep++) {
+      w += nr * K * 3 + K * d;
+      Sn += 1;
+      S.nsc_total++;
+    }
+    if (!p->folding) {
+      w += Sn * 2 * K * d;
+      K *= 2;
+      width /= 2;
+    }
+    if (K > MAX_WROWS) {
+      S.why = "too many witness rows";
+      return S;
+    }
+    if (K > S.max_rows) S.max_rows = (u32)K;
+    const u64 cw = K * 256;
+    if (cw > width || width % cw || cw > CK_BLOCK) {
+      S.why = "projection chunk width (rows*256) exceeds the witness width";
+      return S;
+    }
+    if (width > S.max_fp_width) S.max_fp_width = width;
+    w += Sn * d;
+    w += (K + 1) * d;
+    Sn += 1;
+    w += 2 * d;
+    Sn += 1;
+    S.nsc_total += 2;
+    K = 2;
+    if (p->folding) {
+      w += 1 + Sn * K * 2 * d;
+      K *= 2;
+      if (K * width > S.max_d_rows_width) S.max_d_rows_width = K * width;
+      break;
+    }
+    if (Sn > S.max_stmt) S.max_stmt = (u32)Sn;
+  }
+  if (Sn > S.max_stmt) S.max_stmt = (u32)Sn;
+  if (K > S.max_rows) S.max_rows = (u32)K;
+  if (!p->folding) w += K * width * d;
+  S.proof_words = w;
+  S.ok = true;
+  return S;
+}
+
+extern "C" uint64_t salsaa_proof_size(const salsaa_params* p) {
+  Shapes S = walk(p);
+  return S.ok ? S.proof_words * 8 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// context: parameters + commitment-key tables
+// ---------------------------------------------------------------------------
+struct salsaa_ctx {
+  salsaa_params P;
+  u64 crs_seed;
+  int device;
+  Shapes S;
+  ModQ M;
+  const NttDev* T;
+  u32 d, n;
+  u64 L;
+  u32 ck_bt, ck_nhi;
+  u64* m_slot = nullptr;
+  u64* tlo = nullptr;
+  u64* thi = nullptr;
+  std::mutex mu;
+  salsaa_prover* blocking = nullptr;  // slot used by salsaa_prove()
+};
+
+struct DevBuf {
+  std::vector<void*> ptrs;
+  template <class T>
+  int alloc(T** p, u64 count, const char* what) {
+    void* v = nullptr;
+    cudaError_t e = cudaMalloc(&v, (count ? count : 1) * sizeof(T));
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, what);
+    ptrs.push_back(v);
+    *p = (T*)v;
+    return 0;
+  }
+  void release() {
+    for (void* v : ptrs) cudaFree(v);
+    ptrs.clear();
+  }
+};
+
+static int ctx_build(salsaa_ctx* c, DevBuf& mem) {
+  const u32 d = c->d, n = c->n;
+  const u32 ms = (u32)c->P.module_size;
+  u64* m_coef = nullptr;
+  TRY(mem.alloc(&m_coef, (u64)ms * d, "ctx: module"));
+  TRY(mem.alloc(&c->m_slot, (u64)ms * d, "ctx: module slots"));
+  TRY(mem.alloc(&c->tlo, (u64)ms * c->ck_bt * 3 * n, "ctx: key table lo"));
+  TRY(mem.alloc(&c->thi, (u64)ms * c->ck_nhi * d, "ctx: key table hi"));
+  TRY(launch_gen_crs(m_coef, ms, d, c->P.q, c->crs_seed, 0));
+  TRY(ntt_launch(m_coef, c->m_slot, ms, *c->T, true, false, 0));
+  TRY(launch_ck_tables(c->m_slot, ms, *c->T, c->M, c->L, c->tlo, c->thi, 0));
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ctx: build");
+  return 0;
+}
+
+static std::mutex g_ctx_bufs_mu;
+static std::vector<std::pair<salsaa_ctx*, DevBuf>> g_ctx_bufs;
+
+extern "C" int salsaa_ctx_create(const salsaa_params* p, uint64_t crs_seed, int device, salsaa_ctx** out) {
+  if (!out) return salsaa_set_error(-1, "ctx_create: null output");
+  *out = nullptr;
+  Shapes S = walk(p);
+  if (!S.ok) return salsaa_set_error(-1, ("ctx_create: " + S.why).c_str());
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ctx_create: cudaSetDevice");
+  salsaa_ctx* c = new (std::nothrow) salsaa_ctx;
+  if (!c) return salsaa_set_error(-1, "ctx_create: out of host memory");
+  c->P = *p;
+  c->crs_seed = crs_seed;
+  c->device = device;
+  c->S = S;
+  c->M = make_modq(p->q);
+  c->d = (u32)p->d;
+  c->n = c->d / 2;
+  c->L = p->wit_len;
+  c->ck_bt = (u32)(c->L < CK_BLOCK ? c->L : CK_BLOCK);
+  c->ck_nhi = (u32)(c->L / c->ck_bt);
+  c->T = ntt_tables(c->n, p->q);
+  if (!c->T) {
+    delete c;
+    return salsaa_set_error(-1, "ctx_create: NTT tables unavailable");
+  }
+  DevBuf mem;
+  int rc = ctx_build(c, mem);
+  if (rc) {
+    mem.release();
+    delete c;
+    return rc;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_bufs_mu);
+    g_ctx_bufs.push_back({c, mem});
+  }
+  *out = c;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// one proof in flight
+// ---------------------------------------------------------------------------
+enum Phase { PH_COMMIT = 0, PH_NORM1, PH_NORM2, PH_NORM3, PH_SPLIT, PH_PROJ, PH_FOLD, PH_DECOMP, PH_N };
+constexpr int MAX_EVENTS = 128;
+
+struct salsaa_prover {
+  salsaa_ctx* ctx;
+  cudaStream_t st = nullptr;
+  DevBuf mem;
+  DevState* ds = nullptr;
+  u64 *Dc = nullptr, *Ds = nullptr, *Fc = nullptr, *Fs = nullptr, *Pc = nullptr, *Ps = nullptr;
+  SumcheckBufs sc{};
+  u64* row_base = nullptr;  // TENSOR row bases, nsc_total x d
+  u64* row_cj = nullptr;    // PERIODIC row scalars, rounds x CK_BLOCK
+  u32 *pmask = nullptr, *nmask = nullptr;
+  u64 *c_coef = nullptr, *c_slot = nullptr;
+  ScalarRowDesc* sc_desc = nullptr;
+  const u64** sc_base = nullptr;
+  u64 *sc_lo = nullptr, *sc_hi = nullptr, *acc = nullptr, *cout = nullptr;
+  u64* header_pinned = nullptr;
+  uint8_t* own_proof = nullptr;  // for the blocking API
+  cudaEvent_t ev[MAX_EVENTS];
+  int ev_phase[MAX_EVENTS];
+  int nev = 0;
+  int last_rc = 0;
+};
+
+static int mark(salsaa_prover* pr, int phase) {
+  if (pr->nev >= MAX_EVENTS) return 0;
+  cudaError_t e = cudaEventRecord(pr->ev[pr->nev], pr->st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "event record");
+  pr->ev_phase[pr->nev++] = phase;
+  return 0;
+}
+
+extern "C" uint64_t salsaa_workspace_bytes(const salsaa_params* p) {
+  Shapes S = walk(p);
+  if (!S.ok) return 0;
+  const u64 d = p->d, L = p->wit_len;
+  u64 words = 0;
+  words += 2 * S.max_d_rows_width * d;        // Dc, Ds
+  words += 4 * S.max_fp_width * d;            // Fc, Fs, Pc, Ps
+  words += S.max_nc_rows_width * d;           // sumcheck a
+  words += S.max_nc_rows_width * d / 2;       // sumcheck b
+  words += (u64)S.nsc_total * d + p->nof_rounds * CK_BLOCK;
+  const u64 stmt = S.max_stmt + 2;
+  words += stmt * CK_BLOCK + stmt * (L / CK_BLOCK + 1);
+  words += 2 * stmt * MAX_WROWS * d;
+  return words * 8 + (S.proof_words * 8);
+}
+
+extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
+  if (!c || !out) return salsaa_set_error(-1, "prover_create: null argument");
+  *out = nullptr;
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_create: cudaSetDevice");
+  salsaa_prover* pr = new (std::nothrow) salsaa_prover;
+  if (!pr) return salsaa_set_error(-1, "prover_create: out of host memory");
+  pr->ctx = c;
+  const Shapes& S = c->S;
+  const u64 d = c->d, L = c->L;
+  auto fail = [&](int rc) {
+    pr->mem.release();
+    if (pr->st) cudaStreamDestroy(pr->st);
+    delete pr;
+    return rc;
+  };
+  e = cudaStreamCreateWithFlags(&pr->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(salsaa_set_cuda_error(e, "prover_create: stream"));
+  for (int i = 0; i < MAX_EVENTS; i++) {
+    e = cudaEventCreate(&pr->ev[i]);
+    if (e != cudaSuccess) return fail(salsaa_set_cuda_error(e, "prover_create: event"));
+  }
+  int rc = 0;
+  DevBuf& m = pr->mem;
+  const u64 stmt = S.max_stmt + 2;
+  if ((rc = m.alloc(&pr->ds, 1, "ds")) || (rc = m.alloc(&pr->Dc, S.max_d_rows_width * d, "Dc")) ||
+      (rc = m.alloc(&pr->Ds, S.max_d_rows_width * d, "Ds")) || (rc = m.alloc(&pr->Fc, S.max_fp_width * d, "Fc")) ||
+      (rc = m.alloc(&pr->Fs, S.max_fp_width * d, "Fs")) || (rc = m.alloc(&pr->Pc, S.max_fp_width * d, "Pc")) ||
+      (rc = m.alloc(&pr->Ps, S.max_fp_width * d, "Ps")) ||
+      (rc = m.alloc(&pr->sc.a, S.max_nc_rows_width * d, "sumcheck a")) ||
+      (rc = m.alloc(&pr->sc.b, S.max_nc_rows_width * d / 2 + 1, "sumcheck b")) ||
+      (rc = m.alloc(&pr->sc.sums, 2ULL * 64 * MAX_WROWS * 3, "sumcheck sums")) ||
+      (rc = m.alloc(&pr->sc.cap, 2ULL * MAX_WROWS * d, "sumcheck cap")) ||
+      (rc = m.alloc(&pr->row_base, (u64)S.nsc_total * d + 1, "row bases")) ||
+      (rc = m.alloc(&pr->row_cj, (c->P.nof_rounds + 1) * (u64)CK_BLOCK, "row cj")) ||
+      (rc = m.alloc(&pr->pmask, 256ULL * CK_BLOCK / 32, "pos mask")) ||
+      (rc = m.alloc(&pr->nmask, 256ULL * CK_BLOCK / 32, "neg mask")) ||
+      (rc = m.alloc(&pr->c_coef, (u64)MAX_WROWS * d, "fold c")) ||
+      (rc = m.alloc(&pr->c_slot, (u64)MAX_WROWS * d, "fold c slot")) ||
+      (rc = m.alloc(&pr->sc_desc, (u64)S.nsc_total + 1, "row descriptors")) ||
+      (rc = m.alloc(&pr->sc_base, (u64)S.nsc_total + 1, "row base pointers")) ||
+      (rc = m.alloc(&pr->sc_lo, stmt * CK_BLOCK, "commit s_lo")) ||
+      (rc = m.alloc(&pr->sc_hi, stmt * (L / CK_BLOCK + 1), "commit s_hi")) ||
+      (rc = m.alloc(&pr->acc, stmt * MAX_WROWS * d, "commit acc")) ||
+      (rc = m.alloc(&pr->cout, stmt * MAX_WROWS * d, "commit out")))
+    return fail(rc);
+  // Scalar statement rows of the whole proof, in push order: per round
+  // TENSOR(rep 0), TENSOR(rep 1), PERIODIC (witness_lhs), ONES (projected_lhs).
+  std::vector<ScalarRowDesc> desc;
+  std::vector<const u64*> bases;
+  {
+    u64 K = c->P.init_wit_rep, width = L;
+    for (u64 rd = 0; rd < c->P.nof_rounds; rd++) {
+      const u64 parts = c->P.decomp_parts[rd < 12 ? rd : 11];
+      if (!c->P.folding && parts > 1) K *= parts;
+      for (u32 rep = 0; rep < 2; rep++) {
+        ScalarRowDesc t{};
+        t.type = ROW_TENSOR;
+        t.round = (u32)rd;
+        t.rep = rep;
+        t.K = (u32)ilog2u(width);
+        desc.push_back(t);
+        bases.push_back(pr->row_base + (desc.size() - 1) * d);
+      }
+      if (!c->P.folding) {
+        K *= 2;
+        width /= 2;
+      }
+      ScalarRowDesc per{};
+      per.type = ROW_PERIODIC;
+      per.round = (u32)rd;
+      per.cw = (u32)(K * 256);
+      per.cj = pr->row_cj + rd * CK_BLOCK;
+      desc.push_back(per);
+      bases.push_back(nullptr);
+      ScalarRowDesc ones{};
+      ones.type = ROW_ONES;
+      ones.round = (u32)rd;
+      desc.push_back(ones);
+      bases.push_back(nullptr);
+      K = 2;
+      if (c->P.folding) break;
+    }
+  }
+  if (!desc.empty()) {
+    e = cudaMemcpy(pr->sc_desc, desc.data(), desc.size() * sizeof(ScalarRowDesc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(pr->sc_base, bases.data(), bases.size() * sizeof(u64*), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(salsaa_set_cuda_error(e, "prover_create: descriptors"));
+  }
+  e = cudaMallocHost(&pr->header_pinned, 8 * sizeof(u64));
+  if (e != cudaSuccess) return fail(salsaa_set_cuda_error(e, "prover_create: pinned header"));
+  const salsaa_params& P = c->P;
+  const u64 hdr[8] = {0x31504141534C4153ULL, P.d, P.q, P.module_size, P.wit_len, P.init_wit_rep, P.nof_rounds,
+                      P.folding};
+  memcpy(pr->header_pinned, hdr, sizeof(hdr));
+  *out = pr;
+  return 0;
+}
+
+extern "C" void salsaa_prover_destroy(salsaa_prover* pr) {
+  if (!pr) return;
+  cudaSetDevice(pr->ctx->device);
+  if (pr->st) cudaStreamSynchronize(pr->st);
+  pr->mem.release();
+  if (pr->own_proof) cudaFree(pr->own_proof);
+  if (pr->header_pinned) cudaFreeHost(pr->header_pinned);
+  for (int i = 0; i < MAX_EVENTS; i++) cudaEventDestroy(pr->ev[i]);
+  if (pr->st) cudaStreamDestroy(pr->st);
+  delete pr;
+}
+
+extern "C" void* salsaa_prover_stream(salsaa_prover* pr) { return pr ? (void*)pr->st : nullptr; }
+
+__global__ void set_seed_kernel(DevState* ds, u64 seed) { ds->seed = seed; }
+
+// <statement rows [0, nck) ++ scalar rows [sc_first, sc_first + nsc), witness rows>
+// -> coefficient-form ring elements at proof_out, row-major (statement, witness).
+static int commit_rows(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width, u32 nck, u32 sc_first, u32 nsc,
+                       u64* proof_out) {
+  salsaa_ctx* c = pr->ctx;
+  CommitArgs a{};
+  a.w = ws;
+  a.rows = rows;
+  a.width = width;
+  a.nck = nck;
+  a.tlo = c->tlo;
+  a.thi = c->thi;
+  a.ck_bt = c->ck_bt;
+  a.ck_nhi = c->ck_nhi;
+  a.nsc = nsc;
+  a.sc_desc_dev = pr->sc_desc + sc_first;
+  a.sc_base_dev = pr->sc_base + sc_first;
+  a.sc_lo = pr->sc_lo;
+  a.sc_hi = pr->sc_hi;
+  a.acc = pr->acc;
+  a.out_slot = pr->cout;
+  TRY(launch_commit(a, *c->T, c->M, pr->ds, pr->st));
+  return ntt_launch(pr->cout, proof_out, (u64)(nck + nsc) * rows, *c->T, true, true, pr->st);
+}
+
+static RowSet rows_of(const u64* base, u32 rows, u64 width, u32 d) {
+  RowSet r{};
+  for (u32 k = 0; k < rows; k++) r.p[k] = base + (u64)k * width * d;
+  return r;
+}
+
+static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* proof) {
+  salsaa_ctx* c = pr->ctx;
+  const salsaa_params& P = c->P;
+  const u32 d = c->d, ms = (u32)P.module_size;
+  const u64 q = P.q, L = c->L;
+  const ModQ& M = c->M;
+  const NttDev& T = *c->T;
+  cudaStream_t st = pr->st;
+  pr->nev = 0;
+  u64 cur = 0;
+  TRY(mark(pr, PH_COMMIT));
+  cudaError_t e = cudaMemcpyAsync(proof, pr->header_pinned, 8 * sizeof(u64), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: header");
+  cur = 8;
+  set_seed_kernel<<<1, 1, 0, st>>>(pr->ds, seed);
+  salsaa_count_launch();
+  u32 K = (u32)P.init_wit_rep;
+  u64 width = L;
+  RowSet Wc, Ws;
+  const u64* wbase = d_witness;
+  if (!wbase) {
+    TRY(launch_gen_witness(pr->Dc, K, width, d, q, pr->ds, st));
+    wbase = pr->Dc;
+  }
+  Wc = rows_of(wbase, K, width, d);
+  TRY(ntt_launch(wbase, pr->Ds, (u64)K * width, T, true, false, st));
+  Ws = rows_of(pr->Ds, K, width, d);
+  // commitment: parallel_dot_series_matrix(crs.ck, witness), src/protocol.rs:138
+  TRY(commit_rows(pr, Ws, K, width, ms, 0, 0, proof + cur));
+  cur += (u64)ms * K * d;
+  u32 nsc = 0, didx = 0;
+  for (u32 rd = 0; rd < P.nof_rounds; rd++) {
+    const u32 parts = (u32)P.decomp_parts[rd < 12 ? rd : 11];
+    if (!P.folding && parts > 1) {
+      // decomp_ell (src/subroutines/decomp.rs:32-67)
+      TRY(mark(pr, PH_DECOMP));
+      TRY(launch_decompose(Wc, K, width, d, q, parts, didx++, pr->ds, pr->Dc, proof + cur, st));
+      cur += 1;
+      K *= parts;
+      TRY(ntt_launch(pr->Dc, pr->Ds, (u64)K * width, T, true, false, st));
+      Wc = rows_of(pr->Dc, K, width, d);
+      Ws = rows_of(pr->Ds, K, width, d);
+      TRY(commit_rows(pr, Ws, K, width, ms, 0, nsc, proof + cur));
+      cur += (u64)(ms + nsc) * K * d;
+    }
+    // norm_check_1 / norm_check_2 (x2) / norm_check_3 (x2), src/protocol.rs:206-259
+    TRY(mark(pr, PH_NORM2));
+    const u64 nr = ilog2u(width * d);
+    u64* claims = proof + cur;
+    cur += K;
+    u64* polys0 = proof + cur;
+    u64* rhs0 = polys0 + nr * K * 3;
+    u64* polys1 = rhs0 + (u64)K * d;
+    u64* rhs1 = polys1 + nr * K * 3;
+    cur = (u64)(rhs1 + (u64)K * d - proof);
+    TRY(launch_sumcheck(Wc, K, width * d, d, M, pr->ds, rd, pr->sc, claims, polys0, polys1, st));
+    TRY(mark(pr, PH_NORM3));
+    TRY(launch_norm3(pr->sc.cap, K, (u32)nr, T, M, pr->ds, rd, rhs0, rhs1, pr->row_base + (u64)nsc * d,
+                     pr->row_base + (u64)(nsc + 1) * d, st));
+    nsc += 2;
+    if (!P.folding) {
+      // split (src/subroutines/split.rs:45-76): rows L_0..L_{K-1}, R_0..R_{K-1}
+      TRY(mark(pr, PH_SPLIT));
+      const u64 hw = width / 2;
+      RowSet nc{}, ns{};
+      for (u32 k = 0; k < K; k++) {
+        nc.p[k] = Wc.p[k];
+        nc.p[K + k] = Wc.p[k] + hw * d;
+        ns.p[k] = Ws.p[k];
+        ns.p[K + k] = Ws.p[k] + hw * d;
+      }
+      Wc = nc;
+      Ws = ns;
+      K *= 2;
+      width = hw;
+      TRY(commit_rows(pr, Ws, K, width, ms, 0, nsc, proof + cur));
+      cur += (u64)(ms + nsc) * K * d;
+    }
+    // project (src/subroutines/project.rs:50-103) and its commitment
+    TRY(mark(pr, PH_PROJ));
+    const u32 cw = K * 256;
+    u64* cj = pr->row_cj + (u64)rd * CK_BLOCK;
+    TRY(launch_proj_tables(pr->ds, rd, cw, pr->pmask, pr->nmask, cj, q, st));
+    TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Pc, st));
+    TRY(ntt_launch(pr->Pc, pr->Ps, width, T, true, false, st));
+    RowSet Pr = rows_of(pr->Ps, 1, width, d);
+    TRY(commit_rows(pr, Pr, 1, width, ms, 0, nsc, proof + cur));
+    cur += (u64)(ms + nsc) * d;
+    // batch_projections (src/subroutines/project.rs:131-203): witness_rhs, projection_rhs
+    TRY(commit_rows(pr, Ws, K, width, 0, nsc, 1, proof + cur));
+    cur += (u64)K * d;
+    TRY(commit_rows(pr, Pr, 1, width, 0, nsc + 1, 1, proof + cur));
+    cur += d;
+    nsc += 1;  // witness_lhs joins the statement
+    // fold (src/subroutines/fold.rs:22-27)
+    TRY(mark(pr, PH_FOLD));
+    TRY(launch_fold_challenge(pr->ds, rd, K, d, q, pr->c_coef, st));
+    TRY(ntt_launch(pr->c_coef, pr->c_slot, K, T, true, false, st));
+    TRY(launch_fold(Ws, K, width, T, M, pr->c_slot, pr->Fs, st));
+    TRY(ntt_launch(pr->Fs, pr->Fc, width, T, true, true, st));
+    // send_cross_terms_before_join (src/subroutines/project.rs:229-245)
+    RowSet Fr = rows_of(pr->Fs, 1, width, d);
+    TRY(commit_rows(pr, Fr, 1, width, 0, nsc + 1 - 1 + 1, 1, proof + cur));  // l0 = <projected_lhs, folded>
+    cur += d;
+    TRY(commit_rows(pr, Pr, 1, width, 0, nsc - 1, 1, proof + cur));  // l1 = <witness_lhs, projected>
+    cur += d;
+    nsc += 1;  // projected_lhs joins the statement
+    // join: witness = [folded, projected]
+    K = 2;
+    Wc = RowSet{};
+    Wc.p[0] = pr->Fc;
+    Wc.p[1] = pr->Pc;
+    Ws = RowSet{};
+    Ws.p[0] = pr->Fs;
+    Ws.p[1] = pr->Ps;
+    if (P.folding) {
+      TRY(mark(pr, PH_DECOMP));
+      TRY(launch_decompose(Wc, K, width, d, q, 2, didx++, pr->ds, pr->Dc, proof + cur, st));
+      cur += 1;
+      K *= 2;
+      TRY(ntt_launch(pr->Dc, pr->Ds, (u64)K * width, T, true, false, st));
+      Ws = rows_of(pr->Ds, K, width, d);
+      TRY(commit_rows(pr, Ws, K, width, ms, 0, nsc, proof + cur));
+      cur += (u64)(ms + nsc) * K * d;
+      break;
+    }
+  }
+  if (!P.folding) {
+    for (u32 k = 0; k < K; k++) {
+      e = cudaMemcpyAsync(proof + cur, Wc.p[k], width * d * sizeof(u64), cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: final witness");
+      cur += width * d;
+    }
+  }
+  TRY(mark(pr, PH_N));
+  if (cur != c->S.proof_words) return salsaa_set_error(-9, "enqueue: proof layout mismatch");
+  return 0;
+}
+
+extern "C" int salsaa_prover_enqueue(salsaa_prover* pr, uint64_t seed, const uint64_t* d_witness,
+                                     uint8_t* d_proof) {
+  if (!pr || !d_proof) return salsaa_set_error(-1, "prover_enqueue: null argument");
+  if (((uintptr_t)d_proof) & 7) return salsaa_set_error(-1, "prover_enqueue: proof buffer not 8-byte aligned");
+  cudaError_t e = cudaSetDevice(pr->ctx->device);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue: cudaSetDevice");
+  pr->last_rc = enqueue_impl(pr, seed, d_witness, (u64*)d_proof);
+  return pr->last_rc;
+}
+
+extern "C" int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, const uint64_t* h_witness,
+                                          uint8_t* h_proof) {
+  if (!pr || !h_proof) return salsaa_set_error(-1, "prover_enqueue_host: null argument");
+  salsaa_ctx* c = pr->ctx;
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host: cudaSetDevice");
+  const u64 need = c->S.proof_words * 8;
+  if (!pr->own_proof) {
+    e = cudaMalloc(&pr->own_proof, need);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host: proof buffer");
+  }
+  const u64* dw = nullptr;
+  if (h_witness) {
+    const u64 bytes = c->P.init_wit_rep * c->L * c->d * sizeof(u64);
+    e = cudaMemcpyAsync(pr->Dc, h_witness, bytes, cudaMemcpyHostToDevice, pr->st);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host: witness upload");
+    dw = pr->Dc;
+  }
+  pr->last_rc = enqueue_impl(pr, seed, dw, (u64*)pr->own_proof);
+  if (pr->last_rc) return pr->last_rc;
+  e = cudaMemcpyAsync(h_proof, pr->own_proof, need, cudaMemcpyDeviceToHost, pr->st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host: proof download");
+  return 0;
+}
+
+extern "C" int salsaa_prover_query(salsaa_prover* pr) {
+  if (!pr) return salsaa_set_error(-1, "prover_query: null argument");
+  if (pr->last_rc) return pr->last_rc;
+  cudaError_t e = cudaStreamQuery(pr->st);
+  if (e == cudaErrorNotReady) return 1;
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_query");
+  return 0;
+}
+
+extern "C" int salsaa_prover_sync(salsaa_prover* pr) {
+  if (!pr) return salsaa_set_error(-1, "prover_sync: null argument");
+  cudaError_t e = cudaStreamSynchronize(pr->st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_sync");
+  return pr->last_rc;
+}
+
+extern "C" int salsaa_prover_timing(salsaa_prover* pr, salsaa_timing* t) {
+  if (!pr || !t) return salsaa_set_error(-1, "prover_timing: null argument");
+  double ph[PH_N] = {0};
+  double total = 0;
+  for (int i = 0; i + 1 < pr->nev; i++) {
+    float ms = 0;
+    cudaError_t e = cudaEventElapsedTime(&ms, pr->ev[i], pr->ev[i + 1]);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_timing");
+    if (pr->ev_phase[i] < PH_N) ph[pr->ev_phase[i]] += ms;
+    total += ms;
+  }
+  t->commit = ph[PH_COMMIT];
+  t->norm1 = ph[PH_NORM1];
+  t->norm2 = ph[PH_NORM2];
+  t->norm3 = ph[PH_NORM3];
+  t->split = ph[PH_SPLIT];
+  t->projection = ph[PH_PROJ];
+  t->fold = ph[PH_FOLD];
+  t->decomp = ph[PH_DECOMP];
+  t->total = total;
+  return 0;
+}
+
+extern "C" int salsaa_prove(salsaa_ctx* c, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof,
+                            uint64_t proof_len) {
+  if (!c || !h_proof) return salsaa_set_error(-1, "prove: null argument");
+  const u64 need = c->S.proof_words * 8;
+  if (proof_len < need) return salsaa_set_error(-2, "prove: proof buffer too small");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prove: cudaSetDevice");
+  if (!c->blocking) {
+    TRY(salsaa_prover_create(c, &c->blocking));
+    e = cudaMalloc(&c->blocking->own_proof, need);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prove: proof buffer");
+  }
+  salsaa_prover* pr = c->blocking;
+  const u64* dw = nullptr;
+  if (h_witness) {
+    const u64 bytes = c->P.init_wit_rep * c->L * c->d * sizeof(u64);
+    e = cudaMemcpyAsync(pr->Dc, h_witness, bytes, cudaMemcpyHostToDevice, pr->st);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prove: witness upload");
+    dw = pr->Dc;
+  }
+  TRY(salsaa_prover_enqueue(pr, seed, dw, pr->own_proof));
+  e = cudaMemcpyAsync(h_proof, pr->own_proof, need, cudaMemcpyDeviceToHost, pr->st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prove: proof download");
+  return salsaa_prover_sync(pr);
+}
+
+extern "C" void salsaa_ctx_destroy(salsaa_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->blocking) salsaa_prover_destroy(c->blocking);
+  std::lock_guard<std::mutex> lk(g_ctx_bufs_mu);
+  for (size_t i = 0; i < g_ctx_bufs.size(); i++)
+    if (g_ctx_bufs[i].first == c) {
+      g_ctx_bufs[i].second.release();
+      g_ctx_bufs.erase(g_ctx_bufs.begin() + i);
+      break;
+    }
+  delete c;
+}
+
+// ---------------------------------------------------------------------------
+// subroutine-level entry points (stream-ordered temporary allocations)
+// ---------------------------------------------------------------------------
+namespace {
+struct Tmp {
+  cudaStream_t st;
+  std::vector<void*> v;
+  explicit Tmp(cudaStream_t s) : st(s) {}
+  template <class T>
+  int get(T** p, u64 count) {
+    void* x = nullptr;
+    cudaError_t e = cudaMallocAsync(&x, (count ? count : 1) * sizeof(T), st);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "temporary allocation");
+    v.push_back(x);
+    *p = (T*)x;
+    return 0;
+  }
+  ~Tmp() {
+    for (void* x : v) cudaFreeAsync(x, st);
+  }
+};
+}  // namespace
+
+extern "C" int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uint64_t count, uint64_t q,
+                          int inverse, int incomplete, void* stream) {
+  if (!d_in || !d_out) return salsaa_set_error(-1, "ntt: null pointer");
+  const u64 nn = incomplete ? n / 2 : n;
+  if (incomplete && (n < 4 || n % 2)) return salsaa_set_error(-1, "ntt: incomplete mode needs even d >= 4");
+  const NttDev* T = ntt_tables((u32)nn, q);
+  if (!T || nn > 8192) return salsaa_set_error(-1, "ntt: no NTT for (n, q)");
+  return ntt_launch(d_in, d_out, count, *T, incomplete != 0, inverse != 0, (cudaStream_t)stream);
+}
+
+extern "C" int salsaa_commit(salsaa_ctx* c, const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t* d_out,
+                             void* stream) {
+  if (!c || !d_w || !d_out) return salsaa_set_error(-1, "commit: null argument");
+  if (rows == 0 || rows > (u64)MAX_WROWS || width == 0 || width > c->L || (width & (width - 1)))
+    return salsaa_set_error(-2, "commit: bad witness shape");
+  cudaStream_t st = (cudaStream_t)stream;
+  const u32 d = c->d, ms = (u32)c->P.module_size;
+  Tmp t(st);
+  u64 *ws, *acc, *cout;
+  DevState* ds;
+  TRY(t.get(&ws, rows * width * d));
+  TRY(t.get(&acc, (u64)ms * rows * d));
+  TRY(t.get(&cout, (u64)ms * rows * d));
+  TRY(t.get(&ds, 1));
+  TRY(ntt_launch(d_w, ws, rows * width, *c->T, true, false, st));
+  CommitArgs a{};
+  a.w = rows_of(ws, (u32)rows, width, d);
+  a.rows = (u32)rows;
+  a.width = width;
+  a.nck = ms;
+  a.tlo = c->tlo;
+  a.thi = c->thi;
+  a.ck_bt = c->ck_bt;
+  a.ck_nhi = c->ck_nhi;
+  a.acc = acc;
+  a.out_slot = cout;
+  TRY(launch_commit(a, *c->T, c->M, ds, st));
+  return ntt_launch(cout, d_out, (u64)ms * rows, *c->T, true, true, st);
+}
+
+extern "C" int salsaa_sumcheck(const uint64_t* d_w, uint64_t rows, uint64_t n, uint64_t d, uint64_t q,
+                               uint64_t seed, uint64_t round, uint64_t* d_claims, uint64_t* d_polys,
+                               void* stream) {
+  if (!d_w || !d_claims || !d_polys) return salsaa_set_error(-1, "sumcheck: null argument");
+  if (rows == 0 || rows > (u64)MAX_WROWS || n < 4 || (n & (n - 1)) || d == 0 || n % d)
+    return salsaa_set_error(-2, "sumcheck: bad shape");
+  if (q < 3 || q >= (1ULL << 62)) return salsaa_set_error(-2, "sumcheck: bad modulus");
+  cudaStream_t st = (cudaStream_t)stream;
+  Tmp t(st);
+  SumcheckBufs B{};
+  DevState* ds;
+  TRY(t.get(&B.a, rows * n));
+  TRY(t.get(&B.b, rows * n / 2));
+  TRY(t.get(&B.sums, 2ULL * 64 * rows * 3));
+  TRY(t.get(&B.cap, 2ULL * rows * d));
+  TRY(t.get(&ds, 1));
+  set_seed_kernel<<<1, 1, 0, st>>>(ds, seed);
+  const u64 nr = ilog2u(n);
+  RowSet w = rows_of(d_w, (u32)rows, n / d, (u32)d);
+  return launch_sumcheck(w, (u32)rows, n, (u32)d, make_modq(q), ds, (u32)round, B, d_claims, d_polys,
+                         d_polys + nr * rows * 3, st);
+}
+
+extern "C" int salsaa_decompose(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,
+                                uint64_t parts, uint64_t* d_out, uint64_t* d_radix, void* stream) {
+  if (!d_w || !d_out || !d_radix) return salsaa_set_error(-1, "decompose: null argument");
+  if (rows == 0 || rows > (u64)MAX_WROWS || parts == 0 || parts > 64) return salsaa_set_error(-2, "decompose: bad shape");
+  cudaStream_t st = (cudaStream_t)stream;
+  Tmp t(st);
+  DevState* ds;
+  TRY(t.get(&ds, 1));
+  RowSet w = rows_of(d_w, (u32)rows, width, (u32)d);
+  return launch_decompose(w, (u32)rows, width, (u32)d, q, (u32)parts, 0, ds, d_out, d_radix, st);
+}
+
+extern "C" int salsaa_project(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,
+                              uint64_t seed, uint64_t round, uint64_t* d_out, void* stream) {
+  if (!d_w || !d_out) return salsaa_set_error(-1, "project: null argument");
+  const u64 cw = rows * 256;
+  if (rows == 0 || rows > (u64)MAX_WROWS || cw > width || width % cw || cw > CK_BLOCK)
+    return salsaa_set_error(-3, "project: chunk width (rows*256) exceeds the witness width");
+  cudaStream_t st = (cudaStream_t)stream;
+  Tmp t(st);
+  DevState* ds;
+  u32 *pm, *nm;
+  TRY(t.get(&ds, 1));
+  TRY(t.get(&pm, 256 * cw / 32));
+  TRY(t.get(&nm, 256 * cw / 32));
+  set_seed_kernel<<<1, 1, 0, st>>>(ds, seed);
+  TRY(launch_proj_tables(ds, (u32)round, (u32)cw, pm, nm, nullptr, q, st));
+  RowSet w = rows_of(d_w, (u32)rows, width, (u32)d);
+  return launch_project(w, (u32)rows, width, (u32)d, q, pm, nm, d_out, st);
+}
+
+extern "C" int salsaa_fold(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,
+                           const uint64_t* d_c, uint64_t* d_out, void* stream) {
+  if (!d_w || !d_c || !d_out) return salsaa_set_error(-1, "fold: null argument");
+  if (rows == 0 || rows > (u64)MAX_WROWS || d < 4 || (d & (d - 1))) return salsaa_set_error(-2, "fold: bad shape");
+  const NttDev* T = ntt_tables((u32)(d / 2), q);
+  if (!T) return salsaa_set_error(-1, "fold: no NTT for (d, q)");
+  cudaStream_t st = (cudaStream_t)stream;
+  Tmp t(st);
+  u64 *ws, *cs, *fs;
+  TRY(t.get(&ws, rows * width * d));
+  TRY(t.get(&cs, rows * d));
+  TRY(t.get(&fs, width * d));
+  TRY(ntt_launch(d_w, ws, rows * width, *T, true, false, st));
+  TRY(ntt_launch(d_c, cs, rows, *T, true, false, st));
+  TRY(launch_fold(rows_of(ws, (u32)rows, width, (u32)d), (u32)rows, width, *T, make_modq(q), cs, fs, st));
+  return ntt_launch(fs, d_out, width, *T, true, true, st);
+}

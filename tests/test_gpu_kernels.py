@@ -1,0 +1,200 @@
+"""CUDA kernels against the CPU oracle, bit-exact, through the C ABI."""
+import numpy as np
+import pytest
+
+from helpers import fold_challenge, proj_challenge, rand_mod, small_signed
+from salsaa_b200 import params as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api(gpu_lib, cuda):
+    from salsaa_b200 import api as A
+    return A
+
+
+@pytest.mark.parametrize("n,q", [(2, 17), (8, 65537), (64, P.Q62), (128, P.Q62), (256, P.Q62), (1024, P.Q62),
+                                 (64, P.Q0), (128, P.Q1), (256, P.Q2), (4096, P.Q62)])
+def test_ntt_full(api, oracle, n, q):
+    rng = np.random.default_rng(n)
+    x = rand_mod(rng, (37, n), q)
+    want = oracle.ntt_forward(x, q)
+    d = api.to_dev(x)
+    api.ntt(d, n, q)
+    assert np.array_equal(api.to_host(d), want)
+    api.ntt(d, n, q, inverse=True)
+    assert np.array_equal(api.to_host(d), x)
+
+
+@pytest.mark.parametrize("d,q", [(4, 17), (16, P.Q0), (128, P.Q0), (256, P.Q1), (512, P.Q2), (128, P.Q62)])
+def test_ntt_incomplete(api, oracle, d, q):
+    rng = np.random.default_rng(d)
+    x = rand_mod(rng, (53, d), q)
+    want = oracle.ring_to_slot(x, q)
+    t = api.to_dev(x)
+    out = api.dev_empty(t.shape)
+    api.ntt(t, d, q, incomplete=True, out=out)
+    assert np.array_equal(api.to_host(out), want)
+    api.ntt(out, d, q, inverse=True, incomplete=True)
+    assert np.array_equal(api.to_host(out), x)
+
+
+def test_ntt_large_batch(api, oracle):
+    q, n = P.Q62, 1024
+    rng = np.random.default_rng(9)
+    x = rand_mod(rng, (1 << 14, n), q)
+    t = api.to_dev(x)
+    api.ntt(t, n, q)
+    got = api.to_host(t)
+    idx = rng.choice(x.shape[0], 64, replace=False)
+    assert np.array_equal(got[idx], oracle.ntt_forward(x[idx], q))
+    api.ntt(t, n, q, inverse=True)
+    assert np.array_equal(api.to_host(t), x)
+
+
+@pytest.mark.parametrize("d,q,ms,width,rows", [(16, P.Q0, 3, 64, 1), (16, P.Q0, 5, 4096, 3), (128, P.Q0, 12, 2048, 2),
+                                               (256, P.Q1, 7, 1024, 4), (512, P.Q2, 4, 512, 8),
+                                               (32, P.Q62, 2, 256, 2), (64, P.Q0, 3, 8192, 1)])
+def test_commit(api, oracle, d, q, ms, width, rows):
+    p = P.make_params(d, q, ms, max(width, 16), 1)
+    rng = np.random.default_rng(d + width)
+    w = rand_mod(rng, (rows, width, d), q)
+    want = oracle.commit_ck(p, 21, w)
+    ctx = api.Context(p, crs_seed=21)
+    got = api.to_host(ctx.parallel_dot_series_matrix(api.to_dev(w)))
+    assert np.array_equal(got, want)
+
+
+def test_commit_prefix_layer(api, oracle):
+    """A witness narrower than WIT_LEN uses the matching expanded layer (a prefix of the powers)."""
+    p = P.make_params(16, P.Q0, 3, 1 << 14, 1)
+    rng = np.random.default_rng(3)
+    w = small_signed(rng, (2, 4096, 16), 5, p.q)
+    ctx = api.Context(p, crs_seed=4)
+    got = api.to_host(ctx.parallel_dot_series_matrix(api.to_dev(w)))
+    assert np.array_equal(got, oracle.commit_ck(p, 4, w))
+
+
+@pytest.mark.parametrize("rows,n,d,q", [(1, 4, 4, P.Q0), (1, 1 << 12, 16, P.Q0), (3, 1 << 15, 128, P.Q0),
+                                        (2, 1 << 13, 64, P.Q62), (4, 1 << 16, 256, P.Q1)])
+def test_sumcheck(api, oracle, rows, n, d, q):
+    from helpers import nc_challenges
+    rng = np.random.default_rng(n + rows)
+    w = rand_mod(rng, (rows, n), q)
+    seed, rnd = 99, 3
+    claims, polys = api.sum_check(api.to_dev(w), d, q, seed, rnd)
+    claims, polys = api.to_host(claims), api.to_host(polys)
+    nr = n.bit_length() - 1
+    for rep in range(2):
+        cs = nc_challenges(seed, rnd, rep, nr, q)
+        for k in range(rows):
+            claim, want, _ = oracle.sumcheck(w[k], q, cs)
+            assert int(claims[k]) == claim
+            assert np.array_equal(polys[rep, :, k, :], want)
+
+
+@pytest.mark.parametrize("parts", [1, 2, 3])
+def test_decompose(api, oracle, parts):
+    q, d = P.Q0, 128
+    rng = np.random.default_rng(parts)
+    w = small_signed(rng, (2, 1024, d), 1 << 13, q)
+    want, radix = oracle.decompose(w, q, parts)
+    got, gr = api.decompose_matrix_by_chunks(api.to_dev(w), q, parts)
+    assert int(api.to_host(gr)[0]) == radix
+    assert np.array_equal(api.to_host(got), want)
+
+
+def test_decompose_zero_and_full_range(api, oracle):
+    q, d = P.Q0, 16
+    z = np.zeros((2, 64, d), dtype=np.uint64)
+    got, gr = api.decompose_matrix_by_chunks(api.to_dev(z), q, 2)
+    assert int(api.to_host(gr)[0]) == 1 and not api.to_host(got).any()
+    rng = np.random.default_rng(1)
+    w = rand_mod(rng, (1, 64, d), q)
+    want, radix = oracle.decompose(w, q, 2)
+    got, gr = api.decompose_matrix_by_chunks(api.to_dev(w), q, 2)
+    assert int(api.to_host(gr)[0]) == radix
+    assert np.array_equal(api.to_host(got), want)
+
+
+@pytest.mark.parametrize("rows,width,d,q", [(1, 256, 16, P.Q0), (2, 2048, 128, P.Q0), (4, 4096, 64, P.Q1),
+                                            (8, 2048, 16, P.Q0), (2, 1024, 32, P.Q62)])
+def test_project(api, oracle, rows, width, d, q):
+    rng = np.random.default_rng(rows * width)
+    w = rand_mod(rng, (rows, width, d), q)
+    seed, rnd = 5, 2
+    iz, sg = proj_challenge(seed, rnd, rows * 256)
+    want = oracle.project(w, q, iz, sg)
+    got = api.to_host(api.project(api.to_dev(w), q, seed, rnd))
+    assert np.array_equal(got, want)
+
+
+def test_project_too_narrow_rejected(api):
+    from salsaa_b200.api import SalsaaError
+    w = api.to_dev(np.zeros((4, 512, 16), dtype=np.uint64))
+    with pytest.raises(SalsaaError):
+        api.project(w, P.Q0, 1, 0)
+
+
+@pytest.mark.parametrize("rows,width,d,q", [(2, 512, 16, P.Q0), (8, 1024, 128, P.Q0), (3, 256, 512, P.Q2),
+                                            (2, 128, 32, P.Q62)])
+def test_fold(api, oracle, rows, width, d, q):
+    rng = np.random.default_rng(rows + d)
+    w = rand_mod(rng, (rows, width, d), q)
+    c = fold_challenge(11, 0, rows, d, q)
+    want = oracle.fold(w, q, c)
+    got = api.to_host(api.fold(api.to_dev(w), q, api.to_dev(c)))
+    assert np.array_equal(got, want)
+
+
+# ---- HEXL-compatible tier (host buffers, GPU compute) ---------------------------
+def test_hexl_compat_eltwise(api, oracle):
+    q = P.Q62
+    rng = np.random.default_rng(0)
+    a, b = rand_mod(rng, 5000, q), rand_mod(rng, 5000, q)
+    for name, op in [("eltwise_mult_mod", "mult"), ("eltwise_add_mod", "add"), ("eltwise_sub_mod", "sub")]:
+        r = np.zeros_like(a)
+        api.hexl_call(name, r, a, b, a.size, q)
+        assert np.array_equal(r, oracle.eltwise(op, a, b, q)), name
+    r = np.zeros_like(a)
+    api.hexl_call("eltwise_fma_mod", r, a, 12345, b, a.size, q)
+    assert np.array_equal(r, oracle.eltwise_fma(a, 12345, b, q))
+    big = rng.integers(0, 2 ** 63, size=1000, dtype=np.uint64)
+    r = np.zeros_like(big)
+    api.hexl_call("eltwise_reduce_mod", r, big, big.size, q)
+    assert np.array_equal(r, big % np.uint64(q))
+    assert api.hexl_call("sum", a, a.size, q) == oracle.sum_mod(a, q)
+    assert api.hexl_call("sum_sq", a, a.size, q) == oracle.sum_sq(a, q)
+    assert api.hexl_call("sum_fast", a, a.size, q) == oracle.sum_mod(a, q)
+    assert api.hexl_call("sum_sq_fast", a, a.size, q) == oracle.sum_sq(a, q)
+
+
+def test_hexl_compat_kats(api):
+    """The reference's HEXL-boundary tests (src/hexl/bindings.rs:99-148) against this library."""
+    r = np.zeros(5, dtype=np.uint64)
+    api.hexl_call("eltwise_mult_mod", r, np.array([1, 2, 3, 4, 5], dtype=np.uint64),
+                  np.array([6, 7, 8, 9, 10], dtype=np.uint64), 5, 100)
+    assert r.tolist() == [6, 14, 24, 36, 50]
+    a = np.array([1, 2, 3, 1, 0, 0, 0, 0], dtype=np.uint64)
+    b = np.array([8, 7, 6, 1, 0, 0, 0, 0], dtype=np.uint64)
+    r = np.zeros(8, dtype=np.uint64)
+    api.hexl_call("multiply_poly", r, a, b, 8, 65537)
+    want = [0] * 8
+    for i in range(4):
+        for j in range(4):
+            want[i + j] = (want[i + j] + int(a[i]) * int(b[j])) % 65537
+    assert r.tolist() == want
+    assert api.hexl_call("sum_sq", np.arange(1, 9, dtype=np.uint64), 8, 71) == 62
+
+
+def test_hexl_compat_ntt(api, oracle):
+    q = P.Q62
+    rng = np.random.default_rng(4)
+    for n in (4, 64, 1024):
+        x = rand_mod(rng, n, q)
+        y = x.copy()
+        api.hexl_call("ntt_forward_in_place", y, n, q)
+        assert np.array_equal(y, oracle.ntt_forward(x, q))
+        api.hexl_call("ntt_inverse_in_place", y, n, q)
+        assert np.array_equal(y, x)

@@ -1,0 +1,80 @@
+"""Whole proofs: the device-resident prover's bytes equal the oracle's, and
+the oracle's verifier accepts full-size proofs of the reference parameter
+sets."""
+import numpy as np
+import pytest
+
+from salsaa_b200 import params as P
+
+pytestmark = pytest.mark.gpu
+
+SMALL = {
+    "snark2_d16": P.small_snark(d=16, log_len=13, rounds=2),
+    "snark3_d32_q1": P.small_snark(d=32, q=P.Q1, module_size=2, log_len=14, rounds=3),
+    "snark2_d128": P.make_params(128, P.Q0, 4, 1 << 13, 2, False),
+    "snark2_d512_q2": P.make_params(512, P.Q2, 3, 1 << 13, 2, False),
+    "fold_d16": P.small_folding(d=16, log_len=11),
+    "fold_d128": P.make_params(128, P.Q0, 5, 1 << 12, 1, True),
+}
+
+
+@pytest.fixture(scope="module")
+def api(gpu_lib, cuda):
+    from salsaa_b200 import api as A
+    return A
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_proof_bytes_equal_oracle(api, oracle, name):
+    p = SMALL[name]
+    rc, want, _ = oracle.prove(p, 7, 11)
+    assert rc == 0
+    ctx = api.Context(p, crs_seed=7)
+    got = ctx.prove(11)
+    if not np.array_equal(got, want):
+        w = np.flatnonzero(got.view(np.uint64) != want.view(np.uint64))
+        pytest.fail("first differing word %d of %d" % (w[0], want.size // 8))
+    assert oracle.verify(p, 7, 11, got) == 0
+
+
+def test_explicit_witness(api, oracle):
+    p = SMALL["snark2_d16"]
+    rng = np.random.default_rng(0)
+    w = rng.integers(-3, 4, size=(1, p.wit_len, p.d))
+    w = np.where(w < 0, p.q + w, w).astype(np.uint64)
+    rc, want, _ = oracle.prove(p, 1, 2, witness=w)
+    assert rc == 0
+    got = api.Context(p, crs_seed=1).prove(2, witness=w)
+    assert np.array_equal(got, want)
+
+
+def test_async_slots_match_blocking(api, oracle):
+    """Several proofs in flight on separate slots give the same bytes as one at a time."""
+    import torch
+    p = SMALL["snark3_d32_q1"]
+    ctx = api.Context(p, crs_seed=3)
+    seeds = [10, 11, 12, 13]
+    slots = [api.Prover(ctx) for _ in seeds]
+    bufs = [torch.empty(ctx.proof_bytes // 8, dtype=torch.int64, device="cuda") for _ in seeds]
+    torch.cuda.synchronize()
+    for s, pr, b in zip(seeds, slots, bufs):
+        pr.enqueue(s, b)
+    for pr in slots:
+        pr.sync()
+    for s, b in zip(seeds, bufs):
+        assert np.array_equal(api.to_host(b).view(np.uint8), ctx.prove(s))
+        assert np.array_equal(api.to_host(b).view(np.uint8), oracle.prove(p, 3, s)[1])
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("name", ["F0", "A2", "A0"])
+def test_full_size_proof_verifies(api, oracle, name):
+    """Reference parameter sets at full size: the oracle's verifier (the
+    reference's own checks) accepts the GPU proof, and a flipped word is caught."""
+    p = P.preset(name)
+    ctx = api.Context(p, crs_seed=1)
+    proof = ctx.prove(2)
+    assert oracle.verify(p, 1, 2, proof) == 0
+    bad = proof.copy()
+    bad[8 * 100] ^= 4
+    assert oracle.verify(p, 1, 2, bad) != 0
