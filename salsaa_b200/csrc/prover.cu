@@ -80,7 +80,8 @@ static u64 ilog2u(u64 x) { return x ? 63 - (u64)__builtin_clzll(x) : 0; }
 
 // Walk of the protocol's shapes (identical in every proof of a parameter set).
 struct Shapes {
-  bool ok = false;
+  bool basic_ok = false;  // d, q, wit_len, module_size usable (enough for a context)
+  bool ok = false;        // the whole protocol's shapes are valid (needed to prove)
   std::string why;
   u64 proof_words = 0;
   u64 max_d_rows_width = 0;  // decomposition output / initial witness, rows * width
@@ -120,6 +121,7 @@ static Shapes walk(const salsaa_params* p) {
     S.why = "module_size, init_wit_rep or nof_rounds out of range";
     return S;
   }
+  S.basic_ok = true;
   u64 w = 8, Sn = p->module_size, K = p->init_wit_rep, width = L;
   S.max_d_rows_width = K * width;
   S.max_rows = (u32)K;
@@ -255,7 +257,7 @@ extern "C" int salsaa_ctx_create(const salsaa_params* p, uint64_t crs_seed, int 
   if (!out) return salsaa_set_error(-1, "ctx_create: null output");
   *out = nullptr;
   Shapes S = walk(p);
-  if (!S.ok) return salsaa_set_error(-1, ("ctx_create: " + S.why).c_str());
+  if (!S.basic_ok) return salsaa_set_error(-1, ("ctx_create: " + S.why).c_str());
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ctx_create: cudaSetDevice");
   salsaa_ctx* c = new (std::nothrow) salsaa_ctx;
@@ -347,6 +349,7 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
   *out = nullptr;
   cudaError_t e = cudaSetDevice(c->device);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_create: cudaSetDevice");
+  if (!c->S.ok) return salsaa_set_error(-1, ("prover_create: " + c->S.why).c_str());
   salsaa_prover* pr = new (std::nothrow) salsaa_prover;
   if (!pr) return salsaa_set_error(-1, "prover_create: out of host memory");
   pr->ctx = c;
@@ -463,6 +466,8 @@ __global__ void set_seed_kernel(DevState* ds, u64 seed) { ds->seed = seed; }
 static int commit_rows(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width, u32 nck, u32 sc_first, u32 nsc,
                        u64* proof_out) {
   salsaa_ctx* c = pr->ctx;
+  if ((u64)sc_first + nsc > c->S.nsc_total || nck > c->P.module_size)
+    return salsaa_set_error(-9, "commit: statement row range outside the proof's rows");
   CommitArgs a{};
   a.w = ws;
   a.rows = rows;
@@ -591,7 +596,7 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(ntt_launch(pr->Fs, pr->Fc, width, T, true, true, st));
     // send_cross_terms_before_join (src/subroutines/project.rs:229-245)
     RowSet Fr = rows_of(pr->Fs, 1, width, d);
-    TRY(commit_rows(pr, Fr, 1, width, 0, nsc + 1 - 1 + 1, 1, proof + cur));  // l0 = <projected_lhs, folded>
+    TRY(commit_rows(pr, Fr, 1, width, 0, nsc, 1, proof + cur));  // l0 = <projected_lhs, folded>
     cur += d;
     TRY(commit_rows(pr, Pr, 1, width, 0, nsc - 1, 1, proof + cur));  // l1 = <witness_lhs, projected>
     cur += d;
@@ -705,6 +710,7 @@ extern "C" int salsaa_prover_timing(salsaa_prover* pr, salsaa_timing* t) {
 extern "C" int salsaa_prove(salsaa_ctx* c, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof,
                             uint64_t proof_len) {
   if (!c || !h_proof) return salsaa_set_error(-1, "prove: null argument");
+  if (!c->S.ok) return salsaa_set_error(-1, ("prove: " + c->S.why).c_str());
   const u64 need = c->S.proof_words * 8;
   if (proof_len < need) return salsaa_set_error(-2, "prove: proof buffer too small");
   std::lock_guard<std::mutex> lk(c->mu);
