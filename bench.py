@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--plain-proofs", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ntt", action="store_true")
+    ap.add_argument("--preset", default=PRESET, help="parameter set (profiling; the metric is quoted on A0)")
     return ap.parse_args()
 
 
@@ -200,7 +202,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    params = api.params_preset(PRESET)
+    params = api.params_preset(args.preset)
     q = params.q
     ctx = api.Context(params, crs_seed=1, device=local)
     S = args.slots
@@ -321,7 +323,7 @@ def run_ours(args):
         e2e = {"value": S * args.steps * world / (e_ms / 1000.0), "unit": "proofs/s",
                "h2d_bytes_per_step": S * wbytes, "d2h_bytes_per_step": S * words * 8}
 
-    ntt = ntt_bench(torch, api) if rank == 0 else None
+    ntt = ntt_bench(torch, api) if rank == 0 and not args.no_ntt else None
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(os.cpu_count() or 1)
@@ -331,7 +333,8 @@ def run_ours(args):
             "metric": "proofs/s", "value": value, "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 mod q", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "batch": S, "parallelism": "replicas x%d" % world,
+            "config": {"workload": WORKLOAD if args.preset == PRESET else args.preset, "batch": S,
+                       "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (512 MiB witness per proof)"},
             "p50_ms": statistics.median(lat), "p99_ms": float(np.percentile(lat, 99)),
             "plain": {"proofs_per_s": plain_value, "latency_ms": statistics.mean(plain) if plain else None},

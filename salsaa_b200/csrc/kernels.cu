@@ -538,7 +538,8 @@ int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u3
 // ---------------------------------------------------------------------------
 constexpr u32 PROJ_H = 256;
 
-__global__ void proj_tables_kernel(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask) {
+__global__ void proj_tables_kernel(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask,
+                                   int8_t* J) {
   const u32 words = cw / 32;
   u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (u64)PROJ_H * words) return;
@@ -552,6 +553,7 @@ __global__ void proj_tables_kernel(const DevState* ds, u32 round, u32 cw, u32* p
       if (sg) pm |= 1u << b;
       else nm |= 1u << b;
     }
+    if (J) J[(u64)k * cw + w * 32 + b] = iz ? 0 : (sg ? 1 : -1);
   }
   pos_mask[t] = pm;
   neg_mask[t] = nm;
@@ -569,11 +571,11 @@ __global__ void proj_cj_kernel(u32 cw, const u32* pos_mask, const u32* neg_mask,
   cj[l] = v >= 0 ? (u64)v % q : q - ((u64)(-v) % q);
 }
 
-int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, u64* cj, u64 q,
-                       cudaStream_t st) {
+int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, int8_t* J, u64* cj,
+                       u64 q, cudaStream_t st) {
   if (cw % 32) return salsaa_set_error(-2, "project: chunk width must be a multiple of 32");
   u64 tot = (u64)PROJ_H * (cw / 32);
-  proj_tables_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(ds, round, cw, pos_mask, neg_mask);
+  proj_tables_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(ds, round, cw, pos_mask, neg_mask, J);
   int rc = check_launch("proj_tables");
   if (rc) return rc;
   if (cj) {
@@ -588,8 +590,9 @@ int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32
 // in 64 bits and are reduced once.
 template <int KT, bool LAZY>
 __global__ void project_kernel(RowSet in, u64 width, u32 d, u64 q, u32 cw, u64 nch, const u32* pos_mask,
-                               const u32* neg_mask, u64* out) {
+                               const u32* neg_mask, u64* out, const u64* gate) {
   extern __shared__ u32 msk[];  // KT x words (pos), then KT x words (neg)
+  if (gate && *(volatile const u64*)gate == 0) return;  // the tensor-core pass was exact
   const u32 words = cw / 32;
   const u64 idx = blockIdx.x;
   const u32 i = (u32)(idx / nch);
@@ -630,19 +633,134 @@ __global__ void project_kernel(RowSet in, u64 width, u32 d, u64 q, u32 cw, u64 n
   for (int kk = 0; kk < KT; kk++) out[((idx * PROJ_H) + k0 + kk) * d + pos] = LAZY ? acc[kk] % q : acc[kk];
 }
 
+// Tensor-core projection: per chunk, OUT (256 x d) = J (256 x cw) * W (cw x d)
+// with W centre-lifted to int8, as mma.sync m16n8k32 s8 x s8 -> s32 tiles.
+// A CTA owns 128 outputs x 128 coefficient positions of one chunk; 8 warps in
+// a 4 x 2 grid of 32 x 64 warp tiles.  Shared-memory stages hold 128 columns
+// of J (row-major, l contiguous) and the transposed witness tile (l
+// contiguous per position), both with a 144-byte row stride so that the
+// fragment loads of a warp hit 32 distinct banks.
+constexpr u32 PJ_KS = 128, PJ_LD = 144, PJ_BM = 128, PJ_BN = 128;
+
+__device__ __forceinline__ void mma_s8_16832(int (&c)[4], u32 a0, u32 a1, u32 a2, u32 a3, u32 b0, u32 b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(256, 2) project_mma_kernel(RowSet in, u32 d, u64 q, u32 cw, u64 nch,
+                                                             const int8_t* __restrict__ J, u64* __restrict__ out,
+                                                             u64* flag) {
+  __shared__ __align__(16) int8_t As[PJ_BM * PJ_LD];
+  __shared__ __align__(16) int8_t Bs[PJ_BN * PJ_LD];
+  const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const u32 g = lane >> 2, t4 = lane & 3;
+  const u32 wm = warp & 3, wn = warp >> 2;
+  const u32 mhalf = blockIdx.x & 1, nblk = blockIdx.x >> 1;
+  const u64 idx = blockIdx.y;
+  const u32 i = (u32)(idx / nch);
+  const u64 j = idx % nch;
+  const u64* chunk = in.p[i] + (j * cw) * d + (u64)nblk * PJ_BN;
+  const u32 k0 = mhalf * PJ_BM;
+  const u64 half_q = q >> 1;
+  int acc[2][8][4];
+#pragma unroll
+  for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int b = 0; b < 8; b++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[a][b][c] = 0;
+  bool bad = false;
+  for (u32 l0 = 0; l0 < cw; l0 += PJ_KS) {
+    for (u32 v = tid; v < PJ_BM * PJ_KS / 16; v += 256) {
+      const u32 row = v >> 3, c16 = v & 7;
+      *(int4*)&As[row * PJ_LD + c16 * 16] = *(const int4*)&J[(u64)(k0 + row) * cw + l0 + c16 * 16];
+    }
+    for (u32 t = tid; t < PJ_BN * (PJ_KS / 4); t += 256) {
+      const u32 pos = t & (PJ_BN - 1), l4 = t >> 7;
+      u32 packed = 0;
+#pragma unroll
+      for (u32 e = 0; e < 4; e++) {
+        const u64 v = chunk[(u64)(l0 + l4 * 4 + e) * d + pos];
+        long long c = v > half_q ? (long long)v - (long long)q : (long long)v;
+        if (c < -128 || c > 127) {
+          bad = true;
+          c = 0;
+        }
+        packed |= ((u32)c & 0xffu) << (8 * e);
+      }
+      *(u32*)&Bs[pos * PJ_LD + l4 * 4] = packed;
+    }
+    __syncthreads();
+#pragma unroll
+    for (u32 kk = 0; kk < PJ_KS; kk += 32) {
+      u32 a[2][4], b[8][2];
+#pragma unroll
+      for (int mt = 0; mt < 2; mt++) {
+        const u32 r0 = wm * 32 + mt * 16 + g;
+        a[mt][0] = *(const u32*)&As[r0 * PJ_LD + kk + t4 * 4];
+        a[mt][1] = *(const u32*)&As[(r0 + 8) * PJ_LD + kk + t4 * 4];
+        a[mt][2] = *(const u32*)&As[r0 * PJ_LD + kk + 16 + t4 * 4];
+        a[mt][3] = *(const u32*)&As[(r0 + 8) * PJ_LD + kk + 16 + t4 * 4];
+      }
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        const u32 c0 = wn * 64 + nt * 8 + g;
+        b[nt][0] = *(const u32*)&Bs[c0 * PJ_LD + kk + t4 * 4];
+        b[nt][1] = *(const u32*)&Bs[c0 * PJ_LD + kk + 16 + t4 * 4];
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++)
+          mma_s8_16832(acc[mt][nt], a[mt][0], a[mt][1], a[mt][2], a[mt][3], b[nt][0], b[nt][1]);
+    }
+    __syncthreads();
+  }
+  if (bad) atomicOr((unsigned long long*)flag, 1ULL);
+#pragma unroll
+  for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const u32 row = k0 + wm * 32 + mt * 16 + g + 8 * h;
+        const u32 col = nblk * PJ_BN + wn * 64 + nt * 8 + t4 * 2;
+        u64* dst = out + ((idx * PROJ_H) + row) * d + col;
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int v = acc[mt][nt][h * 2 + e];
+          dst[e] = v >= 0 ? (u64)v : q - (u64)(-(long long)v);
+        }
+      }
+}
+
 int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_mask, const u32* neg_mask,
-                   u64* out, cudaStream_t st) {
+                   const int8_t* J, DevState* ds, u64* out, cudaStream_t st) {
   const u32 cw = rows * PROJ_H;
   if (rows == 0 || rows > MAX_WROWS || cw > width || width % cw)
     return salsaa_set_error(-3, "project: chunk width exceeds witness width");
   if (d > 1024) return salsaa_set_error(-2, "project: ring degree too large");
   const u64 nch = width / cw;
+  if ((u64)rows * nch > 65535) return salsaa_set_error(-2, "project: too many chunks");
+  const u64* gate = nullptr;
+  if (J && ds && d % PJ_BN == 0 && cw % PJ_KS == 0) {
+    cudaError_t e = cudaMemsetAsync(&ds->proj_flag, 0, sizeof(u64), st);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "project memset");
+    dim3 gm(2 * (d / PJ_BN), (unsigned)(rows * nch));
+    project_mma_kernel<<<gm, 256, 0, st>>>(in, d, q, cw, nch, J, out, &ds->proj_flag);
+    int rc = check_launch("project_mma");
+    if (rc) return rc;
+    gate = &ds->proj_flag;
+  }
   constexpr int KT = 16;
   dim3 g((unsigned)(rows * nch), PROJ_H / KT);
   const size_t smem = 2ULL * KT * (cw / 32) * sizeof(u32);
   const bool lazy = q < (1ULL << 52) && cw <= 4096;
-  if (lazy) project_kernel<KT, true><<<g, d, smem, st>>>(in, width, d, q, cw, nch, pos_mask, neg_mask, out);
-  else project_kernel<KT, false><<<g, d, smem, st>>>(in, width, d, q, cw, nch, pos_mask, neg_mask, out);
+  if (lazy) project_kernel<KT, true><<<g, d, smem, st>>>(in, width, d, q, cw, nch, pos_mask, neg_mask, out, gate);
+  else project_kernel<KT, false><<<g, d, smem, st>>>(in, width, d, q, cw, nch, pos_mask, neg_mask, out, gate);
   return check_launch("project");
 }
 

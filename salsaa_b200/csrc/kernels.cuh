@@ -24,6 +24,7 @@ struct DevState {
   u64 seed;
   u64 bw_or[16];   // decomposition: OR of centred magnitudes, per decomposition index
   u64 rlog[16];    // decomposition: radix log2, per decomposition index
+  u64 proj_flag;   // projection: set when a witness value does not fit int8
 };
 
 // ---- statement rows -------------------------------------------------------
@@ -63,10 +64,14 @@ int launch_norm3(const u64* cap, u32 rows, u32 nr, const NttDev& T, const ModQ& 
 int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds,
                      u64* out, u64* proof_radix, cudaStream_t st);
 
-int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, u64* cj, u64 q,
-                       cudaStream_t st);
+// J as bit masks (CUDA-core path), as an int8 matrix 256 x cw (tensor-core
+// path, optional) and cj[l] = sum_k J[k][l] (optional).
+int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, int8_t* J, u64* cj,
+                       u64 q, cudaStream_t st);
+// Tensor-core path when d is a multiple of 128 and J is given; exact CUDA-core
+// recomputation (chosen on the device) whenever a value does not fit int8.
 int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_mask, const u32* neg_mask,
-                   u64* out, cudaStream_t st);
+                   const int8_t* J, DevState* ds, u64* out, cudaStream_t st);
 
 int launch_fold_challenge(const DevState* ds, u32 round, u32 rows, u32 d, u64 q, u64* c_coef, cudaStream_t st);
 int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot,

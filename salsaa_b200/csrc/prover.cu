@@ -308,6 +308,7 @@ struct salsaa_prover {
   u64* row_base = nullptr;  // TENSOR row bases, nsc_total x d
   u64* row_cj = nullptr;    // PERIODIC row scalars, rounds x CK_BLOCK
   u32 *pmask = nullptr, *nmask = nullptr;
+  int8_t* Jm = nullptr;  // projection challenge as int8, 256 x chunk width
   u64 *c_coef = nullptr, *c_slot = nullptr;
   ScalarRowDesc* sc_desc = nullptr;
   const u64** sc_base = nullptr;
@@ -382,6 +383,7 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       (rc = m.alloc(&pr->row_cj, (c->P.nof_rounds + 1) * (u64)CK_BLOCK, "row cj")) ||
       (rc = m.alloc(&pr->pmask, 256ULL * CK_BLOCK / 32, "pos mask")) ||
       (rc = m.alloc(&pr->nmask, 256ULL * CK_BLOCK / 32, "neg mask")) ||
+      (rc = m.alloc(&pr->Jm, 256ULL * CK_BLOCK, "projection J")) ||
       (rc = m.alloc(&pr->c_coef, (u64)MAX_WROWS * d, "fold c")) ||
       (rc = m.alloc(&pr->c_slot, (u64)MAX_WROWS * d, "fold c slot")) ||
       (rc = m.alloc(&pr->sc_desc, (u64)S.nsc_total + 1, "row descriptors")) ||
@@ -576,8 +578,8 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(mark(pr, PH_PROJ));
     const u32 cw = K * 256;
     u64* cj = pr->row_cj + (u64)rd * CK_BLOCK;
-    TRY(launch_proj_tables(pr->ds, rd, cw, pr->pmask, pr->nmask, cj, q, st));
-    TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Pc, st));
+    TRY(launch_proj_tables(pr->ds, rd, cw, pr->pmask, pr->nmask, pr->Jm, cj, q, st));
+    TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Jm, pr->ds, pr->Pc, st));
     TRY(ntt_launch(pr->Pc, pr->Ps, width, T, true, false, st));
     RowSet Pr = rows_of(pr->Ps, 1, width, d);
     TRY(commit_rows(pr, Pr, 1, width, ms, 0, nsc, proof + cur));
@@ -857,13 +859,15 @@ extern "C" int salsaa_project(const uint64_t* d_w, uint64_t rows, uint64_t width
   Tmp t(st);
   DevState* ds;
   u32 *pm, *nm;
+  int8_t* J;
   TRY(t.get(&ds, 1));
   TRY(t.get(&pm, 256 * cw / 32));
   TRY(t.get(&nm, 256 * cw / 32));
+  TRY(t.get(&J, 256 * cw));
   set_seed_kernel<<<1, 1, 0, st>>>(ds, seed);
-  TRY(launch_proj_tables(ds, (u32)round, (u32)cw, pm, nm, nullptr, q, st));
+  TRY(launch_proj_tables(ds, (u32)round, (u32)cw, pm, nm, J, nullptr, q, st));
   RowSet w = rows_of(d_w, (u32)rows, width, (u32)d);
-  return launch_project(w, (u32)rows, width, (u32)d, q, pm, nm, d_out, st);
+  return launch_project(w, (u32)rows, width, (u32)d, q, pm, nm, J, ds, d_out, st);
 }
 
 extern "C" int salsaa_fold(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,

@@ -130,6 +130,23 @@ def test_project(api, oracle, rows, width, d, q):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("rows,width,d,bound", [(2, 2048, 128, 1), (8, 4096, 128, 127), (4, 2048, 256, 128),
+                                                 (2, 1024, 512, 60), (1, 512, 128, 129)])
+def test_project_small_values(api, oracle, rows, width, d, bound):
+    """Witness values in int8 range take the tensor-core path; bound 129 forces
+    the exact fallback for some values."""
+    q = P.Q0
+    rng = np.random.default_rng(bound + d)
+    w = small_signed(rng, (rows, width, d), bound, q)
+    if bound == 128:
+        w[0, 0, :] = q - 128  # the int8 edge
+    seed, rnd = 8, 5
+    iz, sg = proj_challenge(seed, rnd, rows * 256)
+    want = oracle.project(w, q, iz, sg)
+    got = api.to_host(api.project(api.to_dev(w), q, seed, rnd))
+    assert np.array_equal(got, want)
+
+
 def test_project_too_narrow_rejected(api):
     from salsaa_b200.api import SalsaaError
     w = api.to_dev(np.zeros((4, 512, 16), dtype=np.uint64))
