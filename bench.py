@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ntt", action="store_true")
     ap.add_argument("--preset", default=PRESET, help="parameter set (profiling; the metric is quoted on A0)")
+    ap.add_argument("--wit-log", type=int, default=0,
+                    help="profiling: shrink WIT_LEN to 2^L (SNARK rounds L-11), keeping d, q and the rows")
     return ap.parse_args()
 
 
@@ -203,6 +205,10 @@ def run_ours(args):
         return float(t.item())
 
     params = api.params_preset(args.preset)
+    if args.wit_log:
+        params.wit_len = 1 << args.wit_log
+        if not params.folding:
+            params.nof_rounds = args.wit_log - 11
     q = params.q
     ctx = api.Context(params, crs_seed=1, device=local)
     S = args.slots
@@ -333,7 +339,8 @@ def run_ours(args):
             "metric": "proofs/s", "value": value, "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 mod q", "data": "synthetic",
-            "config": {"workload": WORKLOAD if args.preset == PRESET else args.preset, "batch": S,
+            "config": {"workload": WORKLOAD if (args.preset == PRESET and not args.wit_log)
+                       else "%s wit_len=2^%d" % (args.preset, params.wit_len.bit_length() - 1), "batch": S,
                        "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (512 MiB witness per proof)"},
             "p50_ms": statistics.median(lat), "p99_ms": float(np.percentile(lat, 99)),

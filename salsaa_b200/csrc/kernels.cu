@@ -97,6 +97,8 @@ __device__ void slot_pow(const ModQ& M, u64 z, u64 be, u64 bo, u64 e, u64& re, u
   ro = ao;
 }
 
+__device__ __forceinline__ u64 pack25(u64 v) { return ((v >> 25) << 32) | (v & 0x1FFFFFFull); }
+
 __global__ void ck_tlo_kernel(const u64* ms, u32 rows, u32 n, u32 B, ModQ M, const u64* zeta, u64* tlo) {
   u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (u64)rows * B * n) return;
@@ -107,9 +109,16 @@ __global__ void ck_tlo_kernel(const u64* ms, u32 rows, u32 n, u32 B, ModQ M, con
   u64 e, o;
   slot_pow(M, zeta[s], m[s], m[n + s], (u64)lo + 1, e, o);
   u64* dst = tlo + ((u64)r * B + lo) * 3 * n;
-  dst[s] = e;
-  dst[n + s] = o;
-  dst[2 * n + s] = mul_mod(M, zeta[s], o);
+  const u64 z = mul_mod(M, zeta[s], o);
+  if (M.q < (1ULL << 50)) {  // stored as 25-bit limbs in the two 32-bit halves
+    dst[s] = pack25(e);
+    dst[n + s] = pack25(o);
+    dst[2 * n + s] = pack25(z);
+  } else {
+    dst[s] = e;
+    dst[n + s] = o;
+    dst[2 * n + s] = z;
+  }
 }
 
 __global__ void ck_thi_kernel(const u64* ms, u32 rows, u32 n, u32 B, u32 nhi, ModQ M, const u64* zeta,
@@ -176,138 +185,255 @@ int launch_fill(u64* p, u64 n, u64 v, cudaStream_t st) {
 // for all witness rows and both amplification repetitions at once.
 //
 // Round j folds v_j (length L) into v_{j+1} = v_j[:L/2] + c_j (v_j[L/2:] -
-// v_j[:L/2]) and the round polynomial is (f0, f1, f2) = (S00, S01 - S00,
+// v_j[:L/2]); its polynomial is (f0, f1, f2) = (S00, S01 - S00,
 // S11 - 2 S01 + S00) with S00 = sum v0^2, S01 = sum v0 v1, S11 = sum v1^2 over
-// the halves.  Challenges come from the PRF stream, so no host round trip
-// separates the rounds: a kernel that writes v_{j+1} also sums round j+1.
+// the halves.  The challenges are a PRF stream, known before the data, so
+// one pass can run T rounds: a thread owns the 2^T elements
+// v_j[g + m L/2^T] (m < 2^T), which are closed under the next T foldings,
+// sums all T rounds' polynomials and writes v_{j+T}[g].  The first pass reads
+// the witness once for both repetitions (round 0 is shared).
 // sums[((rep * nr + j) * rows + k) * 3 + {0,1,2}] hold S00, S01, S11.
 // ---------------------------------------------------------------------------
-constexpr u32 SC_TAIL = 4096;  // vectors this short finish in one CTA
+constexpr u32 SC_T = 4;          // rounds per streaming pass
+constexpr u32 SC_TAIL = 16384;   // vectors this short finish in one CTA
 
-__global__ void __launch_bounds__(256) sc_first_kernel(RowSet w, u32 rows, u64 nlen, ModQ M,
-                                                       const DevState* ds, u32 round, u64* abuf,
-                                                       u64* sums, u32 nr, bool plain) {
-  __shared__ u64 red[32];
-  const u32 k = blockIdx.y;
-  const u64* x = w.p[k];
-  const u64 q4 = nlen / 4, q = M.q;
-  const u64 c0 = nc_challenge(ds, round, 0, 0, q), c1 = nc_challenge(ds, round, 1, 0, q);
-  u64* o0 = abuf + (0 * (u64)rows + k) * (nlen / 2);
-  u64* o1 = abuf + (1 * (u64)rows + k) * (nlen / 2);
-  u64 s00 = 0, s01 = 0, s11 = 0;
-  u64 t[2][3] = {{0, 0, 0}, {0, 0, 0}};
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < q4; i += (u64)gridDim.x * blockDim.x) {
-    const u64 x0 = x[i], x1 = x[i + q4], x2 = x[i + 2 * q4], x3 = x[i + 3 * q4];
-    s00 = add_mod(s00, add_mod(mul_mod(M, x0, x0), mul_mod(M, x1, x1), q), q);
-    s01 = add_mod(s01, add_mod(mul_mod(M, x0, x2), mul_mod(M, x1, x3), q), q);
-    s11 = add_mod(s11, add_mod(mul_mod(M, x2, x2), mul_mod(M, x3, x3), q), q);
-    const u64 d0 = sub_mod(x2, x0, q), d1 = sub_mod(x3, x1, q);
-#pragma unroll
-    for (int rep = 0; rep < 2; rep++) {
-      const u64 c = rep ? c1 : c0;
-      const u64 a = add_mod(x0, mul_mod(M, c, d0), q), b = add_mod(x1, mul_mod(M, c, d1), q);
-      u64* o = rep ? o1 : o0;
-      o[i] = a;
-      o[i + q4] = b;
-      t[rep][0] = add_mod(t[rep][0], mul_mod(M, a, a), q);
-      t[rep][1] = add_mod(t[rep][1], mul_mod(M, a, b), q);
-      t[rep][2] = add_mod(t[rep][2], mul_mod(M, b, b), q);
-    }
+// Lazy sums: with q < 2^50 each product is < 2^100 and a thread's sum of
+// far fewer than 2^27 products fits in 128 bits.
+struct Sum128 {
+  u64 lo, hi;
+};
+__device__ __forceinline__ void s128_add_prod(Sum128& s, u64 a, u64 b) {
+  const u64 pl = a * b, ph = __umul64hi(a, b);
+  s.lo += pl;
+  s.hi += ph + (s.lo < pl);
+}
+__device__ __forceinline__ void s128_add(Sum128& s, const Sum128& t) {
+  s.lo += t.lo;
+  s.hi += t.hi + (s.lo < t.lo);
+}
+// one accumulator slot: lazy 128-bit sum, or a residue when q >= 2^50
+template <bool LAZY>
+struct ScAcc {
+  Sum128 s;
+  u64 g;
+  __device__ __forceinline__ void zero() {
+    s.lo = s.hi = 0;
+    g = 0;
   }
-  u64 v[9] = {s00, s01, s11, t[0][0], t[0][1], t[0][2], t[1][0], t[1][1], t[1][2]};
-#pragma unroll 1
-  for (int qi = 0; qi < 9; qi++) {
-    u64 r = block_add_mod(v[qi], q, red);
+  __device__ __forceinline__ void mac(const ModQ& M, u64 a, u64 b) {
+    if (LAZY) s128_add_prod(s, a, b);
+    else g = add_mod(g, mul_mod(M, a, b), M.q);
+  }
+};
+// Block total of one accumulator slot, reduced mod q; valid in thread 0.
+template <bool LAZY>
+__device__ u64 block_total(const ModQ& M, ScAcc<LAZY> v, Sum128* sm) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (LAZY) {
+    Sum128 t = v.s;
+    for (int o = 16; o > 0; o >>= 1) {
+      Sum128 u;
+      u.lo = __shfl_down_sync(0xffffffffu, t.lo, o);
+      u.hi = __shfl_down_sync(0xffffffffu, t.hi, o);
+      s128_add(t, u);
+    }
+    __syncthreads();
+    if (lane == 0) sm[wid] = t;
+    __syncthreads();
     if (threadIdx.x == 0) {
-      if (qi < 3) {
-        atomic_add_mod(&sums[((0 * (u64)nr + 0) * rows + k) * 3 + qi], r, q, plain);
-        atomic_add_mod(&sums[((1 * (u64)nr + 0) * rows + k) * 3 + qi], r, q, plain);
-      } else if (nr > 1) {
-        const u32 rep = (qi - 3) / 3, tq = (qi - 3) % 3;
-        atomic_add_mod(&sums[((rep * (u64)nr + 1) * rows + k) * 3 + tq], r, q, plain);
+      Sum128 a = sm[0];
+      for (int w = 1; w < nw; w++) s128_add(a, sm[w]);
+      return reduce128_any(M, a.hi, a.lo);
+    }
+    return 0;
+  } else {
+    u64 t = v.g;
+    for (int o = 16; o > 0; o >>= 1) t = add_mod(t, __shfl_down_sync(0xffffffffu, t, o), M.q);
+    __syncthreads();
+    if (lane == 0) sm[wid].lo = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u64 a = 0;
+      for (int w = 0; w < nw; w++) a = add_mod(a, sm[w].lo, M.q);
+      return a;
+    }
+    return 0;
+  }
+}
+
+__device__ __forceinline__ u64 fold1(u64 a, u64 b, u64 c, u64 cp, u64 q) {
+  return add_mod(a, mul_shoup(sub_mod(b, a, q), c, cp, q), q);
+}
+__device__ __forceinline__ u64 shoup_dev(u64 c, u64 q) { return (u64)((((unsigned __int128)c) << 64) / q); }
+
+// T rounds on a group x[0 .. 2^T): sums of round t go to acc[t][0..2].
+template <bool LAZY, u32 T>
+__device__ __forceinline__ void group_rounds(const ModQ& M, u64 (&x)[1 << T], const u64* c, const u64* cp,
+                                             ScAcc<LAZY> (&acc)[T][3], u32 t0) {
+#pragma unroll
+  for (u32 t = 0; t < T; t++) {
+    const u32 h = (1u << T) >> (t + 1);
+    if (t >= t0) {
+#pragma unroll
+      for (u32 m = 0; m < h; m++) {
+        acc[t][0].mac(M, x[m], x[m]);
+        acc[t][1].mac(M, x[m], x[m + h]);
+        acc[t][2].mac(M, x[m + h], x[m + h]);
       }
     }
+#pragma unroll
+    for (u32 m = 0; m < h; m++) x[m] = fold1(x[m], x[m + h], c[t], cp[t], M.q);
   }
 }
 
-// v_j (length L, per (rep,row) stride sin) -> v_{j+1} (stride sout), sums of round j+1.
-__global__ void __launch_bounds__(256) sc_round_kernel(const u64* in, u64 sin, u64* out, u64 sout, u64 L,
-                                                       u32 rows, ModQ M, const DevState* ds, u32 round,
-                                                       u32 j, u64* sums, u32 nr, bool plain) {
-  __shared__ u64 red[32];
+// First pass: v_0 rows (shared) -> v_T for both repetitions.
+template <bool LAZY>
+__global__ void __launch_bounds__(256) sc_first_kernel(RowSet w, u32 rows, u64 nlen, ModQ M, const DevState* ds,
+                                                       u32 round, u64* out, u64 sout, u64* sums, u32 nr,
+                                                       bool plain) {
+  constexpr u32 T = SC_T, G = 1u << T;
+  __shared__ Sum128 red[32];
+  const u32 k = blockIdx.y;
+  const u64* x = w.p[k];
+  const u64 q = M.q, ng = nlen / G;
+  u64 c[2][T], cp[2][T];
+#pragma unroll
+  for (u32 rep = 0; rep < 2; rep++)
+#pragma unroll
+    for (u32 t = 0; t < T; t++) {
+      c[rep][t] = nc_challenge(ds, round, rep, t, q);
+      cp[rep][t] = shoup_dev(c[rep][t], q);
+    }
+  ScAcc<LAZY> r0[3];
+  ScAcc<LAZY> acc[2][T][3];
+#pragma unroll
+  for (u32 a = 0; a < 3; a++) {
+    r0[a].zero();
+#pragma unroll
+    for (u32 rep = 0; rep < 2; rep++)
+#pragma unroll
+      for (u32 t = 0; t < T; t++) acc[rep][t][a].zero();
+  }
+  for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += (u64)gridDim.x * blockDim.x) {
+    u64 v[G];
+#pragma unroll
+    for (u32 m = 0; m < G; m++) v[m] = __ldg(x + g + m * ng);
+#pragma unroll
+    for (u32 m = 0; m < G / 2; m++) {
+      r0[0].mac(M, v[m], v[m]);
+      r0[1].mac(M, v[m], v[m + G / 2]);
+      r0[2].mac(M, v[m + G / 2], v[m + G / 2]);
+    }
+#pragma unroll
+    for (u32 rep = 0; rep < 2; rep++) {
+      u64 y[G];
+#pragma unroll
+      for (u32 m = 0; m < G; m++) y[m] = v[m];
+      group_rounds<LAZY, T>(M, y, c[rep], cp[rep], acc[rep], 1);
+      out[((u64)rep * rows + k) * sout + g] = y[0];
+    }
+  }
+#pragma unroll
+  for (u32 a = 0; a < 3; a++) {
+    const u64 r = block_total<LAZY>(M, r0[a], red);
+    if (threadIdx.x == 0) {
+      atomic_add_mod(&sums[((0 * (u64)nr + 0) * rows + k) * 3 + a], r, q, plain);
+      atomic_add_mod(&sums[((1 * (u64)nr + 0) * rows + k) * 3 + a], r, q, plain);
+    }
+  }
+#pragma unroll
+  for (u32 rep = 0; rep < 2; rep++)
+#pragma unroll
+    for (u32 t = 1; t < T; t++)
+#pragma unroll
+      for (u32 a = 0; a < 3; a++) {
+        const u64 r = block_total<LAZY>(M, acc[rep][t][a], red);
+        if (threadIdx.x == 0) atomic_add_mod(&sums[((rep * (u64)nr + t) * rows + k) * 3 + a], r, q, plain);
+      }
+}
+
+// Later passes: v_j (per (rep,row), stride sin) -> v_{j+T} (stride sout).
+template <bool LAZY>
+__global__ void __launch_bounds__(256) sc_round_kernel(const u64* in, u64 sin, u64* out, u64 sout, u64 L, u32 rows,
+                                                       ModQ M, const DevState* ds, u32 round, u32 j, u64* sums,
+                                                       u32 nr, bool plain) {
+  constexpr u32 T = SC_T, G = 1u << T;
+  __shared__ Sum128 red[32];
   const u32 pair = blockIdx.y, rep = pair / rows, k = pair % rows;
-  const u64 q = M.q, q4 = L / 4;
+  const u64 q = M.q, ng = L / G;
   const u64* x = in + (u64)pair * sin;
   u64* y = out + (u64)pair * sout;
-  const u64 c = nc_challenge(ds, round, rep, j, q);
-  u64 a00 = 0, a01 = 0, a11 = 0;
-  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < q4; i += (u64)gridDim.x * blockDim.x) {
-    const u64 y0 = x[i], y1 = x[i + q4], y2 = x[i + 2 * q4], y3 = x[i + 3 * q4];
-    const u64 a = add_mod(y0, mul_mod(M, c, sub_mod(y2, y0, q)), q);
-    const u64 b = add_mod(y1, mul_mod(M, c, sub_mod(y3, y1, q)), q);
-    y[i] = a;
-    y[i + q4] = b;
-    a00 = add_mod(a00, mul_mod(M, a, a), q);
-    a01 = add_mod(a01, mul_mod(M, a, b), q);
-    a11 = add_mod(a11, mul_mod(M, b, b), q);
+  u64 c[T], cp[T];
+#pragma unroll
+  for (u32 t = 0; t < T; t++) {
+    c[t] = nc_challenge(ds, round, rep, j + t, q);
+    cp[t] = shoup_dev(c[t], q);
   }
-  u64 v[3] = {a00, a01, a11};
-#pragma unroll 1
-  for (int qi = 0; qi < 3; qi++) {
-    u64 r = block_add_mod(v[qi], q, red);
-    if (threadIdx.x == 0) atomic_add_mod(&sums[((rep * (u64)nr + j + 1) * rows + k) * 3 + qi], r, q, plain);
+  ScAcc<LAZY> acc[T][3];
+#pragma unroll
+  for (u32 t = 0; t < T; t++)
+#pragma unroll
+    for (u32 a = 0; a < 3; a++) acc[t][a].zero();
+  for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += (u64)gridDim.x * blockDim.x) {
+    u64 v[G];
+#pragma unroll
+    for (u32 m = 0; m < G; m++) v[m] = __ldg(x + g + m * ng);
+    group_rounds<LAZY, T>(M, v, c, cp, acc, 0);
+    y[g] = v[0];
   }
+#pragma unroll
+  for (u32 t = 0; t < T; t++)
+#pragma unroll
+    for (u32 a = 0; a < 3; a++) {
+      const u64 r = block_total<LAZY>(M, acc[t][a], red);
+      if (threadIdx.x == 0) atomic_add_mod(&sums[((rep * (u64)nr + j + t) * rows + k) * 3 + a], r, q, plain);
+    }
 }
 
-// One CTA per (rep,row): finish all rounds from v_j (length L <= SC_TAIL).
-__global__ void __launch_bounds__(1024) sc_tail_kernel(const u64* in, u64 sin, u64 L, u32 rows, ModQ M,
-                                                       const DevState* ds, u32 round, u32 j0, u64* sums,
-                                                       u32 nr, u32 d, u64* cap) {
-  __shared__ u64 v[SC_TAIL];
-  __shared__ u64 red[32];
+// One CTA per (rep,row) finishes rounds j0.. from v_{j0} (length L <= SC_TAIL),
+// reading either a per-pair buffer or (j0 = 0) the witness row itself.
+template <bool LAZY>
+__global__ void __launch_bounds__(1024) sc_tail_kernel(const u64* in, u64 sin, RowSet w0, u64 L, u32 rows, ModQ M,
+                                                       const DevState* ds, u32 round, u32 j0, u64* sums, u32 nr,
+                                                       u32 d, u64* cap) {
+  extern __shared__ u64 v[];
+  __shared__ Sum128 red[32];
   const u32 pair = blockIdx.x, rep = pair / rows, k = pair % rows;
   const u64 q = M.q;
-  const u64* x = in + (u64)pair * sin;
+  const u64* x = (j0 == 0) ? w0.p[k] : in + (u64)pair * sin;
   for (u32 i = threadIdx.x; i < L; i += blockDim.x) v[i] = x[i];
   __syncthreads();
   u64 cur = L;
   u32 j = j0;
-  if (cur == d)
-    for (u32 i = threadIdx.x; i < d; i += blockDim.x) cap[(u64)pair * d + i] = v[i];
   while (cur > 1) {
-    const u64 c = nc_challenge(ds, round, rep, j, q);
+    if (cur == d)
+      for (u32 i = threadIdx.x; i < d; i += blockDim.x) cap[(u64)pair * d + i] = v[i];
     const u64 h = cur / 2;
-    u64 a[SC_TAIL / 1024 / 2 + 1];
-    u32 cnt = 0;
-    for (u32 i = threadIdx.x; i < h; i += blockDim.x) a[cnt++] = add_mod(v[i], mul_mod(M, c, sub_mod(v[i + h], v[i], q)), q);
+    ScAcc<LAZY> a0, a1, a2;
+    a0.zero();
+    a1.zero();
+    a2.zero();
+    for (u32 i = threadIdx.x; i < h; i += blockDim.x) {
+      const u64 p0 = v[i], p1 = v[i + h];
+      a0.mac(M, p0, p0);
+      a1.mac(M, p0, p1);
+      a2.mac(M, p1, p1);
+    }
+    const u64 r0 = block_total<LAZY>(M, a0, red);
+    const u64 r1 = block_total<LAZY>(M, a1, red);
+    const u64 r2 = block_total<LAZY>(M, a2, red);
+    if (threadIdx.x == 0) {
+      u64* sp = &sums[((rep * (u64)nr + j) * rows + k) * 3];
+      sp[0] = r0;
+      sp[1] = r1;
+      sp[2] = r2;
+    }
+    const u64 c = nc_challenge(ds, round, rep, j, q), cp = shoup_dev(c, q);
     __syncthreads();
-    cnt = 0;
-    for (u32 i = threadIdx.x; i < h; i += blockDim.x) v[i] = a[cnt++];
+    for (u32 i = threadIdx.x; i < h; i += blockDim.x) v[i] = fold1(v[i], v[i + h], c, cp, q);
     __syncthreads();
     cur = h;
     j++;
-    if (cur == d)
-      for (u32 i = threadIdx.x; i < d; i += blockDim.x) cap[(u64)pair * d + i] = v[i];
-    if (cur >= 2) {
-      const u64 hh = cur / 2;
-      u64 s00 = 0, s01 = 0, s11 = 0;
-      for (u32 i = threadIdx.x; i < hh; i += blockDim.x) {
-        const u64 p0 = v[i], p1 = v[i + hh];
-        s00 = add_mod(s00, mul_mod(M, p0, p0), q);
-        s01 = add_mod(s01, mul_mod(M, p0, p1), q);
-        s11 = add_mod(s11, mul_mod(M, p1, p1), q);
-      }
-      u64 r0 = block_add_mod(s00, q, red);
-      u64 r1 = block_add_mod(s01, q, red);
-      u64 r2 = block_add_mod(s11, q, red);
-      if (threadIdx.x == 0) {
-        u64* s = &sums[((rep * (u64)nr + j) * rows + k) * 3];
-        s[0] = r0;
-        s[1] = r1;
-        s[2] = r2;
-      }
-    }
-    __syncthreads();
   }
 }
 
@@ -329,40 +455,67 @@ __global__ void sc_finalize_kernel(const u64* sums, u32 rows, u32 nr, u64 q, u64
   if (rep == 0 && jk < rows) claims[jk] = add_mod(s00, s11, q);  // round 0: sum of squares
 }
 
-int launch_sumcheck(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, const DevState* ds, u32 round,
-                    SumcheckBufs B, u64* proof_claims, u64* proof_rep0, u64* proof_rep1, cudaStream_t st) {
-  if (nlen < 4 || (nlen & (nlen - 1)) || rows == 0 || rows > MAX_WROWS)
-    return salsaa_set_error(-2, "sumcheck: bad shape");
-  const u32 nr = 63u - (u32)__builtin_clzll(nlen);
-  const bool plain = M.q < (1ULL << 50);
-  cudaError_t e = cudaMemsetAsync(B.sums, 0, 2ULL * nr * rows * 3 * sizeof(u64), st);
-  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sumcheck memset");
-  {
-    dim3 g(grid_1d(nlen / 4, 256, 1024), rows);
-    sc_first_kernel<<<g, 256, 0, st>>>(w, rows, nlen, M, ds, round, B.a, B.sums, nr, plain);
+template <bool LAZY>
+static int sumcheck_passes(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, const DevState* ds, u32 round,
+                           SumcheckBufs B, u32 nr, bool plain, cudaStream_t st) {
+  const u64 sa = nlen / 2, sb = nlen / 4;  // strides of the two ping-pong buffers
+  u64 L = nlen;
+  u32 j = 0;
+  const u64* in = nullptr;
+  u64 sin = 0;
+  bool to_a = true;
+  auto grid_for = [](u64 groups, u32 pairs) {
+    u64 want = (148ULL * 8 + pairs - 1) / pairs;  // about eight CTAs per SM in total
+    u64 g = (groups + 255) / 256;
+    return (unsigned)(g < want ? (g ? g : 1) : want);
+  };
+  if (L > SC_TAIL) {
+    dim3 g(grid_for(L / (1u << SC_T), rows), rows);
+    sc_first_kernel<LAZY><<<g, 256, 0, st>>>(w, rows, L, M, ds, round, B.a, sa, B.sums, nr, plain);
     int rc = check_launch("sc_first");
     if (rc) return rc;
+    in = B.a;
+    sin = sa;
+    to_a = false;
+    L >>= SC_T;
+    j = SC_T;
+    while (L > SC_TAIL) {
+      u64* out = to_a ? B.a : B.b;
+      const u64 so = to_a ? sa : sb;
+      dim3 gr(grid_for(L / (1u << SC_T), 2 * rows), 2 * rows);
+      sc_round_kernel<LAZY><<<gr, 256, 0, st>>>(in, sin, out, so, L, rows, M, ds, round, j, B.sums, nr, plain);
+      rc = check_launch("sc_round");
+      if (rc) return rc;
+      in = out;
+      sin = so;
+      to_a = !to_a;
+      L >>= SC_T;
+      j += SC_T;
+    }
   }
-  // ping-pong: v_1 in a (stride nlen/2), v_2 in b (stride nlen/4), v_3 in a ...
-  u64 L = nlen / 2;
-  u32 j = 1;
-  const u64 sa = nlen / 2, sb = nlen / 4;
-  bool in_a = true;
-  while (L > SC_TAIL) {
-    const u64* in = in_a ? B.a : B.b;
-    u64* out = in_a ? B.b : B.a;
-    dim3 g(grid_1d(L / 4, 256, 1024), 2 * rows);
-    sc_round_kernel<<<g, 256, 0, st>>>(in, in_a ? sa : sb, out, in_a ? sb : sa, L, rows, M, ds, round, j, B.sums,
-                                      nr, plain);
-    int rc = check_launch("sc_round");
-    if (rc) return rc;
-    in_a = !in_a;
-    L /= 2;
-    j++;
+  const size_t smem = L * sizeof(u64);
+  auto kern = sc_tail_kernel<LAZY>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sc_tail smem attribute");
   }
-  sc_tail_kernel<<<2 * rows, 1024, 0, st>>>(in_a ? B.a : B.b, in_a ? sa : sb, L, rows, M, ds, round, j, B.sums,
-                                           nr, d, B.cap);
-  int rc = check_launch("sc_tail");
+  kern<<<2 * rows, 1024, smem, st>>>(in, sin, w, L, rows, M, ds, round, j, B.sums, nr, d, B.cap);
+  return check_launch("sc_tail");
+}
+
+int launch_sumcheck(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, const DevState* ds, u32 round,
+                    SumcheckBufs B, u64* proof_claims, u64* proof_rep0, u64* proof_rep1, cudaStream_t st) {
+  if (nlen < 4 || (nlen & (nlen - 1)) || rows == 0 || rows > MAX_WROWS || nlen < d)
+    return salsaa_set_error(-2, "sumcheck: bad shape");
+  const u32 nr = 63u - (u32)__builtin_clzll(nlen);
+  const bool lazy = M.q < (1ULL << 50);
+  // the lazy per-thread / per-block sums stay far below 2^128; with fewer than
+  // 2^13 contributions per address the plain 64-bit atomics cannot overflow
+  const bool plain = lazy;
+  cudaError_t e = cudaMemsetAsync(B.sums, 0, 2ULL * nr * rows * 3 * sizeof(u64), st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sumcheck memset");
+  int rc = lazy ? sumcheck_passes<true>(w, rows, nlen, d, M, ds, round, B, nr, plain, st)
+                : sumcheck_passes<false>(w, rows, nlen, d, M, ds, round, B, nr, plain, st);
   if (rc) return rc;
   u64 tot = 2ULL * nr * rows;
   sc_finalize_kernel<<<(unsigned)((tot + 127) / 128), 128, 0, st>>>(B.sums, rows, nr, M.q, proof_claims,
@@ -821,10 +974,12 @@ template <int RT, int KT, bool LIMB>
 __global__ void __launch_bounds__(256) ck_commit_kernel(RowSet w, u32 rows, u32 nck, const u64* tlo,
                                                         const u64* thi, u32 Bt, u32 nhi_t, u32 CH, ModQ M,
                                                         const u64* zeta, u64* acc, bool plain) {
+  // grid: x = row tile (fastest, so co-scheduled CTAs share the witness chunk in L2),
+  //       y = element chunk, z = witness-row tile
   const u32 n = blockDim.x, s = threadIdx.x, d = 2 * n;
-  const u64 i0 = (u64)blockIdx.x * CH;
+  const u64 i0 = (u64)blockIdx.y * CH;
   const u32 hi = (u32)(i0 / Bt), lo0 = (u32)(i0 % Bt);
-  const u32 r0 = blockIdx.y * RT, k0 = blockIdx.z * KT;
+  const u32 r0 = blockIdx.x * RT, k0 = blockIdx.z * KT;
   const u64 q = M.q;
   Acc3 re[RT][KT], im[RT][KT];
   u64 gre[RT][KT], gim[RT][KT];
@@ -838,44 +993,77 @@ __global__ void __launch_bounds__(256) ck_commit_kernel(RowSet w, u32 rows, u32 
     }
   const u64* wp[KT];
 #pragma unroll
-  for (int b = 0; b < KT; b++) wp[b] = (k0 + b < rows) ? w.p[k0 + b] : w.p[k0];
+  for (int b = 0; b < KT; b++) wp[b] = ((k0 + b < rows) ? w.p[k0 + b] : w.p[k0]) + i0 * d + s;
   const u64* tp[RT];
 #pragma unroll
-  for (int a = 0; a < RT; a++) tp[a] = tlo + ((u64)((r0 + a < nck) ? r0 + a : r0) * Bt + lo0) * 3 * n;
+  for (int a = 0; a < RT; a++) tp[a] = tlo + ((u64)((r0 + a < nck) ? r0 + a : r0) * Bt + lo0) * 3 * n + s;
+  // operands of the current element, prefetched one element ahead
+  u64 we[KT], wo[KT], tc[RT], td[RT], tz[RT];
+#pragma unroll
+  for (int b = 0; b < KT; b++) {
+    we[b] = __ldg(wp[b]);
+    wo[b] = __ldg(wp[b] + n);
+  }
+#pragma unroll
+  for (int a = 0; a < RT; a++) {
+    tc[a] = __ldg(tp[a]);
+    td[a] = __ldg(tp[a] + n);
+    tz[a] = __ldg(tp[a] + 2 * n);
+  }
   for (u32 e = 0; e < CH; e++) {
-    const u64 i = i0 + e;
-    u64 we[KT], wo[KT];
+    const u32 en = (e + 1 < CH) ? e + 1 : e;
+    u64 nwe[KT], nwo[KT], ntc[RT], ntd[RT], ntz[RT];
 #pragma unroll
     for (int b = 0; b < KT; b++) {
-      we[b] = wp[b][i * d + s];
-      wo[b] = wp[b][i * d + n + s];
+      nwe[b] = __ldg(wp[b] + (u64)en * d);
+      nwo[b] = __ldg(wp[b] + (u64)en * d + n);
     }
 #pragma unroll
     for (int a = 0; a < RT; a++) {
-      const u64* t = tp[a] + (u64)e * 3 * n;
-      const u64 c = t[s], dd = t[n + s], zd = t[2 * n + s];
-      if (LIMB) {
-        u32 c1, c0, d1, d0, z1, z0;
-        split25(c, c1, c0);
-        split25(dd, d1, d0);
-        split25(zd, z1, z0);
+      const u64* t = tp[a] + (u64)en * 3 * n;
+      ntc[a] = __ldg(t);
+      ntd[a] = __ldg(t + n);
+      ntz[a] = __ldg(t + 2 * n);
+    }
+    if (LIMB) {
+      u32 e1[KT], e0[KT], o1[KT], o0[KT];
+#pragma unroll
+      for (int b = 0; b < KT; b++) {
+        split25(we[b], e1[b], e0[b]);
+        split25(wo[b], o1[b], o0[b]);
+      }
+#pragma unroll
+      for (int a = 0; a < RT; a++) {
+        const u32 c1 = (u32)(tc[a] >> 32), c0 = (u32)tc[a];
+        const u32 d1 = (u32)(td[a] >> 32), d0 = (u32)td[a];
+        const u32 z1 = (u32)(tz[a] >> 32), z0 = (u32)tz[a];
 #pragma unroll
         for (int b = 0; b < KT; b++) {
-          u32 e1, e0, o1, o0;
-          split25(we[b], e1, e0);
-          split25(wo[b], o1, o0);
-          acc_mac(re[a][b], e1, e0, c1, c0);
-          acc_mac(re[a][b], o1, o0, z1, z0);
-          acc_mac(im[a][b], o1, o0, c1, c0);
-          acc_mac(im[a][b], e1, e0, d1, d0);
-        }
-      } else {
-#pragma unroll
-        for (int b = 0; b < KT; b++) {
-          gre[a][b] = add_mod(gre[a][b], add_mod(mul_mod(M, we[b], c), mul_mod(M, wo[b], zd), q), q);
-          gim[a][b] = add_mod(gim[a][b], add_mod(mul_mod(M, wo[b], c), mul_mod(M, we[b], dd), q), q);
+          acc_mac(re[a][b], e1[b], e0[b], c1, c0);
+          acc_mac(re[a][b], o1[b], o0[b], z1, z0);
+          acc_mac(im[a][b], o1[b], o0[b], c1, c0);
+          acc_mac(im[a][b], e1[b], e0[b], d1, d0);
         }
       }
+    } else {
+#pragma unroll
+      for (int a = 0; a < RT; a++)
+#pragma unroll
+        for (int b = 0; b < KT; b++) {
+          gre[a][b] = add_mod(gre[a][b], add_mod(mul_mod(M, we[b], tc[a]), mul_mod(M, wo[b], tz[a]), q), q);
+          gim[a][b] = add_mod(gim[a][b], add_mod(mul_mod(M, wo[b], tc[a]), mul_mod(M, we[b], td[a]), q), q);
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < KT; b++) {
+      we[b] = nwe[b];
+      wo[b] = nwo[b];
+    }
+#pragma unroll
+    for (int a = 0; a < RT; a++) {
+      tc[a] = ntc[a];
+      td[a] = ntd[a];
+      tz[a] = ntz[a];
     }
   }
   const u64 z = zeta[s];
@@ -887,26 +1075,30 @@ __global__ void __launch_bounds__(256) ck_commit_kernel(RowSet w, u32 rows, u32 
 #pragma unroll
     for (int b = 0; b < KT; b++) {
       if (k0 + b >= rows) break;
-      u64 e = LIMB ? acc_reduce(M, re[a][b]) : gre[a][b];
-      u64 o = LIMB ? acc_reduce(M, im[a][b]) : gim[a][b];
-      slot_mul(M, e, o, he, ho, z, e, o);
+      u64 ev = LIMB ? acc_reduce(M, re[a][b]) : gre[a][b];
+      u64 ov = LIMB ? acc_reduce(M, im[a][b]) : gim[a][b];
+      slot_mul(M, ev, ov, he, ho, z, ev, ov);
       u64* dst = acc + ((u64)(r0 + a) * rows + k0 + b) * d;
-      atomic_add_mod(dst + s, e, q, plain);
-      atomic_add_mod(dst + n + s, o, q, plain);
+      atomic_add_mod(dst + s, ev, q, plain);
+      atomic_add_mod(dst + n + s, ov, q, plain);
     }
   }
 }
 
 // Scalar-structured rows: value(i) = s_hi[i/Bw] * s_lo[i%Bw]; one thread per
-// coefficient position of the slot-form witness.
+// coefficient position of the slot-form witness, operands prefetched one
+// element ahead.  Row tiles are RT consecutive scalar rows; a launch handles
+// either the TENSOR tiles (want_tensor = 1, over the witness) or the others
+// (over the witness' column sums, since their s_hi is identically 1).
 template <int RT, int KT, bool LIMB>
-__global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 nsc, const u64* s_lo,
-                                                        const u64* s_hi, u32 Bw, u32 nhi, u32 CH, ModQ M,
-                                                        u64* acc, bool plain) {
+__global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 nsc, const ScalarRowDesc* desc,
+                                                        int want_tensor, const u64* s_lo, const u64* s_hi, u32 Bw,
+                                                        u32 nhi, u32 CH, ModQ M, u64* acc, bool plain) {
   const u32 d = blockDim.x, p = threadIdx.x;
-  const u64 i0 = (u64)blockIdx.x * CH;
+  const u32 r0 = blockIdx.x * RT, k0 = blockIdx.z * KT;
+  if ((desc[r0].type == ROW_TENSOR) != (want_tensor != 0)) return;
+  const u64 i0 = (u64)blockIdx.y * CH;
   const u32 hi = (u32)(i0 / Bw), lo0 = (u32)(i0 % Bw);
-  const u32 r0 = blockIdx.y * RT, k0 = blockIdx.z * KT;
   const u64 q = M.q;
   Acc3 ac[RT][KT];
   u64 g[RT][KT];
@@ -919,32 +1111,43 @@ __global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 
     }
   const u64* wp[KT];
 #pragma unroll
-  for (int b = 0; b < KT; b++) wp[b] = (k0 + b < rows) ? w.p[k0 + b] : w.p[k0];
+  for (int b = 0; b < KT; b++) wp[b] = ((k0 + b < rows) ? w.p[k0 + b] : w.p[k0]) + i0 * d + p;
   const u64* sp[RT];
 #pragma unroll
   for (int a = 0; a < RT; a++) sp[a] = s_lo + (u64)((r0 + a < nsc) ? r0 + a : r0) * Bw + lo0;
+  u64 x[KT], sv[RT];
+#pragma unroll
+  for (int b = 0; b < KT; b++) x[b] = __ldg(wp[b]);
+#pragma unroll
+  for (int a = 0; a < RT; a++) sv[a] = __ldg(sp[a]);
   for (u32 e = 0; e < CH; e++) {
-    const u64 i = i0 + e;
-    u64 x[KT];
+    const u32 en = (e + 1 < CH) ? e + 1 : e;
+    u64 nx[KT], ns[RT];
 #pragma unroll
-    for (int b = 0; b < KT; b++) x[b] = wp[b][i * d + p];
+    for (int b = 0; b < KT; b++) nx[b] = __ldg(wp[b] + (u64)en * d);
 #pragma unroll
-    for (int a = 0; a < RT; a++) {
-      const u64 sv = sp[a][e];
-      if (LIMB) {
+    for (int a = 0; a < RT; a++) ns[a] = __ldg(sp[a] + en);
+    if (LIMB) {
+      u32 x1[KT], x0[KT];
+#pragma unroll
+      for (int b = 0; b < KT; b++) split25(x[b], x1[b], x0[b]);
+#pragma unroll
+      for (int a = 0; a < RT; a++) {
         u32 s1, s0;
-        split25(sv, s1, s0);
+        split25(sv[a], s1, s0);
 #pragma unroll
-        for (int b = 0; b < KT; b++) {
-          u32 x1, x0;
-          split25(x[b], x1, x0);
-          acc_mac(ac[a][b], x1, x0, s1, s0);
-        }
-      } else {
-#pragma unroll
-        for (int b = 0; b < KT; b++) g[a][b] = add_mod(g[a][b], mul_mod(M, x[b], sv), q);
+        for (int b = 0; b < KT; b++) acc_mac(ac[a][b], x1[b], x0[b], s1, s0);
       }
+    } else {
+#pragma unroll
+      for (int a = 0; a < RT; a++)
+#pragma unroll
+        for (int b = 0; b < KT; b++) g[a][b] = add_mod(g[a][b], mul_mod(M, x[b], sv[a]), q);
     }
+#pragma unroll
+    for (int b = 0; b < KT; b++) x[b] = nx[b];
+#pragma unroll
+    for (int a = 0; a < RT; a++) sv[a] = ns[a];
   }
 #pragma unroll
   for (int a = 0; a < RT; a++) {
@@ -957,6 +1160,25 @@ __global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 
       v = mul_mod(M, v, h);
       atomic_add_mod(acc + ((u64)(r0 + a) * rows + k0 + b) * d + p, v, q, plain);
     }
+  }
+}
+
+// Column sums U_k[lo] = sum_h W_k[h*Bw + lo] (mod q) for the rows whose
+// weights repeat with a period dividing Bw (witness_lhs and projected_lhs).
+__global__ void colsum_kernel(RowSet w, u32 rows, u64 width, u32 Bw, u32 d, ModQ M, u64* out) {
+  const u64 per = (u64)Bw * d, tot = rows * per, nhi = width / Bw;
+  const bool lazy = M.q < (1ULL << 50) && nhi <= 4096;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u64 k = t / per, r = t % per;
+    const u64* x = w.p[k] + r;
+    u64 sacc = 0;
+    if (lazy) {
+      for (u64 h = 0; h < nhi; h++) sacc += __ldg(x + h * per);
+      sacc %= M.q;
+    } else {
+      for (u64 h = 0; h < nhi; h++) sacc = add_mod(sacc, __ldg(x + h * per), M.q);
+    }
+    out[t] = sacc;
   }
 }
 
@@ -1012,7 +1234,7 @@ __global__ void commit_finalize_kernel(const u64* acc, u32 nck, u32 nsc, u32 row
 template <int RT, int KT>
 static void launch_ck_variant(const CommitArgs& a, u32 n, u32 Bt, u32 nhi_t, u32 CH, const ModQ& M,
                               const u64* zeta, bool plain, cudaStream_t st) {
-  dim3 g((unsigned)(a.width / CH), (a.nck + RT - 1) / RT, (a.rows + KT - 1) / KT);
+  dim3 g((a.nck + RT - 1) / RT, (unsigned)(a.width / CH), (a.rows + KT - 1) / KT);
   if (M.q < (1ULL << 50))
     ck_commit_kernel<RT, KT, true><<<g, n, 0, st>>>(a.w, a.rows, a.nck, a.tlo, a.thi, Bt, nhi_t, CH, M, zeta, a.acc,
                                                    plain);
@@ -1022,15 +1244,22 @@ static void launch_ck_variant(const CommitArgs& a, u32 n, u32 Bt, u32 nhi_t, u32
 }
 
 template <int RT, int KT>
-static void launch_sc_variant(const CommitArgs& a, u32 d, u32 Bw, u32 nhi, u32 CH, const ModQ& M, bool plain,
-                              u64* acc_sc, cudaStream_t st) {
-  dim3 g((unsigned)(a.width / CH), (a.nsc + RT - 1) / RT, (a.rows + KT - 1) / KT);
+static void launch_sc_variant(const CommitArgs& a, const RowSet& w, u64 width, int want_tensor, u32 d, u32 Bw,
+                              u32 nhi, u32 CH, const ModQ& M, bool plain, u64* acc_sc, cudaStream_t st) {
+  dim3 g((a.nsc + RT - 1) / RT, (unsigned)(width / CH), (a.rows + KT - 1) / KT);
   if (M.q < (1ULL << 50))
-    sc_commit_kernel<RT, KT, true><<<g, d, 0, st>>>(a.w, a.rows, a.nsc, a.sc_lo, a.sc_hi, Bw, nhi, CH, M, acc_sc,
-                                                   plain);
+    sc_commit_kernel<RT, KT, true><<<g, d, 0, st>>>(w, a.rows, a.nsc, a.sc_desc_dev, want_tensor, a.sc_lo, a.sc_hi,
+                                                   Bw, nhi, CH, M, acc_sc, plain);
   else
-    sc_commit_kernel<RT, KT, false><<<g, d, 0, st>>>(a.w, a.rows, a.nsc, a.sc_lo, a.sc_hi, Bw, nhi, CH, M, acc_sc,
-                                                    plain);
+    sc_commit_kernel<RT, KT, false><<<g, d, 0, st>>>(w, a.rows, a.nsc, a.sc_desc_dev, want_tensor, a.sc_lo, a.sc_hi,
+                                                    Bw, nhi, CH, M, acc_sc, plain);
+}
+
+static void launch_sc_pass(const CommitArgs& a, const RowSet& w, u64 width, int want_tensor, u32 d, u32 Bw, u32 nhi,
+                           u32 CH, const ModQ& M, bool plain, u64* acc_sc, cudaStream_t st) {
+  if (a.rows == 1) launch_sc_variant<2, 1>(a, w, width, want_tensor, d, Bw, nhi, CH, M, plain, acc_sc, st);
+  else if (a.rows == 2) launch_sc_variant<2, 2>(a, w, width, want_tensor, d, Bw, nhi, CH, M, plain, acc_sc, st);
+  else launch_sc_variant<2, 4>(a, w, width, want_tensor, d, Bw, nhi, CH, M, plain, acc_sc, st);
 }
 
 int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st) {
@@ -1050,7 +1279,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit memset");
   if (a.nck) {
     if (Bw > a.ck_bt || a.ck_bt % CH) return salsaa_set_error(-2, "commit: witness wider than the key tables");
-    if (a.rows == 1) launch_ck_variant<8, 1>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);
+    if (a.rows == 1) launch_ck_variant<4, 1>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);
     else if (a.rows == 2) launch_ck_variant<4, 2>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);
     else launch_ck_variant<2, 4>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);
     int rc = check_launch("ck_commit");
@@ -1062,10 +1291,24 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
     int rc = check_launch("sc_tables");
     if (rc) return rc;
     u64* acc_sc = a.acc + (u64)a.nck * a.rows * d;
-    if (a.rows == 1) launch_sc_variant<8, 1>(a, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
-    else if (a.rows == 2) launch_sc_variant<4, 2>(a, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
-    else launch_sc_variant<4, 4>(a, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
-    rc = check_launch("sc_commit");
+    // TENSOR rows over the witness
+    launch_sc_pass(a, a.w, a.width, 1, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
+    rc = check_launch("sc_commit (tensor rows)");
+    if (rc) return rc;
+    // periodic and all-ones rows over the column sums
+    RowSet u = a.w;
+    if (nhi > 1) {
+      if (!a.colsum) return salsaa_set_error(-2, "commit: column-sum scratch missing");
+      colsum_kernel<<<grid_1d((u64)a.rows * Bw * d, 256), 256, 0, st>>>(a.w, a.rows, a.width, Bw, d, M, a.colsum);
+      rc = check_launch("colsum");
+      if (rc) return rc;
+      for (u32 k = 0; k < a.rows; k++) u.p[k] = a.colsum + (u64)k * Bw * d;
+    }
+    u64 CHu = Bw / 64;
+    if (CHu < 16) CHu = 16;
+    if (CHu > Bw) CHu = Bw;
+    launch_sc_pass(a, u, Bw, 0, d, Bw, nhi, (u32)CHu, M, plain, acc_sc, st);
+    rc = check_launch("sc_commit (periodic rows)");
     if (rc) return rc;
   }
   const u64 tot = (u64)(a.nck + a.nsc) * a.rows * n;

@@ -93,6 +93,7 @@ struct CommitArgs {
   const u64* const* sc_base_dev;     // nsc ring bases (slot form) or null (= 1)
   u64* sc_lo;        // scratch nsc x CK_BLOCK
   u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)
+  u64* colsum;       // scratch rows x min(width, CK_BLOCK) x d (scalar rows only)
   u64* acc;          // scratch (nck + nsc) x rows x d
   u64* out_slot;     // (nck + nsc) x rows x d, statement order = CK rows then scalar rows
 };

@@ -312,7 +312,7 @@ struct salsaa_prover {
   u64 *c_coef = nullptr, *c_slot = nullptr;
   ScalarRowDesc* sc_desc = nullptr;
   const u64** sc_base = nullptr;
-  u64 *sc_lo = nullptr, *sc_hi = nullptr, *acc = nullptr, *cout = nullptr;
+  u64 *sc_lo = nullptr, *sc_hi = nullptr, *acc = nullptr, *cout = nullptr, *colsum = nullptr;
   u64* header_pinned = nullptr;
   uint8_t* own_proof = nullptr;  // for the blocking API
   cudaEvent_t ev[MAX_EVENTS];
@@ -342,6 +342,7 @@ extern "C" uint64_t salsaa_workspace_bytes(const salsaa_params* p) {
   const u64 stmt = S.max_stmt + 2;
   words += stmt * CK_BLOCK + stmt * (L / CK_BLOCK + 1);
   words += 2 * stmt * MAX_WROWS * d;
+  words += (u64)S.max_rows * (L < CK_BLOCK ? L : CK_BLOCK) * d;
   return words * 8 + (S.proof_words * 8);
 }
 
@@ -391,6 +392,7 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       (rc = m.alloc(&pr->sc_lo, stmt * CK_BLOCK, "commit s_lo")) ||
       (rc = m.alloc(&pr->sc_hi, stmt * (L / CK_BLOCK + 1), "commit s_hi")) ||
       (rc = m.alloc(&pr->acc, stmt * MAX_WROWS * d, "commit acc")) ||
+      (rc = m.alloc(&pr->colsum, (u64)S.max_rows * (L < CK_BLOCK ? L : CK_BLOCK) * d, "commit column sums")) ||
       (rc = m.alloc(&pr->cout, stmt * MAX_WROWS * d, "commit out")))
     return fail(rc);
   // Scalar statement rows of the whole proof, in push order: per round
@@ -485,6 +487,7 @@ static int commit_rows(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width,
   a.sc_lo = pr->sc_lo;
   a.sc_hi = pr->sc_hi;
   a.acc = pr->acc;
+  a.colsum = pr->colsum;
   a.out_slot = pr->cout;
   TRY(launch_commit(a, *c->T, c->M, pr->ds, pr->st));
   return ntt_launch(pr->cout, proof_out, (u64)(nck + nsc) * rows, *c->T, true, true, pr->st);
