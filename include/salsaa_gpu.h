@@ -189,6 +189,18 @@ int salsaa_decompose(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_
 int salsaa_project(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q, uint64_t seed,
                    uint64_t round, uint64_t* d_out, void* stream);
 
+/* No counterpart in the reference: salsaa_project() for callers that must not
+ * allocate device memory on the call path, such as a serving loop that has
+ * already divided HBM among in-flight proofs, or a host runtime that owns all
+ * device allocations.  All scratch lives in a fixed 641 KiB array inside this
+ * library (one per GPU, kept until the process exits), so at most 8 rows
+ * (chunk width rows*256 <= 2048); larger inputs return -3 with a message.
+ * The first call on a device looks up that array's address and should come
+ * before any stream capture on that device.  Calls share the array: two calls
+ * whose work overlaps on the GPU race; serialise them on one stream. */
+int salsaa_project_noalloc(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,
+                           uint64_t seed, uint64_t round, uint64_t* d_out, void* stream);
+
 /* fold (src/subroutines/fold.rs:22-27): d_w rows x width x d coefficients,
  * d_c rows ring challenges (coefficients) -> d_out width x d coefficients. */
 int salsaa_fold(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,

@@ -68,6 +68,7 @@ DEVICE_SYMBOLS = {
     "salsaa_decompose": (INT, [VP, U64, U64, U64, U64, U64, VP, VP, VP]),
     "salsaa_project": (INT, [VP, U64, U64, U64, U64, U64, U64, VP, VP]),
     "salsaa_fold": (INT, [VP, U64, U64, U64, U64, VP, VP, VP]),
+    "salsaa_project_noalloc": (INT, [VP, U64, U64, U64, U64, U64, U64, VP, VP]),
 }
 
 ALL_SYMBOLS = {**HEXL_SYMBOLS, **DEVICE_SYMBOLS}
