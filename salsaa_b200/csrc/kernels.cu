@@ -1231,6 +1231,254 @@ __global__ void commit_finalize_kernel(const u64* acc, u32 nck, u32 nsc, u32 row
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core commitment-key rows (q < 2^56).  Per NTT slot s the key rows'
+// contribution is a matrix product over F_q: with T = m^(lo+1) = (c, d) and
+// W = (a, b) in F_q[X]/(X^2 - zeta),
+//   re = sum_lo c a + (zeta d) b,   im = sum_lo c b + d a.
+// Every value is split into 7 bytes, so G = A * B^T is an exact u8 x u8 ->
+// s32 product (sums of 2048 byte products stay below 2^31), with
+//   A rows (r, comp, byte) from the key tables (comp = c, d, zeta d) and
+//   B rows (k, part, byte) from the witness (part = a, b);
+// then value = sum_{x,y} 2^(8(x+y)) G[(.., x), (.., y)] mod q.
+// ---------------------------------------------------------------------------
+constexpr u32 CKM_KS = 128, CKM_LD = 144;
+
+__global__ void ck_tl8_kernel(const u64* tlo, u32 nck, u32 n, u32 bt, u32 nmt, bool packed, uint8_t* tl8) {
+  const u64 tot = (u64)n * nmt * CKM_BM * bt;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u32 lo = (u32)(t % bt);
+    u64 rest = t / bt;
+    const u32 m = (u32)(rest % CKM_BM);
+    rest /= CKM_BM;
+    const u32 mt = (u32)(rest % nmt), s = (u32)(rest / nmt);
+    uint8_t v = 0;
+    if (m < CKM_ROWS * 21) {
+      const u32 r = mt * CKM_ROWS + m / 21, comp = (m / 7) % 3, b = m % 7;
+      if (r < nck) {
+        u64 x = tlo[((u64)r * bt + lo) * 3 * n + comp * n + s];
+        if (packed) x = ((x >> 32) << 25) | (x & 0x1FFFFFFull);
+        v = (uint8_t)(x >> (8 * b));
+      }
+    }
+    tl8[t] = v;
+  }
+}
+
+int launch_ck_tl8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* tl8, cudaStream_t st) {
+  const u32 nmt = (nck + CKM_ROWS - 1) / CKM_ROWS;
+  ck_tl8_kernel<<<grid_1d((u64)n * nmt * CKM_BM * bt, 256), 256, 0, st>>>(tlo, nck, n, bt, nmt, packed, tl8);
+  return check_launch("ck_tl8");
+}
+
+__device__ __forceinline__ void mma_u8_16832(int (&c)[4], u32 a0, u32 a1, u32 a2, u32 a3, u32 b0, u32 b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k32.row.col.s32.u8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+r"(c[0]), "+r"(c[1]), "+r"(c[2]), "+r"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldsm_x4(u32 (&r)[4], const void* p) {
+  const u32 a = (u32)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x2(u32 (&r)[2], const void* p) {
+  const u32 a = (u32)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r[0]), "=r"(r[1]) : "r"(a));
+}
+
+// CTA = (slot s, M tile of 6 key rows, block of Bw elements), slot fastest in
+// the grid so the 64 CTAs of one block share the witness rows in L2.  The
+// witness is read in its slot-form u64 layout and split into bytes while it
+// is staged; the next stage is prefetched into registers during the MMAs.
+// 8 warps as 4 (M, 32 rows) x 2 (N, NTW n-tiles of 8).
+template <int NTW>
+__global__ void __launch_bounds__(256) ck_mma_kernel(const uint8_t* __restrict__ tl8, RowSet w, u32 rows, u64 width,
+                                                     u32 nck, u32 nmt, u32 n, u32 bt, u32 Bw, const u64* thi,
+                                                     u32 nhi_t, ModQ M, const u64* zeta, u64* acc, bool plain) {
+  constexpr u32 NP = 2 * NTW * 8;
+  constexpr u32 TPT = 2;  // witness staging tasks per thread (rows <= 8)
+  extern __shared__ __align__(16) uint8_t smem[];
+  uint8_t* As = smem;
+  uint8_t* Bs = smem + CKM_BM * CKM_LD;
+  const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const u32 g = lane >> 2, t4 = lane & 3, wm = warp & 3, wn = warp >> 2;
+  const u32 s = blockIdx.x, mt = blockIdx.y, hb = blockIdx.z;
+  const u32 d = 2 * n, NR = rows * 14;
+  const u64 i0 = (u64)hb * Bw;
+  const uint8_t* Ag = tl8 + ((u64)s * nmt + mt) * CKM_BM * bt + (i0 % bt);
+  const u32 ntask = rows * 2 * (CKM_KS / 4);  // (k, part, 4 consecutive elements)
+  // zero the padding rows of the witness tile once
+  for (u32 v = tid; v < (NP - NR) * CKM_LD / 4; v += 256) ((u32*)(Bs + NR * CKM_LD))[v] = 0;
+  uint4 ra[4];
+  u64 rb[TPT][4];
+  auto fetch = [&](u32 l0) {
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const u32 v = tid + x * 256, row = v >> 3, c16 = v & 7;
+      ra[x] = *(const uint4*)&Ag[(u64)row * bt + l0 + c16 * 16];
+    }
+#pragma unroll
+    for (int x = 0; x < TPT; x++) {
+      const u32 task = tid + x * 256;
+      if (task < ntask) {
+        const u32 i4 = task % (CKM_KS / 4), kp = task / (CKM_KS / 4), k = kp >> 1, part = kp & 1;
+        const u64* src = w.p[k] + (i0 + l0 + i4 * 4) * d + part * n + s;
+#pragma unroll
+        for (int e = 0; e < 4; e++) rb[x][e] = __ldg(src + (u64)e * d);
+      }
+    }
+  };
+  auto stash = [&]() {
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const u32 v = tid + x * 256, row = v >> 3, c16 = v & 7;
+      *(uint4*)&As[row * CKM_LD + c16 * 16] = ra[x];
+    }
+#pragma unroll
+    for (int x = 0; x < TPT; x++) {
+      const u32 task = tid + x * 256;
+      if (task < ntask) {
+        const u32 i4 = task % (CKM_KS / 4), kp = task / (CKM_KS / 4);
+#pragma unroll
+        for (int b = 0; b < 7; b++) {
+          u32 word = 0;
+#pragma unroll
+          for (int e = 0; e < 4; e++) word |= ((u32)(rb[x][e] >> (8 * b)) & 0xffu) << (8 * e);
+          *(u32*)&Bs[(kp * 7 + b) * CKM_LD + i4 * 4] = word;
+        }
+      }
+    }
+  };
+  int c[2][NTW][4];
+#pragma unroll
+  for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int b = 0; b < NTW; b++)
+#pragma unroll
+      for (int e = 0; e < 4; e++) c[a][b][e] = 0;
+  fetch(0);
+  stash();
+  __syncthreads();
+  for (u32 l0 = 0; l0 < Bw; l0 += CKM_KS) {
+    const bool more = l0 + CKM_KS < Bw;
+    if (more) fetch(l0 + CKM_KS);
+#pragma unroll
+    for (u32 kk = 0; kk < CKM_KS; kk += 32) {
+      u32 a[2][4], b[NTW][2];
+#pragma unroll
+      for (int mi = 0; mi < 2; mi++) {
+        const u32 r = wm * 32 + mi * 16 + (lane & 7) + ((lane >> 3) & 1) * 8;
+        ldsm_x4(a[mi], &As[r * CKM_LD + kk + (lane >> 4) * 16]);
+      }
+#pragma unroll
+      for (int ni = 0; ni < NTW; ni++) {
+        const u32 r = wn * NTW * 8 + ni * 8 + (lane & 7);
+        ldsm_x2(b[ni], &Bs[r * CKM_LD + kk + ((lane >> 3) & 1) * 16]);
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+        for (int ni = 0; ni < NTW; ni++)
+          mma_u8_16832(c[mi][ni], a[mi][0], a[mi][1], a[mi][2], a[mi][3], b[ni][0], b[ni][1]);
+    }
+    __syncthreads();
+    if (more) {
+      stash();
+      __syncthreads();
+    }
+  }
+  // G[m][nn] in shared memory
+  int* G = (int*)smem;
+#pragma unroll
+  for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+    for (int ni = 0; ni < NTW; ni++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const u32 m = wm * 32 + mi * 16 + g + 8 * h;
+        const u32 nn = wn * NTW * 8 + ni * 8 + t4 * 2;
+        G[m * NP + nn] = c[mi][ni][h * 2];
+        G[m * NP + nn + 1] = c[mi][ni][h * 2 + 1];
+      }
+  __syncthreads();
+  // partial[rl][k][term][x] = (sum_y 2^(8y) G[(rl,comp,x)][(k,part,y)]) * 2^(8x) mod q
+  // terms: 0 = (c, a), 1 = (zeta d, b)  [re];  2 = (c, b), 3 = (d, a)  [im]
+  u64* part = (u64*)(smem + (u64)CKM_BM * NP * sizeof(int));
+  const u32 ntk = CKM_ROWS * rows * 4 * 7;
+  for (u32 t = tid; t < ntk; t += 256) {
+    const u32 x = t % 7, term = (t / 7) % 4, k = (t / 28) % rows, rl = t / (28 * rows);
+    const u32 comp = (term == 0 || term == 2) ? 0 : (term == 1 ? 2 : 1);
+    const u32 pr = (term == 0 || term == 3) ? 0 : 1;
+    const int* grow = G + ((rl * 3 + comp) * 7 + x) * NP + (k * 2 + pr) * 7;
+    u64 lo = 0, hi = 0;
+#pragma unroll
+    for (u32 y = 0; y < 7; y++) {
+      const u64 v = (u64)(u32)grow[y];
+      const u64 sl = v << (8 * y), sh = (y == 0) ? 0 : (v >> (64 - 8 * y));
+      lo += sl;
+      hi += sh + (lo < sl);
+    }
+    u64 r = reduce128_any(M, hi, lo);
+    r = mul_mod(M, r, ((1ULL << (8 * x)) % M.q));
+    part[t] = r;
+  }
+  __syncthreads();
+  for (u32 t = tid; t < CKM_ROWS * rows; t += 256) {
+    const u32 k = t % rows, rl = t / rows, r = mt * CKM_ROWS + rl;
+    if (r >= nck) continue;
+    const u64* pp = part + (u64)(rl * rows + k) * 28;
+    u64 re = 0, im = 0;
+#pragma unroll
+    for (u32 x = 0; x < 7; x++) {
+      re = add_mod(re, add_mod(pp[0 * 7 + x], pp[1 * 7 + x], M.q), M.q);
+      im = add_mod(im, add_mod(pp[2 * 7 + x], pp[3 * 7 + x], M.q), M.q);
+    }
+    const u32 hi_t = (u32)(i0 / bt);
+    const u64* th = thi + ((u64)r * nhi_t + hi_t) * d;
+    slot_mul(M, re, im, th[s], th[n + s], zeta[s], re, im);
+    u64* dst = acc + ((u64)r * rows + k) * d;
+    atomic_add_mod(dst + s, re, M.q, plain);
+    atomic_add_mod(dst + n + s, im, M.q, plain);
+  }
+}
+
+template <int NTW>
+static int launch_ck_mma_t(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, const u64* zeta, bool plain,
+                           cudaStream_t st) {
+  constexpr u32 NP = 2 * NTW * 8;
+  const u32 nmt = (a.nck + CKM_ROWS - 1) / CKM_ROWS;
+  const size_t stage = (size_t)(CKM_BM + NP) * CKM_LD;
+  const size_t epi = (size_t)CKM_BM * NP * sizeof(int) + (size_t)CKM_ROWS * a.rows * 28 * sizeof(u64);
+  const size_t smem = stage > epi ? stage : epi;
+  auto kern = ck_mma_kernel<NTW>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ck_mma smem attribute");
+  }
+  dim3 g(n, nmt, (unsigned)(a.width / Bw));
+  kern<<<g, 256, smem, st>>>(a.tl8, a.w, a.rows, a.width, a.nck, nmt, n, a.ck_bt, Bw, a.thi, a.ck_nhi, M, zeta,
+                             a.acc, plain);
+  return check_launch("ck_mma");
+}
+
+static int launch_ck_mma(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, const u64* zeta, bool plain,
+                         cudaStream_t st) {
+  switch ((a.rows * 14 + 15) / 16) {
+    case 1: return launch_ck_mma_t<1>(a, n, Bw, M, zeta, plain, st);
+    case 2: return launch_ck_mma_t<2>(a, n, Bw, M, zeta, plain, st);
+    case 3: return launch_ck_mma_t<3>(a, n, Bw, M, zeta, plain, st);
+    case 4: return launch_ck_mma_t<4>(a, n, Bw, M, zeta, plain, st);
+    case 5: return launch_ck_mma_t<5>(a, n, Bw, M, zeta, plain, st);
+    case 6: return launch_ck_mma_t<6>(a, n, Bw, M, zeta, plain, st);
+    case 7: return launch_ck_mma_t<7>(a, n, Bw, M, zeta, plain, st);
+    default: return salsaa_set_error(-2, "ck_mma: too many witness rows");
+  }
+}
+
 template <int RT, int KT>
 static void launch_ck_variant(const CommitArgs& a, u32 n, u32 Bt, u32 nhi_t, u32 CH, const ModQ& M,
                               const u64* zeta, bool plain, cudaStream_t st) {
@@ -1277,7 +1525,11 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   cudaError_t e =
       cudaMemsetAsync(a.acc, 0, (u64)(a.nck + a.nsc) * a.rows * d * sizeof(u64), st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit memset");
-  if (a.nck) {
+  if (a.nck && a.tl8 && M.q < (1ULL << 56) && a.width >= CKM_KS && a.rows <= 8 && n <= 512) {
+    if (Bw > a.ck_bt) return salsaa_set_error(-2, "commit: witness wider than the key tables");
+    int rc = launch_ck_mma(a, n, Bw, M, T.zeta, plain, st);
+    if (rc) return rc;
+  } else if (a.nck) {
     if (Bw > a.ck_bt || a.ck_bt % CH) return salsaa_set_error(-2, "commit: witness wider than the key tables");
     if (a.rows == 1) launch_ck_variant<4, 1>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);
     else if (a.rows == 2) launch_ck_variant<4, 2>(a, n, a.ck_bt, a.ck_nhi, (u32)CH, M, T.zeta, plain, st);

@@ -44,6 +44,12 @@ struct ScalarRowDesc {
 int launch_gen_crs(u64* m_coef, u32 rows, u32 d, u64 q, u64 crs_seed, cudaStream_t st);
 int launch_ck_tables(const u64* m_slot, u32 rows, const NttDev& T, const ModQ& M, u64 L, u64* tlo, u64* thi,
                      cudaStream_t st);
+// Byte planes of the key tables for the tensor-core commitment (q < 2^56):
+// tl8[s][mt][m][lo], m = (r_local * 3 + comp) * 7 + byte for the 6 key rows
+// of M tile mt, comp = (even, odd, zeta * odd); rows m >= 126 are zero.
+constexpr u32 CKM_ROWS = 6, CKM_BM = 128;
+inline u64 ck_tl8_bytes(u32 nck, u32 n, u32 bt) { return (u64)n * ((nck + CKM_ROWS - 1) / CKM_ROWS) * CKM_BM * bt; }
+int launch_ck_tl8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* tl8, cudaStream_t st);
 int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState* ds, cudaStream_t st);
 int launch_fill(u64* p, u64 n, u64 v, cudaStream_t st);
 
@@ -93,6 +99,7 @@ struct CommitArgs {
   const u64* const* sc_base_dev;     // nsc ring bases (slot form) or null (= 1)
   u64* sc_lo;        // scratch nsc x CK_BLOCK
   u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)
+  const uint8_t* tl8;  // tensor-core key table (see launch_ck_tl8) or null
   u64* colsum;       // scratch rows x min(width, CK_BLOCK) x d (scalar rows only)
   u64* acc;          // scratch (nck + nsc) x rows x d
   u64* out_slot;     // (nck + nsc) x rows x d, statement order = CK rows then scalar rows

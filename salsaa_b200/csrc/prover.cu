@@ -213,6 +213,7 @@ struct salsaa_ctx {
   u64* m_slot = nullptr;
   u64* tlo = nullptr;
   u64* thi = nullptr;
+  uint8_t* tl8 = nullptr;  // tensor-core key table (q < 2^56), else null
   std::mutex mu;
   salsaa_prover* blocking = nullptr;  // slot used by salsaa_prove()
 };
@@ -245,6 +246,10 @@ static int ctx_build(salsaa_ctx* c, DevBuf& mem) {
   TRY(launch_gen_crs(m_coef, ms, d, c->P.q, c->crs_seed, 0));
   TRY(ntt_launch(m_coef, c->m_slot, ms, *c->T, true, false, 0));
   TRY(launch_ck_tables(c->m_slot, ms, *c->T, c->M, c->L, c->tlo, c->thi, 0));
+  if (c->P.q < (1ULL << 56)) {
+    TRY(mem.alloc(&c->tl8, ck_tl8_bytes(ms, n, c->ck_bt), "ctx: key byte planes"));
+    TRY(launch_ck_tl8(c->tlo, ms, n, c->ck_bt, c->P.q < (1ULL << 50), c->tl8, 0));
+  }
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ctx: build");
   return 0;
@@ -487,6 +492,7 @@ static int commit_rows(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width,
   a.sc_lo = pr->sc_lo;
   a.sc_hi = pr->sc_hi;
   a.acc = pr->acc;
+  a.tl8 = c->tl8;
   a.colsum = pr->colsum;
   a.out_slot = pr->cout;
   TRY(launch_commit(a, *c->T, c->M, pr->ds, pr->st));
@@ -803,6 +809,7 @@ extern "C" int salsaa_commit(salsaa_ctx* c, const uint64_t* d_w, uint64_t rows, 
   TRY(t.get(&ds, 1));
   TRY(ntt_launch(d_w, ws, rows * width, *c->T, true, false, st));
   CommitArgs a{};
+  a.tl8 = c->tl8;
   a.w = rows_of(ws, (u32)rows, width, d);
   a.rows = (u32)rows;
   a.width = width;
