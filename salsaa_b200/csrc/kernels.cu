@@ -1300,7 +1300,7 @@ __global__ void __launch_bounds__(256) ck_mma_kernel(const uint8_t* __restrict__
                                                      u32 nck, u32 nmt, u32 n, u32 bt, u32 Bw, const u64* thi,
                                                      u32 nhi_t, ModQ M, const u64* zeta, u64* acc, bool plain) {
   constexpr u32 NP = 2 * NTW * 8;
-  constexpr u32 TPT = 2;  // witness staging tasks per thread (rows <= 8)
+  constexpr u32 TPT = 3;  // witness staging tasks per thread (rows <= 12)
   extern __shared__ __align__(16) uint8_t smem[];
   uint8_t* As = smem;
   uint8_t* Bs = smem + CKM_BM * CKM_LD;
@@ -1475,6 +1475,7 @@ static int launch_ck_mma(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, cons
     case 5: return launch_ck_mma_t<5>(a, n, Bw, M, zeta, plain, st);
     case 6: return launch_ck_mma_t<6>(a, n, Bw, M, zeta, plain, st);
     case 7: return launch_ck_mma_t<7>(a, n, Bw, M, zeta, plain, st);
+    case 8: return launch_ck_mma_t<8>(a, n, Bw, M, zeta, plain, st);
     default: return salsaa_set_error(-2, "ck_mma: too many witness rows");
   }
 }
@@ -1525,7 +1526,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   cudaError_t e =
       cudaMemsetAsync(a.acc, 0, (u64)(a.nck + a.nsc) * a.rows * d * sizeof(u64), st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit memset");
-  if (a.nck && a.tl8 && M.q < (1ULL << 56) && a.width >= CKM_KS && a.rows <= 8 && n <= 512) {
+  if (a.nck && a.tl8 && M.q < (1ULL << 56) && a.width >= CKM_KS && a.rows <= 9 && n <= 512) {
     if (Bw > a.ck_bt) return salsaa_set_error(-2, "commit: witness wider than the key tables");
     int rc = launch_ck_mma(a, n, Bw, M, T.zeta, plain, st);
     if (rc) return rc;
@@ -1550,7 +1551,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
     // periodic and all-ones rows over the column sums
     RowSet u = a.w;
     if (nhi > 1) {
-      if (!a.colsum) return salsaa_set_error(-2, "commit: column-sum scratch missing");
+      if (!a.colsum || a.rows > a.colsum_rows) return salsaa_set_error(-2, "commit: column-sum scratch too small");
       colsum_kernel<<<grid_1d((u64)a.rows * Bw * d, 256), 256, 0, st>>>(a.w, a.rows, a.width, Bw, d, M, a.colsum);
       rc = check_launch("colsum");
       if (rc) return rc;
@@ -1567,6 +1568,63 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   commit_finalize_kernel<<<grid_1d(tot, 256), 256, 0, st>>>(a.acc, a.nck, a.nsc, a.rows, n, M, T.zeta,
                                                           a.sc_base_dev, a.out_slot);
   return check_launch("commit_finalize");
+}
+
+// ---------------------------------------------------------------------------
+// Derived commitments (see launch_derive in kernels.cuh).
+// ---------------------------------------------------------------------------
+__global__ void derive_kernel(DeriveArgs a, u32 n, ModQ M, const u64* zeta, const DevState* ds) {
+  const u64 tot = (u64)(a.nck + a.nsc) * a.K * n;
+  const u32 d = 2 * n;
+  const u32 logw = 63u - (u32)__clzll((long long)a.w);
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u32 s = (u32)(t % n);
+    const u64 jk = t / n;
+    const u32 k = (u32)(jk % a.K), j = (u32)(jk / a.K);
+    const u64* x = a.R + ((u64)j * a.ncols + k) * d;
+    const u64* y = a.R + ((u64)j * a.ncols + a.K + k) * d;
+    u64 re, ro;
+    if (j < a.nck) {
+      // t0 = 1, t1 = m^(w/2)
+      const u64 e = a.w / 2;
+      u64 te, to;
+      if (e >= a.ck_bt) {
+        const u64* th = a.thi + ((u64)j * a.ck_nhi + e / a.ck_bt) * d;
+        te = th[s];
+        to = th[n + s];
+      } else {
+        const u64* tl = a.tlo + ((u64)j * a.ck_bt + (e - 1)) * 3 * n;
+        te = tl[s];
+        to = tl[n + s];
+        if (a.packed) {
+          te = ((te >> 32) << 25) | (te & 0x1FFFFFFull);
+          to = ((to >> 32) << 25) | (to & 0x1FFFFFFull);
+        }
+      }
+      slot_mul(M, te, to, y[s], y[n + s], zeta[s], re, ro);
+      re = add_mod(re, x[s], M.q);
+      ro = add_mod(ro, x[n + s], M.q);
+    } else {
+      const ScalarRowDesc D = a.sc_desc_dev[j - a.nck];
+      u64 t0 = 1 % M.q, t1 = 1 % M.q;
+      if (D.type == ROW_TENSOR) {
+        const u64 c = uni_mod(prf_at(prf_key(ds->seed, domain_id(DOM_NC, D.round, D.rep)), D.K - logw), M.q);
+        t0 = sub_mod(1 % M.q, c, M.q);
+        t1 = c;
+      }
+      re = add_mod(mul_mod(M, t0, x[s]), mul_mod(M, t1, y[s]), M.q);
+      ro = add_mod(mul_mod(M, t0, x[n + s]), mul_mod(M, t1, y[n + s]), M.q);
+    }
+    a.out[jk * d + s] = re;
+    a.out[jk * d + n + s] = ro;
+  }
+}
+
+int launch_derive(const DeriveArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st) {
+  if (a.w < 2 || (a.w & (a.w - 1)) || a.ncols < 2 * a.K) return salsaa_set_error(-2, "derive: bad shape");
+  const u64 tot = (u64)(a.nck + a.nsc) * a.K * T.n;
+  derive_kernel<<<grid_1d(tot, 256), 256, 0, st>>>(a, T.n, M, T.zeta, ds);
+  return check_launch("derive");
 }
 
 }  // namespace salsaa

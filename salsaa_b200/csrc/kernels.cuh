@@ -100,10 +100,29 @@ struct CommitArgs {
   u64* sc_lo;        // scratch nsc x CK_BLOCK
   u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)
   const uint8_t* tl8;  // tensor-core key table (see launch_ck_tl8) or null
-  u64* colsum;       // scratch rows x min(width, CK_BLOCK) x d (scalar rows only)
+  u64* colsum;       // scratch colsum_rows x min(width, CK_BLOCK) x d (scalar rows only)
+  u32 colsum_rows;   // capacity of colsum in witness rows
   u64* acc;          // scratch (nck + nsc) x rows x d
   u64* out_slot;     // (nck + nsc) x rows x d, statement order = CK rows then scalar rows
 };
 int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st);
+
+// Commitment of a witness of width w from the commitment of its split halves
+// (slot form): out[j][k] = t0_j * R[j][k] + t1_j * R[j][K + k] for statement
+// rows j < nck + nsc, where (t0_j, t1_j) is row j's tensor factor of the
+// layer of length w (verifier_split's relation, src/subroutines/split.rs:171-221).
+// R has `ncols` witness columns per row; out has K.
+struct DeriveArgs {
+  const u64* R;
+  u32 ncols, K, nck, nsc;
+  u64 w;
+  const u64* tlo;
+  const u64* thi;
+  u32 ck_bt, ck_nhi;
+  bool packed;  // tlo stored as 25-bit limbs
+  const ScalarRowDesc* sc_desc_dev;
+  u64* out;
+};
+int launch_derive(const DeriveArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st);
 
 }  // namespace salsaa

@@ -318,6 +318,7 @@ struct salsaa_prover {
   ScalarRowDesc* sc_desc = nullptr;
   const u64** sc_base = nullptr;
   u64 *sc_lo = nullptr, *sc_hi = nullptr, *acc = nullptr, *cout = nullptr, *colsum = nullptr;
+  u64* cout2 = nullptr;  // coefficient-form staging of a merged commitment
   u64* header_pinned = nullptr;
   uint8_t* own_proof = nullptr;  // for the blocking API
   cudaEvent_t ev[MAX_EVENTS];
@@ -347,7 +348,7 @@ extern "C" uint64_t salsaa_workspace_bytes(const salsaa_params* p) {
   const u64 stmt = S.max_stmt + 2;
   words += stmt * CK_BLOCK + stmt * (L / CK_BLOCK + 1);
   words += 2 * stmt * MAX_WROWS * d;
-  words += (u64)S.max_rows * (L < CK_BLOCK ? L : CK_BLOCK) * d;
+  words += (u64)(S.max_rows + 1) * (L < CK_BLOCK ? L : CK_BLOCK) * d;
   return words * 8 + (S.proof_words * 8);
 }
 
@@ -397,8 +398,9 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       (rc = m.alloc(&pr->sc_lo, stmt * CK_BLOCK, "commit s_lo")) ||
       (rc = m.alloc(&pr->sc_hi, stmt * (L / CK_BLOCK + 1), "commit s_hi")) ||
       (rc = m.alloc(&pr->acc, stmt * MAX_WROWS * d, "commit acc")) ||
-      (rc = m.alloc(&pr->colsum, (u64)S.max_rows * (L < CK_BLOCK ? L : CK_BLOCK) * d, "commit column sums")) ||
-      (rc = m.alloc(&pr->cout, stmt * MAX_WROWS * d, "commit out")))
+      (rc = m.alloc(&pr->colsum, (u64)(S.max_rows + 1) * (L < CK_BLOCK ? L : CK_BLOCK) * d, "commit column sums")) ||
+      (rc = m.alloc(&pr->cout, stmt * MAX_WROWS * d, "commit out")) ||
+      (rc = m.alloc(&pr->cout2, stmt * MAX_WROWS * d, "commit out (coefficients)")))
     return fail(rc);
   // Scalar statement rows of the whole proof, in push order: per round
   // TENSOR(rep 0), TENSOR(rep 1), PERIODIC (witness_lhs), ONES (projected_lhs).
@@ -471,9 +473,9 @@ extern "C" void* salsaa_prover_stream(salsaa_prover* pr) { return pr ? (void*)pr
 __global__ void set_seed_kernel(DevState* ds, u64 seed) { ds->seed = seed; }
 
 // <statement rows [0, nck) ++ scalar rows [sc_first, sc_first + nsc), witness rows>
-// -> coefficient-form ring elements at proof_out, row-major (statement, witness).
-static int commit_rows(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width, u32 nck, u32 sc_first, u32 nsc,
-                       u64* proof_out) {
+// -> slot-form ring elements in pr->cout, row-major (statement, witness).
+static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width, u32 nck, u32 sc_first,
+                            u32 nsc) {
   salsaa_ctx* c = pr->ctx;
   if ((u64)sc_first + nsc > c->S.nsc_total || nck > c->P.module_size)
     return salsaa_set_error(-9, "commit: statement row range outside the proof's rows");
@@ -494,9 +496,16 @@ static int commit_rows(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width,
   a.acc = pr->acc;
   a.tl8 = c->tl8;
   a.colsum = pr->colsum;
+  a.colsum_rows = c->S.max_rows + 1;  // the merged split/projection pass has 2K + 1 rows
   a.out_slot = pr->cout;
-  TRY(launch_commit(a, *c->T, c->M, pr->ds, pr->st));
-  return ntt_launch(pr->cout, proof_out, (u64)(nck + nsc) * rows, *c->T, true, true, pr->st);
+  return launch_commit(a, *c->T, c->M, pr->ds, pr->st);
+}
+
+// Same, in coefficient form at proof_out.
+static int commit_rows(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width, u32 nck, u32 sc_first, u32 nsc,
+                       u64* proof_out) {
+  TRY(commit_rows_slot(pr, ws, rows, width, nck, sc_first, nsc));
+  return ntt_launch(pr->cout, proof_out, (u64)(nck + nsc) * rows, *pr->ctx->T, true, true, pr->st);
 }
 
 static RowSet rows_of(const u64* base, u32 rows, u64 width, u32 d) {
@@ -532,8 +541,13 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
   Wc = rows_of(wbase, K, width, d);
   TRY(ntt_launch(wbase, pr->Ds, (u64)K * width, T, true, false, st));
   Ws = rows_of(pr->Ds, K, width, d);
-  // commitment: parallel_dot_series_matrix(crs.ck, witness), src/protocol.rs:138
-  TRY(commit_rows(pr, Ws, K, width, ms, 0, 0, proof + cur));
+  // commitment: parallel_dot_series_matrix(crs.ck, witness), src/protocol.rs:138.
+  // In the SNARK it is derived from round 0's split commitment through the
+  // split relation (exact mod q), so the witness is not streamed twice.
+  u64 pend_off = cur;             // pending derived commitment: proof offset,
+  u32 pend_rows = ms, pend_K = K; // statement rows and witness rows
+  bool pending = !P.folding && P.nof_rounds > 0;
+  if (!pending) TRY(commit_rows(pr, Ws, K, width, ms, 0, 0, proof + cur));
   cur += (u64)ms * K * d;
   u32 nsc = 0, didx = 0;
   for (u32 rd = 0; rd < P.nof_rounds; rd++) {
@@ -547,7 +561,11 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       TRY(ntt_launch(pr->Dc, pr->Ds, (u64)K * width, T, true, false, st));
       Wc = rows_of(pr->Dc, K, width, d);
       Ws = rows_of(pr->Ds, K, width, d);
-      TRY(commit_rows(pr, Ws, K, width, ms, 0, nsc, proof + cur));
+      // decomp rhs: derived after this round's split (see below)
+      pend_off = cur;
+      pend_rows = ms + nsc;
+      pend_K = K;
+      pending = true;
       cur += (u64)(ms + nsc) * K * d;
     }
     // norm_check_1 / norm_check_2 (x2) / norm_check_3 (x2), src/protocol.rs:206-259
@@ -580,10 +598,8 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       Ws = ns;
       K *= 2;
       width = hw;
-      TRY(commit_rows(pr, Ws, K, width, ms, 0, nsc, proof + cur));
-      cur += (u64)(ms + nsc) * K * d;
     }
-    // project (src/subroutines/project.rs:50-103) and its commitment
+    // project (src/subroutines/project.rs:50-103)
     TRY(mark(pr, PH_PROJ));
     const u32 cw = K * 256;
     u64* cj = pr->row_cj + (u64)rd * CK_BLOCK;
@@ -591,8 +607,50 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Jm, pr->ds, pr->Pc, st));
     TRY(ntt_launch(pr->Pc, pr->Ps, width, T, true, false, st));
     RowSet Pr = rows_of(pr->Ps, 1, width, d);
-    TRY(commit_rows(pr, Pr, 1, width, ms, 0, nsc, proof + cur));
-    cur += (u64)(ms + nsc) * d;
+    const u32 S = ms + nsc;
+    if (!P.folding) {
+      // split rhs and projected commitment in one pass over the statement
+      // rows: witness columns L_0..L_{K/2-1}, R_0..R_{K/2-1}, P.  The
+      // challenges are fixed in advance, so computing P first changes nothing.
+      TRY(mark(pr, PH_SPLIT));
+      RowSet both = Ws;
+      both.p[K] = pr->Ps;
+      TRY(commit_rows_slot(pr, both, K + 1, width, ms, 0, nsc));
+      TRY(ntt_launch(pr->cout, pr->cout2, (u64)S * (K + 1), T, true, true, st));
+      const size_t row_bytes = (size_t)(K + 1) * d * sizeof(u64);
+      e = cudaMemcpy2DAsync(proof + cur, (size_t)K * d * sizeof(u64), pr->cout2, row_bytes,
+                            (size_t)K * d * sizeof(u64), S, cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: split rhs");
+      cur += (u64)S * K * d;
+      e = cudaMemcpy2DAsync(proof + cur, (size_t)d * sizeof(u64), pr->cout2 + (u64)K * d, row_bytes,
+                            (size_t)d * sizeof(u64), S, cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: projected commitment");
+      cur += (u64)S * d;
+      if (pending) {
+        // commitment of the unsplit witness (initial commitment or decomp rhs)
+        DeriveArgs da{};
+        da.R = pr->cout;
+        da.ncols = K + 1;
+        da.K = K / 2;
+        da.nck = ms;
+        da.nsc = pend_rows - ms;
+        da.w = 2 * width;
+        da.tlo = c->tlo;
+        da.thi = c->thi;
+        da.ck_bt = c->ck_bt;
+        da.ck_nhi = c->ck_nhi;
+        da.packed = q < (1ULL << 50);
+        da.sc_desc_dev = pr->sc_desc;
+        da.out = pr->acc;
+        if (da.K != pend_K) return salsaa_set_error(-9, "enqueue: derived commitment shape mismatch");
+        TRY(launch_derive(da, T, M, pr->ds, st));
+        TRY(ntt_launch(pr->acc, proof + pend_off, (u64)pend_rows * pend_K, T, true, true, st));
+        pending = false;
+      }
+    } else {
+      TRY(commit_rows(pr, Pr, 1, width, ms, 0, nsc, proof + cur));
+      cur += (u64)S * d;
+    }
     // batch_projections (src/subroutines/project.rs:131-203): witness_rhs, projection_rhs
     TRY(commit_rows(pr, Ws, K, width, 0, nsc, 1, proof + cur));
     cur += (u64)K * d;
@@ -632,6 +690,7 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       break;
     }
   }
+  if (pending) return salsaa_set_error(-9, "enqueue: a derived commitment was never produced");
   if (!P.folding) {
     for (u32 k = 0; k < K; k++) {
       e = cudaMemcpyAsync(proof + cur, Wc.p[k], width * d * sizeof(u64), cudaMemcpyDeviceToDevice, st);
