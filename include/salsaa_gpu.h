@@ -157,6 +157,27 @@ int salsaa_prover_timing(salsaa_prover* pr, salsaa_timing* t);
 int salsaa_prove(salsaa_ctx* ctx, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof,
                  uint64_t proof_len);
 
+/* ---- serving: continuous batching on one GPU ---- */
+/* No reference counterpart (the reference proves one statement per process,
+ * src/main.rs:1-11).  A service holds parameter sets, each with a fixed number
+ * of proof slots allocated at registration inside an HBM budget; requests are
+ * admitted onto free slots as earlier proofs finish, and admitted proofs run
+ * concurrently.  Proof bytes equal those of salsaa_prove() for the same
+ * (parameters, CRS seed, seed, witness). */
+typedef struct salsaa_server salsaa_server;
+int salsaa_server_create(int device, uint64_t hbm_budget_bytes, salsaa_server** out);
+int salsaa_server_register(salsaa_server* s, const salsaa_params* p, uint64_t crs_seed, uint32_t slots,
+                           int* set_id);
+/* Queue one proof; d_witness may be NULL (sampled from seed); d_proof is a
+ * device buffer of salsaa_proof_size() bytes that must stay valid until done. */
+int salsaa_server_submit(salsaa_server* s, int set_id, uint64_t seed, const uint64_t* d_witness, uint8_t* d_proof,
+                         uint64_t* ticket);
+/* Retire finished proofs and admit queued ones; returns requests in flight. */
+int salsaa_server_progress(salsaa_server* s);
+/* 1 pending, 0 done (latency from submit and from admission, ms), < 0 failed. */
+int salsaa_server_poll(salsaa_server* s, uint64_t ticket, double* latency_ms, double* run_ms);
+void salsaa_server_destroy(salsaa_server* s);
+
 /* ---- subroutine-level entry points (device pointers, cudaStream_t) ---- */
 
 /* Batched negacyclic NTT.  incomplete = 0: `count` polynomials of n

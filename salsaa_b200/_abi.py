@@ -69,6 +69,12 @@ DEVICE_SYMBOLS = {
     "salsaa_project": (INT, [VP, U64, U64, U64, U64, U64, U64, VP, VP]),
     "salsaa_fold": (INT, [VP, U64, U64, U64, U64, VP, VP, VP]),
     "salsaa_project_noalloc": (INT, [VP, U64, U64, U64, U64, U64, U64, VP, VP]),
+    "salsaa_server_create": (INT, [INT, U64, ctypes.POINTER(VP)]),
+    "salsaa_server_register": (INT, [VP, PP, U64, ctypes.c_uint32, ctypes.POINTER(INT)]),
+    "salsaa_server_submit": (INT, [VP, INT, U64, VP, VP, ctypes.POINTER(U64)]),
+    "salsaa_server_progress": (INT, [VP]),
+    "salsaa_server_poll": (INT, [VP, U64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "salsaa_server_destroy": (None, [VP]),
 }
 
 ALL_SYMBOLS = {**HEXL_SYMBOLS, **DEVICE_SYMBOLS}

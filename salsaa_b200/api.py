@@ -222,3 +222,53 @@ def hexl_call(name, *args):
     """Call a HEXL-compatible symbol; numpy arrays are passed as uint64*."""
     conv = [(_u64p(a) if isinstance(a, np.ndarray) else a) for a in args]
     return getattr(lib(), name)(*conv)
+
+
+# ---- serving --------------------------------------------------------------------
+class Server:
+    """Continuous-batching proof service on one GPU (salsaa_server_* in the C ABI)."""
+
+    def __init__(self, hbm_budget_bytes, device=0):
+        h = ctypes.c_void_p()
+        _check(lib().salsaa_server_create(device, hbm_budget_bytes, ctypes.byref(h)), "server_create")
+        self.h = h
+        self.sets = []
+
+    def register(self, params, crs_seed=0, slots=1):
+        sid = ctypes.c_int()
+        _check(lib().salsaa_server_register(self.h, ctypes.byref(params), crs_seed, slots, ctypes.byref(sid)),
+               "server_register")
+        self.sets.append(params)
+        return sid.value
+
+    def submit(self, set_id, seed, d_proof, d_witness=None):
+        t = ctypes.c_uint64()
+        _check(lib().salsaa_server_submit(self.h, set_id, seed, _p(d_witness), _p(d_proof), ctypes.byref(t)),
+               "server_submit")
+        return t.value
+
+    def progress(self):
+        rc = lib().salsaa_server_progress(self.h)
+        if rc < 0:
+            _check(rc, "server_progress")
+        return rc
+
+    def poll(self, ticket):
+        """None while pending, else (latency_ms, run_ms)."""
+        lat, run = ctypes.c_double(), ctypes.c_double()
+        rc = lib().salsaa_server_poll(self.h, ticket, ctypes.byref(lat), ctypes.byref(run))
+        if rc == 1:
+            return None
+        _check(rc, "server_poll")
+        return lat.value, run.value
+
+    def close(self):
+        if self.h:
+            lib().salsaa_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
