@@ -54,19 +54,29 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ntt", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--preset", default=PRESET, help="parameter set (profiling; the metric is quoted on A0)")
     ap.add_argument("--wit-log", type=int, default=0,
                     help="profiling: shrink WIT_LEN to 2^L (SNARK rounds L-11), keeping d, q and the rows")
+    ap.add_argument("--ntt-only", action="store_true",
+                    help="profiling: run only the NTT microbench and print its JSON")
+    ap.add_argument("--ntt-log-coeffs", type=int, default=28,
+                    help="log2 of the coefficients per NTT batch (28 = 2 GiB per buffer)")
     return ap.parse_args()
 
 
-def measured_peaks():
+def measured_peaks(tensor=False):
+    """HBM copy GB/s, or (tensor=True) the sustained dense bf16 TFLOP/s, which
+    applies to a kernel timed inside a long step."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        if tensor:
+            return float(d["bf16_tflops_sustained"]), "measured (cuBLAS bf16 dense, sustained)"
+        return float(d["hbm_gbs"]), "measured (copy)"
     except Exception:
-        return 6650.0, "fallback"
+        return (1400.0, "fallback") if tensor else (6650.0, "fallback")
 
 
 # ---------------------------------------------------------------------------
@@ -183,7 +193,7 @@ def ternary_witness(torch, shape, q, gen):
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from salsaa_b200 import api, lib
+    from salsaa_b200 import api, lib, replicas
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -227,7 +237,7 @@ def run_ours(args):
         done = []
         for i in range(S):
             ext[i].wait_event(start_ev)
-            slots[i].enqueue(seed=(rank << 40) + step * S + i + 1, d_proof=proofs[i], d_witness=witnesses[i])
+            slots[i].enqueue(seed=replicas.proof_seed(rank, step, i, S), d_proof=proofs[i], d_witness=witnesses[i])
             e = torch.cuda.Event(enable_timing=True)
             e.record(ext[i])
             main.wait_event(e)
@@ -274,13 +284,18 @@ def run_ours(args):
         try:
             import oracle as O
             pb = api.to_host(proofs[0]).view(np.uint8)
-            check = O.verify(params, 1, (rank << 40) + (args.steps - 1) * S + 1, pb) == 0
+            check = O.verify(params, 1, replicas.proof_seed(rank, args.steps - 1, 0, S), pb) == 0
         except Exception as e:  # the checker is optional here; tests own parity
             check = "not run: %s" % e
 
-    # plain path: one proof at a time on one slot
+    # plain path: one proof at a time on one slot.  The per-kernel trace runs
+    # here, where nothing else shares the GPU, so each launch's events bracket
+    # that launch alone.
     plain = []
     for i in range(args.plain_proofs):
+        if i == 1:
+            torch.cuda.synchronize()
+            lib().salsaa_trace_enable(1)
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(ext[0])
@@ -289,6 +304,9 @@ def run_ours(args):
         b.synchronize()
         if i > 0:
             plain.append(a.elapsed_time(b))
+    torch.cuda.synchronize()
+    traced = trace_read("ck_mma_kernel") if args.plain_proofs > 1 else None
+    lib().salsaa_trace_enable(0)
     plain_value = 1000.0 / statistics.mean(plain) if plain else None
 
     # e2e: the same batches through host buffers (pinned), copies inside the timing
@@ -329,7 +347,13 @@ def run_ours(args):
         e2e = {"value": S * args.steps * world / (e_ms / 1000.0), "unit": "proofs/s",
                "h2d_bytes_per_step": S * wbytes, "d2h_bytes_per_step": S * words * 8}
 
+    for pr in slots:
+        pr.close()
+    slots = []
+    del witnesses, proofs
+    torch.cuda.empty_cache()
     ntt = ntt_bench(torch, api) if rank == 0 and not args.no_ntt else None
+    serving = serving_bench(torch, api, args.serve_requests, rank) if not args.no_serve else None
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(os.cpu_count() or 1)
@@ -350,70 +374,218 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "e2e": e2e,
             "ntt": ntt,
-            "roofline": roofline_from(ntt, peak, kind),
+            "serving": serving,
+            "roofline": roofline_ck(traced, measured_peaks(tensor=True),
+                                    statistics.mean(plain) * len(plain) if plain else None),
+            "ntt_roofline": roofline_ntt(ntt, peak, kind),
             "cpu_baseline": cpu,
             "clocks": clk,
             "verified": check,
         }
         print(json.dumps(line), flush=True)
-    for pr in slots:
-        pr.close()
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
     return 0
 
 
-def ntt_bench(torch, api):
-    """forward -> pointwise -> inverse, n=1024, the 62-bit prime,
-    2^18 polynomials (2 GiB, larger than L2); forward/inverse timed alone."""
-    from salsaa_b200 import params as P
-    q, n, count = P.Q62, 1024, 1 << 18
-    x = torch.randint(0, 1 << 62, (count, n), dtype=torch.int64, device="cuda") % q
-    reps = 5
-    res = {}
-    for inv in (False, True):
-        for _ in range(2):
-            api.ntt(x, n, q, inverse=inv)
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(reps):
-            api.ntt(x, n, q, inverse=inv)
-        b.record()
-        b.synchronize()
-        ms = a.elapsed_time(b) / reps
-        res["inverse" if inv else "forward"] = {"ms": ms, "GB/s": 16.0 * n * count / (ms * 1e6)}
-    # protocol-shaped incomplete NTT: d=128 (two n=64 halves), 2^19 ring elements
-    y = torch.randint(0, 1 << 50, (1 << 19, 128), dtype=torch.int64, device="cuda") % P.Q0
-    out = torch.empty_like(y)
-    api.ntt(y, 128, P.Q0, incomplete=True, out=out)
-    a = torch.cuda.Event(enable_timing=True)
-    b = torch.cuda.Event(enable_timing=True)
-    a.record()
+SERVE_SLOTS = {"A0": 4, "A1": 4, "A2": 4, "F0": 4, "F1": 2, "F2": 1}
+SERVE_BUDGET = 140 << 30
+
+
+def serving_bench(torch, api, nreq, rank):
+    """Poisson arrivals of A0/A1/A2 SNARK proves and F0/F1/F2 folding
+    steps (size classes 0/1/2 drawn 40/30/30, SNARK or folding 50/50), each with
+    its own seed and a witness sampled on the GPU.  The same stream is run
+    through the continuous-batching server and through the plain path (one
+    proof at a time, in arrival order); latency counts from arrival."""
+    import time as _t
+    rng = np.random.default_rng(4242 + rank)
+    cls = rng.choice(3, size=nreq, p=[0.4, 0.3, 0.3])
+    kind = rng.integers(0, 2, size=nreq)
+    names = [("A%d" if k == 0 else "F%d") % c for c, k in zip(cls, kind)]
+    params = {nm: api.params_preset(nm) for nm in SERVE_SLOTS}
+    # plain path first: one slot per set, proofs strictly one after another
+    ctxs = {nm: api.Context(params[nm], crs_seed=3) for nm in SERVE_SLOTS}
+    provers = {nm: api.Prover(ctxs[nm]) for nm in SERVE_SLOTS}
+    bufs = {nm: torch.empty(ctxs[nm].proof_bytes // 8, dtype=torch.int64, device="cuda") for nm in SERVE_SLOTS}
+    service = {}
+    for nm in SERVE_SLOTS:  # warm-up and per-set service time
+        provers[nm].enqueue(1, bufs[nm])
+        provers[nm].sync()
+        t0 = _t.perf_counter()
+        provers[nm].enqueue(2, bufs[nm])
+        provers[nm].sync()
+        service[nm] = _t.perf_counter() - t0
+    mean_service = float(np.mean([service[nm] for nm in names]))
+    rate = 1.5 / mean_service  # offered load 1.5x the plain path's capacity
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
+    seeds = [10 ** 7 + rank * 10 ** 5 + i for i in range(nreq)]
+    plain_lat = []
+    t0 = _t.perf_counter()
+    for i, nm in enumerate(names):
+        while _t.perf_counter() - t0 < arrivals[i]:
+            pass
+        provers[nm].enqueue(seeds[i], bufs[nm])
+        provers[nm].sync()
+        plain_lat.append(_t.perf_counter() - t0 - arrivals[i])
+    plain_span = _t.perf_counter() - t0
+    for nm in SERVE_SLOTS:
+        provers[nm].close()
+        ctxs[nm].close()
+    del bufs
+    torch.cuda.empty_cache()
+    # served path
+    srv = api.Server(SERVE_BUDGET)
+    sets = {nm: srv.register(params[nm], crs_seed=3, slots=SERVE_SLOTS[nm]) for nm in SERVE_SLOTS}
+    outs = [torch.empty(api.proof_size(params[nm]) // 8, dtype=torch.int64, device="cuda") for nm in names]
+    warm = [srv.submit(sets[nm], 1, torch.empty(api.proof_size(params[nm]) // 8, dtype=torch.int64,
+                                                device="cuda")) for nm in SERVE_SLOTS]
+    while srv.progress() > 0:
+        pass
+    for t in warm:
+        srv.poll(t)
+    tickets = [None] * nreq
+    done = {}
+    nsub = 0
+    t0 = _t.perf_counter()
+    while len(done) < nreq:
+        now = _t.perf_counter() - t0
+        while nsub < nreq and arrivals[nsub] <= now:
+            tickets[nsub] = srv.submit(sets[names[nsub]], seeds[nsub], outs[nsub])
+            nsub += 1
+        srv.progress()
+        for i in range(nsub):
+            if i not in done:
+                r = srv.poll(tickets[i])
+                if r is not None:
+                    done[i] = _t.perf_counter() - t0 - arrivals[i]
+    span = _t.perf_counter() - t0
+    srv.close()
+    lat = [done[i] for i in range(nreq)]
+    served = {"proofs_per_s": nreq / span, "p50_ms": 1e3 * float(np.median(lat)),
+              "p99_ms": 1e3 * float(np.percentile(lat, 99))}
+    plain = {"proofs_per_s": nreq / plain_span, "p50_ms": 1e3 * float(np.median(plain_lat)),
+             "p99_ms": 1e3 * float(np.percentile(plain_lat, 99))}
+    return {"requests": nreq, "offered_per_s": rate, "mix": {nm: names.count(nm) for nm in SERVE_SLOTS},
+            "slots": SERVE_SLOTS, "served": served, "plain": plain,
+            "served_over_plain": served["proofs_per_s"] / plain["proofs_per_s"],
+            "service_ms_alone": {nm: 1e3 * v for nm, v in service.items()}}
+
+
+def trace_read(name):
+    """(launches, total device ms, total algorithmic work) of a traced kernel."""
+    import ctypes
+    from salsaa_b200 import lib
+    ms, work, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_uint64()
+    rc = lib().salsaa_trace_read(name.encode(), ctypes.byref(ms), ctypes.byref(work), ctypes.byref(n))
+    if rc:
+        raise RuntimeError("trace_read failed for %s" % name)
+    return {"launches": int(n.value), "ms": ms.value, "work": work.value}
+
+
+def timed_launches(torch, fn, name, reps):
+    """Run fn reps times with the trace on; per-launch device time of `name`."""
+    from salsaa_b200 import lib
+    torch.cuda.synchronize()
+    lib().salsaa_trace_enable(1)
     for _ in range(reps):
-        api.ntt(y, 128, P.Q0, incomplete=True, out=out)
-    b.record()
-    b.synchronize()
-    ms = a.elapsed_time(b) / reps
-    res["incomplete_d128"] = {"ms": ms, "GB/s": 16.0 * 128 * (1 << 19) / (ms * 1e6)}
-    res["config"] = "n=1024 q=4546383823830515713 2^18 polys; incomplete d=128 q=1125899904679937 2^19 elements"
+        fn()
+    torch.cuda.synchronize()
+    t = trace_read(name)
+    lib().salsaa_trace_enable(0)
+    return t
+
+
+def flush_l2(torch, buf):
+    buf.add_(1)
+
+
+def ntt_bench(torch, api, log_coeffs=28):
+    """Batched negacyclic NTT microbench (62-bit prime, coefficients uniform in
+    [0, q)): forward, inverse and the fused forward-product-inverse for
+    n in {64, 128, 256, 1024}, plus the protocol-shaped incomplete transform
+    (d = 128, 50-bit prime).  Every batch is >= 512 MiB (larger than L2) and
+    each launch is timed by CUDA events on its own stream."""
+    from salsaa_b200 import params as P
+    q = P.Q62
+    res = {}
+    reps = 5
+    for n in (64, 128, 256, 1024):
+        count = min(1 << 20, (1 << log_coeffs) // n)
+        x = torch.randint(0, 1 << 62, (count, n), dtype=torch.int64, device="cuda") % q
+        y = torch.randint(0, 1 << 62, (count, n), dtype=torch.int64, device="cuda") % q
+        r = torch.empty_like(x)
+        row = {"polys": count}
+        for inv in (False, True):
+            api.ntt(x, n, q, inverse=inv)
+            t = timed_launches(torch, lambda: api.ntt(x, n, q, inverse=inv), "ntt_kernel", reps)
+            ms = t["ms"] / t["launches"]
+            row["inverse" if inv else "forward"] = {"ms": ms, "GB/s": t["work"] / t["launches"] / (ms * 1e6)}
+        api.poly_mul(x, y, n, q, out=r)
+        t = timed_launches(torch, lambda: api.poly_mul(x, y, n, q, out=r), "ntt_mul_kernel", reps)
+        ms = t["ms"] / t["launches"]
+        row["fused_product"] = {"ms": ms, "GB/s": t["work"] / t["launches"] / (ms * 1e6)}
+        res["n%d" % n] = row
+        del x, y, r
+    ne = min(1 << 19, (1 << log_coeffs) // 128)
+    z = torch.randint(0, 1 << 50, (ne, 128), dtype=torch.int64, device="cuda") % P.Q0
+    out = torch.empty_like(z)
+    api.ntt(z, 128, P.Q0, incomplete=True, out=out)
+    t = timed_launches(torch, lambda: api.ntt(z, 128, P.Q0, incomplete=True, out=out), "ntt_kernel", reps)
+    ms = t["ms"] / t["launches"]
+    res["incomplete_d128"] = {"ms": ms, "GB/s": t["work"] / t["launches"] / (ms * 1e6), "elements": ne}
+    res["q"] = q
+    res["bytes"] = "forward/inverse 16 B per coefficient, fused product 24 B per coefficient (read a, b; write r)"
     return res
 
 
-def roofline_from(ntt, peak, kind):
+def roofline_ntt(ntt, peak, kind):
     if not ntt:
         return None
-    f = ntt["forward"]
-    return {"kernel": "ntt_kernel (forward, n=1024, 62-bit q)", "bound": "hbm", "achieved": f["GB/s"],
-            "peak": peak, "unit": "GB/s", "frac": f["GB/s"] / peak, "peak_kind": kind,
-            "traffic": None, "algorithmic_bytes_per_launch": 16 * 1024 * (1 << 18)}
+    f = ntt["n1024"]["forward"]
+    return {"kernel": "ntt_reg_kernel (forward, n=1024, 62-bit q, 2^18 polynomials)", "bound": "hbm",
+            "achieved": f["GB/s"], "peak": peak, "unit": "GB/s", "frac": f["GB/s"] / peak, "peak_kind": kind,
+            "algorithmic_bytes_per_launch": 16 * 1024 * (1 << 18)}
+
+
+# DRAM bytes (read + write) per int8 operation of ck_mma_kernel, from one ncu
+# capture of a 9-row x 16384-element commitment against 12 key rows:
+# 285.13 MB for 6.66e10 operations.  Traffic grows with rows x elements, as
+# the operations do, so a launch's traffic is estimated from its operations.
+CK_MMA_BYTES_PER_OP = 285.13e6 / (588.0 * 12 * 9 * 16384 * 64)
+
+
+def roofline_ck(traced, peak_info, elapsed_ms):
+    # elapsed_ms: summed device time of the traced plain proofs
+    """Dominant kernel of the prove: the tensor-core commitment product.  Work
+    is counted as int8 operations (2 per byte-limb product) and set against
+    the measured dense bf16 rate, the only tensor peak measured here."""
+    peak, kind = peak_info
+    if not traced or not traced["launches"]:
+        return None
+    per_ms = traced["ms"] / traced["launches"]
+    work = traced["work"] / traced["launches"]
+    achieved = work / (per_ms * 1e-3) / 1e12
+    return {"kernel": "ck_mma_kernel (exact int8 limb-split commitment, mma.sync m16n8k32)", "bound": "tensor",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_kind": kind, "traffic": work * CK_MMA_BYTES_PER_OP,
+            "traffic_note": "DRAM bytes per launch, scaled by operations from an ncu capture of a smaller launch",
+            "launches": traced["launches"],
+            "ms_per_launch": per_ms, "ops_per_launch": work,
+            "share_of_plain_prove": traced["ms"] / elapsed_ms if elapsed_ms else None,
+            "measured_on": "plain path (one proof at a time), CUDA events around each launch"}
 
 
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.ntt_only:
+        import torch
+        from salsaa_b200 import api
+        print(json.dumps({"ntt": ntt_bench(torch, api, args.ntt_log_coeffs)}), flush=True)
+        return 0
     return run_ours(args)
 
 

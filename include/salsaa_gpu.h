@@ -117,6 +117,14 @@ typedef struct salsaa_timing {
 const char* salsaa_last_error(void);
 /* Kernel launches this library has issued since it was loaded. */
 uint64_t salsaa_kernel_launches(void);
+/* Device-time trace for measurement (off by default): enable/reset, then read
+ * the summed device time (CUDA events on the launching stream), summed
+ * algorithmic work and launch count of a traced kernel by name.  Traced:
+ * "ck_mma_kernel" (work = exact int8 limb products x 2, as operations) and
+ * "ntt_kernel" (work = 16 bytes per coefficient).  Reading waits for the
+ * traced launches. */
+void salsaa_trace_enable(int on);
+int salsaa_trace_read(const char* name, double* total_ms, double* total_work, uint64_t* launches);
 /* Fill *out with preset "A0".."C2", "F0".."F2" (src/protocol.rs:28-123). */
 int salsaa_params_preset(const char* name, salsaa_params* out);
 /* Proof length in bytes for a parameter set (0 if the set is invalid). */
@@ -186,6 +194,15 @@ void salsaa_server_destroy(salsaa_server* s);
  * d_in may equal d_out. */
 int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uint64_t count, uint64_t q, int inverse,
                int incomplete, void* stream);
+
+/* Batched negacyclic product r = a * b mod (Y^n + 1) of `count` polynomial
+ * pairs: the device-resident, batched form of multiply_poly
+ * (hexl-bindings/hexl_wrapper.cpp, called from src/hexl/bindings.rs:60-66).
+ * Inputs canonical in [0, q).  For 16 <= n <= 4096 and 16-byte aligned
+ * buffers one fused kernel does forward, product and inverse per tile;
+ * otherwise three passes with a temporary buffer.  d_r may alias d_a/d_b. */
+int salsaa_poly_mul(const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_r, uint64_t n, uint64_t count, uint64_t q,
+                    void* stream);
 
 /* parallel_dot_series_matrix with the commitment-key rows of ctx
  * (src/arithmetic.rs:459-505): d_w is rows x width x d coefficient form;

@@ -341,7 +341,8 @@ typedef struct {
 
 static int ring_init(Ring* R, u64 d, u64 q) {
   memset(R, 0, sizeof(*R));
-  if (d < 4 || (d & (d - 1))) return -1;
+  /* ring buffers below are sized for d <= 2048 (the reference's sets use d <= 512) */
+  if (d < 4 || d > 2048 || (d & (d - 1))) return -1;
   R->d = d;
   R->n = d / 2;
   R->q = q;

@@ -48,6 +48,9 @@ PP = ctypes.POINTER(SalsaaParams)
 DEVICE_SYMBOLS = {
     "salsaa_last_error": (ctypes.c_char_p, []),
     "salsaa_kernel_launches": (U64, []),
+    "salsaa_trace_enable": (None, [INT]),
+    "salsaa_trace_read": (INT, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(U64)]),
     "salsaa_params_preset": (INT, [ctypes.c_char_p, PP]),
     "salsaa_proof_size": (U64, [PP]),
     "salsaa_workspace_bytes": (U64, [PP]),
@@ -63,6 +66,7 @@ DEVICE_SYMBOLS = {
     "salsaa_prover_timing": (INT, [VP, ctypes.POINTER(SalsaaTiming)]),
     "salsaa_prove": (INT, [VP, U64, VP, VP, U64]),
     "salsaa_ntt": (INT, [VP, VP, U64, U64, U64, INT, INT, VP]),
+    "salsaa_poly_mul": (INT, [VP, VP, VP, U64, U64, U64, VP]),
     "salsaa_commit": (INT, [VP, VP, U64, U64, VP, VP]),
     "salsaa_sumcheck": (INT, [VP, U64, U64, U64, U64, U64, U64, VP, VP, VP]),
     "salsaa_decompose": (INT, [VP, U64, U64, U64, U64, U64, VP, VP, VP]),

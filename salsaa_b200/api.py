@@ -176,6 +176,15 @@ def ntt(x, n, q, inverse=False, incomplete=False, out=None):
     return out
 
 
+def poly_mul(a, b, n, q, out=None):
+    """Batched negacyclic product of CUDA tensors whose last axis has n words
+    (multiply_poly, hexl-bindings/hexl_wrapper.cpp, for many pairs at once)."""
+    count = a.numel() // n
+    out = dev_empty(a.shape) if out is None else out
+    _check(lib().salsaa_poly_mul(_p(a), _p(b), _p(out), n, count, q, _stream()), "poly_mul")
+    return out
+
+
 def sum_check(w, d, q, seed, round_):
     """norm_check_1 + both sum_check repetitions (src/subroutines/fast_norm_check.rs:135-320).
     w: CUDA tensor rows x n -> (claims[rows], polys[2, log2 n, rows, 3])."""

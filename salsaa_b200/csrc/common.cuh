@@ -128,3 +128,8 @@ int salsaa_set_cuda_error(cudaError_t e, const char* what);
 int salsaa_set_error(int code, const char* msg);
 // Counts kernel launches issued by this library (reported by the benchmark).
 void salsaa_count_launch();
+// Optional device-time trace of named kernels (off unless enabled through the
+// C ABI): an event pair on the launching stream around each traced launch.
+// `work` is the launch's algorithmic work (bytes or operations, per kernel).
+int salsaa_trace_begin(const char* name, cudaStream_t st, double work);
+void salsaa_trace_end(int token, cudaStream_t st);

@@ -27,22 +27,6 @@ inline unsigned grid_1d(u64 work, unsigned threads, unsigned cap = 148 * 32) {
   return (unsigned)g;
 }
 
-// Warp + block reduction of a value mod q; result valid in thread 0.
-__device__ __forceinline__ u64 warp_add_mod(u64 v, u64 q) {
-  for (int o = 16; o > 0; o >>= 1) v = add_mod(v, __shfl_down_sync(0xffffffffu, v, o), q);
-  return v;
-}
-__device__ u64 block_add_mod(u64 v, u64 q, u64* sm /* >= 32 words */) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  v = warp_add_mod(v, q);
-  __syncthreads();
-  if (lane == 0) sm[wid] = v;
-  __syncthreads();
-  v = (threadIdx.x < (unsigned)nw) ? sm[threadIdx.x] : 0;
-  if (wid == 0) v = warp_add_mod(v, q);
-  return v;
-}
-
 // Accumulate a reduced value into a global sum kept mod q.  With q < 2^50
 // and fewer than 2^13 contributions a plain 64-bit add cannot overflow and
 // the consumer reduces at the end; otherwise add modulo q with a CAS loop.
@@ -178,6 +162,17 @@ int launch_fill(u64* p, u64 n, u64 v, cudaStream_t st) {
   if (!n) return 0;
   fill_kernel<<<grid_1d(n, 256), 256, 0, st>>>(p, n, v);
   return check_launch("fill");
+}
+
+__global__ void pointwise_mul_kernel(u64* r, const u64* b, u64 n, ModQ M) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    r[i] = mul_mod(M, r[i], b[i]);
+}
+
+int launch_pointwise_mul(u64* r, const u64* b, u64 n, u64 q, cudaStream_t st) {
+  if (!n) return 0;
+  pointwise_mul_kernel<<<grid_1d(n, 256), 256, 0, st>>>(r, b, n, make_modq(q));
+  return check_launch("pointwise_mul");
 }
 
 // ---------------------------------------------------------------------------
@@ -1460,8 +1455,12 @@ static int launch_ck_mma_t(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, co
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ck_mma smem attribute");
   }
   dim3 g(n, nmt, (unsigned)(a.width / Bw));
+  // algorithmic work: the exact byte-limb products, 3 key components x 7 bytes
+  // against 2 witness parts x 7 bytes per (key row, witness row, element, slot)
+  const int tr = salsaa_trace_begin("ck_mma_kernel", st, 2.0 * 294.0 * a.nck * a.rows * (double)a.width * n);
   kern<<<g, 256, smem, st>>>(a.tl8, a.w, a.rows, a.width, a.nck, nmt, n, a.ck_bt, Bw, a.thi, a.ck_nhi, M, zeta,
                              a.acc, plain);
+  salsaa_trace_end(tr, st);
   return check_launch("ck_mma");
 }
 

@@ -52,6 +52,8 @@ inline u64 ck_tl8_bytes(u32 nck, u32 n, u32 bt) { return (u64)n * ((nck + CKM_RO
 int launch_ck_tl8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* tl8, cudaStream_t st);
 int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState* ds, cudaStream_t st);
 int launch_fill(u64* p, u64 n, u64 v, cudaStream_t st);
+// r[i] = r[i] * b[i] mod q (canonical inputs)
+int launch_pointwise_mul(u64* r, const u64* b, u64 n, u64 q, cudaStream_t st);
 
 // sumcheck of `rows` witness rows (coefficient form, length nlen each), both
 // amplification repetitions at once; see sumcheck implementation for buffers.

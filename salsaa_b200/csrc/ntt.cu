@@ -157,10 +157,385 @@ __global__ void __launch_bounds__(256) ntt_kernel(const u64* in, u64* out, u64 c
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident NTT for 16 <= n <= 4096 (q < 2^62, which the tables
+// guarantee).  Each thread holds 16 coefficients of one transform unit (a
+// full polynomial, or one half of a ring element in incomplete mode) and runs
+// up to 4 butterfly stages on them in registers between exchanges through
+// shared memory, so a 1024-point transform takes 3 exchanges instead of 10.
+// Butterflies are Harvey's lazy variants of the Cooley-Tukey (forward) and
+// Gentleman-Sande (inverse) butterflies with Shoup multiplication: forward
+// values stay in [0, 4q) and inverse values in [0, 2q), which needs 4q < 2^64;
+// one correction at the end makes the outputs canonical, so they equal the
+// fully reduced transform exactly.
+//
+// Stage numbering follows the generic kernel above: forward stage g pairs
+// elements t = n >> (g+1) apart with twiddle fwd[2^g + j / 2t]; inverse stage
+// g pairs elements t = 2^g apart with twiddle inv[(n >> (g+1)) + j / 2t].  A
+// phase covering stages g0 .. g0+S-1 gives each thread "mini-blocks" of 2^S
+// elements e = blk * (stride << S) + r + k * stride, k < 2^S, whose pairs in
+// all S stages stay inside the mini-block (stride = n >> (g0+S) forward,
+// 2^g0 inverse).
+//
+// The first phase reads global memory and the last writes it directly: the
+// strided side (forward input, inverse output) is coalesced across lanes,
+// including the even/odd interleave of incomplete mode (lanes alternate
+// halves); the contiguous side (forward output, inverse input: 2^S
+// consecutive coefficients per thread) uses 16-byte vector accesses, so it
+// needs 16-byte aligned buffers.  Shared memory holds 4096 coefficients with
+// one padding word every 16 to spread the strided phases over the banks.
+// ---------------------------------------------------------------------------
+namespace {
+
+__host__ __device__ constexpr int ph_count(int L) { return (L + 3) / 4; }
+__host__ __device__ constexpr int ph_size(int L, int p) { return L / ph_count(L) + (p < L % ph_count(L) ? 1 : 0); }
+__host__ __device__ constexpr int ph_start(int L, int p) { return p == 0 ? 0 : ph_start(L, p - 1) + ph_size(L, p - 1); }
+
+constexpr u32 NR_TILE = 4096;  // coefficients per CTA
+__device__ __forceinline__ u32 npad(u32 p) { return p + (p >> 4); }
+
+// x * w mod q in [0, 2q) for any 64-bit x (Shoup, without the final correction)
+__device__ __forceinline__ u64 shoup_lazy(u64 x, u64 w, u64 wp, u64 q) { return x * w - __umul64hi(x, wp) * q; }
+
+struct NrCtx {
+  const NttDev* T;
+  u64 q, q2;
+};
+
+template <int LOGN, int P, bool INV>
+__device__ __forceinline__ void nr_compute(u64 (&x)[16], u32 tu, const NttDev& T, u64 q, u64 q2) {
+  constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
+  constexpr u32 N = 1u << LOGN, TPU = N / 16, MB = 16 >> S, K = 1u << S;
+  constexpr u32 LSTR = INV ? G0 : LOGN - G0 - S;  // log2(stride)
+#pragma unroll
+  for (u32 j = 0; j < MB; j++) {
+    const u32 mb = tu + j * TPU, blk = mb >> LSTR;
+    u64* v = x + j * (1u << S);
+    // pairs p < 2^(S-1) of level l: k = (sb << (l'+1)) + kk, one twiddle per sb
+#pragma unroll
+    for (int l = 0; l < S; l++) {
+      const u32 lt = INV ? l : S - 1 - l;  // log2 of the pair distance in k
+      const u32 t = 1u << lt;
+      u64 w = 0, wp = 0;
+#pragma unroll
+      for (u32 p = 0; p < K / 2; p++) {
+        const u32 sb = p >> lt, kk = p & (t - 1), k = (sb << (lt + 1)) + kk;
+        if (kk == 0) {
+          const u32 idx = INV ? (N >> (G0 + l + 1)) + (blk << (S - l - 1)) + sb : (1u << (G0 + l)) + (blk << l) + sb;
+          w = __ldg((INV ? T.inv : T.fwd) + idx);
+          wp = __ldg((INV ? T.invp : T.fwdp) + idx);
+        }
+        if (!INV) {
+          u64 a = v[k];
+          a = a >= q2 ? a - q2 : a;
+          const u64 b = shoup_lazy(v[k + t], w, wp, q);
+          v[k] = a + b;
+          v[k + t] = a - b + q2;
+        } else {
+          const u64 a = v[k], b = v[k + t];
+          u64 s2 = a + b;
+          s2 = s2 >= q2 ? s2 - q2 : s2;
+          v[k] = s2;
+          v[k + t] = shoup_lazy(a - b + q2, w, wp, q);
+        }
+      }
+    }
+  }
+}
+
+// element index (within its unit) of register (j, k) in phase P
+template <int LOGN, int P, bool INV>
+__device__ __forceinline__ u32 nr_elem(u32 tu, u32 j, u32 k) {
+  constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
+  constexpr u32 N = 1u << LOGN, TPU = N / 16;
+  constexpr u32 LSTR = INV ? G0 : LOGN - G0 - S;
+  const u32 mb = tu + j * TPU, blk = mb >> LSTR, r = mb & ((1u << LSTR) - 1);
+  return (blk << (LSTR + S)) + r + (k << LSTR);
+}
+
+// Shared-memory exchange: a thread reads and writes the same positions within
+// a phase, so a phase can update the tile in place.
+template <int LOGN, int P, bool INV>
+__device__ __forceinline__ void nr_load_smem(u64 (&x)[16], const u64* sm, u32 unit, u32 tu) {
+  constexpr int S = ph_size(LOGN, P);
+  constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
+#pragma unroll
+  for (u32 j = 0; j < MB; j++)
+#pragma unroll
+    for (u32 k = 0; k < K; k++) x[j * K + k] = sm[npad(unit * N + nr_elem<LOGN, P, INV>(tu, j, k))];
+}
+template <int LOGN, int P, bool INV>
+__device__ __forceinline__ void nr_store_smem(const u64 (&x)[16], u64* sm, u32 unit, u32 tu) {
+  constexpr int S = ph_size(LOGN, P);
+  constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
+#pragma unroll
+  for (u32 j = 0; j < MB; j++)
+#pragma unroll
+    for (u32 k = 0; k < K; k++) sm[npad(unit * N + nr_elem<LOGN, P, INV>(tu, j, k))] = x[j * K + k];
+}
+
+// Global side of the first phase (P = 0).
+template <int LOGN, bool INC, bool INV>
+__device__ __forceinline__ void nr_load_global(u64 (&x)[16], const u64* __restrict__ in, u64 ug, u32 tu) {
+  constexpr int S = ph_size(LOGN, 0);
+  constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
+  if (!INV) {  // strided: e = r + k * stride (blk = 0), coalesced across lanes
+#pragma unroll
+    for (u32 j = 0; j < MB; j++)
+#pragma unroll
+      for (u32 k = 0; k < K; k++) {
+        const u32 e = nr_elem<LOGN, 0, INV>(tu, j, k);
+        const u64 g = INC ? (ug >> 1) * (2 * N) + 2 * e + (ug & 1) : ug * N + e;
+        x[j * K + k] = __ldg(in + g);
+      }
+  } else {  // contiguous 2^S coefficients per mini-block
+#pragma unroll
+    for (u32 j = 0; j < MB; j++) {
+      const ulonglong2* src = (const ulonglong2*)(in + ug * N + nr_elem<LOGN, 0, INV>(tu, j, 0));
+#pragma unroll
+      for (u32 k = 0; k < K / 2; k++) {
+        const ulonglong2 v = __ldg(src + k);
+        x[j * K + 2 * k] = v.x;
+        x[j * K + 2 * k + 1] = v.y;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ u64 nr_canon4(u64 a, u64 q, u64 q2) {  // [0, 4q) -> [0, q)
+  a = a >= q2 ? a - q2 : a;
+  return a >= q ? a - q : a;
+}
+
+// Global side of the last phase: canonical forward output (contiguous), or
+// the inverse output scaled by 1/n (strided).
+template <int LOGN, bool INC, bool INV>
+__device__ __forceinline__ void nr_store_global(const u64 (&x)[16], u64* __restrict__ out, u64 ug, u32 tu,
+                                                const NttDev& T, u64 q, u64 q2) {
+  constexpr int P = ph_count(LOGN) - 1, S = ph_size(LOGN, P);
+  constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
+  if (!INV) {
+#pragma unroll
+    for (u32 j = 0; j < MB; j++) {
+      ulonglong2* dst = (ulonglong2*)(out + ug * N + nr_elem<LOGN, P, INV>(tu, j, 0));
+#pragma unroll
+      for (u32 k = 0; k < K / 2; k++)
+        dst[k] = make_ulonglong2(nr_canon4(x[j * K + 2 * k], q, q2), nr_canon4(x[j * K + 2 * k + 1], q, q2));
+    }
+  } else {
+#pragma unroll
+    for (u32 j = 0; j < MB; j++)
+#pragma unroll
+      for (u32 k = 0; k < K; k++) {
+        const u32 e = nr_elem<LOGN, P, INV>(tu, j, k);
+        u64 v = shoup_lazy(x[j * K + k], T.ninv, T.ninvp, q);
+        v = v >= q ? v - q : v;
+        const u64 g = INC ? (ug >> 1) * (2 * N) + 2 * e + (ug & 1) : ug * N + e;
+        out[g] = v;
+      }
+  }
+}
+
+// Phases P .. PEND-1 entirely through shared memory.
+template <int LOGN, int P, int PEND, bool INV>
+__device__ __forceinline__ void nr_mid(u64 (&x)[16], u64* sm, u32 unit, u32 tu, bool active, const NttDev& T,
+                                       u64 q, u64 q2) {
+  if constexpr (P < PEND) {
+    if (active) {
+      nr_load_smem<LOGN, P, INV>(x, sm, unit, tu);
+      nr_compute<LOGN, P, INV>(x, tu, T, q, q2);
+      nr_store_smem<LOGN, P, INV>(x, sm, unit, tu);
+    }
+    __syncthreads();
+    nr_mid<LOGN, P + 1, PEND, INV>(x, sm, unit, tu, active, T, q, q2);
+  }
+}
+
+// Thread -> (unit in tile, thread within unit); in incomplete mode lanes
+// alternate the two halves of an element so the interleaved side coalesces.
+template <int LOGN, bool INC>
+__device__ __forceinline__ void nr_map(u32 tid, u32& unit, u32& tu) {
+  constexpr u32 TPU = (1u << LOGN) / 16;
+  if (INC) {
+    unit = 2 * (tid / (2 * TPU)) + (tid & 1);
+    tu = (tid % (2 * TPU)) >> 1;
+  } else {
+    unit = tid / TPU;
+    tu = tid % TPU;
+  }
+}
+
+template <int LOGN, bool INC, bool INV>
+__global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u64 units, NttDev T) {
+  constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
+  constexpr int NPH = ph_count(LOGN);
+  static_assert(!INC || UPT % 2 == 0, "incomplete mode keeps both halves of an element in one tile");
+  __shared__ u64 sm[NR_TILE + NR_TILE / 16];
+  u32 unit, tu;
+  nr_map<LOGN, INC>(threadIdx.x, unit, tu);
+  const u64 ug = (u64)blockIdx.x * UPT + unit;
+  const bool active = ug < units;
+  const u64 q = T.q, q2 = 2 * T.q;
+  u64 x[16];
+  if (active) {
+    nr_load_global<LOGN, INC, INV>(x, in, ug, tu);
+    nr_compute<LOGN, 0, INV>(x, tu, T, q, q2);
+  }
+  if constexpr (NPH > 1) {
+    if (active) nr_store_smem<LOGN, 0, INV>(x, sm, unit, tu);
+    __syncthreads();
+    nr_mid<LOGN, 1, NPH - 1, INV>(x, sm, unit, tu, active, T, q, q2);
+    if (active) {
+      nr_load_smem<LOGN, NPH - 1, INV>(x, sm, unit, tu);
+      nr_compute<LOGN, NPH - 1, INV>(x, tu, T, q, q2);
+    }
+  }
+  if (active) nr_store_global<LOGN, INC, INV>(x, out, ug, tu, T, q, q2);
+}
+
+// Fused negacyclic product r = a * b mod (Y^n + 1) for a batch of polynomials:
+// forward transforms of a and b, the pointwise product and the inverse
+// transform in one pass over a tile, so HBM sees a and b read once and r
+// written once (24 bytes per coefficient instead of 72 for three separate
+// passes).  Same value as NTT^-1(NTT(a) . NTT(b)) with the generic kernels.
+template <int LOGN>
+__global__ void __launch_bounds__(256) ntt_mul_kernel(const u64* a, const u64* b, u64* r, u64 units, NttDev T,
+                                                      ModQ M) {
+  constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
+  constexpr int NPH = ph_count(LOGN), PL = NPH - 1, SL = ph_size(LOGN, PL);
+  constexpr u32 MBL = 16 >> SL, KL = 1u << SL;
+  extern __shared__ u64 nm_smem[];  // two padded tiles
+  u64* sa = nm_smem;
+  u64* sb = nm_smem + NR_TILE + NR_TILE / 16;
+  u32 unit, tu;
+  nr_map<LOGN, false>(threadIdx.x, unit, tu);
+  const u64 ug = (u64)blockIdx.x * UPT + unit;
+  const bool active = ug < units;
+  const u64 q = T.q, q2 = 2 * T.q;
+  u64 x[16];
+  // forward transform of a, left canonical in sa
+  if (active) {
+    nr_load_global<LOGN, false, false>(x, a, ug, tu);
+    nr_compute<LOGN, 0, false>(x, tu, T, q, q2);
+  }
+  if constexpr (NPH > 1) {
+    if (active) nr_store_smem<LOGN, 0, false>(x, sa, unit, tu);
+    __syncthreads();
+    nr_mid<LOGN, 1, PL, false>(x, sa, unit, tu, active, T, q, q2);
+    if (active) {
+      nr_load_smem<LOGN, PL, false>(x, sa, unit, tu);
+      nr_compute<LOGN, PL, false>(x, tu, T, q, q2);
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (u32 i = 0; i < 16; i++) x[i] = nr_canon4(x[i], q, q2);
+    nr_store_smem<LOGN, PL, false>(x, sa, unit, tu);
+  }
+  // forward transform of b through sb, ending in registers
+  if (active) {
+    nr_load_global<LOGN, false, false>(x, b, ug, tu);
+    nr_compute<LOGN, 0, false>(x, tu, T, q, q2);
+  }
+  if constexpr (NPH > 1) {
+    if (active) nr_store_smem<LOGN, 0, false>(x, sb, unit, tu);
+    __syncthreads();
+    nr_mid<LOGN, 1, PL, false>(x, sb, unit, tu, active, T, q, q2);
+    if (active) {
+      nr_load_smem<LOGN, PL, false>(x, sb, unit, tu);
+      nr_compute<LOGN, PL, false>(x, tu, T, q, q2);
+    }
+  }
+  // pointwise product into sa (each thread owns these positions of sa)
+  if (active) {
+#pragma unroll
+    for (u32 j = 0; j < MBL; j++)
+#pragma unroll
+      for (u32 k = 0; k < KL; k++) {
+        const u32 pos = npad(unit * N + nr_elem<LOGN, PL, false>(tu, j, k));
+        sa[pos] = mul_mod(M, nr_canon4(x[j * KL + k], q, q2), sa[pos]);
+      }
+  }
+  __syncthreads();
+  // inverse transform from sa to r
+  if (active) {
+    nr_load_smem<LOGN, 0, true>(x, sa, unit, tu);
+    nr_compute<LOGN, 0, true>(x, tu, T, q, q2);
+  }
+  if constexpr (NPH > 1) {
+    if (active) nr_store_smem<LOGN, 0, true>(x, sa, unit, tu);
+    __syncthreads();
+    nr_mid<LOGN, 1, PL, true>(x, sa, unit, tu, active, T, q, q2);
+    if (active) {
+      nr_load_smem<LOGN, PL, true>(x, sa, unit, tu);
+      nr_compute<LOGN, PL, true>(x, tu, T, q, q2);
+    }
+  }
+  if (active) nr_store_global<LOGN, false, true>(x, r, ug, tu, T, q, q2);
+}
+
+template <int LOGN>
+int nm_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& T, cudaStream_t st) {
+  constexpr u32 UPT = NR_TILE >> LOGN;
+  const u64 blocks = (count + UPT - 1) / UPT;
+  if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt_mul: batch too large");
+  const size_t smem = 2 * (NR_TILE + NR_TILE / 16) * sizeof(u64);
+  cudaError_t e = cudaFuncSetAttribute(ntt_mul_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ntt_mul smem attribute");
+  ntt_mul_kernel<LOGN><<<(unsigned)blocks, 256, smem, st>>>(a, b, r, count, T, make_modq(T.q));
+  return 0;
+}
+
+template <int LOGN>
+int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomplete, bool inverse, cudaStream_t st) {
+  constexpr u32 UPT = NR_TILE >> LOGN;
+  const u64 blocks = (units + UPT - 1) / UPT;
+  if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt: batch too large");
+  if (incomplete) {
+    if constexpr (UPT >= 2) {
+      if (inverse)
+        ntt_reg_kernel<LOGN, true, true><<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
+      else
+        ntt_reg_kernel<LOGN, true, false><<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
+    } else {
+      return salsaa_set_error(-2, "ntt: incomplete register path needs two halves per tile");
+    }
+  } else if (inverse) {
+    ntt_reg_kernel<LOGN, false, true><<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
+  } else {
+    ntt_reg_kernel<LOGN, false, false><<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
+  }
+  return 0;
+}
+
+}  // namespace
+
 int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incomplete, bool inverse,
                cudaStream_t st) {
   if (count == 0) return 0;
   const u32 d = incomplete ? 2 * T.n : T.n;
+  const bool aligned = ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
+  if (aligned && T.n >= 16 && T.n <= (incomplete ? 2048u : 4096u)) {
+    const u64 units = incomplete ? 2 * count : count;
+    const int tr = salsaa_trace_begin("ntt_kernel", st, 16.0 * (double)count * d);
+    int rc = 0;
+    switch (T.logn) {
+      case 4: rc = nr_launch<4>(in, out, units, T, incomplete, inverse, st); break;
+      case 5: rc = nr_launch<5>(in, out, units, T, incomplete, inverse, st); break;
+      case 6: rc = nr_launch<6>(in, out, units, T, incomplete, inverse, st); break;
+      case 7: rc = nr_launch<7>(in, out, units, T, incomplete, inverse, st); break;
+      case 8: rc = nr_launch<8>(in, out, units, T, incomplete, inverse, st); break;
+      case 9: rc = nr_launch<9>(in, out, units, T, incomplete, inverse, st); break;
+      case 10: rc = nr_launch<10>(in, out, units, T, incomplete, inverse, st); break;
+      case 11: rc = nr_launch<11>(in, out, units, T, incomplete, inverse, st); break;
+      default: rc = nr_launch<12>(in, out, units, T, incomplete, inverse, st); break;
+    }
+    salsaa_trace_end(tr, st);
+    if (rc) return rc;
+    salsaa_count_launch();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ntt launch");
+  }
   // 32 KiB of elements per CTA (at least one element).
   u32 epb = 4096 / d;
   if (epb == 0) epb = 1;
@@ -172,13 +547,43 @@ int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incompl
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ntt smem attribute");
     }
+    // algorithmic bytes: every coefficient read once and written once
+    const int tr = salsaa_trace_begin("ntt_kernel", st, 16.0 * (double)count * d);
     kern<<<(unsigned)blocks, 256, smem, st>>>(in, out, count, T, epb);
+    salsaa_trace_end(tr, st);
     salsaa_count_launch();
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ntt launch");
   };
   if (incomplete) return inverse ? launch(ntt_kernel<true, true>) : launch(ntt_kernel<true, false>);
   return inverse ? launch(ntt_kernel<false, true>) : launch(ntt_kernel<false, false>);
+}
+
+bool ntt_mul_fused_ok(const u64* a, const u64* b, const u64* r, const NttDev& T) {
+  return T.n >= 16 && T.n <= 4096 && (uintptr_t)a % 16 == 0 && (uintptr_t)b % 16 == 0 && (uintptr_t)r % 16 == 0;
+}
+
+int ntt_mul_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& T, cudaStream_t st) {
+  if (count == 0) return 0;
+  if (!ntt_mul_fused_ok(a, b, r, T)) return salsaa_set_error(-2, "ntt_mul: size or alignment not supported");
+  const int tr = salsaa_trace_begin("ntt_mul_kernel", st, 24.0 * (double)count * T.n);
+  int rc = 0;
+  switch (T.logn) {
+    case 4: rc = nm_launch<4>(a, b, r, count, T, st); break;
+    case 5: rc = nm_launch<5>(a, b, r, count, T, st); break;
+    case 6: rc = nm_launch<6>(a, b, r, count, T, st); break;
+    case 7: rc = nm_launch<7>(a, b, r, count, T, st); break;
+    case 8: rc = nm_launch<8>(a, b, r, count, T, st); break;
+    case 9: rc = nm_launch<9>(a, b, r, count, T, st); break;
+    case 10: rc = nm_launch<10>(a, b, r, count, T, st); break;
+    case 11: rc = nm_launch<11>(a, b, r, count, T, st); break;
+    default: rc = nm_launch<12>(a, b, r, count, T, st); break;
+  }
+  salsaa_trace_end(tr, st);
+  if (rc) return rc;
+  salsaa_count_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ntt_mul launch");
 }
 
 }  // namespace salsaa

@@ -32,6 +32,12 @@ const NttDev* ntt_tables(u32 n, u64 q);
 int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incomplete, bool inverse,
                cudaStream_t st);
 
+// Fused batched negacyclic product r = a * b mod (Y^n + 1), count polynomials
+// of n words each (r may alias a or b).  Needs 16 <= n <= 4096 and 16-byte
+// aligned buffers (ntt_mul_fused_ok); the C ABI falls back to three passes.
+bool ntt_mul_fused_ok(const u64* a, const u64* b, const u64* r, const NttDev& T);
+int ntt_mul_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& T, cudaStream_t st);
+
 // ---- ring helpers in slot form, used by several kernels ----
 // (a_e + X a_o)(b_e + X b_o) = a_e b_e + zeta a_o b_o + X (a_o b_e + a_e b_o)
 // Inputs are taken by value, so outputs may alias them.

@@ -33,6 +33,69 @@ int salsaa_set_cuda_error(cudaError_t e, const char* what) {
 }
 extern "C" const char* salsaa_last_error(void) { return g_err.c_str(); }
 
+// ---- device-time trace ------------------------------------------------------
+namespace {
+constexpr int TRACE_MAX = 8192;
+struct TraceRec {
+  const char* name;
+  cudaEvent_t a, b;
+  double work;
+  int done;
+};
+std::mutex g_trace_mu;
+std::atomic<int> g_trace_on{0};
+std::vector<TraceRec> g_trace;
+}  // namespace
+
+int salsaa_trace_begin(const char* name, cudaStream_t st, double work) {
+  if (!g_trace_on.load(std::memory_order_relaxed)) return -1;
+  std::lock_guard<std::mutex> lk(g_trace_mu);
+  if ((int)g_trace.size() >= TRACE_MAX) return -1;
+  TraceRec r{name, nullptr, nullptr, work, 0};
+  if (cudaEventCreate(&r.a) != cudaSuccess || cudaEventCreate(&r.b) != cudaSuccess) return -1;
+  cudaEventRecord(r.a, st);
+  g_trace.push_back(r);
+  return (int)g_trace.size() - 1;
+}
+void salsaa_trace_end(int token, cudaStream_t st) {
+  if (token < 0) return;
+  std::lock_guard<std::mutex> lk(g_trace_mu);
+  if (token < (int)g_trace.size()) {
+    cudaEventRecord(g_trace[token].b, st);
+    g_trace[token].done = 1;
+  }
+}
+extern "C" void salsaa_trace_enable(int on) {
+  std::lock_guard<std::mutex> lk(g_trace_mu);
+  for (TraceRec& r : g_trace) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  g_trace.clear();
+  g_trace_on.store(on ? 1 : 0);
+}
+extern "C" int salsaa_trace_read(const char* name, double* total_ms, double* total_work, uint64_t* launches) {
+  if (!name || !total_ms || !total_work || !launches) return salsaa_set_error(-1, "trace_read: null argument");
+  std::lock_guard<std::mutex> lk(g_trace_mu);
+  double t = 0, wk = 0;
+  uint64_t n = 0;
+  for (TraceRec& r : g_trace) {
+    if (!r.done || strcmp(r.name, name)) continue;
+    cudaError_t e = cudaEventSynchronize(r.b);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "trace_read");
+    float ms = 0;
+    e = cudaEventElapsedTime(&ms, r.a, r.b);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "trace_read");
+    t += ms;
+    wk += r.work;
+    n++;
+  }
+  *total_ms = t;
+  *total_work = wk;
+  *launches = n;
+  return 0;
+}
+
 static std::atomic<uint64_t> g_launches{0};
 void salsaa_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 extern "C" uint64_t salsaa_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
@@ -850,6 +913,24 @@ extern "C" int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uin
   const NttDev* T = ntt_tables((u32)nn, q);
   if (!T || nn > 8192) return salsaa_set_error(-1, "ntt: no NTT for (n, q)");
   return ntt_launch(d_in, d_out, count, *T, incomplete != 0, inverse != 0, (cudaStream_t)stream);
+}
+
+extern "C" int salsaa_poly_mul(const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_r, uint64_t n,
+                               uint64_t count, uint64_t q, void* stream) {
+  if (!d_a || !d_b || !d_r) return salsaa_set_error(-1, "poly_mul: null pointer");
+  const NttDev* T = ntt_tables((u32)n, q);
+  if (!T || n > 8192) return salsaa_set_error(-1, "poly_mul: no NTT for (n, q)");
+  if (count == 0) return 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (ntt_mul_fused_ok(d_a, d_b, d_r, *T)) return ntt_mul_launch(d_a, d_b, d_r, count, *T, st);
+  // three passes: NTT(a) -> r, NTT(b) -> tmp, r *= tmp, INTT(r)
+  Tmp t(st);
+  u64* tb;
+  TRY(t.get(&tb, count * n));
+  TRY(ntt_launch(d_b, tb, count, *T, false, false, st));
+  TRY(ntt_launch(d_a, d_r, count, *T, false, false, st));
+  TRY(launch_pointwise_mul(d_r, tb, count * n, q, st));
+  return ntt_launch(d_r, d_r, count, *T, false, true, st);
 }
 
 extern "C" int salsaa_commit(salsaa_ctx* c, const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t* d_out,

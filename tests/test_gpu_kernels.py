@@ -14,8 +14,9 @@ def api(gpu_lib, cuda):
     return A
 
 
-@pytest.mark.parametrize("n,q", [(2, 17), (8, 65537), (64, P.Q62), (128, P.Q62), (256, P.Q62), (1024, P.Q62),
-                                 (64, P.Q0), (128, P.Q1), (256, P.Q2), (4096, P.Q62)])
+@pytest.mark.parametrize("n,q", [(2, 17), (8, 65537), (16, P.Q62), (32, P.Q62), (64, P.Q62), (128, P.Q62),
+                                 (256, P.Q62), (512, P.Q62), (1024, P.Q62), (2048, P.Q62), (64, P.Q0), (128, P.Q1),
+                                 (256, P.Q2), (4096, P.Q62), (8192, P.Q62)])
 def test_ntt_full(api, oracle, n, q):
     rng = np.random.default_rng(n)
     x = rand_mod(rng, (37, n), q)
@@ -27,17 +28,84 @@ def test_ntt_full(api, oracle, n, q):
     assert np.array_equal(api.to_host(d), x)
 
 
-@pytest.mark.parametrize("d,q", [(4, 17), (16, P.Q0), (128, P.Q0), (256, P.Q1), (512, P.Q2), (128, P.Q62)])
+@pytest.mark.parametrize("d,q", [(4, 17), (16, P.Q0), (32, P.Q62), (64, P.Q62), (128, P.Q0), (256, P.Q1),
+                                 (512, P.Q2), (128, P.Q62), (1024, P.Q62), (4096, P.Q62), (8192, P.Q62)])
 def test_ntt_incomplete(api, oracle, d, q):
     rng = np.random.default_rng(d)
     x = rand_mod(rng, (53, d), q)
-    want = oracle.ring_to_slot(x, q)
+    if d <= 2048:
+        want = oracle.ring_to_slot(x, q)
+    else:  # beyond the oracle's ring size: [NTT(even) | NTT(odd)] by definition
+        want = np.concatenate([oracle.ntt_forward(x[:, 0::2].copy(), q), oracle.ntt_forward(x[:, 1::2].copy(), q)],
+                              axis=1)
     t = api.to_dev(x)
     out = api.dev_empty(t.shape)
     api.ntt(t, d, q, incomplete=True, out=out)
     assert np.array_equal(api.to_host(out), want)
     api.ntt(out, d, q, inverse=True, incomplete=True)
     assert np.array_equal(api.to_host(out), x)
+
+
+@pytest.mark.parametrize("incomplete", [False, True])
+def test_ntt_unaligned_and_out_of_place(api, oracle, incomplete):
+    """Buffers that are only 8-byte aligned take the generic kernel; results agree."""
+    import torch
+    q, n = P.Q62, 256
+    rng = np.random.default_rng(17)
+    x = rand_mod(rng, (9, n), q)
+    want = oracle.ring_to_slot(x, q) if incomplete else oracle.ntt_forward(x, q)
+    big = torch.zeros(9 * n + 1, dtype=torch.int64, device="cuda")
+    big[1:] = api.to_dev(x).view(-1)
+    view = big[1:].view(9, n)
+    out = api.dev_empty((9, n))
+    api.ntt(view, n, q, incomplete=incomplete, out=out)
+    assert np.array_equal(api.to_host(out), want)
+    api.ntt(view, n, q, incomplete=incomplete)  # in place, unaligned
+    assert np.array_equal(api.to_host(view), want)
+    api.ntt(view, n, q, inverse=True, incomplete=incomplete)
+    assert np.array_equal(api.to_host(view), x)
+
+
+def test_ntt_ragged_tiles(api, oracle):
+    """Batch sizes that leave the last tile of 4096 coefficients partly empty."""
+    q = P.Q0
+    rng = np.random.default_rng(23)
+    for count in (1, 31, 33, 95):
+        x = rand_mod(rng, (count, 128), q)
+        out = api.dev_empty(x.shape)
+        api.ntt(api.to_dev(x), 128, q, incomplete=True, out=out)
+        assert np.array_equal(api.to_host(out), oracle.ring_to_slot(x, q))
+        y = rand_mod(rng, (count, 1024), P.Q62)
+        t = api.to_dev(y)
+        api.ntt(t, 1024, P.Q62)
+        assert np.array_equal(api.to_host(t), oracle.ntt_forward(y, P.Q62))
+
+
+@pytest.mark.parametrize("n,q,count", [(16, P.Q62, 7), (64, P.Q62, 65), (128, P.Q0, 33), (256, P.Q62, 17),
+                                       (1024, P.Q62, 9), (4096, P.Q62, 3), (8, 65537, 5), (8192, P.Q62, 2)])
+def test_poly_mul(api, oracle, n, q, count):
+    """Batched negacyclic product against the oracle's multiply_poly, per pair."""
+    rng = np.random.default_rng(n + count)
+    a, b = rand_mod(rng, (count, n), q), rand_mod(rng, (count, n), q)
+    got = api.to_host(api.poly_mul(api.to_dev(a), api.to_dev(b), n, q))
+    for i in range(count):
+        assert np.array_equal(got[i], oracle.multiply_poly(a[i], b[i], q)), i
+
+
+def test_poly_mul_in_place_and_unaligned(api, oracle):
+    import torch
+    q, n, count = P.Q62, 64, 5
+    rng = np.random.default_rng(2)
+    a, b = rand_mod(rng, (count, n), q), rand_mod(rng, (count, n), q)
+    want = np.stack([oracle.multiply_poly(a[i], b[i], q) for i in range(count)])
+    ta, tb = api.to_dev(a), api.to_dev(b)
+    api.poly_mul(ta, tb, n, q, out=ta)  # r aliases a
+    assert np.array_equal(api.to_host(ta), want)
+    big = torch.zeros(count * n + 1, dtype=torch.int64, device="cuda")
+    big[1:] = api.to_dev(a).view(-1)
+    va = big[1:].view(count, n)
+    got = api.poly_mul(va, tb, n, q)  # 8-byte aligned input: three-pass path
+    assert np.array_equal(api.to_host(got), want)
 
 
 def test_ntt_large_batch(api, oracle):
