@@ -195,6 +195,15 @@ void salsaa_server_destroy(salsaa_server* s);
 int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uint64_t count, uint64_t q, int inverse,
                int incomplete, void* stream);
 
+/* Self-test of the int8 tensor-core building block used by the commitment
+ * kernels (tcgen05.mma kind::i8, accumulator in tensor memory): d_out (128 x n,
+ * int32, row-major) = A (128 x k bytes, row-major) * B (n x k bytes)^T, with
+ * 16 <= n <= 256 a multiple of 16 and k a multiple of 32 up to 256.  No
+ * reference counterpart; it exists so the operand and descriptor encoding can
+ * be checked against an exact integer product. */
+int salsaa_selftest_umma_i8(const uint8_t* d_a, const uint8_t* d_b, uint32_t n, uint32_t k, int32_t* d_out,
+                            void* stream);
+
 /* Batched negacyclic product r = a * b mod (Y^n + 1) of `count` polynomial
  * pairs: the device-resident, batched form of multiply_poly
  * (hexl-bindings/hexl_wrapper.cpp, called from src/hexl/bindings.rs:60-66).

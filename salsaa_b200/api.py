@@ -185,6 +185,20 @@ def poly_mul(a, b, n, q, out=None):
     return out
 
 
+def selftest_umma_i8(a, b):
+    """Exact u8 product on the tensor cores: a (128 x k), b (n x k) uint8 numpy
+    arrays -> int32 numpy (128 x n) = a @ b.T."""
+    torch = _torch()
+    a = np.ascontiguousarray(a, dtype=np.uint8)
+    b = np.ascontiguousarray(b, dtype=np.uint8)
+    n, k = b.shape
+    ta = torch.from_numpy(a).cuda()
+    tb = torch.from_numpy(b).cuda()
+    out = torch.empty((128, n), dtype=torch.int32, device="cuda")
+    _check(lib().salsaa_selftest_umma_i8(_p(ta), _p(tb), n, k, _p(out), _stream()), "selftest_umma_i8")
+    return out.cpu().numpy()
+
+
 def sum_check(w, d, q, seed, round_):
     """norm_check_1 + both sum_check repetitions (src/subroutines/fast_norm_check.rs:135-320).
     w: CUDA tensor rows x n -> (claims[rows], polys[2, log2 n, rows, 3])."""

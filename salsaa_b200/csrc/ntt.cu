@@ -77,6 +77,7 @@ const NttDev* ntt_tables(u32 n, u64 q) {
   T->zetap = d + 5 * n;
   T->ninv = host::invmod(n % q, q);
   T->ninvp = shoup_pre(T->ninv, q);
+  T->onep = shoup_pre(1, q);
   g_tabs[key] = T;
   return T;
 }
@@ -169,6 +170,14 @@ __global__ void __launch_bounds__(256) ntt_kernel(const u64* in, u64* out, u64 c
 // one correction at the end makes the outputs canonical, so they equal the
 // fully reduced transform exactly.
 //
+// For q < 2^50 (the protocol's primes) the RELAX variants drop the per-
+// butterfly corrections: forward values grow by at most 2q per stage, so stay
+// below (2 log n + 1) q, and inverse sums at most double per stage, so stay
+// below 2^(log n) q, with the difference offset by C = 2^(log n) q instead of
+// 2q; both bounds are far below 2^63 for log n <= 12.  One Shoup reduction by
+// 1 (x - floor(x floor(2^64/q) / 2^64) q, in [0, 2q)) and a subtraction make
+// the outputs canonical.
+//
 // Stage numbering follows the generic kernel above: forward stage g pairs
 // elements t = n >> (g+1) apart with twiddle fwd[2^g + j / 2t]; inverse stage
 // g pairs elements t = 2^g apart with twiddle inv[(n >> (g+1)) + j / 2t].  A
@@ -192,6 +201,7 @@ __host__ __device__ constexpr int ph_size(int L, int p) { return L / ph_count(L)
 __host__ __device__ constexpr int ph_start(int L, int p) { return p == 0 ? 0 : ph_start(L, p - 1) + ph_size(L, p - 1); }
 
 constexpr u32 NR_TILE = 4096;  // coefficients per CTA
+constexpr u64 NR_RELAX_Q = 1ULL << 50;  // below this, butterflies skip their corrections
 __device__ __forceinline__ u32 npad(u32 p) { return p + (p >> 4); }
 
 // x * w mod q in [0, 2q) for any 64-bit x (Shoup, without the final correction)
@@ -202,8 +212,10 @@ struct NrCtx {
   u64 q, q2;
 };
 
-template <int LOGN, int P, bool INV>
+template <int LOGN, int P, bool INV, bool RELAX>
 __device__ __forceinline__ void nr_compute(u64 (&x)[16], u32 tu, const NttDev& T, u64 q, u64 q2) {
+  // inverse difference offset: 2q, or 2^LOGN q when sums are left unreduced
+  const u64 cdiff = RELAX ? (q << LOGN) : q2;
   constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
   constexpr u32 N = 1u << LOGN, TPU = N / 16, MB = 16 >> S, K = 1u << S;
   constexpr u32 LSTR = INV ? G0 : LOGN - G0 - S;  // log2(stride)
@@ -227,16 +239,16 @@ __device__ __forceinline__ void nr_compute(u64 (&x)[16], u32 tu, const NttDev& T
         }
         if (!INV) {
           u64 a = v[k];
-          a = a >= q2 ? a - q2 : a;
+          if (!RELAX) a = a >= q2 ? a - q2 : a;
           const u64 b = shoup_lazy(v[k + t], w, wp, q);
           v[k] = a + b;
           v[k + t] = a - b + q2;
         } else {
           const u64 a = v[k], b = v[k + t];
           u64 s2 = a + b;
-          s2 = s2 >= q2 ? s2 - q2 : s2;
+          if (!RELAX) s2 = s2 >= q2 ? s2 - q2 : s2;
           v[k] = s2;
-          v[k + t] = shoup_lazy(a - b + q2, w, wp, q);
+          v[k + t] = shoup_lazy(a - b + cdiff, w, wp, q);
         }
       }
     }
@@ -306,10 +318,17 @@ __device__ __forceinline__ u64 nr_canon4(u64 a, u64 q, u64 q2) {  // [0, 4q) -> 
   a = a >= q2 ? a - q2 : a;
   return a >= q ? a - q : a;
 }
+// forward output -> [0, q): [0, 4q) normally, any value below 2^64 when relaxed
+template <bool RELAX>
+__device__ __forceinline__ u64 nr_canon(u64 a, u64 q, u64 q2, u64 onep) {
+  if (!RELAX) return nr_canon4(a, q, q2);
+  a = shoup_lazy(a, 1, onep, q);
+  return a >= q ? a - q : a;
+}
 
 // Global side of the last phase: canonical forward output (contiguous), or
 // the inverse output scaled by 1/n (strided).
-template <int LOGN, bool INC, bool INV>
+template <int LOGN, bool INC, bool INV, bool RELAX>
 __device__ __forceinline__ void nr_store_global(const u64 (&x)[16], u64* __restrict__ out, u64 ug, u32 tu,
                                                 const NttDev& T, u64 q, u64 q2) {
   constexpr int P = ph_count(LOGN) - 1, S = ph_size(LOGN, P);
@@ -320,7 +339,8 @@ __device__ __forceinline__ void nr_store_global(const u64 (&x)[16], u64* __restr
       ulonglong2* dst = (ulonglong2*)(out + ug * N + nr_elem<LOGN, P, INV>(tu, j, 0));
 #pragma unroll
       for (u32 k = 0; k < K / 2; k++)
-        dst[k] = make_ulonglong2(nr_canon4(x[j * K + 2 * k], q, q2), nr_canon4(x[j * K + 2 * k + 1], q, q2));
+        dst[k] = make_ulonglong2(nr_canon<RELAX>(x[j * K + 2 * k], q, q2, T.onep),
+                                 nr_canon<RELAX>(x[j * K + 2 * k + 1], q, q2, T.onep));
     }
   } else {
 #pragma unroll
@@ -337,17 +357,17 @@ __device__ __forceinline__ void nr_store_global(const u64 (&x)[16], u64* __restr
 }
 
 // Phases P .. PEND-1 entirely through shared memory.
-template <int LOGN, int P, int PEND, bool INV>
+template <int LOGN, int P, int PEND, bool INV, bool RELAX>
 __device__ __forceinline__ void nr_mid(u64 (&x)[16], u64* sm, u32 unit, u32 tu, bool active, const NttDev& T,
                                        u64 q, u64 q2) {
   if constexpr (P < PEND) {
     if (active) {
       nr_load_smem<LOGN, P, INV>(x, sm, unit, tu);
-      nr_compute<LOGN, P, INV>(x, tu, T, q, q2);
+      nr_compute<LOGN, P, INV, RELAX>(x, tu, T, q, q2);
       nr_store_smem<LOGN, P, INV>(x, sm, unit, tu);
     }
     __syncthreads();
-    nr_mid<LOGN, P + 1, PEND, INV>(x, sm, unit, tu, active, T, q, q2);
+    nr_mid<LOGN, P + 1, PEND, INV, RELAX>(x, sm, unit, tu, active, T, q, q2);
   }
 }
 
@@ -365,7 +385,7 @@ __device__ __forceinline__ void nr_map(u32 tid, u32& unit, u32& tu) {
   }
 }
 
-template <int LOGN, bool INC, bool INV>
+template <int LOGN, bool INC, bool INV, bool RELAX>
 __global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u64 units, NttDev T) {
   constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
   constexpr int NPH = ph_count(LOGN);
@@ -379,18 +399,18 @@ __global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u
   u64 x[16];
   if (active) {
     nr_load_global<LOGN, INC, INV>(x, in, ug, tu);
-    nr_compute<LOGN, 0, INV>(x, tu, T, q, q2);
+    nr_compute<LOGN, 0, INV, RELAX>(x, tu, T, q, q2);
   }
   if constexpr (NPH > 1) {
     if (active) nr_store_smem<LOGN, 0, INV>(x, sm, unit, tu);
     __syncthreads();
-    nr_mid<LOGN, 1, NPH - 1, INV>(x, sm, unit, tu, active, T, q, q2);
+    nr_mid<LOGN, 1, NPH - 1, INV, RELAX>(x, sm, unit, tu, active, T, q, q2);
     if (active) {
       nr_load_smem<LOGN, NPH - 1, INV>(x, sm, unit, tu);
-      nr_compute<LOGN, NPH - 1, INV>(x, tu, T, q, q2);
+      nr_compute<LOGN, NPH - 1, INV, RELAX>(x, tu, T, q, q2);
     }
   }
-  if (active) nr_store_global<LOGN, INC, INV>(x, out, ug, tu, T, q, q2);
+  if (active) nr_store_global<LOGN, INC, INV, RELAX>(x, out, ug, tu, T, q, q2);
 }
 
 // Fused negacyclic product r = a * b mod (Y^n + 1) for a batch of polynomials:
@@ -398,7 +418,7 @@ __global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u
 // transform in one pass over a tile, so HBM sees a and b read once and r
 // written once (24 bytes per coefficient instead of 72 for three separate
 // passes).  Same value as NTT^-1(NTT(a) . NTT(b)) with the generic kernels.
-template <int LOGN>
+template <int LOGN, bool RELAX>
 __global__ void __launch_bounds__(256) ntt_mul_kernel(const u64* a, const u64* b, u64* r, u64 units, NttDev T,
                                                       ModQ M) {
   constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
@@ -416,34 +436,34 @@ __global__ void __launch_bounds__(256) ntt_mul_kernel(const u64* a, const u64* b
   // forward transform of a, left canonical in sa
   if (active) {
     nr_load_global<LOGN, false, false>(x, a, ug, tu);
-    nr_compute<LOGN, 0, false>(x, tu, T, q, q2);
+    nr_compute<LOGN, 0, false, RELAX>(x, tu, T, q, q2);
   }
   if constexpr (NPH > 1) {
     if (active) nr_store_smem<LOGN, 0, false>(x, sa, unit, tu);
     __syncthreads();
-    nr_mid<LOGN, 1, PL, false>(x, sa, unit, tu, active, T, q, q2);
+    nr_mid<LOGN, 1, PL, false, RELAX>(x, sa, unit, tu, active, T, q, q2);
     if (active) {
       nr_load_smem<LOGN, PL, false>(x, sa, unit, tu);
-      nr_compute<LOGN, PL, false>(x, tu, T, q, q2);
+      nr_compute<LOGN, PL, false, RELAX>(x, tu, T, q, q2);
     }
   }
   if (active) {
 #pragma unroll
-    for (u32 i = 0; i < 16; i++) x[i] = nr_canon4(x[i], q, q2);
+    for (u32 i = 0; i < 16; i++) x[i] = nr_canon<RELAX>(x[i], q, q2, T.onep);
     nr_store_smem<LOGN, PL, false>(x, sa, unit, tu);
   }
   // forward transform of b through sb, ending in registers
   if (active) {
     nr_load_global<LOGN, false, false>(x, b, ug, tu);
-    nr_compute<LOGN, 0, false>(x, tu, T, q, q2);
+    nr_compute<LOGN, 0, false, RELAX>(x, tu, T, q, q2);
   }
   if constexpr (NPH > 1) {
     if (active) nr_store_smem<LOGN, 0, false>(x, sb, unit, tu);
     __syncthreads();
-    nr_mid<LOGN, 1, PL, false>(x, sb, unit, tu, active, T, q, q2);
+    nr_mid<LOGN, 1, PL, false, RELAX>(x, sb, unit, tu, active, T, q, q2);
     if (active) {
       nr_load_smem<LOGN, PL, false>(x, sb, unit, tu);
-      nr_compute<LOGN, PL, false>(x, tu, T, q, q2);
+      nr_compute<LOGN, PL, false, RELAX>(x, tu, T, q, q2);
     }
   }
   // pointwise product into sa (each thread owns these positions of sa)
@@ -453,25 +473,25 @@ __global__ void __launch_bounds__(256) ntt_mul_kernel(const u64* a, const u64* b
 #pragma unroll
       for (u32 k = 0; k < KL; k++) {
         const u32 pos = npad(unit * N + nr_elem<LOGN, PL, false>(tu, j, k));
-        sa[pos] = mul_mod(M, nr_canon4(x[j * KL + k], q, q2), sa[pos]);
+        sa[pos] = mul_mod(M, nr_canon<RELAX>(x[j * KL + k], q, q2, T.onep), sa[pos]);
       }
   }
   __syncthreads();
   // inverse transform from sa to r
   if (active) {
     nr_load_smem<LOGN, 0, true>(x, sa, unit, tu);
-    nr_compute<LOGN, 0, true>(x, tu, T, q, q2);
+    nr_compute<LOGN, 0, true, RELAX>(x, tu, T, q, q2);
   }
   if constexpr (NPH > 1) {
     if (active) nr_store_smem<LOGN, 0, true>(x, sa, unit, tu);
     __syncthreads();
-    nr_mid<LOGN, 1, PL, true>(x, sa, unit, tu, active, T, q, q2);
+    nr_mid<LOGN, 1, PL, true, RELAX>(x, sa, unit, tu, active, T, q, q2);
     if (active) {
       nr_load_smem<LOGN, PL, true>(x, sa, unit, tu);
-      nr_compute<LOGN, PL, true>(x, tu, T, q, q2);
+      nr_compute<LOGN, PL, true, RELAX>(x, tu, T, q, q2);
     }
   }
-  if (active) nr_store_global<LOGN, false, true>(x, r, ug, tu, T, q, q2);
+  if (active) nr_store_global<LOGN, false, true, RELAX>(x, r, ug, tu, T, q, q2);
 }
 
 template <int LOGN>
@@ -480,10 +500,13 @@ int nm_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& T, cu
   const u64 blocks = (count + UPT - 1) / UPT;
   if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt_mul: batch too large");
   const size_t smem = 2 * (NR_TILE + NR_TILE / 16) * sizeof(u64);
-  cudaError_t e = cudaFuncSetAttribute(ntt_mul_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ntt_mul smem attribute");
-  ntt_mul_kernel<LOGN><<<(unsigned)blocks, 256, smem, st>>>(a, b, r, count, T, make_modq(T.q));
-  return 0;
+  auto go = [&](auto kern) -> int {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ntt_mul smem attribute");
+    kern<<<(unsigned)blocks, 256, smem, st>>>(a, b, r, count, T, make_modq(T.q));
+    return 0;
+  };
+  return T.q < NR_RELAX_Q ? go(ntt_mul_kernel<LOGN, true>) : go(ntt_mul_kernel<LOGN, false>);
 }
 
 template <int LOGN>
@@ -491,21 +514,23 @@ int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomple
   constexpr u32 UPT = NR_TILE >> LOGN;
   const u64 blocks = (units + UPT - 1) / UPT;
   if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt: batch too large");
+  const bool relax = T.q < NR_RELAX_Q;
+  auto go = [&](auto kern) -> int {
+    kern<<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
+    return 0;
+  };
   if (incomplete) {
     if constexpr (UPT >= 2) {
       if (inverse)
-        ntt_reg_kernel<LOGN, true, true><<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
-      else
-        ntt_reg_kernel<LOGN, true, false><<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
+        return relax ? go(ntt_reg_kernel<LOGN, true, true, true>) : go(ntt_reg_kernel<LOGN, true, true, false>);
+      return relax ? go(ntt_reg_kernel<LOGN, true, false, true>) : go(ntt_reg_kernel<LOGN, true, false, false>);
     } else {
       return salsaa_set_error(-2, "ntt: incomplete register path needs two halves per tile");
     }
-  } else if (inverse) {
-    ntt_reg_kernel<LOGN, false, true><<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
-  } else {
-    ntt_reg_kernel<LOGN, false, false><<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
   }
-  return 0;
+  if (inverse)
+    return relax ? go(ntt_reg_kernel<LOGN, false, true, true>) : go(ntt_reg_kernel<LOGN, false, true, false>);
+  return relax ? go(ntt_reg_kernel<LOGN, false, false, true>) : go(ntt_reg_kernel<LOGN, false, false, false>);
 }
 
 }  // namespace

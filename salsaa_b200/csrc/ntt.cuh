@@ -20,6 +20,7 @@ struct NttDev {
   const u64* inv;   // bit-reversed psi^-i
   const u64* invp;
   u64 ninv, ninvp;  // 1/n mod q and its Shoup companion
+  u64 onep;         // Shoup companion of 1: floor(2^64 / q), for reductions
   const u64* zeta;  // shift factors NTT_n(Y) (slot order), for ring products
   const u64* zetap;
 };

@@ -16,7 +16,8 @@ def api(gpu_lib, cuda):
 
 @pytest.mark.parametrize("n,q", [(2, 17), (8, 65537), (16, P.Q62), (32, P.Q62), (64, P.Q62), (128, P.Q62),
                                  (256, P.Q62), (512, P.Q62), (1024, P.Q62), (2048, P.Q62), (64, P.Q0), (128, P.Q1),
-                                 (256, P.Q2), (4096, P.Q62), (8192, P.Q62)])
+                                 (256, P.Q2), (4096, P.Q62), (8192, P.Q62), (16, P.Q0), (1024, P.Q0),
+                                 (4096, P.Q0)])
 def test_ntt_full(api, oracle, n, q):
     rng = np.random.default_rng(n)
     x = rand_mod(rng, (37, n), q)
@@ -29,7 +30,8 @@ def test_ntt_full(api, oracle, n, q):
 
 
 @pytest.mark.parametrize("d,q", [(4, 17), (16, P.Q0), (32, P.Q62), (64, P.Q62), (128, P.Q0), (256, P.Q1),
-                                 (512, P.Q2), (128, P.Q62), (1024, P.Q62), (4096, P.Q62), (8192, P.Q62)])
+                                 (512, P.Q2), (128, P.Q62), (1024, P.Q62), (4096, P.Q62), (8192, P.Q62),
+                                 (32, P.Q0), (2048, P.Q0), (4096, P.Q0)])
 def test_ntt_incomplete(api, oracle, d, q):
     rng = np.random.default_rng(d)
     x = rand_mod(rng, (53, d), q)
@@ -82,7 +84,8 @@ def test_ntt_ragged_tiles(api, oracle):
 
 
 @pytest.mark.parametrize("n,q,count", [(16, P.Q62, 7), (64, P.Q62, 65), (128, P.Q0, 33), (256, P.Q62, 17),
-                                       (1024, P.Q62, 9), (4096, P.Q62, 3), (8, 65537, 5), (8192, P.Q62, 2)])
+                                       (1024, P.Q62, 9), (4096, P.Q62, 3), (8, 65537, 5), (8192, P.Q62, 2),
+                                       (1024, P.Q0, 5), (4096, P.Q0, 3), (16, P.Q1, 9)])
 def test_poly_mul(api, oracle, n, q, count):
     """Batched negacyclic product against the oracle's multiply_poly, per pair."""
     rng = np.random.default_rng(n + count)
@@ -231,6 +234,19 @@ def test_fold(api, oracle, rows, width, d, q):
     want = oracle.fold(w, q, c)
     got = api.to_host(api.fold(api.to_dev(w), q, api.to_dev(c)))
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("n,k", [(16, 32), (112, 128), (176, 128), (256, 256), (128, 64)])
+def test_umma_i8_selftest(api, n, k):
+    """tcgen05.mma kind::i8 with our shared-memory descriptors equals the exact integer product."""
+    rng = np.random.default_rng(n * k)
+    a = rng.integers(0, 256, size=(128, k), dtype=np.uint8)
+    b = rng.integers(0, 256, size=(n, k), dtype=np.uint8)
+    a[0, :] = 255
+    b[0, :] = 255
+    got = api.selftest_umma_i8(a, b)
+    want = a.astype(np.int64) @ b.astype(np.int64).T
+    assert np.array_equal(got.astype(np.int64), want)
 
 
 # ---- HEXL-compatible tier (host buffers, GPU compute) ---------------------------
