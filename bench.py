@@ -305,7 +305,7 @@ def run_ours(args):
         if i > 0:
             plain.append(a.elapsed_time(b))
     torch.cuda.synchronize()
-    traced = trace_read("ck_mma_kernel") if args.plain_proofs > 1 else None
+    traced = trace_read("ck_umma_kernel") if args.plain_proofs > 1 else None
     lib().salsaa_trace_enable(0)
     plain_value = 1000.0 / statistics.mean(plain) if plain else None
 
@@ -549,11 +549,9 @@ def roofline_ntt(ntt, peak, kind):
             "algorithmic_bytes_per_launch": 16 * 1024 * (1 << 18)}
 
 
-# DRAM bytes (read + write) per int8 operation of ck_mma_kernel, from one ncu
-# capture of a 9-row x 16384-element commitment against 12 key rows:
-# 285.13 MB for 6.66e10 operations.  Traffic grows with rows x elements, as
-# the operations do, so a launch's traffic is estimated from its operations.
-CK_MMA_BYTES_PER_OP = 285.13e6 / (588.0 * 12 * 9 * 16384 * 64)
+# DRAM bytes (read + write) per launch of the commitment kernel are not
+# measured live; the ncu summaries under profiles/ give them for named launches.
+CK_TRAFFIC_NOTE = "DRAM bytes per launch: see the ncu summary of ck_umma_kernel under profiles/"
 
 
 def roofline_ck(traced, peak_info, elapsed_ms):
@@ -567,10 +565,10 @@ def roofline_ck(traced, peak_info, elapsed_ms):
     per_ms = traced["ms"] / traced["launches"]
     work = traced["work"] / traced["launches"]
     achieved = work / (per_ms * 1e-3) / 1e12
-    return {"kernel": "ck_mma_kernel (exact int8 limb-split commitment, mma.sync m16n8k32)", "bound": "tensor",
+    return {"kernel": "ck_umma_kernel (exact int8 limb-split commitment, tcgen05.mma kind::i8, TMEM)",
+            "bound": "tensor",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_kind": kind, "traffic": work * CK_MMA_BYTES_PER_OP,
-            "traffic_note": "DRAM bytes per launch, scaled by operations from an ncu capture of a smaller launch",
+            "peak_kind": kind, "traffic": None, "traffic_note": CK_TRAFFIC_NOTE,
             "launches": traced["launches"],
             "ms_per_launch": per_ms, "ops_per_launch": work,
             "share_of_plain_prove": traced["ms"] / elapsed_ms if elapsed_ms else None,

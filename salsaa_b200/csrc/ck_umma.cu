@@ -4,6 +4,7 @@
 
 #include "../../include/salsaa_gpu.h"
 #include "kernels.cuh"
+#include "ntt.cuh"
 #include "umma.cuh"
 
 using namespace salsaa;
@@ -68,7 +69,287 @@ __global__ void __launch_bounds__(128) umma_selftest_kernel(const uint8_t* A, co
   if (warp == 0) umma::tmem_dealloc(tmem, 256);
 }
 
+// ---------------------------------------------------------------------------
+// Commitment-key rows on tcgen05 (q < 2^56).  Per NTT slot s the key rows'
+// contribution to the commitment is a matrix product over F_q[X]/(X^2 - zeta):
+// with the key power T = (c, d) and the witness value W = (a, b),
+//   re = sum c a + zeta sum d b,    im = sum c b + sum d a.
+// Every value is split into 7 bytes, so one u8 x u8 -> s32 tensor-core
+// product per slot gives all four sums exactly (2048 byte products per block
+// stay below 2^27):
+//   A (M = 128): witness rows (k, part a|b, byte y), y-th byte of W,
+//   B (N = nkp): key rows (r, comp c|d, byte x), x-th byte of T,
+//   D[(k,p,y)][(r,c,x)] = sum_i byte_y(W_k,p(i)) byte_x(T_r,c(i)),
+// and value = sum_{x,y} 2^(8(x+y)) D mod q.  The key bytes are laid out once
+// per context in the operand's shared-memory image (ck_tk8), so each
+// 128-element chunk of both slots' key tiles is one bulk copy.
+//
+// CTA = (slot pair s0, s0 + 1; block of Bw elements).  Per 128-element chunk:
+// thread 0 bulk-copies the two key tiles, all 256 threads load the witness
+// pairs (one 16-byte load covers both slots), split them into byte planes in
+// shared memory, and thread 0 issues 2 x 4 MMAs (K = 32) into two TMEM
+// accumulators.  Two stages: the witness of chunk c + 1 is staged while the
+// MMAs of chunk c run.  Epilogue: each thread reads its TMEM lane (one
+// witness byte row), folds the key bytes x, the block's 7 y-rows are folded
+// through shared memory, and the result is multiplied by the block's high
+// key factor and added into the accumulator as in the CUDA-core path.
+// ---------------------------------------------------------------------------
+constexpr u32 CKU_CHUNK = 128;  // elements per pipeline step (K of 4 MMAs)
+constexpr u32 CKU_THREADS = 256;
+constexpr u32 CKU_ATILE = 128 * CKU_CHUNK;  // witness byte tile of one slot
+
+__global__ void ck_tk8_kernel(const u64* tlo, u32 nck, u32 n, u32 bt, u32 nkp, bool packed, uint8_t* tk8) {
+  const u64 tot = (u64)bt * n * nkp;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u32 b = (u32)(t % 16);
+    u64 rest = t / 16;
+    const u32 row = (u32)(rest % nkp);
+    rest /= nkp;
+    const u32 j = (u32)(rest % 8);
+    rest /= 8;
+    const u32 s = (u32)(rest % n), cc = (u32)(rest / n);
+    uint8_t v = 0;
+    if (row < nck * 14) {
+      const u32 r = row / 14, comp = (row / 7) % 2, x = row % 7;
+      const u32 lo = cc * CKU_CHUNK + j * 16 + b;
+      u64 val = tlo[((u64)r * bt + lo) * 3 * n + (u64)comp * n + s];
+      if (packed) val = ((val >> 32) << 25) | (val & 0x1FFFFFFull);
+      v = (uint8_t)(val >> (8 * x));
+    }
+    tk8[t] = v;
+  }
+}
+
+__device__ u32 g_tc_error;  // set when a tensor-core wait gave up
+
+__global__ void __launch_bounds__(CKU_THREADS, 1)
+    ck_umma_kernel(const uint8_t* __restrict__ tk8, RowSet w, u32 rows, u32 nck, u32 nkp, u32 n, u32 bt, u32 Bw,
+                   const u64* thi, u32 nhi_t, ModQ M, const u64* zeta, u64* acc, bool plain) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t full_bar[2], done_bar[2];
+  __shared__ uint32_t tslot;
+  const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const u32 s0 = 2 * blockIdx.x, d = 2 * n;
+  const u64 i0 = (u64)blockIdx.y * Bw;
+  const u32 btile = nkp * CKU_CHUNK;                  // one slot's key tile
+  const u32 stage_bytes = 2 * CKU_ATILE + 2 * btile;  // A0 A1 B0 B1
+  const u32 nchunks = Bw / CKU_CHUNK;
+  const u32 cc0 = (u32)((i0 % bt) / CKU_CHUNK);
+  u32* err = &g_tc_error;
+
+  // zero both stages' witness tiles once: rows >= 14 * rows stay zero
+  for (u32 v = tid; v < 2 * 2 * CKU_ATILE / 16; v += CKU_THREADS) {
+    const u32 st = v / (2 * CKU_ATILE / 16), o = v % (2 * CKU_ATILE / 16);
+    *(uint4*)(smem + st * stage_bytes + o * 16) = make_uint4(0, 0, 0, 0);
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 2; i++) {
+      umma::mbar_init(&full_bar[i], 1);
+      umma::mbar_init(&done_bar[i], 1);
+    }
+    umma::mbar_fence_init();
+  }
+  // two accumulators of nkp columns: 2 x 128 columns when they fit, so two
+  // CTAs with small key tables can share an SM's 512 TMEM columns
+  const u32 cs = nkp <= 128 ? 128 : 256;
+  if (warp == 0) umma::tmem_alloc(&tslot, 2 * cs);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const u32 tmem = tslot;
+
+  // witness task t: (i4lo, kp within a group of 8, kp group, i4hi)
+  const u32 nkpw = 2 * rows, kpb = (nkpw + 7) / 8;
+  uint4 wv[3][4];
+  auto fetch = [&](u32 c) {
+#pragma unroll
+    for (u32 x = 0; x < 3; x++) {
+      const u32 t = tid + x * CKU_THREADS;
+      const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
+      const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
+      if (x < kpb && kp < nkpw) {
+        const u32 k = kp >> 1, part = kp & 1;
+        const u64 e0 = i0 + (u64)c * CKU_CHUNK + (i4hi * 4 + i4lo) * 4;
+        const u64* src = w.p[k] + e0 * d + part * n + s0;
+#pragma unroll
+        for (u32 e = 0; e < 4; e++) wv[x][e] = __ldg((const uint4*)(src + (u64)e * d));
+      }
+    }
+  };
+  auto stash = [&](u32 st) {
+    uint8_t* A = smem + st * stage_bytes;
+#pragma unroll
+    for (u32 x = 0; x < 3; x++) {
+      const u32 t = tid + x * CKU_THREADS;
+      const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
+      const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
+      if (x < kpb && kp < nkpw) {
+        const u32 i4 = i4hi * 4 + i4lo;  // elements 4 * i4 .. + 3 of the chunk
+        const u32 off = (i4 >> 2) * (128 * 16) + (kp * 7) * 16 + (i4 & 3) * 4;
+#pragma unroll
+        for (u32 sg = 0; sg < 2; sg++)
+#pragma unroll
+          for (u32 b = 0; b < 7; b++) {
+            u32 word = 0;
+#pragma unroll
+            for (u32 e = 0; e < 4; e++) {
+              const u64 v = sg ? ((const u64*)&wv[x][e])[1] : ((const u64*)&wv[x][e])[0];
+              word |= ((u32)(v >> (8 * b)) & 0xffu) << (8 * e);
+            }
+            *(u32*)(A + sg * CKU_ATILE + off + b * 16) = word;
+          }
+      }
+    }
+  };
+
+  const u32 idesc = umma::idesc_u8(128, nkp);
+  bool ok = true;
+  fetch(0);
+  for (u32 c = 0; c < nchunks; c++) {
+    const u32 st = c & 1;
+    uint8_t* stage = smem + st * stage_bytes;
+    if (c >= 2) ok &= umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1);
+    if (tid == 0) {
+      umma::mbar_expect_tx(&full_bar[st], 2 * btile);
+      umma::bulk_g2s(stage + 2 * CKU_ATILE, tk8 + ((u64)(cc0 + c) * n + s0) * btile, 2 * btile, &full_bar[st]);
+    }
+    stash(st);
+    if (c + 1 < nchunks) fetch(c + 1);
+    umma::fence_proxy_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      ok &= umma::mbar_wait(&full_bar[st], (c >> 1) & 1, err, 2);
+#pragma unroll
+      for (u32 sg = 0; sg < 2; sg++)
+#pragma unroll
+        for (u32 ks = 0; ks < CKU_CHUNK / 32; ks++) {
+          const uint64_t ad =
+              umma::desc_kmajor(umma::smem_u32(stage + sg * CKU_ATILE + ks * 2 * 128 * 16), 128 * 16, 128);
+          const uint64_t bd =
+              umma::desc_kmajor(umma::smem_u32(stage + 2 * CKU_ATILE + sg * btile + ks * 2 * nkp * 16), nkp * 16, 128);
+          umma::mma_i8(tmem + sg * cs, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+        }
+      umma::commit(&done_bar[st]);
+    }
+  }
+  // all MMAs done (the last commit covers every earlier MMA of thread 0)
+  ok &= umma::mbar_wait(&done_bar[(nchunks - 1) & 1], ((nchunks - 1) >> 1) & 1, err, 3);
+  ok = __syncthreads_and(ok);
+  umma::fence_after_sync();
+
+  // ---- epilogue ----
+  u64* Pm = (u64*)smem;  // [slot][128 lanes][2 nck] partial sums over x
+  const u32 ng = 2 * nck;
+  const u32 sg = warp >> 2, row = (warp & 3) * 32 + lane;
+  if (ok) {
+    const bool valid = row < rows * 14;
+    const u32 y = row % 7;
+    const u64 pw = ((u64)1 << (8 * y)) % M.q;
+    u64 hi = 0, lo = 0;
+    for (u32 cb = 0; cb * 16 < nkp; cb++) {
+      uint32_t r[16];
+      umma::tmem_ld16(tmem + (((warp & 3) * 32) << 16) + sg * cs + cb * 16, r);
+      umma::tmem_wait_ld();
+#pragma unroll
+      for (u32 i = 0; i < 16; i++) {
+        const u32 j = cb * 16 + i;
+        if (j < nck * 14) {
+          const u32 x = j % 7;
+          const u64 v = (u64)r[i];
+          const u64 sl = v << (8 * x), sh = x ? (v >> (64 - 8 * x)) : 0;
+          lo += sl;
+          hi += sh + (lo < sl);
+          if (x == 6) {
+            u64 p = (M.s >= 39) ? barrett128(M, hi, lo) : reduce128_any(M, hi, lo);
+            if (valid) Pm[((u64)sg * 128 + row) * ng + j / 7] = mul_mod(M, p, pw);
+            hi = lo = 0;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (ok) {
+    const u32 hi_t = (u32)(i0 / bt);
+    for (u32 t = tid; t < 2 * rows * nck; t += CKU_THREADS) {
+      const u32 r = t % nck, k = (t / nck) % rows, g2 = t / (nck * rows);
+      const u32 s = s0 + g2;
+      const u64* P = Pm + (u64)g2 * 128 * ng;
+      u64 ca = 0, db = 0, cb = 0, da = 0;
+#pragma unroll
+      for (u32 y = 0; y < 7; y++) {
+        const u64* pa = P + (u64)((2 * k) * 7 + y) * ng;      // part a rows
+        const u64* pb = P + (u64)((2 * k + 1) * 7 + y) * ng;  // part b rows
+        ca = salsaa::add_mod(ca, pa[2 * r], M.q);
+        da = salsaa::add_mod(da, pa[2 * r + 1], M.q);
+        cb = salsaa::add_mod(cb, pb[2 * r], M.q);
+        db = salsaa::add_mod(db, pb[2 * r + 1], M.q);
+      }
+      u64 re = salsaa::add_mod(ca, mul_mod(M, zeta[s], db), M.q);
+      u64 im = salsaa::add_mod(cb, da, M.q);
+      const u64* th = thi + ((u64)r * nhi_t + hi_t) * d;
+      slot_mul(M, re, im, th[s], th[n + s], zeta[s], re, im);
+      u64* dst = acc + ((u64)r * rows + k) * d;
+      atomic_add_mod(dst + s, re, M.q, plain);
+      atomic_add_mod(dst + n + s, im, M.q, plain);
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 2 * cs);
+}
+
 }  // namespace
+
+namespace salsaa {
+
+int launch_ck_tk8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* tk8, cudaStream_t st) {
+  const u32 nkp = ck_tk8_nkp(nck);
+  const u64 tot = (u64)bt * n * nkp;
+  u64 g = (tot + 255) / 256;
+  if (g > 65535 * 16) g = 65535 * 16;
+  ck_tk8_kernel<<<(unsigned)g, 256, 0, st>>>(tlo, nck, n, bt, nkp, packed, tk8);
+  salsaa_count_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ck_tk8");
+}
+
+bool ck_umma_ok(const CommitArgs& a, u32 n) {
+  if (!a.tk8 || a.rows == 0 || a.rows > CKU_MAX_WROWS || a.nck == 0 || a.nck > CKU_MAX_KEYS || (n & 1)) return false;
+  if (a.width < CKU_CHUNK || a.ck_bt < CKU_CHUNK) return false;
+  for (u32 k = 0; k < a.rows; k++)
+    if ((uintptr_t)a.w.p[k] % 16) return false;
+  return true;
+}
+
+int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, const u64* zeta, bool plain, cudaStream_t st) {
+  const u32 nkp = ck_tk8_nkp(a.nck);
+  const size_t stage = 2 * (size_t)CKU_ATILE + 2 * (size_t)nkp * CKU_CHUNK;
+  const size_t epi = 2 * 128 * (size_t)(2 * a.nck) * sizeof(u64);
+  const size_t smem = 2 * stage > epi ? 2 * stage : epi;
+  cudaError_t e = cudaFuncSetAttribute(ck_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ck_umma smem attribute");
+  dim3 g(n / 2, (unsigned)(a.width / Bw));
+  const int tr = salsaa_trace_begin("ck_umma_kernel", st, 2.0 * 196.0 * a.nck * a.rows * (double)a.width * n);
+  ck_umma_kernel<<<g, CKU_THREADS, smem, st>>>(a.tk8, a.w, a.rows, a.nck, nkp, n, a.ck_bt, Bw, a.thi, a.ck_nhi, M,
+                                               zeta, a.acc, plain);
+  salsaa_trace_end(tr, st);
+  salsaa_count_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ck_umma launch");
+}
+
+int tc_error_check() {
+  u32 h = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&h, g_tc_error, sizeof(u32));
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "tensor-core status");
+  if (h) return salsaa_set_error(-4, "a tensor-core wait timed out; results of that launch are invalid");
+  return 0;
+}
+
+}  // namespace salsaa
 
 extern "C" int salsaa_selftest_umma_i8(const uint8_t* d_a, const uint8_t* d_b, uint32_t n, uint32_t k,
                                        int32_t* d_out, void* stream) {

@@ -69,6 +69,22 @@ __device__ __forceinline__ u64 mul_shoup(u64 x, u64 w, u64 wp, u64 q) {
   return r >= q ? r - q : r;
 }
 
+// Accumulate a reduced value into a global sum kept mod q.  With q < 2^50
+// and fewer than 2^13 contributions a plain 64-bit add cannot overflow and
+// the consumer reduces at the end; otherwise add modulo q with a CAS loop.
+__device__ __forceinline__ void atomic_add_mod(u64* addr, u64 v, u64 q, bool plain) {
+  if (plain) {
+    atomicAdd((unsigned long long*)addr, (unsigned long long)v);
+    return;
+  }
+  unsigned long long old = *(volatile unsigned long long*)addr, assumed;
+  do {
+    assumed = old;
+    u64 nv = add_mod((u64)assumed % q, v, q);
+    old = atomicCAS((unsigned long long*)addr, assumed, (unsigned long long)nv);
+  } while (old != assumed);
+}
+
 // ---- lazy limb accumulator (q < 2^50) -------------------------------------
 struct Acc3 {
   u64 lo, mid, hi;

@@ -27,21 +27,6 @@ inline unsigned grid_1d(u64 work, unsigned threads, unsigned cap = 148 * 32) {
   return (unsigned)g;
 }
 
-// Accumulate a reduced value into a global sum kept mod q.  With q < 2^50
-// and fewer than 2^13 contributions a plain 64-bit add cannot overflow and
-// the consumer reduces at the end; otherwise add modulo q with a CAS loop.
-__device__ __forceinline__ void atomic_add_mod(u64* addr, u64 v, u64 q, bool plain) {
-  if (plain) {
-    atomicAdd((unsigned long long*)addr, (unsigned long long)v);
-    return;
-  }
-  unsigned long long old = *(volatile unsigned long long*)addr, assumed;
-  do {
-    assumed = old;
-    u64 nv = add_mod((u64)assumed % q, v, q);
-    old = atomicCAS((unsigned long long*)addr, assumed, (unsigned long long)nv);
-  } while (old != assumed);
-}
 
 __device__ __forceinline__ u64 nc_challenge(const DevState* ds, u32 round, u32 rep, u64 j, u64 q) {
   return uni_mod(prf_at(prf_key(ds->seed, domain_id(DOM_NC, round, rep)), j), q);
@@ -1525,7 +1510,11 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   cudaError_t e =
       cudaMemsetAsync(a.acc, 0, (u64)(a.nck + a.nsc) * a.rows * d * sizeof(u64), st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit memset");
-  if (a.nck && a.tl8 && M.q < (1ULL << 56) && a.width >= CKM_KS && a.rows <= 9 && n <= 512) {
+  if (a.nck && ck_umma_ok(a, n)) {
+    if (Bw > a.ck_bt) return salsaa_set_error(-2, "commit: witness wider than the key tables");
+    int rc = launch_ck_umma(a, n, Bw, M, T.zeta, plain, st);
+    if (rc) return rc;
+  } else if (a.nck && a.tl8 && M.q < (1ULL << 56) && a.width >= CKM_KS && a.rows <= 9 && n <= 512) {
     if (Bw > a.ck_bt) return salsaa_set_error(-2, "commit: witness wider than the key tables");
     int rc = launch_ck_mma(a, n, Bw, M, T.zeta, plain, st);
     if (rc) return rc;

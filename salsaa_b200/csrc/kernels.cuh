@@ -50,6 +50,15 @@ int launch_ck_tables(const u64* m_slot, u32 rows, const NttDev& T, const ModQ& M
 constexpr u32 CKM_ROWS = 6, CKM_BM = 128;
 inline u64 ck_tl8_bytes(u32 nck, u32 n, u32 bt) { return (u64)n * ((nck + CKM_ROWS - 1) / CKM_ROWS) * CKM_BM * bt; }
 int launch_ck_tl8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* tl8, cudaStream_t st);
+// tcgen05 key table: for each 128-element chunk position cc and slot s, the
+// byte image of the B operand (rows (key row, comp c|d, byte), padded to nkp)
+// in the canonical K-major shared-memory layout; q < 2^56, nck <= 18.
+constexpr u32 CKU_MAX_KEYS = 18, CKU_MAX_WROWS = 9;
+inline u32 ck_tk8_nkp(u32 nck) { return ((nck * 14 + 15) / 16) * 16; }
+inline u64 ck_tk8_bytes(u32 nck, u32 n, u32 bt) { return (u64)bt * n * ck_tk8_nkp(nck); }
+int launch_ck_tk8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* tk8, cudaStream_t st);
+// Nonzero (and the last error set) when a tensor-core kernel's bounded wait gave up.
+int tc_error_check();
 int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState* ds, cudaStream_t st);
 int launch_fill(u64* p, u64 n, u64 v, cudaStream_t st);
 // r[i] = r[i] * b[i] mod q (canonical inputs)
@@ -102,12 +111,16 @@ struct CommitArgs {
   u64* sc_lo;        // scratch nsc x CK_BLOCK
   u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)
   const uint8_t* tl8;  // tensor-core key table (see launch_ck_tl8) or null
+  const uint8_t* tk8;  // tcgen05 key table (see launch_ck_tk8) or null
   u64* colsum;       // scratch colsum_rows x min(width, CK_BLOCK) x d (scalar rows only)
   u32 colsum_rows;   // capacity of colsum in witness rows
   u64* acc;          // scratch (nck + nsc) x rows x d
   u64* out_slot;     // (nck + nsc) x rows x d, statement order = CK rows then scalar rows
 };
 int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st);
+// Key rows of launch_commit on tcgen05 when ck_umma_ok (see ck_umma.cu).
+bool ck_umma_ok(const CommitArgs& a, u32 n);
+int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, const u64* zeta, bool plain, cudaStream_t st);
 
 // Commitment of a witness of width w from the commitment of its split halves
 // (slot form): out[j][k] = t0_j * R[j][k] + t1_j * R[j][K + k] for statement

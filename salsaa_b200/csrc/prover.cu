@@ -277,6 +277,7 @@ struct salsaa_ctx {
   u64* tlo = nullptr;
   u64* thi = nullptr;
   uint8_t* tl8 = nullptr;  // tensor-core key table (q < 2^56), else null
+  uint8_t* tk8 = nullptr;  // tcgen05 key table (q < 2^56, <= 18 key rows, blocks of >= 128), else null
   std::mutex mu;
   salsaa_prover* blocking = nullptr;  // slot used by salsaa_prove()
 };
@@ -312,6 +313,10 @@ static int ctx_build(salsaa_ctx* c, DevBuf& mem) {
   if (c->P.q < (1ULL << 56)) {
     TRY(mem.alloc(&c->tl8, ck_tl8_bytes(ms, n, c->ck_bt), "ctx: key byte planes"));
     TRY(launch_ck_tl8(c->tlo, ms, n, c->ck_bt, c->P.q < (1ULL << 50), c->tl8, 0));
+    if (ms <= CKU_MAX_KEYS && c->ck_bt >= 128 && n % 2 == 0) {
+      TRY(mem.alloc(&c->tk8, ck_tk8_bytes(ms, n, c->ck_bt), "ctx: tcgen05 key tiles"));
+      TRY(launch_ck_tk8(c->tlo, ms, n, c->ck_bt, c->P.q < (1ULL << 50), c->tk8, 0));
+    }
   }
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ctx: build");
@@ -558,6 +563,7 @@ static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 w
   a.sc_hi = pr->sc_hi;
   a.acc = pr->acc;
   a.tl8 = c->tl8;
+  a.tk8 = c->tk8;
   a.colsum = pr->colsum;
   a.colsum_rows = c->S.max_rows + 1;  // the merged split/projection pass has 2K + 1 rows
   a.out_slot = pr->cout;
@@ -814,7 +820,8 @@ extern "C" int salsaa_prover_sync(salsaa_prover* pr) {
   if (!pr) return salsaa_set_error(-1, "prover_sync: null argument");
   cudaError_t e = cudaStreamSynchronize(pr->st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_sync");
-  return pr->last_rc;
+  if (pr->last_rc) return pr->last_rc;
+  return tc_error_check();
 }
 
 extern "C" int salsaa_prover_timing(salsaa_prover* pr, salsaa_timing* t) {
@@ -950,6 +957,7 @@ extern "C" int salsaa_commit(salsaa_ctx* c, const uint64_t* d_w, uint64_t rows, 
   TRY(ntt_launch(d_w, ws, rows * width, *c->T, true, false, st));
   CommitArgs a{};
   a.tl8 = c->tl8;
+  a.tk8 = c->tk8;
   a.w = rows_of(ws, (u32)rows, width, d);
   a.rows = (u32)rows;
   a.width = width;

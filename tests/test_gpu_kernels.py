@@ -126,7 +126,10 @@ def test_ntt_large_batch(api, oracle):
 
 @pytest.mark.parametrize("d,q,ms,width,rows", [(16, P.Q0, 3, 64, 1), (16, P.Q0, 5, 4096, 3), (128, P.Q0, 12, 2048, 2),
                                                (256, P.Q1, 7, 1024, 4), (512, P.Q2, 4, 512, 8),
-                                               (32, P.Q62, 2, 256, 2), (64, P.Q0, 3, 8192, 1)])
+                                               (32, P.Q62, 2, 256, 2), (64, P.Q0, 3, 8192, 1),
+                                               (128, P.Q0, 18, 4096, 9), (128, P.Q0, 13, 2048, 9),
+                                               (256, P.Q1, 1, 128, 1), (16, P.Q0, 12, 16384, 7),
+                                               (4, P.Q0, 2, 256, 3)])
 def test_commit(api, oracle, d, q, ms, width, rows):
     p = P.make_params(d, q, ms, max(width, 16), 1)
     rng = np.random.default_rng(d + width)
