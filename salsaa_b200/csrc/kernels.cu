@@ -266,70 +266,50 @@ __device__ __forceinline__ void group_rounds(const ModQ& M, u64 (&x)[1 << T], co
   }
 }
 
-// First pass: v_0 rows (shared) -> v_T for both repetitions.
+// First pass: v_0 rows (shared) -> v_T for each repetition.  The two
+// repetitions run in neighbouring CTAs (blockIdx.x = 2 * block + rep) over
+// the same witness range, so the second read of each range hits L2; this
+// halves the per-thread accumulators (two CTAs per SM).  Round 0 is the same
+// for both repetitions: the rep-0 CTA adds its sums to both.
 template <bool LAZY>
-__global__ void __launch_bounds__(256) sc_first_kernel(RowSet w, u32 rows, u64 nlen, ModQ M, const DevState* ds,
-                                                       u32 round, u64* out, u64 sout, u64* sums, u32 nr,
-                                                       bool plain) {
+__global__ void __launch_bounds__(256, 2) sc_first_kernel(RowSet w, u32 rows, u64 nlen, ModQ M, const DevState* ds,
+                                                          u32 round, u64* out, u64 sout, u64* sums, u32 nr,
+                                                          bool plain) {
   constexpr u32 T = SC_T, G = 1u << T;
   __shared__ Sum128 red[32];
-  const u32 k = blockIdx.y;
+  const u32 k = blockIdx.y, rep = blockIdx.x & 1, bx = blockIdx.x >> 1, nbx = gridDim.x >> 1;
   const u64* x = w.p[k];
   const u64 q = M.q, ng = nlen / G;
-  u64 c[2][T], cp[2][T];
+  u64 c[T], cp[T];
 #pragma unroll
-  for (u32 rep = 0; rep < 2; rep++)
-#pragma unroll
-    for (u32 t = 0; t < T; t++) {
-      c[rep][t] = nc_challenge(ds, round, rep, t, q);
-      cp[rep][t] = shoup_dev(c[rep][t], q);
-    }
-  ScAcc<LAZY> r0[3];
-  ScAcc<LAZY> acc[2][T][3];
-#pragma unroll
-  for (u32 a = 0; a < 3; a++) {
-    r0[a].zero();
-#pragma unroll
-    for (u32 rep = 0; rep < 2; rep++)
-#pragma unroll
-      for (u32 t = 0; t < T; t++) acc[rep][t][a].zero();
+  for (u32 t = 0; t < T; t++) {
+    c[t] = nc_challenge(ds, round, rep, t, q);
+    cp[t] = shoup_dev(c[t], q);
   }
-  for (u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += (u64)gridDim.x * blockDim.x) {
+  ScAcc<LAZY> acc[T][3];  // acc[0] = round 0, only kept by the rep-0 CTAs
+#pragma unroll
+  for (u32 t = 0; t < T; t++)
+#pragma unroll
+    for (u32 a = 0; a < 3; a++) acc[t][a].zero();
+  for (u64 g = (u64)bx * blockDim.x + threadIdx.x; g < ng; g += (u64)nbx * blockDim.x) {
     u64 v[G];
 #pragma unroll
     for (u32 m = 0; m < G; m++) v[m] = __ldg(x + g + m * ng);
-#pragma unroll
-    for (u32 m = 0; m < G / 2; m++) {
-      r0[0].mac(M, v[m], v[m]);
-      r0[1].mac(M, v[m], v[m + G / 2]);
-      r0[2].mac(M, v[m + G / 2], v[m + G / 2]);
-    }
-#pragma unroll
-    for (u32 rep = 0; rep < 2; rep++) {
-      u64 y[G];
-#pragma unroll
-      for (u32 m = 0; m < G; m++) y[m] = v[m];
-      group_rounds<LAZY, T>(M, y, c[rep], cp[rep], acc[rep], 1);
-      out[((u64)rep * rows + k) * sout + g] = y[0];
-    }
+    group_rounds<LAZY, T>(M, v, c, cp, acc, rep == 0 ? 0 : 1);
+    out[((u64)rep * rows + k) * sout + g] = v[0];
   }
 #pragma unroll
-  for (u32 a = 0; a < 3; a++) {
-    const u64 r = block_total<LAZY>(M, r0[a], red);
-    if (threadIdx.x == 0) {
-      atomic_add_mod(&sums[((0 * (u64)nr + 0) * rows + k) * 3 + a], r, q, plain);
-      atomic_add_mod(&sums[((1 * (u64)nr + 0) * rows + k) * 3 + a], r, q, plain);
-    }
-  }
+  for (u32 t = 0; t < T; t++) {
+    if (t == 0 && rep != 0) continue;  // uniform per CTA
 #pragma unroll
-  for (u32 rep = 0; rep < 2; rep++)
-#pragma unroll
-    for (u32 t = 1; t < T; t++)
-#pragma unroll
-      for (u32 a = 0; a < 3; a++) {
-        const u64 r = block_total<LAZY>(M, acc[rep][t][a], red);
-        if (threadIdx.x == 0) atomic_add_mod(&sums[((rep * (u64)nr + t) * rows + k) * 3 + a], r, q, plain);
+    for (u32 a = 0; a < 3; a++) {
+      const u64 r = block_total<LAZY>(M, acc[t][a], red);
+      if (threadIdx.x == 0) {
+        atomic_add_mod(&sums[((rep * (u64)nr + t) * rows + k) * 3 + a], r, q, plain);
+        if (t == 0) atomic_add_mod(&sums[((1 * (u64)nr + 0) * rows + k) * 3 + a], r, q, plain);
       }
+    }
+  }
 }
 
 // Later passes: v_j (per (rep,row), stride sin) -> v_{j+T} (stride sout).
@@ -450,7 +430,7 @@ static int sumcheck_passes(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, c
     return (unsigned)(g < want ? (g ? g : 1) : want);
   };
   if (L > SC_TAIL) {
-    dim3 g(grid_for(L / (1u << SC_T), rows), rows);
+    dim3 g(2 * grid_for(L / (1u << SC_T), rows), rows);
     sc_first_kernel<LAZY><<<g, 256, 0, st>>>(w, rows, L, M, ds, round, B.a, sa, B.sums, nr, plain);
     int rc = check_launch("sc_first");
     if (rc) return rc;
