@@ -55,11 +55,16 @@ __device__ __forceinline__ u64 barrett128(const ModQ& M, u64 hi, u64 lo) {
 __device__ __forceinline__ u64 mul_mod(const ModQ& M, u64 a, u64 b) {
   return barrett128(M, __umul64hi(a, b), a * b);
 }
+// x mod q for any 64-bit x: Barrett applies directly when 2^64 <= 2^(2s),
+// i.e. q >= 2^31; smaller moduli use the hardware-less division.
+__device__ __forceinline__ u64 reduce64(const ModQ& M, u64 x) {
+  return M.s >= 32 ? barrett128(M, 0, x) : x % M.q;
+}
 // Reduction of an arbitrary 128-bit value: hi*2^64 + lo = (hi mod q)*(2^64 mod q) + lo.
 __device__ __forceinline__ u64 reduce128_any(const ModQ& M, u64 hi, u64 lo) {
-  u64 h = hi % M.q;  // rare path (final flushes only)
+  u64 h = reduce64(M, hi);
   u64 t = mul_mod(M, h, M.r64);
-  u64 l = lo % M.q;
+  u64 l = reduce64(M, lo);
   return add_mod(t, l, M.q);
 }
 // Shoup: x * w mod q for any x < 2^64, w < q, wp = floor(w 2^64 / q).

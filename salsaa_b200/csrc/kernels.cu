@@ -1482,9 +1482,10 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   if (d > 512) return salsaa_set_error(-2, "commit: ring degree above 512");
   const u32 Bw = (u32)(a.width < CK_BLOCK ? a.width : CK_BLOCK);
   const u32 nhi = (u32)(a.width / Bw);
-  // chunk: >= 32 elements, at most 4096 chunks, inside one block of either table
-  u64 CH = a.width / 4096;
-  if (CH < 32) CH = 32;
+  // chunk: >= 128 elements (each thread's lazy sums are reduced once per
+  // chunk), at most 512 chunks, inside one block of either table
+  u64 CH = a.width / 512;
+  if (CH < 128) CH = 128;
   if (CH > Bw) CH = Bw;
   const bool plain = M.q < (1ULL << 50) && (a.width / CH) < (1ULL << 13);
   cudaError_t e =
