@@ -120,9 +120,10 @@ uint64_t salsaa_kernel_launches(void);
 /* Device-time trace for measurement (off by default): enable/reset, then read
  * the summed device time (CUDA events on the launching stream), summed
  * algorithmic work and launch count of a traced kernel by name.  Traced:
- * "ck_mma_kernel" (work = exact int8 limb products x 2, as operations) and
- * "ntt_kernel" (work = 16 bytes per coefficient).  Reading waits for the
- * traced launches. */
+ * "ck_umma_kernel" and "ck_mma_kernel" (work = 2 x the exact byte-limb
+ * products, as int8 operations), "ntt_kernel" (16 bytes per coefficient) and
+ * "ntt_mul_kernel" (24 bytes per coefficient).  Reading waits for the traced
+ * launches. */
 void salsaa_trace_enable(int on);
 int salsaa_trace_read(const char* name, double* total_ms, double* total_work, uint64_t* launches);
 /* Fill *out with preset "A0".."C2", "F0".."F2" (src/protocol.rs:28-123). */
