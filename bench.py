@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--preset", default=PRESET, help="parameter set (profiling; the metric is quoted on A0)")
     ap.add_argument("--wit-log", type=int, default=0,
                     help="profiling: shrink WIT_LEN to 2^L (SNARK rounds L-11), keeping d, q and the rows")
+    ap.add_argument("--no-dense", action="store_true", help="skip the dense commitment microbench")
+    ap.add_argument("--dense-only", action="store_true",
+                    help="profiling: run only the dense commitment microbench and print its JSON")
     ap.add_argument("--ntt-only", action="store_true",
                     help="profiling: run only the NTT microbench and print its JSON")
     ap.add_argument("--ntt-log-coeffs", type=int, default=28,
@@ -353,6 +356,7 @@ def run_ours(args):
     del witnesses, proofs
     torch.cuda.empty_cache()
     ntt = ntt_bench(torch, api) if rank == 0 and not args.no_ntt else None
+    dense = dense_bench(torch, api) if rank == 0 and not args.no_dense else None
     serving = serving_bench(torch, api, args.serve_requests, rank) if not args.no_serve else None
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -374,6 +378,7 @@ def run_ours(args):
             "gpu_launches": int(launches),
             "e2e": e2e,
             "ntt": ntt,
+            "commit_dense": dense,
             "serving": serving,
             "roofline": roofline_ck(traced, measured_peaks(tensor=True),
                                     statistics.mean(plain) * len(plain) if plain else None),
@@ -471,6 +476,57 @@ def serving_bench(torch, api, nreq, rank):
             "slots": SERVE_SLOTS, "served": served, "plain": plain,
             "served_over_plain": served["proofs_per_s"] / plain["proofs_per_s"],
             "service_ms_alone": {nm: 1e3 * v for nm, v in service.items()}}
+
+
+def dense_bench(torch, api):
+    """Ajtai commitment microbench: C = A W over R_q (d = 128, the 50-bit
+    prime), A n x m uniform, W m x r base-b digits uniform in [-b/2, b/2)
+    (seeded), for n in {8, 16}, m in {2^12, 2^16}, r in {1, 8, 32},
+    b in {2, 16}.  A is prepared once (its byte image for the tensor cores);
+    each timed call includes W's NTT, the product and C's inverse NTT, and
+    W's NTT is also timed alone."""
+    from salsaa_b200 import params as P
+    q, d, reps = P.Q0, 128, 5
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(77)
+    out = []
+    for n in (8, 16):
+        for mlog in (12, 16):
+            m = 1 << mlog
+            A = torch.randint(0, 1 << 62, (n, m, d), dtype=torch.int64, device="cuda", generator=gen) % q
+            key = api.DenseKey(A, q)
+            del A
+            for r in (1, 8, 32):
+                ws = api.dev_empty((r, m, d))
+                C = api.dev_empty((n, r, d))
+                for b in (2, 16):
+                    W = torch.randint(-(b // 2), b // 2, (r, m, d), dtype=torch.int64, device="cuda",
+                                      generator=gen) % q
+                    key.commit(W, out=C, w_slot=ws)
+                    a = torch.cuda.Event(enable_timing=True)
+                    e = torch.cuda.Event(enable_timing=True)
+                    a.record()
+                    for _ in range(reps):
+                        key.commit(W, out=C, w_slot=ws)
+                    e.record()
+                    e.synchronize()
+                    ms = a.elapsed_time(e) / reps
+                    a.record()
+                    for _ in range(reps):
+                        api.ntt(W, d, q, incomplete=True, out=ws)
+                    e.record()
+                    e.synchronize()
+                    ntt_ms = a.elapsed_time(e) / reps
+                    nbytes = 8 * d * (n * m + m * r + n * r)
+                    out.append({"n": n, "m": m, "r": r, "b": b, "ms": ms, "w_ntt_ms": ntt_ms,
+                                "GB/s": nbytes / (ms * 1e6),
+                                "Gmulmod/s": n * m * r * 2 * d / (ms * 1e6)})
+                    del W
+                del ws, C
+            key.close()
+            torch.cuda.empty_cache()
+    return {"q": q, "d": d, "bytes": "8 d (n m + m r + n r) per call", "mulmods": "n m r 2d per call",
+            "runs": out}
 
 
 def trace_read(name):
@@ -579,6 +635,11 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.dense_only:
+        import torch
+        from salsaa_b200 import api
+        print(json.dumps({"commit_dense": dense_bench(torch, api)}), flush=True)
+        return 0
     if args.ntt_only:
         import torch
         from salsaa_b200 import api

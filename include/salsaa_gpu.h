@@ -196,6 +196,23 @@ void salsaa_server_destroy(salsaa_server* s);
 int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uint64_t count, uint64_t q, int inverse,
                int incomplete, void* stream);
 
+/* Dense ring-matrix commitment C = A * W over R_q: parallel_dot_matrix_matrix
+ * (src/arithmetic.rs:429-457) in the Ajtai shape, C[j][c] = sum_i A[j][i] W[c][i].
+ * The key holds A (n x m ring elements of degree d, coefficient form, given
+ * once) prepared for the tensor cores (q < 2^56, n <= 18) or CUDA cores.
+ * m is a power of two >= 128, n <= 64, d in 4..512, q = 1 mod d. */
+typedef struct salsaa_dense_key salsaa_dense_key;
+int salsaa_dense_key_create(const uint64_t* d_a, uint64_t n, uint64_t m, uint64_t d, uint64_t q, void* stream,
+                            salsaa_dense_key** out);
+void salsaa_dense_key_destroy(salsaa_dense_key* key);
+/* d_w: r columns of m ring elements each (r x m x d, coefficient form);
+ * d_c: n x r ring elements (coefficient form, row j = key row j).  d_w_slot is
+ * an optional r x m x d workspace for W's NTT (NULL: allocated on the stream).
+ * Calls sharing one key must not overlap on the GPU (the key holds the
+ * accumulators). */
+int salsaa_dense_commit(salsaa_dense_key* key, const uint64_t* d_w, uint64_t r, uint64_t* d_c, uint64_t* d_w_slot,
+                        void* stream);
+
 /* Self-test of the int8 tensor-core building block used by the commitment
  * kernels (tcgen05.mma kind::i8, accumulator in tensor memory): d_out (128 x n,
  * int32, row-major) = A (128 x k bytes, row-major) * B (n x k bytes)^T, with

@@ -71,6 +71,8 @@ def lib():
             getattr(L, name).argtypes = [U64P, U64P, U64, U64]
         L.so_ring_mul.restype = ctypes.c_int
         L.so_ring_mul.argtypes = [U64P, U64P, U64P, U64, U64]
+        L.so_dense_commit.restype = ctypes.c_int
+        L.so_dense_commit.argtypes = [U64P, U64P, U64P, U64, U64, U64, U64, U64]
         L.so_conjugate.restype = None
         L.so_conjugate.argtypes = [U64P, U64P, U64, U64]
         L.so_shift_factors.restype = ctypes.c_int
@@ -233,6 +235,16 @@ def ring_mul(a, b, q):
     r = np.zeros_like(a)
     assert lib().so_ring_mul(_p(r), _p(a), _p(b), a.size, q) == 0
     return r
+
+
+def dense_commit(A, W, q):
+    """C = A * W (src/arithmetic.rs:429-457): A n x m x d, W r x m x d -> n x r x d."""
+    A, W = u64(A), u64(W)
+    n, m, d = A.shape
+    r = W.shape[0]
+    C = np.zeros((n, r, d), dtype=np.uint64)
+    assert lib().so_dense_commit(_p(C), _p(A), _p(W), n, m, r, d, q) == 0
+    return C
 
 
 def conjugate(a, q):

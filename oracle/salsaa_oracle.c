@@ -424,6 +424,41 @@ int so_ring_mul(u64* r, const u64* a, const u64* b, u64 d, u64 q) {
   ring_free(&R);
   return 0;
 }
+/* parallel_dot_matrix_matrix (src/arithmetic.rs:429-457) in the Ajtai shape:
+ * C[j][c] = sum_i A[j][i] * W[c][i] in R_q; A is n x m, W is r x m, C is
+ * n x r ring elements (coefficient form).  Products in slot form. */
+int so_dense_commit(u64* C, const u64* A, const u64* W, u64 n, u64 m, u64 r, u64 d, u64 q) {
+  Ring R;
+  if (ring_init(&R, d, q)) return -1;
+  u64* as = (u64*)malloc(n * m * d * sizeof(u64));
+  u64* ws = (u64*)malloc(r * m * d * sizeof(u64));
+  if (!as || !ws) {
+    free(as);
+    free(ws);
+    ring_free(&R);
+    return -1;
+  }
+#pragma omp parallel for schedule(static)
+  for (long long t = 0; t < (long long)(n * m); t++) to_slot(&R, A + (u64)t * d, as + (u64)t * d);
+#pragma omp parallel for schedule(static)
+  for (long long t = 0; t < (long long)(r * m); t++) to_slot(&R, W + (u64)t * d, ws + (u64)t * d);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long long jc = 0; jc < (long long)(n * r); jc++) {
+    const u64 j = (u64)jc / r, c = (u64)jc % r;
+    u64 acc[2048], prod[2048];
+    memset(acc, 0, d * sizeof(u64));
+    for (u64 i = 0; i < m; i++) {
+      slot_mul(&R, as + (j * m + i) * d, ws + (c * m + i) * d, prod);
+      for (u64 x = 0; x < d; x++) acc[x] = mod_add(acc[x], prod[x], q);
+    }
+    from_slot(&R, acc, C + (u64)jc * d);
+  }
+  free(as);
+  free(ws);
+  ring_free(&R);
+  return 0;
+}
+
 int so_shift_factors(u64* out, u64 d, u64 q) {
   Ring R;
   if (ring_init(&R, d, q)) return -1;

@@ -67,6 +67,8 @@ uint64_t so_sum_sq(const uint64_t* a, uint64_t n, uint64_t q);
 int so_ring_to_slot(uint64_t* out, const uint64_t* coef, uint64_t d, uint64_t q);
 int so_ring_from_slot(uint64_t* out, const uint64_t* slot, uint64_t d, uint64_t q);
 int so_ring_mul(uint64_t* r, const uint64_t* a, const uint64_t* b, uint64_t d, uint64_t q);
+int so_dense_commit(uint64_t* C, const uint64_t* A, const uint64_t* W, uint64_t n, uint64_t m, uint64_t r,
+                    uint64_t d, uint64_t q);
 void so_conjugate(uint64_t* r, const uint64_t* a, uint64_t d, uint64_t q);
 int so_shift_factors(uint64_t* out, uint64_t d, uint64_t q);
 void so_tensor(uint64_t* out, const uint64_t* cs, uint64_t k, uint64_t q);

@@ -185,6 +185,37 @@ def poly_mul(a, b, n, q, out=None):
     return out
 
 
+class DenseKey:
+    """Ajtai commitment key A (n x m ring elements, coefficient form) for
+    C = A * W (parallel_dot_matrix_matrix, src/arithmetic.rs:429-457)."""
+
+    def __init__(self, a, q):
+        n, m, d = a.shape
+        self.n, self.m, self.d, self.q = n, m, d, q
+        self._h = ctypes.c_void_p()
+        _check(lib().salsaa_dense_key_create(_p(a), n, m, d, q, _stream(), ctypes.byref(self._h)),
+               "dense_key_create")
+
+    def commit(self, w, out=None, w_slot=None):
+        """w: r x m x d CUDA tensor (columns of W) -> n x r x d commitment."""
+        r = w.shape[0]
+        out = dev_empty((self.n, r, self.d)) if out is None else out
+        _check(lib().salsaa_dense_commit(self._h, _p(w), r, _p(out), _p(w_slot) if w_slot is not None else None,
+                                         _stream()), "dense_commit")
+        return out
+
+    def close(self):
+        if self._h:
+            lib().salsaa_dense_key_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def selftest_umma_i8(a, b):
     """Exact u8 product on the tensor cores: a (128 x k), b (n x k) uint8 numpy
     arrays -> int32 numpy (128 x n) = a @ b.T."""

@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsalsaa_gpu.so")
-SOURCES = ["ntt.cu", "kernels.cu", "prover.cu", "hexl_compat.cu", "no_alloc.cu", "server.cu", "ck_umma.cu"]
+SOURCES = ["ntt.cu", "kernels.cu", "prover.cu", "hexl_compat.cu", "no_alloc.cu", "server.cu", "ck_umma.cu", "dense.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",

@@ -1181,7 +1181,7 @@ __global__ void commit_finalize_kernel(const u64* acc, u32 nck, u32 nsc, u32 row
     const u64 jk = t / n;
     const u32 j = (u32)(jk / rows);
     const u64* a = acc + jk * 2 * n;
-    u64 e = a[s] % M.q, o = a[n + s] % M.q;
+    u64 e = reduce64(M, a[s]), o = reduce64(M, a[n + s]);
     if (j >= nck && bases) {
       const u64* bs = bases[j - nck];
       if (bs) slot_mul(M, e, o, bs[s], bs[n + s], zeta[s], e, o);

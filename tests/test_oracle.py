@@ -237,3 +237,21 @@ def test_nc_challenges_helper(oracle):
     got = nc_challenges(5, 2, 1, 4, q)
     dom = domain(DOM_NC, 2, 1)
     assert [int(x) for x in got] == [(oracle.prf(5, dom, j) * q) >> 64 for j in range(4)]
+
+
+def test_dense_commit_matches_ring_products(oracle):
+    """The oracle's dense commitment (src/arithmetic.rs:429-457) is the sum of ring products."""
+    from helpers import rand_mod
+    from salsaa_b200 import params as P
+    q = P.Q0
+    rng = np.random.default_rng(5)
+    A = rand_mod(rng, (2, 4, 16), q)
+    W = rand_mod(rng, (3, 4, 16), q)
+    C = oracle.dense_commit(A, W, q)
+    for j in range(2):
+        for c in range(3):
+            acc = [0] * 16
+            for i in range(4):
+                pr = oracle.ring_mul(A[j, i], W[c, i], q)
+                acc = [(x + int(y)) % q for x, y in zip(acc, pr)]
+            assert [int(v) for v in C[j, c]] == acc
