@@ -59,9 +59,10 @@ def parse():
     ap.add_argument("--preset", default=PRESET, help="parameter set (profiling; the metric is quoted on A0)")
     ap.add_argument("--wit-log", type=int, default=0,
                     help="profiling: shrink WIT_LEN to 2^L (SNARK rounds L-11), keeping d, q and the rows")
-    ap.add_argument("--no-dense", action="store_true", help="skip the dense commitment microbench")
+    ap.add_argument("--no-dense", action="store_true",
+                    help="skip the dense commitment and batched sumcheck microbenches")
     ap.add_argument("--dense-only", action="store_true",
-                    help="profiling: run only the dense commitment microbench and print its JSON")
+                    help="profiling: run only the dense commitment and batched sumcheck microbenches")
     ap.add_argument("--ntt-only", action="store_true",
                     help="profiling: run only the NTT microbench and print its JSON")
     ap.add_argument("--ntt-log-coeffs", type=int, default=28,
@@ -357,6 +358,7 @@ def run_ours(args):
     torch.cuda.empty_cache()
     ntt = ntt_bench(torch, api) if rank == 0 and not args.no_ntt else None
     dense = dense_bench(torch, api) if rank == 0 and not args.no_dense else None
+    scb = sumcheck_batch_bench(torch, api) if rank == 0 and not args.no_dense else None
     serving = serving_bench(torch, api, args.serve_requests, rank) if not args.no_serve else None
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -379,6 +381,7 @@ def run_ours(args):
             "e2e": e2e,
             "ntt": ntt,
             "commit_dense": dense,
+            "sumcheck_batch": scb,
             "serving": serving,
             "roofline": roofline_ck(traced, measured_peaks(tensor=True),
                                     statistics.mean(plain) * len(plain) if plain else None),
@@ -529,6 +532,42 @@ def dense_bench(torch, api):
             "runs": out}
 
 
+def sumcheck_batch_bench(torch, api):
+    """Norm-check sumcheck microbench: 64 instances with lengths log-uniform in
+    2^16..2^22 (seeded), ternary coefficients, the 50-bit prime; all rounds of
+    all instances in one batched call, against the same instances one call
+    each.  Bytes: 8 per coefficient (each vector is read once)."""
+    from salsaa_b200 import params as P
+    q, reps = P.Q0, 5
+    rng = np.random.default_rng(2024)
+    logs = np.sort(rng.integers(16, 23, size=64))
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(5)
+    vecs = [(torch.randint(-1, 2, (1 << int(k),), dtype=torch.int64, device="cuda", generator=gen) % q)
+            for k in logs]
+    total = sum(v.numel() for v in vecs)
+
+    def timed(fn):
+        fn()
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        e.synchronize()
+        return a.elapsed_time(e) / reps
+
+    batched = timed(lambda: api.sum_check_batch(vecs, q, 1, 0))
+    single = timed(lambda: [api.sum_check_batch([v], q, 1, 0) for v in vecs])
+    res = {"instances": len(vecs), "lengths_log2": [int(k) for k in logs], "coefficients": int(total),
+           "batched_ms": batched, "one_call_each_ms": single, "batched_GB/s": 8.0 * total / (batched * 1e6),
+           "speedup": single / batched}
+    del vecs
+    torch.cuda.empty_cache()
+    return res
+
+
 def trace_read(name):
     """(launches, total device ms, total algorithmic work) of a traced kernel."""
     import ctypes
@@ -638,7 +677,8 @@ def main():
     if args.dense_only:
         import torch
         from salsaa_b200 import api
-        print(json.dumps({"commit_dense": dense_bench(torch, api)}), flush=True)
+        print(json.dumps({"commit_dense": dense_bench(torch, api),
+                          "sumcheck_batch": sumcheck_batch_bench(torch, api)}), flush=True)
         return 0
     if args.ntt_only:
         import torch

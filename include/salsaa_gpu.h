@@ -196,6 +196,18 @@ void salsaa_server_destroy(salsaa_server* s);
 int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uint64_t count, uint64_t q, int inverse,
                int incomplete, void* stream);
 
+/* Many independent norm-check sumchecks in a few launches: the batched form
+ * of norm_check_1 + sum_check (src/subroutines/fast_norm_check.rs:135-320) for
+ * `count` <= 64 vectors of uneven power-of-two lengths (2..2^30), one
+ * repetition each.  Instance i draws its round challenges from the
+ * norm-check stream of (seed, round, repetition i).  d_vecs and lens are
+ * host arrays (device pointers, lengths); d_claims gets count sums of squares
+ * and d_polys the round polynomials (f0, f1, f2) of instance 0, then 1, ...
+ * (log2 len_i rounds each).  Each pass level over all instances is one
+ * persistent launch over equal tiles; one launch finishes every instance. */
+int salsaa_sumcheck_batch(const uint64_t* const* d_vecs, const uint64_t* lens, uint32_t count, uint64_t q,
+                          uint64_t seed, uint64_t round, uint64_t* d_claims, uint64_t* d_polys, void* stream);
+
 /* Dense ring-matrix commitment C = A * W over R_q: parallel_dot_matrix_matrix
  * (src/arithmetic.rs:429-457) in the Ajtai shape, C[j][c] = sum_i A[j][i] W[c][i].
  * The key holds A (n x m ring elements of degree d, coefficient form, given

@@ -67,6 +67,8 @@ DEVICE_SYMBOLS = {
     "salsaa_prove": (INT, [VP, U64, VP, VP, U64]),
     "salsaa_ntt": (INT, [VP, VP, U64, U64, U64, INT, INT, VP]),
     "salsaa_poly_mul": (INT, [VP, VP, VP, U64, U64, U64, VP]),
+    "salsaa_sumcheck_batch": (INT, [ctypes.POINTER(VP), ctypes.POINTER(U64), ctypes.c_uint32, U64, U64, U64, VP,
+                                    VP, VP]),
     "salsaa_dense_key_create": (INT, [VP, U64, U64, U64, U64, VP, ctypes.POINTER(VP)]),
     "salsaa_dense_key_destroy": (None, [VP]),
     "salsaa_dense_commit": (INT, [VP, VP, U64, VP, VP, VP]),

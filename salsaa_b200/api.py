@@ -185,6 +185,25 @@ def poly_mul(a, b, n, q, out=None):
     return out
 
 
+def sum_check_batch(vecs, q, seed, round_):
+    """Independent sumchecks of a list of CUDA vectors (power-of-two lengths,
+    one repetition each, instance i on the challenge stream (round, i)) ->
+    (claims[count], [polys_i of shape (log2 len_i, 3)])."""
+    count = len(vecs)
+    ptrs = (ctypes.c_void_p * count)(*[v.data_ptr() for v in vecs])
+    lens = (ctypes.c_uint64 * count)(*[v.numel() for v in vecs])
+    nrs = [v.numel().bit_length() - 1 for v in vecs]
+    claims = dev_empty((count,))
+    polys = dev_empty((max(sum(nrs), 1), 3))
+    _check(lib().salsaa_sumcheck_batch(ptrs, lens, count, q, seed, round_, _p(claims), _p(polys), _stream()),
+           "sumcheck_batch")
+    out, o = [], 0
+    for nr in nrs:
+        out.append(polys[o:o + nr])
+        o += nr
+    return claims, out
+
+
 class DenseKey:
     """Ajtai commitment key A (n x m ring elements, coefficient form) for
     C = A * W (parallel_dot_matrix_matrix, src/arithmetic.rs:429-457)."""

@@ -8,6 +8,7 @@
 //   projection               src/subroutines/project.rs:26-103
 //   fold                     src/subroutines/fold.rs:22-27,70-75
 //   structured dot products  src/arithmetic.rs:459-536
+#include <vector>
 #include "kernels.cuh"
 
 namespace salsaa {
@@ -397,7 +398,274 @@ __global__ void __launch_bounds__(1024) sc_tail_kernel(const u64* in, u64 sin, R
   }
 }
 
-// Round polynomials and claims from the raw sums, canonical mod q.
+// ---------------------------------------------------------------------------
+// Batched uneven sumchecks: many independent vectors (one repetition each),
+// instance i drawing its challenges from the norm-check stream of
+// (round, repetition = i).  Every pass level is one persistent launch over
+// equal tiles of all instances still longer than SC_TAIL (a tile = 1024
+// groups of 16 elements; the tile -> instance map is a prefix table in shared
+// memory), four rounds per pass; a final launch finishes every instance in
+// shared memory (one CTA each).
+// ---------------------------------------------------------------------------
+struct SbInst {
+  const u64* in;
+  u64* out;
+  u64 L;     // current length
+  u64 tile0; // first tile of this instance in the level's tile space
+  u32 j;     // index of the next round
+  u32 id;    // instance index: its challenge stream and its rows of sums
+};
+constexpr u32 SB_MAX_INST = 64, SB_GPT = 4, SB_TILE_GROUPS = 256 * SB_GPT;
+
+__device__ __forceinline__ u64 sb_challenge(u64 seed, u32 round, u32 inst, u64 j, u64 q) {
+  return uni_mod(prf_at(prf_key(seed, domain_id(DOM_NC, round, inst)), j), q);
+}
+
+template <bool LAZY>
+__global__ void __launch_bounds__(256, 2) sb_pass_kernel(const SbInst* inst, u32 ninst, u64 ntiles, ModQ M,
+                                                         u64 seed, u32 round, u64* sums, u32 nrmax, bool plain) {
+  constexpr u32 T = SC_T, G = 1u << T;
+  __shared__ Sum128 red[32];
+  __shared__ u64 t0s[SB_MAX_INST + 1];
+  for (u32 i = threadIdx.x; i <= ninst; i += blockDim.x) t0s[i] = i < ninst ? inst[i].tile0 : ntiles;
+  __syncthreads();
+  const u64 q = M.q;
+  for (u64 tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    u32 lo = 0, hi = ninst;  // t0s[lo] <= tile < t0s[hi]
+    while (hi - lo > 1) {
+      const u32 mid = (lo + hi) / 2;
+      if (t0s[mid] <= tile) lo = mid;
+      else hi = mid;
+    }
+    const SbInst I = inst[lo];
+    const u64 ng = I.L / G, gbase = (tile - t0s[lo]) * SB_TILE_GROUPS;
+    u64 c[T], cp[T];
+#pragma unroll
+    for (u32 t = 0; t < T; t++) {
+      c[t] = sb_challenge(seed, round, I.id, I.j + t, q);
+      cp[t] = shoup_dev(c[t], q);
+    }
+    ScAcc<LAZY> acc[T][3];
+#pragma unroll
+    for (u32 t = 0; t < T; t++)
+#pragma unroll
+      for (u32 a = 0; a < 3; a++) acc[t][a].zero();
+#pragma unroll 1
+    for (u32 x = 0; x < SB_GPT; x++) {
+      const u64 g = gbase + x * 256 + threadIdx.x;
+      u64 v[G];
+#pragma unroll
+      for (u32 m = 0; m < G; m++) v[m] = __ldg(I.in + g + m * ng);
+      group_rounds<LAZY, T>(M, v, c, cp, acc, 0);
+      I.out[g] = v[0];
+    }
+#pragma unroll
+    for (u32 t = 0; t < T; t++)
+#pragma unroll
+      for (u32 a = 0; a < 3; a++) {
+        const u64 r = block_total<LAZY>(M, acc[t][a], red);
+        if (threadIdx.x == 0) atomic_add_mod(&sums[((u64)I.id * nrmax + I.j + t) * 3 + a], r, q, plain);
+      }
+  }
+}
+
+template <bool LAZY>
+__global__ void __launch_bounds__(1024) sb_tail_kernel(const SbInst* inst, ModQ M, u64 seed, u32 round, u64* sums,
+                                                       u32 nrmax) {
+  extern __shared__ u64 v[];
+  __shared__ Sum128 red[32];
+  const u32 i = blockIdx.x;
+  const SbInst I = inst[i];
+  const u64 q = M.q;
+  for (u64 e = threadIdx.x; e < I.L; e += blockDim.x) v[e] = I.in[e];
+  __syncthreads();
+  u64 cur = I.L;
+  u32 j = I.j;
+  while (cur > 1) {
+    const u64 h = cur / 2;
+    ScAcc<LAZY> a0, a1, a2;
+    a0.zero();
+    a1.zero();
+    a2.zero();
+    for (u64 e = threadIdx.x; e < h; e += blockDim.x) {
+      const u64 p0 = v[e], p1 = v[e + h];
+      a0.mac(M, p0, p0);
+      a1.mac(M, p0, p1);
+      a2.mac(M, p1, p1);
+    }
+    const u64 r0 = block_total<LAZY>(M, a0, red);
+    const u64 r1 = block_total<LAZY>(M, a1, red);
+    const u64 r2 = block_total<LAZY>(M, a2, red);
+    if (threadIdx.x == 0) {
+      u64* sp = &sums[((u64)i * nrmax + j) * 3];
+      sp[0] = r0;
+      sp[1] = r1;
+      sp[2] = r2;
+    }
+    const u64 c = sb_challenge(seed, round, i, j, q), cp = shoup_dev(c, q);
+    __syncthreads();
+    for (u64 e = threadIdx.x; e < h; e += blockDim.x) v[e] = fold1(v[e], v[e + h], c, cp, q);
+    __syncthreads();
+    cur = h;
+    j++;
+  }
+}
+
+// polys: instance i's nr_i x 3 block starts at offs[i] * 3
+__global__ void sb_finalize_kernel(const u64* sums, const u32* nrs, const u64* offs, u32 ninst, u32 nrmax, u64 q,
+                                   u64* claims, u64* polys) {
+  const u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (u64)ninst * nrmax) return;
+  const u32 i = (u32)(t / nrmax), j = (u32)(t % nrmax);
+  if (j >= nrs[i]) return;
+  const u64* s = sums + t * 3;
+  const u64 s00 = s[0] % q, s01 = s[1] % q, s11 = s[2] % q;
+  u64* o = polys + (offs[i] + j) * 3;
+  o[0] = s00;
+  o[1] = sub_mod(s01, s00, q);
+  o[2] = add_mod(sub_mod(sub_mod(s11, s01, q), s01, q), s00, q);
+  if (j == 0) claims[i] = add_mod(s00, s11, q);
+}
+
+int launch_sumcheck_batch(const u64* const* vecs, const u64* lens, u32 count, const ModQ& M, u64 seed, u32 round,
+                          u64* claims, u64* polys, cudaStream_t st) {
+  if (count == 0) return 0;
+  if (count > SB_MAX_INST) return salsaa_set_error(-2, "sumcheck_batch: at most 64 instances");
+  u32 nrmax = 0;
+  std::vector<u32> nrs(count);
+  std::vector<u64> offs(count);
+  u64 tot_a = 0, tot_b = 0, off = 0, max_tiles = 0;
+  for (u32 i = 0; i < count; i++) {
+    const u64 L = lens[i];
+    if (!vecs[i] || L < 2 || (L & (L - 1)) || L > (1ULL << 30))
+      return salsaa_set_error(-2, "sumcheck_batch: lengths must be powers of two in 2..2^30");
+    nrs[i] = 63u - (u32)__builtin_clzll(L);
+    nrmax = nrs[i] > nrmax ? nrs[i] : nrmax;
+    offs[i] = off;
+    off += nrs[i];
+    if (L > SC_TAIL) {
+      tot_a += L / 16;
+      tot_b += L / 256;
+      const u64 tiles = L / 16 / SB_TILE_GROUPS;
+      max_tiles = tiles > max_tiles ? tiles : max_tiles;
+    }
+  }
+  const bool lazy = M.q < (1ULL << 50);
+  const bool plain = lazy && max_tiles < (1ULL << 13);
+  // device scratch: sums, two ping-pong areas, descriptors, nrs / offs
+  const u32 maxlev = 8;  // 16^8 > 2^30
+  const u64 desc_bytes = (u64)(maxlev + 1) * SB_MAX_INST * sizeof(SbInst);
+  u64 *sums = nullptr, *bufa = nullptr, *bufb = nullptr, *doffs = nullptr;
+  SbInst* ddesc = nullptr;
+  u32* dnrs = nullptr;
+  auto alloc = [&](void** p, u64 bytes) {
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, st);
+    return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "sumcheck_batch: workspace");
+  };
+  struct Guard {
+    std::vector<void*> v;
+    cudaStream_t s;
+    ~Guard() {
+      for (void* p : v) cudaFreeAsync(p, s);
+    }
+  } guard{{}, st};
+  int rc = 0;
+  if ((rc = alloc((void**)&sums, (u64)count * nrmax * 3 * 8))) return rc;
+  guard.v.push_back(sums);
+  if ((rc = alloc((void**)&bufa, tot_a * 8))) return rc;
+  guard.v.push_back(bufa);
+  if ((rc = alloc((void**)&bufb, tot_b * 8))) return rc;
+  guard.v.push_back(bufb);
+  if ((rc = alloc((void**)&ddesc, desc_bytes))) return rc;
+  guard.v.push_back(ddesc);
+  if ((rc = alloc((void**)&dnrs, count * 4))) return rc;
+  guard.v.push_back(dnrs);
+  if ((rc = alloc((void**)&doffs, count * 8))) return rc;
+  guard.v.push_back(doffs);
+  cudaError_t e = cudaMemsetAsync(sums, 0, (u64)count * nrmax * 3 * 8, st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sumcheck_batch: memset");
+  // host plan: per level, the instances still longer than SC_TAIL, then the tail
+  std::vector<SbInst> plan((maxlev + 1) * SB_MAX_INST);
+  std::vector<u32> lev_n;
+  std::vector<u64> lev_tiles;
+  std::vector<const u64*> cur_in(vecs, vecs + count);
+  std::vector<u64> cur_L(lens, lens + count);
+  std::vector<u32> cur_j(count, 0);
+  std::vector<u64> oa(count), ob(count);
+  {
+    u64 ta = 0, tb = 0;
+    for (u32 i = 0; i < count; i++) {
+      oa[i] = ta;
+      ob[i] = tb;
+      if (lens[i] > SC_TAIL) {
+        ta += lens[i] / 16;
+        tb += lens[i] / 256;
+      }
+    }
+  }
+  for (u32 lev = 0; lev < maxlev; lev++) {
+    u64 tiles = 0;
+    u32 n = 0;
+    for (u32 i = 0; i < count; i++) {
+      if (cur_L[i] <= SC_TAIL) continue;
+      SbInst I{};
+      I.in = cur_in[i];
+      I.out = (lev % 2 == 0) ? bufa + oa[i] : bufb + ob[i];
+      I.L = cur_L[i];
+      I.tile0 = tiles;
+      I.j = cur_j[i];
+      I.id = i;
+      plan[lev * SB_MAX_INST + n++] = I;
+      tiles += cur_L[i] / 16 / SB_TILE_GROUPS;
+      cur_in[i] = I.out;
+      cur_L[i] /= 16;
+      cur_j[i] += SC_T;
+    }
+    if (!n) break;
+    lev_n.push_back(n);
+    lev_tiles.push_back(tiles);
+  }
+  const u32 nlev = (u32)lev_n.size();
+  u64 tail_max = 0;
+  for (u32 i = 0; i < count; i++) {
+    SbInst I{};
+    I.in = cur_in[i];
+    I.L = cur_L[i];
+    I.j = cur_j[i];
+    I.id = i;
+    plan[maxlev * SB_MAX_INST + i] = I;
+    tail_max = cur_L[i] > tail_max ? cur_L[i] : tail_max;
+  }
+  e = cudaMemcpyAsync(ddesc, plan.data(), desc_bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dnrs, nrs.data(), count * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(doffs, offs.data(), count * 8, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sumcheck_batch: plan");
+  // (from pageable memory the copies are staged before cudaMemcpyAsync returns)
+  for (u32 lev = 0; lev < nlev; lev++) {
+    const u64 grid = lev_tiles[lev] < 296 ? lev_tiles[lev] : 296;
+    if (lazy)
+      sb_pass_kernel<true><<<(unsigned)grid, 256, 0, st>>>(ddesc + lev * SB_MAX_INST, lev_n[lev], lev_tiles[lev],
+                                                            M, seed, round, sums, nrmax, plain);
+    else
+      sb_pass_kernel<false><<<(unsigned)grid, 256, 0, st>>>(ddesc + lev * SB_MAX_INST, lev_n[lev],
+                                                             lev_tiles[lev], M, seed, round, sums, nrmax, plain);
+    if ((rc = check_launch("sb_pass"))) return rc;
+  }
+  const size_t smem = tail_max * sizeof(u64);
+  auto tail = lazy ? sb_tail_kernel<true> : sb_tail_kernel<false>;
+  if (smem > 48 * 1024) {
+    e = cudaFuncSetAttribute(tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sumcheck_batch: tail smem");
+  }
+  tail<<<count, 1024, smem, st>>>(ddesc + maxlev * SB_MAX_INST, M, seed, round, sums, nrmax);
+  if ((rc = check_launch("sb_tail"))) return rc;
+  const u64 tot = (u64)count * nrmax;
+  sb_finalize_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(sums, dnrs, doffs, count, nrmax, M.q, claims,
+                                                                   polys);
+  return check_launch("sb_finalize");
+}
+
+// Round polynomials and claims from the raw sums, canonical mod q.// Round polynomials and claims from the raw sums, canonical mod q.
 __global__ void sc_finalize_kernel(const u64* sums, u32 rows, u32 nr, u64 q, u64* claims, u64* polys0,
                                    u64* polys1) {
   u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;

@@ -74,6 +74,11 @@ struct SumcheckBufs {
 };
 int launch_sumcheck(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, const DevState* ds, u32 round,
                     SumcheckBufs B, u64* proof_claims, u64* proof_rep0, u64* proof_rep1, cudaStream_t st);
+// Independent sumchecks of `count` <= 64 vectors of power-of-two lengths (one
+// repetition each; instance i uses the norm-check challenges of (round, i)):
+// claims[i] and the round polynomials of instance i at polys + 3 * sum_{i'<i} log2 len.
+int launch_sumcheck_batch(const u64* const* vecs, const u64* lens, u32 count, const ModQ& M, u64 seed, u32 round,
+                          u64* claims, u64* polys, cudaStream_t st);
 // norm_check_3 outputs: rhs (coef, into proof) and each repetition's ring base (slot).
 int launch_norm3(const u64* cap, u32 rows, u32 nr, const NttDev& T, const ModQ& M, const DevState* ds,
                  u32 round, u64* proof_rep0, u64* proof_rep1, u64* base0, u64* base1, cudaStream_t st);

@@ -940,6 +940,15 @@ extern "C" int salsaa_poly_mul(const uint64_t* d_a, const uint64_t* d_b, uint64_
   return ntt_launch(d_r, d_r, count, *T, false, true, st);
 }
 
+extern "C" int salsaa_sumcheck_batch(const uint64_t* const* d_vecs, const uint64_t* lens, uint32_t count, uint64_t q,
+                                     uint64_t seed, uint64_t round, uint64_t* d_claims, uint64_t* d_polys,
+                                     void* stream) {
+  if (!d_vecs || !lens || !d_claims || !d_polys) return salsaa_set_error(-1, "sumcheck_batch: null argument");
+  if (q < 3 || q >= (1ULL << 62)) return salsaa_set_error(-1, "sumcheck_batch: modulus must be in [3, 2^62)");
+  return launch_sumcheck_batch(d_vecs, lens, count, make_modq(q), seed, (u32)round, d_claims, d_polys,
+                               (cudaStream_t)stream);
+}
+
 extern "C" int salsaa_commit(salsaa_ctx* c, const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t* d_out,
                              void* stream) {
   if (!c || !d_w || !d_out) return salsaa_set_error(-1, "commit: null argument");

@@ -1,0 +1,69 @@
+"""Batched uneven sumchecks (salsaa_sumcheck_batch) against the CPU oracle,
+bit-exact: instance i follows sum_check (src/subroutines/fast_norm_check.rs:
+135-199) with the norm-check challenge stream of (round, repetition i)."""
+import numpy as np
+import pytest
+
+from helpers import nc_challenges, rand_mod, small_signed
+from salsaa_b200 import params as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api(gpu_lib, cuda):
+    from salsaa_b200 import api as A
+    return A
+
+
+def _check(api, oracle, vecs, q, seed, rnd):
+    claims, polys = api.sum_check_batch([api.to_dev(v) for v in vecs], q, seed, rnd)
+    claims = api.to_host(claims)
+    for i, v in enumerate(vecs):
+        nr = v.size.bit_length() - 1
+        cs = nc_challenges(seed, rnd, i, nr, q)
+        claim, want, _ = oracle.sumcheck(v, q, cs)
+        assert int(claims[i]) == claim, i
+        assert np.array_equal(api.to_host(polys[i]), want), i
+
+
+def test_sumcheck_batch_uneven(api, oracle):
+    """Tail-only, one-level and two-level instances in one batch."""
+    q = P.Q0
+    rng = np.random.default_rng(41)
+    logs = [4, 14, 15, 16, 19, 18, 1]
+    vecs = [small_signed(rng, 1 << k, 1, q) if k % 2 else rand_mod(rng, 1 << k, q) for k in logs]
+    _check(api, oracle, vecs, q, seed=12, rnd=3)
+
+
+def test_sumcheck_batch_64_instances(api, oracle):
+    q = P.Q1
+    rng = np.random.default_rng(7)
+    logs = rng.integers(10, 18, size=64)
+    vecs = [small_signed(rng, 1 << int(k), 1, q) for k in logs]
+    _check(api, oracle, vecs, q, seed=99, rnd=0)
+
+
+def test_sumcheck_batch_wide_modulus(api, oracle):
+    """q >= 2^50: exact residues instead of lazy 128-bit sums."""
+    q = P.Q62
+    rng = np.random.default_rng(3)
+    vecs = [rand_mod(rng, 1 << 17, q), rand_mod(rng, 1 << 9, q)]
+    _check(api, oracle, vecs, q, seed=5, rnd=1)
+
+
+def test_sumcheck_batch_matches_single_call(api, oracle):
+    """Instance 0 of a batch equals repetition 0 of the single-vector entry point."""
+    q = P.Q0
+    rng = np.random.default_rng(8)
+    w = small_signed(rng, (1, 1 << 16), 1, q)
+    claims, polys = api.sum_check(api.to_dev(w), 16, q, 21, 2)
+    bc, bp = api.sum_check_batch([api.to_dev(w[0])], q, 21, 2)
+    assert int(api.to_host(bc)[0]) == int(api.to_host(claims)[0])
+    assert np.array_equal(api.to_host(bp[0]), api.to_host(polys)[0, :, 0, :])
+
+
+def test_sumcheck_batch_rejects_bad_lengths(api):
+    from salsaa_b200.api import SalsaaError
+    with pytest.raises(SalsaaError):
+        api.sum_check_batch([api.to_dev(np.zeros(100, dtype=np.uint64))], P.Q0, 1, 0)
