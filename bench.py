@@ -399,6 +399,7 @@ def run_ours(args):
 
 SERVE_SLOTS = {"A0": 4, "A1": 4, "A2": 4, "F0": 4, "F1": 2, "F2": 1}
 SERVE_BUDGET = 140 << 30
+SERVE_MAX_INFLIGHT = 2  # proofs running at once in the served path
 
 
 def serving_bench(torch, api, nreq, rank):
@@ -445,6 +446,7 @@ def serving_bench(torch, api, nreq, rank):
     torch.cuda.empty_cache()
     # served path
     srv = api.Server(SERVE_BUDGET)
+    srv.limit(SERVE_MAX_INFLIGHT)
     sets = {nm: srv.register(params[nm], crs_seed=3, slots=SERVE_SLOTS[nm]) for nm in SERVE_SLOTS}
     outs = [torch.empty(api.proof_size(params[nm]) // 8, dtype=torch.int64, device="cuda") for nm in names]
     warm = [srv.submit(sets[nm], 1, torch.empty(api.proof_size(params[nm]) // 8, dtype=torch.int64,
@@ -476,7 +478,7 @@ def serving_bench(torch, api, nreq, rank):
     plain = {"proofs_per_s": nreq / plain_span, "p50_ms": 1e3 * float(np.median(plain_lat)),
              "p99_ms": 1e3 * float(np.percentile(plain_lat, 99))}
     return {"requests": nreq, "offered_per_s": rate, "mix": {nm: names.count(nm) for nm in SERVE_SLOTS},
-            "slots": SERVE_SLOTS, "served": served, "plain": plain,
+            "slots": SERVE_SLOTS, "max_in_flight": SERVE_MAX_INFLIGHT, "served": served, "plain": plain,
             "served_over_plain": served["proofs_per_s"] / plain["proofs_per_s"],
             "service_ms_alone": {nm: 1e3 * v for nm, v in service.items()}}
 

@@ -181,6 +181,8 @@ int salsaa_server_register(salsaa_server* s, const salsaa_params* p, uint64_t cr
  * device buffer of salsaa_proof_size() bytes that must stay valid until done. */
 int salsaa_server_submit(salsaa_server* s, int set_id, uint64_t seed, const uint64_t* d_witness, uint8_t* d_proof,
                          uint64_t* ticket);
+/* Cap the proofs running at once over all sets (0 = only the slots limit). */
+int salsaa_server_limit(salsaa_server* s, uint32_t max_inflight);
 /* Retire finished proofs and admit queued ones; returns requests in flight. */
 int salsaa_server_progress(salsaa_server* s);
 /* 1 pending, 0 done (latency from submit and from admission, ms), < 0 failed. */

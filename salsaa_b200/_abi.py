@@ -82,6 +82,7 @@ DEVICE_SYMBOLS = {
     "salsaa_server_create": (INT, [INT, U64, ctypes.POINTER(VP)]),
     "salsaa_server_register": (INT, [VP, PP, U64, ctypes.c_uint32, ctypes.POINTER(INT)]),
     "salsaa_server_submit": (INT, [VP, INT, U64, VP, VP, ctypes.POINTER(U64)]),
+    "salsaa_server_limit": (INT, [VP, ctypes.c_uint32]),
     "salsaa_server_progress": (INT, [VP]),
     "salsaa_server_poll": (INT, [VP, U64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "salsaa_server_destroy": (None, [VP]),

@@ -320,6 +320,10 @@ class Server:
                "server_submit")
         return t.value
 
+    def limit(self, max_inflight):
+        """Cap the proofs running at once (0 = only the slots limit)."""
+        _check(lib().salsaa_server_limit(self.h, max_inflight), "server_limit")
+
     def progress(self):
         rc = lib().salsaa_server_progress(self.h)
         if rc < 0:

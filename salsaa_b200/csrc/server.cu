@@ -59,6 +59,7 @@ struct salsaa_server {
   std::unordered_map<uint64_t, Req> reqs;
   std::deque<uint64_t> queue;
   uint64_t next_ticket = 1;
+  uint32_t max_inflight = 0;  // 0 = as many as there are slots
   std::mutex mu;
 };
 
@@ -151,7 +152,12 @@ extern "C" int salsaa_server_progress(salsaa_server* s) {
       r.t_done = now_ms();
       sl.ticket = 0;
     }
+  uint32_t running = 0;
+  for (PSet& ps : s->sets)
+    for (Slot& sl : ps.slots)
+      if (sl.ticket) running++;
   for (auto it = s->queue.begin(); it != s->queue.end();) {
+    if (s->max_inflight && running >= s->max_inflight) break;
     Req& r = s->reqs[*it];
     PSet& ps = s->sets[r.set];
     int free_slot = -1;
@@ -177,6 +183,7 @@ extern "C" int salsaa_server_progress(salsaa_server* s) {
       r.state = RQ_RUNNING;
       r.slot = free_slot;
       sl.ticket = *it;
+      running++;
     }
     it = s->queue.erase(it);
   }
@@ -185,6 +192,17 @@ extern "C" int salsaa_server_progress(salsaa_server* s) {
     for (Slot& sl : ps.slots)
       if (sl.ticket) pending++;
   return pending;
+}
+
+// Cap on proofs running at once over all parameter sets (0 = no cap beyond
+// the slots).  Every admitted proof shares the GPU with the others, so a
+// small cap keeps completion close to arrival order (tail latency) while
+// still overlapping one proof's short kernels with another's.
+extern "C" int salsaa_server_limit(salsaa_server* s, uint32_t max_inflight) {
+  if (!s) return salsaa_set_error(-1, "server_limit: null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->max_inflight = max_inflight;
+  return 0;
 }
 
 // 1 queued or running, 0 done (latencies in ms: from submit, and on the GPU

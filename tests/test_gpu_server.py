@@ -22,9 +22,11 @@ def api(gpu_lib, cuda):
     return A
 
 
-def test_mixed_stream_equals_alone(api, oracle, cuda):
+@pytest.mark.parametrize("max_inflight", [0, 1, 2])
+def test_mixed_stream_equals_alone(api, oracle, cuda, max_inflight):
     torch = cuda
     srv = api.Server(hbm_budget_bytes=16 << 30)
+    srv.limit(max_inflight)
     names = sorted(MIX)
     sets = {nm: srv.register(MIX[nm], crs_seed=7, slots=2) for nm in names}
     jobs = []
