@@ -90,6 +90,9 @@ __device__ __forceinline__ void atomic_add_mod(u64* addr, u64 v, u64 q, bool pla
   } while (old != assumed);
 }
 
+// Shoup without the final correction: x * w mod q in [0, 2q) for any 64-bit x.
+__device__ __forceinline__ u64 mul_shoup_lazy(u64 x, u64 w, u64 wp, u64 q) { return x * w - __umul64hi(x, wp) * q; }
+
 // ---- lazy limb accumulator (q < 2^50) -------------------------------------
 struct Acc3 {
   u64 lo, mid, hi;

@@ -1163,29 +1163,72 @@ int launch_fold_challenge(const DevState* ds, u32 round, u32 rows, u32 d, u64 q,
   return check_launch("fold_challenge");
 }
 
-__global__ void fold_kernel(RowSet w, u32 rows, u64 width, u32 n, ModQ M, const u64* zeta, const u64* c,
+// Fold constants per (row k, slot s): c_e, c_o and zeta c_o with their Shoup
+// companions, so each slot product is four Shoup multiplications:
+// (c_e + X c_o)(w_e + X w_o) = c_e w_e + (zeta c_o) w_o + X (c_o w_e + c_e w_o).
+__global__ void fold_pre_kernel(const u64* c, u32 rows, u32 n, ModQ M, const u64* zeta, u64* pre) {
+  const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= rows * n) return;
+  const u32 k = t / n, s = t % n;
+  const u64 ce = c[(u64)k * 2 * n + s], co = c[(u64)k * 2 * n + n + s], zco = mul_mod(M, zeta[s], co);
+  u64* p = pre + (u64)t * 6;
+  p[0] = ce;
+  p[1] = shoup_dev(ce, M.q);
+  p[2] = co;
+  p[3] = shoup_dev(co, M.q);
+  p[4] = zco;
+  p[5] = shoup_dev(zco, M.q);
+}
+
+// out = sum_k c_k w_k in slot form.  LAZY (q < 2^57, at most 16 rows): the
+// per-row terms (each below 4q) are summed without reduction and reduced once.
+template <bool LAZY>
+__global__ void fold_kernel(RowSet w, u32 rows, u64 width, u32 logn, ModQ M, const u64* __restrict__ pre,
                             u64* out) {
-  const u64 tot = width * n;
+  const u32 n = 1u << logn;
+  const u64 tot = width << logn, q = M.q, q2 = 2 * q;
   for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
-    const u64 i = t / n;
-    const u32 s = (u32)(t % n);
-    const u64 z = zeta[s];
+    const u64 i = t >> logn;
+    const u32 s = (u32)t & (n - 1);
     u64 ae = 0, ao = 0;
     for (u32 k = 0; k < rows; k++) {
-      const u64* x = w.p[k] + i * 2 * n;
-      u64 e, o;
-      slot_mul(M, x[s], x[n + s], c[(u64)k * 2 * n + s], c[(u64)k * 2 * n + n + s], z, e, o);
-      ae = add_mod(ae, e, M.q);
-      ao = add_mod(ao, o, M.q);
+      const u64* x = w.p[k] + (i << (logn + 1));
+      const u64 we = x[s], wo = x[n + s];
+      const u64* p = pre + ((u64)(k << logn) + s) * 6;
+      u64 e = mul_shoup_lazy(we, __ldg(p), __ldg(p + 1), q) + mul_shoup_lazy(wo, __ldg(p + 4), __ldg(p + 5), q);
+      u64 o = mul_shoup_lazy(we, __ldg(p + 2), __ldg(p + 3), q) + mul_shoup_lazy(wo, __ldg(p), __ldg(p + 1), q);
+      if (LAZY) {
+        ae += e;
+        ao += o;
+      } else {  // e, o < 4q < 2^64
+        e = e >= q2 ? e - q2 : e;
+        e = e >= q ? e - q : e;
+        o = o >= q2 ? o - q2 : o;
+        o = o >= q ? o - q : o;
+        ae = add_mod(ae, e, q);
+        ao = add_mod(ao, o, q);
+      }
     }
-    out[i * 2 * n + s] = ae;
-    out[i * 2 * n + n + s] = ao;
+    if (LAZY) {
+      ae = reduce64(M, ae);
+      ao = reduce64(M, ao);
+    }
+    out[(i << (logn + 1)) + s] = ae;
+    out[(i << (logn + 1)) + n + s] = ao;
   }
 }
 
-int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot,
+int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot, u64* pre,
                 u64* out_slot, cudaStream_t st) {
-  fold_kernel<<<grid_1d(width * T.n, 256), 256, 0, st>>>(w_slot, rows, width, T.n, M, T.zeta, c_slot, out_slot);
+  if (rows == 0 || rows > MAX_WROWS) return salsaa_set_error(-2, "fold: bad row count");
+  fold_pre_kernel<<<(rows * T.n + 127) / 128, 128, 0, st>>>(c_slot, rows, T.n, M, T.zeta, pre);
+  int rc = check_launch("fold_pre");
+  if (rc) return rc;
+  const bool lazy = M.q < (1ULL << 57);
+  if (lazy)
+    fold_kernel<true><<<grid_1d(width * T.n, 256), 256, 0, st>>>(w_slot, rows, width, T.logn, M, pre, out_slot);
+  else
+    fold_kernel<false><<<grid_1d(width * T.n, 256), 256, 0, st>>>(w_slot, rows, width, T.logn, M, pre, out_slot);
   return check_launch("fold");
 }
 

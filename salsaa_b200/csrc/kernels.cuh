@@ -96,7 +96,8 @@ int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_
                    const int8_t* J, DevState* ds, u64* out, cudaStream_t st);
 
 int launch_fold_challenge(const DevState* ds, u32 round, u32 rows, u32 d, u64 q, u64* c_coef, cudaStream_t st);
-int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot,
+// pre: scratch of rows x n x 6 words (Shoup constants of the challenges)
+int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot, u64* pre,
                 u64* out_slot, cudaStream_t st);
 
 // <statement rows, witness rows> in slot form.  acc: (nck + nsc) x rows x d

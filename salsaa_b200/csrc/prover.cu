@@ -382,7 +382,7 @@ struct salsaa_prover {
   u64* row_cj = nullptr;    // PERIODIC row scalars, rounds x CK_BLOCK
   u32 *pmask = nullptr, *nmask = nullptr;
   int8_t* Jm = nullptr;  // projection challenge as int8, 256 x chunk width
-  u64 *c_coef = nullptr, *c_slot = nullptr;
+  u64 *c_coef = nullptr, *c_slot = nullptr, *fold_pre = nullptr;
   ScalarRowDesc* sc_desc = nullptr;
   const u64** sc_base = nullptr;
   u64 *sc_lo = nullptr, *sc_hi = nullptr, *acc = nullptr, *cout = nullptr, *colsum = nullptr;
@@ -461,6 +461,7 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       (rc = m.alloc(&pr->Jm, 256ULL * CK_BLOCK, "projection J")) ||
       (rc = m.alloc(&pr->c_coef, (u64)MAX_WROWS * d, "fold c")) ||
       (rc = m.alloc(&pr->c_slot, (u64)MAX_WROWS * d, "fold c slot")) ||
+      (rc = m.alloc(&pr->fold_pre, (u64)MAX_WROWS * (d / 2) * 6, "fold constants")) ||
       (rc = m.alloc(&pr->sc_desc, (u64)S.nsc_total + 1, "row descriptors")) ||
       (rc = m.alloc(&pr->sc_base, (u64)S.nsc_total + 1, "row base pointers")) ||
       (rc = m.alloc(&pr->sc_lo, stmt * CK_BLOCK, "commit s_lo")) ||
@@ -730,7 +731,7 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(mark(pr, PH_FOLD));
     TRY(launch_fold_challenge(pr->ds, rd, K, d, q, pr->c_coef, st));
     TRY(ntt_launch(pr->c_coef, pr->c_slot, K, T, true, false, st));
-    TRY(launch_fold(Ws, K, width, T, M, pr->c_slot, pr->Fs, st));
+    TRY(launch_fold(Ws, K, width, T, M, pr->c_slot, pr->fold_pre, pr->Fs, st));
     TRY(ntt_launch(pr->Fs, pr->Fc, width, T, true, true, st));
     // send_cross_terms_before_join (src/subroutines/project.rs:229-245)
     RowSet Fr = rows_of(pr->Fs, 1, width, d);
@@ -1045,12 +1046,13 @@ extern "C" int salsaa_fold(const uint64_t* d_w, uint64_t rows, uint64_t width, u
   if (!T) return salsaa_set_error(-1, "fold: no NTT for (d, q)");
   cudaStream_t st = (cudaStream_t)stream;
   Tmp t(st);
-  u64 *ws, *cs, *fs;
+  u64 *ws, *cs, *fs, *pre;
   TRY(t.get(&ws, rows * width * d));
   TRY(t.get(&cs, rows * d));
   TRY(t.get(&fs, width * d));
+  TRY(t.get(&pre, rows * (d / 2) * 6));
   TRY(ntt_launch(d_w, ws, rows * width, *T, true, false, st));
   TRY(ntt_launch(d_c, cs, rows, *T, true, false, st));
-  TRY(launch_fold(rows_of(ws, (u32)rows, width, (u32)d), (u32)rows, width, *T, make_modq(q), cs, fs, st));
+  TRY(launch_fold(rows_of(ws, (u32)rows, width, (u32)d), (u32)rows, width, *T, make_modq(q), cs, pre, fs, st));
   return ntt_launch(fs, d_out, width, *T, true, true, st);
 }
