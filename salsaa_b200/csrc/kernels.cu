@@ -1362,22 +1362,30 @@ __global__ void __launch_bounds__(256) ck_commit_kernel(RowSet w, u32 rows, u32 
 // either the TENSOR tiles (want_tensor = 1, over the witness) or the others
 // (over the witness' column sums, since their s_hi is identically 1).
 template <int RT, int KT, bool LIMB>
-__global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 nsc, const ScalarRowDesc* desc,
-                                                        int want_tensor, const u64* s_lo, const u64* s_hi, u32 Bw,
-                                                        u32 nhi, u32 CH, ModQ M, u64* acc, bool plain) {
+__global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, ScRowList list, const u64* s_lo,
+                                                        const u64* s_hi, u32 Bw, u32 nhi, u32 CH, ModQ M, u64* acc,
+                                                        bool plain) {
   const u32 d = blockDim.x, p = threadIdx.x;
-  const u32 r0 = blockIdx.x * RT, k0 = blockIdx.z * KT;
-  if ((desc[r0].type == ROW_TENSOR) != (want_tensor != 0)) return;
+  const u32 t0 = blockIdx.x * RT, k0 = blockIdx.z * KT;
+  u32 row[RT];  // statement rows of this tile (the last one repeated past the list's end)
+#pragma unroll
+  for (int a = 0; a < RT; a++) row[a] = list.idx[(t0 + a < list.n) ? t0 + a : list.n - 1];
   const u64 i0 = (u64)blockIdx.y * CH;
   const u32 hi = (u32)(i0 / Bw), lo0 = (u32)(i0 % Bw);
-  const u64 q = M.q;
-  Acc3 ac[RT][KT];
+  const u64 q = M.q, qh = q / 2;
+  // LIMB (q < 2^50): the centred witness value c = wh 2^25 + wl (|wl| <= 2^24)
+  // times the row value s = s1 2^25 + s0 accumulates as three signed sums
+  // A0 = sum s0 wl, A1 = sum (s1 wl + s0 wh), A2 = sum s1 wh; each term is
+  // below 2^51, so 2048 terms stay below 2^63.  When no value of the warp
+  // needs wh (small witness, the common case in coefficient form) the two
+  // wh products are skipped for the whole warp.
+  long long A0[RT][KT], A1[RT][KT], A2[RT][KT];
   u64 g[RT][KT];
 #pragma unroll
   for (int a = 0; a < RT; a++)
 #pragma unroll
     for (int b = 0; b < KT; b++) {
-      acc_zero(ac[a][b]);
+      A0[a][b] = A1[a][b] = A2[a][b] = 0;
       g[a][b] = 0;
     }
   const u64* wp[KT];
@@ -1385,7 +1393,7 @@ __global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 
   for (int b = 0; b < KT; b++) wp[b] = ((k0 + b < rows) ? w.p[k0 + b] : w.p[k0]) + i0 * d + p;
   const u64* sp[RT];
 #pragma unroll
-  for (int a = 0; a < RT; a++) sp[a] = s_lo + (u64)((r0 + a < nsc) ? r0 + a : r0) * Bw + lo0;
+  for (int a = 0; a < RT; a++) sp[a] = s_lo + (u64)row[a] * Bw + lo0;
   u64 x[KT], sv[RT];
 #pragma unroll
   for (int b = 0; b < KT; b++) x[b] = __ldg(wp[b]);
@@ -1399,15 +1407,42 @@ __global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 
 #pragma unroll
     for (int a = 0; a < RT; a++) ns[a] = __ldg(sp[a] + en);
     if (LIMB) {
-      u32 x1[KT], x0[KT];
+      int wl[KT], wh[KT];
+      bool big = false;
 #pragma unroll
-      for (int b = 0; b < KT; b++) split25(x[b], x1[b], x0[b]);
+      for (int b = 0; b < KT; b++) {
+        // small (|centred value| < 2^24): x < 2^24 or x > q - 2^24; then the
+        // low 32 bits of x or x - q are the signed value itself
+        const bool neg = x[b] > qh;
+        wl[b] = (int)((u32)x[b] - (neg ? (u32)q : 0u));
+        wh[b] = 0;
+        big |= neg ? (x[b] <= q - (1ULL << 24)) : (x[b] >= (1ULL << 24));
+      }
+      big = __any_sync(0xffffffffu, big);
+      if (big) {  // exact split of every value of this step
+#pragma unroll
+        for (int b = 0; b < KT; b++) {
+          const long long c = x[b] > qh ? (long long)x[b] - (long long)q : (long long)x[b];
+          const long long l = ((c + (1LL << 24)) & ((1LL << 25) - 1)) - (1LL << 24);
+          wl[b] = (int)l;
+          wh[b] = (int)((c - l) >> 25);
+        }
+      }
 #pragma unroll
       for (int a = 0; a < RT; a++) {
-        u32 s1, s0;
-        split25(sv[a], s1, s0);
+        const int s0 = (int)(sv[a] & 0x1FFFFFFull), s1 = (int)(sv[a] >> 25);
 #pragma unroll
-        for (int b = 0; b < KT; b++) acc_mac(ac[a][b], x1[b], x0[b], s1, s0);
+        for (int b = 0; b < KT; b++) {
+          A0[a][b] += (long long)s0 * wl[b];
+          A1[a][b] += (long long)s1 * wl[b];
+        }
+        if (big) {
+#pragma unroll
+          for (int b = 0; b < KT; b++) {
+            A1[a][b] += (long long)s0 * wh[b];
+            A2[a][b] += (long long)s1 * wh[b];
+          }
+        }
       }
     } else {
 #pragma unroll
@@ -1420,16 +1455,26 @@ __global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, u32 
 #pragma unroll
     for (int a = 0; a < RT; a++) sv[a] = ns[a];
   }
+  // signed sums -> residues: add a multiple of q above 2^62 to negative ones
+  const u64 cpos = LIMB ? ((((u64)1 << 62) / q) + 1) * q : 0;
+  const u64 p25 = LIMB ? ((u64)1 << 25) % q : 0, p50 = LIMB ? ((u64)1 << 50) % q : 0;
+  auto smod = [&](long long v) -> u64 { return reduce64(M, v < 0 ? (u64)(v + (long long)cpos) : (u64)v); };
 #pragma unroll
   for (int a = 0; a < RT; a++) {
-    if (r0 + a >= nsc) break;
-    const u64 h = s_hi[(u64)(r0 + a) * nhi + hi];
+    if (t0 + a >= list.n) break;
+    const u64 h = s_hi[(u64)row[a] * nhi + hi];
 #pragma unroll
     for (int b = 0; b < KT; b++) {
       if (k0 + b >= rows) break;
-      u64 v = LIMB ? acc_reduce(M, ac[a][b]) : g[a][b];
+      u64 v;
+      if (LIMB) {
+        v = add_mod(smod(A0[a][b]), mul_mod(M, smod(A1[a][b]), p25), q);
+        v = add_mod(v, mul_mod(M, smod(A2[a][b]), p50), q);
+      } else {
+        v = g[a][b];
+      }
       v = mul_mod(M, v, h);
-      atomic_add_mod(acc + ((u64)(r0 + a) * rows + k0 + b) * d + p, v, q, plain);
+      atomic_add_mod(acc + ((u64)row[a] * rows + k0 + b) * d + p, v, q, plain);
     }
   }
 }
@@ -1768,22 +1813,30 @@ static void launch_ck_variant(const CommitArgs& a, u32 n, u32 Bt, u32 nhi_t, u32
 }
 
 template <int RT, int KT>
-static void launch_sc_variant(const CommitArgs& a, const RowSet& w, u64 width, int want_tensor, u32 d, u32 Bw,
+static void launch_sc_variant(const CommitArgs& a, const RowSet& w, u64 width, const ScRowList& list, u32 d, u32 Bw,
                               u32 nhi, u32 CH, const ModQ& M, bool plain, u64* acc_sc, cudaStream_t st) {
-  dim3 g((a.nsc + RT - 1) / RT, (unsigned)(width / CH), (a.rows + KT - 1) / KT);
+  dim3 g((list.n + RT - 1) / RT, (unsigned)(width / CH), (a.rows + KT - 1) / KT);
   if (M.q < (1ULL << 50))
-    sc_commit_kernel<RT, KT, true><<<g, d, 0, st>>>(w, a.rows, a.nsc, a.sc_desc_dev, want_tensor, a.sc_lo, a.sc_hi,
-                                                   Bw, nhi, CH, M, acc_sc, plain);
+    sc_commit_kernel<RT, KT, true><<<g, d, 0, st>>>(w, a.rows, list, a.sc_lo, a.sc_hi, Bw, nhi, CH, M, acc_sc, plain);
   else
-    sc_commit_kernel<RT, KT, false><<<g, d, 0, st>>>(w, a.rows, a.nsc, a.sc_desc_dev, want_tensor, a.sc_lo, a.sc_hi,
-                                                    Bw, nhi, CH, M, acc_sc, plain);
+    sc_commit_kernel<RT, KT, false><<<g, d, 0, st>>>(w, a.rows, list, a.sc_lo, a.sc_hi, Bw, nhi, CH, M, acc_sc,
+                                                    plain);
 }
 
-static void launch_sc_pass(const CommitArgs& a, const RowSet& w, u64 width, int want_tensor, u32 d, u32 Bw, u32 nhi,
-                           u32 CH, const ModQ& M, bool plain, u64* acc_sc, cudaStream_t st) {
-  if (a.rows == 1) launch_sc_variant<2, 1>(a, w, width, want_tensor, d, Bw, nhi, CH, M, plain, acc_sc, st);
-  else if (a.rows == 2) launch_sc_variant<2, 2>(a, w, width, want_tensor, d, Bw, nhi, CH, M, plain, acc_sc, st);
-  else launch_sc_variant<2, 4>(a, w, width, want_tensor, d, Bw, nhi, CH, M, plain, acc_sc, st);
+// One launch per row list (TENSOR rows over the witness; periodic / all-ones
+// rows over its column sums), tiles of 2 rows x up to 4 witness rows.
+static void launch_sc_pass(const CommitArgs& a, const RowSet& w, u64 width, const ScRowList& list, bool tensor, u32 d,
+                           u32 Bw, u32 nhi, u32 CH, const ModQ& M, bool plain, u64* acc_sc, cudaStream_t st) {
+  if (!list.n) return;
+  (void)tensor;
+  if (a.rows == 1) launch_sc_variant<2, 1>(a, w, width, list, d, Bw, nhi, CH, M, plain, acc_sc, st);
+  else if (a.rows == 2) launch_sc_variant<2, 2>(a, w, width, list, d, Bw, nhi, CH, M, plain, acc_sc, st);
+  else launch_sc_variant<2, 4>(a, w, width, list, d, Bw, nhi, CH, M, plain, acc_sc, st);
+}
+
+__global__ void reduce_inplace_kernel(u64* x, u64 n, ModQ M) {
+  for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    x[i] = reduce64(M, x[i]);
 }
 
 int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st) {
@@ -1824,15 +1877,24 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
     int rc = check_launch("sc_tables");
     if (rc) return rc;
     u64* acc_sc = a.acc + (u64)a.nck * a.rows * d;
+    // scalar rows are linear in the witness: with its coefficient form given,
+    // sum there (small centred values) and move the sums to slot form after
+    const RowSet& wsrc = a.coef_sc ? a.wc : a.w;
+    if (!a.sc_types_host || a.nsc > SC_MAX_ROWS) return salsaa_set_error(-2, "commit: scalar row types missing");
+    ScRowList tl{}, ol{};
+    for (u32 j = 0; j < a.nsc; j++) {
+      if (a.sc_types_host[j] == ROW_TENSOR) tl.idx[tl.n++] = (unsigned char)j;
+      else ol.idx[ol.n++] = (unsigned char)j;
+    }
     // TENSOR rows over the witness
-    launch_sc_pass(a, a.w, a.width, 1, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
+    launch_sc_pass(a, wsrc, a.width, tl, true, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
     rc = check_launch("sc_commit (tensor rows)");
     if (rc) return rc;
     // periodic and all-ones rows over the column sums
-    RowSet u = a.w;
+    RowSet u = wsrc;
     if (nhi > 1) {
       if (!a.colsum || a.rows > a.colsum_rows) return salsaa_set_error(-2, "commit: column-sum scratch too small");
-      colsum_kernel<<<grid_1d((u64)a.rows * Bw * d, 256), 256, 0, st>>>(a.w, a.rows, a.width, Bw, d, M, a.colsum);
+      colsum_kernel<<<grid_1d((u64)a.rows * Bw * d, 256), 256, 0, st>>>(wsrc, a.rows, a.width, Bw, d, M, a.colsum);
       rc = check_launch("colsum");
       if (rc) return rc;
       for (u32 k = 0; k < a.rows; k++) u.p[k] = a.colsum + (u64)k * Bw * d;
@@ -1840,9 +1902,17 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
     u64 CHu = Bw / 64;
     if (CHu < 16) CHu = 16;
     if (CHu > Bw) CHu = Bw;
-    launch_sc_pass(a, u, Bw, 0, d, Bw, nhi, (u32)CHu, M, plain, acc_sc, st);
+    launch_sc_pass(a, u, Bw, ol, false, d, Bw, nhi, (u32)CHu, M, plain, acc_sc, st);
     rc = check_launch("sc_commit (periodic rows)");
     if (rc) return rc;
+    if (a.coef_sc) {
+      const u64 cnt = (u64)a.nsc * a.rows;
+      reduce_inplace_kernel<<<grid_1d(cnt * d, 256), 256, 0, st>>>(acc_sc, cnt * d, M);
+      rc = check_launch("reduce");
+      if (rc) return rc;
+      rc = ntt_launch(acc_sc, acc_sc, cnt, T, true, false, st);
+      if (rc) return rc;
+    }
   }
   const u64 tot = (u64)(a.nck + a.nsc) * a.rows * n;
   commit_finalize_kernel<<<grid_1d(tot, 256), 256, 0, st>>>(a.acc, a.nck, a.nsc, a.rows, n, M, T.zeta,

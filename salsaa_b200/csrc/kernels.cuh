@@ -27,6 +27,13 @@ struct DevState {
   u64 proj_flag;   // projection: set when a witness value does not fit int8
 };
 
+// Indices of the scalar rows one commitment pass covers (passed by value).
+constexpr u32 SC_MAX_ROWS = 64;
+struct ScRowList {
+  u32 n;
+  unsigned char idx[SC_MAX_ROWS];
+};
+
 // ---- statement rows -------------------------------------------------------
 enum RowType : int { ROW_CK = 0, ROW_TENSOR = 1, ROW_PERIODIC = 2, ROW_ONES = 3 };
 
@@ -104,6 +111,8 @@ int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ&
 // scratch; out_slot: results in statement order given by `order`.
 struct CommitArgs {
   RowSet w;          // slot-form witness rows
+  RowSet wc;         // the same rows in coefficient form (used when coef_sc)
+  bool coef_sc;      // scalar rows over wc, their sums moved to slot form after
   u32 rows;
   u64 width;
   u32 nck;           // commitment-key rows (statement rows 0..nck-1)
@@ -113,6 +122,7 @@ struct CommitArgs {
   u32 ck_nhi;        // L / ck_bt
   u32 nsc;           // scalar rows
   const ScalarRowDesc* sc_desc_dev;  // nsc descriptors in device memory
+  const int* sc_types_host;          // their types, on the host (required when nsc > 0)
   const u64* const* sc_base_dev;     // nsc ring bases (slot form) or null (= 1)
   u64* sc_lo;        // scratch nsc x CK_BLOCK
   u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)

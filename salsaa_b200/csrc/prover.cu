@@ -384,6 +384,7 @@ struct salsaa_prover {
   int8_t* Jm = nullptr;  // projection challenge as int8, 256 x chunk width
   u64 *c_coef = nullptr, *c_slot = nullptr, *fold_pre = nullptr;
   ScalarRowDesc* sc_desc = nullptr;
+  std::vector<int> sc_types;  // host copy of the scalar rows' types (launch tiling)
   const u64** sc_base = nullptr;
   u64 *sc_lo = nullptr, *sc_hi = nullptr, *acc = nullptr, *cout = nullptr, *colsum = nullptr;
   u64* cout2 = nullptr;  // coefficient-form staging of a merged commitment
@@ -509,6 +510,7 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       if (c->P.folding) break;
     }
   }
+  for (const ScalarRowDesc& sd : desc) pr->sc_types.push_back(sd.type);
   if (!desc.empty()) {
     e = cudaMemcpy(pr->sc_desc, desc.data(), desc.size() * sizeof(ScalarRowDesc), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
@@ -543,13 +545,18 @@ __global__ void set_seed_kernel(DevState* ds, u64 seed) { ds->seed = seed; }
 
 // <statement rows [0, nck) ++ scalar rows [sc_first, sc_first + nsc), witness rows>
 // -> slot-form ring elements in pr->cout, row-major (statement, witness).
-static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width, u32 nck, u32 sc_first,
-                            u32 nsc) {
+// wc: the same witness rows in coefficient form (scalar rows are summed there), or null.
+static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, const RowSet* wc, u32 rows, u64 width, u32 nck,
+                            u32 sc_first, u32 nsc) {
   salsaa_ctx* c = pr->ctx;
   if ((u64)sc_first + nsc > c->S.nsc_total || nck > c->P.module_size)
     return salsaa_set_error(-9, "commit: statement row range outside the proof's rows");
   CommitArgs a{};
   a.w = ws;
+  if (wc && nsc) {
+    a.wc = *wc;
+    a.coef_sc = true;
+  }
   a.rows = rows;
   a.width = width;
   a.nck = nck;
@@ -559,6 +566,7 @@ static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 w
   a.ck_nhi = c->ck_nhi;
   a.nsc = nsc;
   a.sc_desc_dev = pr->sc_desc + sc_first;
+  a.sc_types_host = nsc ? pr->sc_types.data() + sc_first : nullptr;
   a.sc_base_dev = pr->sc_base + sc_first;
   a.sc_lo = pr->sc_lo;
   a.sc_hi = pr->sc_hi;
@@ -572,9 +580,9 @@ static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 w
 }
 
 // Same, in coefficient form at proof_out.
-static int commit_rows(salsaa_prover* pr, const RowSet& ws, u32 rows, u64 width, u32 nck, u32 sc_first, u32 nsc,
-                       u64* proof_out) {
-  TRY(commit_rows_slot(pr, ws, rows, width, nck, sc_first, nsc));
+static int commit_rows(salsaa_prover* pr, const RowSet& ws, const RowSet* wc, u32 rows, u64 width, u32 nck,
+                       u32 sc_first, u32 nsc, u64* proof_out) {
+  TRY(commit_rows_slot(pr, ws, wc, rows, width, nck, sc_first, nsc));
   return ntt_launch(pr->cout, proof_out, (u64)(nck + nsc) * rows, *pr->ctx->T, true, true, pr->st);
 }
 
@@ -617,7 +625,7 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
   u64 pend_off = cur;             // pending derived commitment: proof offset,
   u32 pend_rows = ms, pend_K = K; // statement rows and witness rows
   bool pending = !P.folding && P.nof_rounds > 0;
-  if (!pending) TRY(commit_rows(pr, Ws, K, width, ms, 0, 0, proof + cur));
+  if (!pending) TRY(commit_rows(pr, Ws, &Wc, K, width, ms, 0, 0, proof + cur));
   cur += (u64)ms * K * d;
   u32 nsc = 0, didx = 0;
   for (u32 rd = 0; rd < P.nof_rounds; rd++) {
@@ -677,15 +685,17 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Jm, pr->ds, pr->Pc, st));
     TRY(ntt_launch(pr->Pc, pr->Ps, width, T, true, false, st));
     RowSet Pr = rows_of(pr->Ps, 1, width, d);
+    RowSet Prc = rows_of(pr->Pc, 1, width, d);
     const u32 S = ms + nsc;
     if (!P.folding) {
       // split rhs and projected commitment in one pass over the statement
       // rows: witness columns L_0..L_{K/2-1}, R_0..R_{K/2-1}, P.  The
       // challenges are fixed in advance, so computing P first changes nothing.
       TRY(mark(pr, PH_SPLIT));
-      RowSet both = Ws;
+      RowSet both = Ws, bothc = Wc;
       both.p[K] = pr->Ps;
-      TRY(commit_rows_slot(pr, both, K + 1, width, ms, 0, nsc));
+      bothc.p[K] = pr->Pc;
+      TRY(commit_rows_slot(pr, both, &bothc, K + 1, width, ms, 0, nsc));
       TRY(ntt_launch(pr->cout, pr->cout2, (u64)S * (K + 1), T, true, true, st));
       const size_t row_bytes = (size_t)(K + 1) * d * sizeof(u64);
       e = cudaMemcpy2DAsync(proof + cur, (size_t)K * d * sizeof(u64), pr->cout2, row_bytes,
@@ -718,13 +728,13 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
         pending = false;
       }
     } else {
-      TRY(commit_rows(pr, Pr, 1, width, ms, 0, nsc, proof + cur));
+      TRY(commit_rows(pr, Pr, &Prc, 1, width, ms, 0, nsc, proof + cur));
       cur += (u64)S * d;
     }
     // batch_projections (src/subroutines/project.rs:131-203): witness_rhs, projection_rhs
-    TRY(commit_rows(pr, Ws, K, width, 0, nsc, 1, proof + cur));
+    TRY(commit_rows(pr, Ws, &Wc, K, width, 0, nsc, 1, proof + cur));
     cur += (u64)K * d;
-    TRY(commit_rows(pr, Pr, 1, width, 0, nsc + 1, 1, proof + cur));
+    TRY(commit_rows(pr, Pr, &Prc, 1, width, 0, nsc + 1, 1, proof + cur));
     cur += d;
     nsc += 1;  // witness_lhs joins the statement
     // fold (src/subroutines/fold.rs:22-27)
@@ -734,10 +744,10 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(launch_fold(Ws, K, width, T, M, pr->c_slot, pr->fold_pre, pr->Fs, st));
     TRY(ntt_launch(pr->Fs, pr->Fc, width, T, true, true, st));
     // send_cross_terms_before_join (src/subroutines/project.rs:229-245)
-    RowSet Fr = rows_of(pr->Fs, 1, width, d);
-    TRY(commit_rows(pr, Fr, 1, width, 0, nsc, 1, proof + cur));  // l0 = <projected_lhs, folded>
+    RowSet Fr = rows_of(pr->Fs, 1, width, d), Frc = rows_of(pr->Fc, 1, width, d);
+    TRY(commit_rows(pr, Fr, &Frc, 1, width, 0, nsc, 1, proof + cur));  // l0 = <projected_lhs, folded>
     cur += d;
-    TRY(commit_rows(pr, Pr, 1, width, 0, nsc - 1, 1, proof + cur));  // l1 = <witness_lhs, projected>
+    TRY(commit_rows(pr, Pr, &Prc, 1, width, 0, nsc - 1, 1, proof + cur));  // l1 = <witness_lhs, projected>
     cur += d;
     nsc += 1;  // projected_lhs joins the statement
     // join: witness = [folded, projected]
@@ -755,7 +765,8 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       K *= 2;
       TRY(ntt_launch(pr->Dc, pr->Ds, (u64)K * width, T, true, false, st));
       Ws = rows_of(pr->Ds, K, width, d);
-      TRY(commit_rows(pr, Ws, K, width, ms, 0, nsc, proof + cur));
+      const RowSet Dcr = rows_of(pr->Dc, K, width, d);
+      TRY(commit_rows(pr, Ws, &Dcr, K, width, ms, 0, nsc, proof + cur));
       cur += (u64)(ms + nsc) * K * d;
       break;
     }
