@@ -206,40 +206,45 @@ struct ScAcc {
     else g = add_mod(g, mul_mod(M, a, b), M.q);
   }
 };
-// Block total of one accumulator slot, reduced mod q; valid in thread 0.
-template <bool LAZY>
-__device__ u64 block_total(const ModQ& M, ScAcc<LAZY> v, Sum128* sm) {
+// Block totals of NV accumulator slots at once (one barrier for all of them,
+// one more so the shared buffer can be reused); thread i < NV gets total i.
+// red: NV x 32 slots of shared memory.
+template <bool LAZY, int NV>
+__device__ __forceinline__ u64 block_totals(const ModQ& M, ScAcc<LAZY> (&v)[NV], Sum128* red) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  if (LAZY) {
-    Sum128 t = v.s;
-    for (int o = 16; o > 0; o >>= 1) {
-      Sum128 u;
-      u.lo = __shfl_down_sync(0xffffffffu, t.lo, o);
-      u.hi = __shfl_down_sync(0xffffffffu, t.hi, o);
-      s128_add(t, u);
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+    if (LAZY) {
+      Sum128 t = v[i].s;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        Sum128 u;
+        u.lo = __shfl_down_sync(0xffffffffu, t.lo, o);
+        u.hi = __shfl_down_sync(0xffffffffu, t.hi, o);
+        s128_add(t, u);
+      }
+      if (lane == 0) red[i * 32 + wid] = t;
+    } else {
+      u64 t = v[i].g;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t = add_mod(t, __shfl_down_sync(0xffffffffu, t, o), M.q);
+      if (lane == 0) red[i * 32 + wid].lo = t;
     }
-    __syncthreads();
-    if (lane == 0) sm[wid] = t;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      Sum128 a = sm[0];
-      for (int w = 1; w < nw; w++) s128_add(a, sm[w]);
-      return reduce128_any(M, a.hi, a.lo);
-    }
-    return 0;
-  } else {
-    u64 t = v.g;
-    for (int o = 16; o > 0; o >>= 1) t = add_mod(t, __shfl_down_sync(0xffffffffu, t, o), M.q);
-    __syncthreads();
-    if (lane == 0) sm[wid].lo = t;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      u64 a = 0;
-      for (int w = 0; w < nw; w++) a = add_mod(a, sm[w].lo, M.q);
-      return a;
-    }
-    return 0;
   }
+  __syncthreads();
+  u64 r = 0;
+  if (threadIdx.x < NV) {
+    const int i = threadIdx.x;
+    if (LAZY) {
+      Sum128 a = red[i * 32];
+      for (int w = 1; w < nw; w++) s128_add(a, red[i * 32 + w]);
+      r = reduce128_any(M, a.hi, a.lo);
+    } else {
+      for (int w = 0; w < nw; w++) r = add_mod(r, red[i * 32 + w].lo, M.q);
+    }
+  }
+  __syncthreads();
+  return r;
 }
 
 __device__ __forceinline__ u64 fold1(u64 a, u64 b, u64 c, u64 cp, u64 q) {
@@ -277,7 +282,7 @@ __global__ void __launch_bounds__(256, 2) sc_first_kernel(RowSet w, u32 rows, u6
                                                           u32 round, u64* out, u64 sout, u64* sums, u32 nr,
                                                           bool plain) {
   constexpr u32 T = SC_T, G = 1u << T;
-  __shared__ Sum128 red[32];
+  __shared__ Sum128 red[SC_T * 3 * 32];
   const u32 k = blockIdx.y, rep = blockIdx.x & 1, bx = blockIdx.x >> 1, nbx = gridDim.x >> 1;
   const u64* x = w.p[k];
   const u64 q = M.q, ng = nlen / G;
@@ -299,17 +304,16 @@ __global__ void __launch_bounds__(256, 2) sc_first_kernel(RowSet w, u32 rows, u6
     group_rounds<LAZY, T>(M, v, c, cp, acc, rep == 0 ? 0 : 1);
     out[((u64)rep * rows + k) * sout + g] = v[0];
   }
+  ScAcc<LAZY> flat[T * 3];
 #pragma unroll
-  for (u32 t = 0; t < T; t++) {
-    if (t == 0 && rep != 0) continue;  // uniform per CTA
+  for (u32 t = 0; t < T; t++)
 #pragma unroll
-    for (u32 a = 0; a < 3; a++) {
-      const u64 r = block_total<LAZY>(M, acc[t][a], red);
-      if (threadIdx.x == 0) {
-        atomic_add_mod(&sums[((rep * (u64)nr + t) * rows + k) * 3 + a], r, q, plain);
-        if (t == 0) atomic_add_mod(&sums[((1 * (u64)nr + 0) * rows + k) * 3 + a], r, q, plain);
-      }
-    }
+    for (u32 a = 0; a < 3; a++) flat[t * 3 + a] = acc[t][a];
+  const u64 r = block_totals<LAZY, T * 3>(M, flat, red);
+  if (threadIdx.x < T * 3) {
+    const u32 t = threadIdx.x / 3, a = threadIdx.x % 3;
+    if (t > 0 || rep == 0) atomic_add_mod(&sums[((rep * (u64)nr + t) * rows + k) * 3 + a], r, q, plain);
+    if (t == 0 && rep == 0) atomic_add_mod(&sums[((1 * (u64)nr + 0) * rows + k) * 3 + a], r, q, plain);
   }
 }
 
@@ -319,7 +323,7 @@ __global__ void __launch_bounds__(256) sc_round_kernel(const u64* in, u64 sin, u
                                                        ModQ M, const DevState* ds, u32 round, u32 j, u64* sums,
                                                        u32 nr, bool plain) {
   constexpr u32 T = SC_T, G = 1u << T;
-  __shared__ Sum128 red[32];
+  __shared__ Sum128 red[SC_T * 3 * 32];
   const u32 pair = blockIdx.y, rep = pair / rows, k = pair % rows;
   const u64 q = M.q, ng = L / G;
   const u64* x = in + (u64)pair * sin;
@@ -342,13 +346,16 @@ __global__ void __launch_bounds__(256) sc_round_kernel(const u64* in, u64 sin, u
     group_rounds<LAZY, T>(M, v, c, cp, acc, 0);
     y[g] = v[0];
   }
+  ScAcc<LAZY> flat[T * 3];
 #pragma unroll
   for (u32 t = 0; t < T; t++)
 #pragma unroll
-    for (u32 a = 0; a < 3; a++) {
-      const u64 r = block_total<LAZY>(M, acc[t][a], red);
-      if (threadIdx.x == 0) atomic_add_mod(&sums[((rep * (u64)nr + j + t) * rows + k) * 3 + a], r, q, plain);
-    }
+    for (u32 a = 0; a < 3; a++) flat[t * 3 + a] = acc[t][a];
+  const u64 r = block_totals<LAZY, T * 3>(M, flat, red);
+  if (threadIdx.x < T * 3) {
+    const u32 t = threadIdx.x / 3, a = threadIdx.x % 3;
+    atomic_add_mod(&sums[((rep * (u64)nr + j + t) * rows + k) * 3 + a], r, q, plain);
+  }
 }
 
 // One CTA per (rep,row) finishes rounds j0.. from v_{j0} (length L <= SC_TAIL),
@@ -358,7 +365,7 @@ __global__ void __launch_bounds__(1024) sc_tail_kernel(const u64* in, u64 sin, R
                                                        const DevState* ds, u32 round, u32 j0, u64* sums, u32 nr,
                                                        u32 d, u64* cap) {
   extern __shared__ u64 v[];
-  __shared__ Sum128 red[32];
+  __shared__ Sum128 red[3 * 32];
   const u32 pair = blockIdx.x, rep = pair / rows, k = pair % rows;
   const u64 q = M.q;
   const u64* x = (j0 == 0) ? w0.p[k] : in + (u64)pair * sin;
@@ -380,15 +387,9 @@ __global__ void __launch_bounds__(1024) sc_tail_kernel(const u64* in, u64 sin, R
       a1.mac(M, p0, p1);
       a2.mac(M, p1, p1);
     }
-    const u64 r0 = block_total<LAZY>(M, a0, red);
-    const u64 r1 = block_total<LAZY>(M, a1, red);
-    const u64 r2 = block_total<LAZY>(M, a2, red);
-    if (threadIdx.x == 0) {
-      u64* sp = &sums[((rep * (u64)nr + j) * rows + k) * 3];
-      sp[0] = r0;
-      sp[1] = r1;
-      sp[2] = r2;
-    }
+    ScAcc<LAZY> tri[3] = {a0, a1, a2};
+    const u64 r = block_totals<LAZY, 3>(M, tri, red);
+    if (threadIdx.x < 3) sums[((rep * (u64)nr + j) * rows + k) * 3 + threadIdx.x] = r;
     const u64 c = nc_challenge(ds, round, rep, j, q), cp = shoup_dev(c, q);
     __syncthreads();
     for (u32 i = threadIdx.x; i < h; i += blockDim.x) v[i] = fold1(v[i], v[i + h], c, cp, q);
@@ -425,7 +426,7 @@ template <bool LAZY>
 __global__ void __launch_bounds__(256, 2) sb_pass_kernel(const SbInst* inst, u32 ninst, u64 ntiles, ModQ M,
                                                          u64 seed, u32 round, u64* sums, u32 nrmax, bool plain) {
   constexpr u32 T = SC_T, G = 1u << T;
-  __shared__ Sum128 red[32];
+  __shared__ Sum128 red[SC_T * 3 * 32];
   __shared__ u64 t0s[SB_MAX_INST + 1];
   for (u32 i = threadIdx.x; i <= ninst; i += blockDim.x) t0s[i] = i < ninst ? inst[i].tile0 : ntiles;
   __syncthreads();
@@ -459,13 +460,14 @@ __global__ void __launch_bounds__(256, 2) sb_pass_kernel(const SbInst* inst, u32
       group_rounds<LAZY, T>(M, v, c, cp, acc, 0);
       I.out[g] = v[0];
     }
+    ScAcc<LAZY> flat[T * 3];
 #pragma unroll
     for (u32 t = 0; t < T; t++)
 #pragma unroll
-      for (u32 a = 0; a < 3; a++) {
-        const u64 r = block_total<LAZY>(M, acc[t][a], red);
-        if (threadIdx.x == 0) atomic_add_mod(&sums[((u64)I.id * nrmax + I.j + t) * 3 + a], r, q, plain);
-      }
+      for (u32 a = 0; a < 3; a++) flat[t * 3 + a] = acc[t][a];
+    const u64 r = block_totals<LAZY, T * 3>(M, flat, red);
+    if (threadIdx.x < T * 3)
+      atomic_add_mod(&sums[((u64)I.id * nrmax + I.j + threadIdx.x / 3) * 3 + threadIdx.x % 3], r, q, plain);
   }
 }
 
@@ -473,7 +475,7 @@ template <bool LAZY>
 __global__ void __launch_bounds__(1024) sb_tail_kernel(const SbInst* inst, ModQ M, u64 seed, u32 round, u64* sums,
                                                        u32 nrmax) {
   extern __shared__ u64 v[];
-  __shared__ Sum128 red[32];
+  __shared__ Sum128 red[3 * 32];
   const u32 i = blockIdx.x;
   const SbInst I = inst[i];
   const u64 q = M.q;
@@ -493,15 +495,9 @@ __global__ void __launch_bounds__(1024) sb_tail_kernel(const SbInst* inst, ModQ 
       a1.mac(M, p0, p1);
       a2.mac(M, p1, p1);
     }
-    const u64 r0 = block_total<LAZY>(M, a0, red);
-    const u64 r1 = block_total<LAZY>(M, a1, red);
-    const u64 r2 = block_total<LAZY>(M, a2, red);
-    if (threadIdx.x == 0) {
-      u64* sp = &sums[((u64)i * nrmax + j) * 3];
-      sp[0] = r0;
-      sp[1] = r1;
-      sp[2] = r2;
-    }
+    ScAcc<LAZY> tri[3] = {a0, a1, a2};
+    const u64 r = block_totals<LAZY, 3>(M, tri, red);
+    if (threadIdx.x < 3) sums[((u64)i * nrmax + j) * 3 + threadIdx.x] = r;
     const u64 c = sb_challenge(seed, round, i, j, q), cp = shoup_dev(c, q);
     __syncthreads();
     for (u64 e = threadIdx.x; e < h; e += blockDim.x) v[e] = fold1(v[e], v[e + h], c, cp, q);
@@ -693,12 +689,14 @@ static int sumcheck_passes(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, c
   u64 sin = 0;
   bool to_a = true;
   auto grid_for = [](u64 groups, u32 pairs) {
-    u64 want = (148ULL * 8 + pairs - 1) / pairs;  // about eight CTAs per SM in total
+    // one resident wave in total (two CTAs per SM): few CTAs, each streaming
+    // many groups, so the per-CTA reductions stay a small share
+    u64 want = (148ULL * 2 + pairs - 1) / pairs;
     u64 g = (groups + 255) / 256;
     return (unsigned)(g < want ? (g ? g : 1) : want);
   };
   if (L > SC_TAIL) {
-    dim3 g(2 * grid_for(L / (1u << SC_T), rows), rows);
+    dim3 g(2 * grid_for(L / (1u << SC_T), 2 * rows), rows);
     sc_first_kernel<LAZY><<<g, 256, 0, st>>>(w, rows, L, M, ds, round, B.a, sa, B.sums, nr, plain);
     int rc = check_launch("sc_first");
     if (rc) return rc;
