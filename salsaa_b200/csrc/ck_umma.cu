@@ -341,6 +341,139 @@ int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, const u64*
   return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ck_umma launch");
 }
 
+// ---------------------------------------------------------------------------
+// Projection on tcgen05 (project, src/subroutines/project.rs:50-103): per
+// chunk of cw witness elements, out[256 x d] = J (256 x cw, entries -1/0/1) x
+// W (cw x d, centre-lifted, int8).  CTA = (chunk, block of 128 coefficient
+// positions); per 128-element step thread 0 bulk-copies both 128-row halves
+// of J from their canonical image (Jc, see launch_proj_tables) and issues
+// 2 x 4 MMAs (kind::i8, signed x signed, M = 128 J rows, N = 128 positions,
+// K = 32) into two TMEM accumulators; the threads convert the witness step to
+// int8 in the canonical layout.  A value outside [-128, 127] sets the flag and
+// the exact CUDA-core kernel recomputes every output (same as the mma.sync
+// path).  Two stages: the witness of step c + 1 is staged while the MMAs of
+// step c run.
+// ---------------------------------------------------------------------------
+constexpr u32 PU_POS = 128, PU_KS = 128;
+constexpr u32 PU_A = 2 * 128 * PU_KS;  // both J halves of one step (32 KiB)
+constexpr u32 PU_B = PU_POS * PU_KS;   // witness int8 tile (16 KiB)
+constexpr u32 PU_STAGE = PU_A + PU_B;
+
+__global__ void __launch_bounds__(256, 2)
+    project_umma_kernel(RowSet in, u32 d, u64 q, u32 cw, u64 nch, const int8_t* __restrict__ Jc,
+                        u64* __restrict__ out, u64* flag) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t full_bar[2], done_bar[2];
+  __shared__ uint32_t tslot;
+  const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const u32 nblk = blockIdx.x;
+  const u64 idx = blockIdx.y;
+  const u32 i = (u32)(idx / nch);
+  const u64 j = idx % nch;
+  const u64* chunk = in.p[i] + (j * cw) * d + (u64)nblk * PU_POS;
+  const u64 half_q = q >> 1;
+  const u32 nsteps = cw / PU_KS;
+  u32* err = &g_tc_error;
+  if (tid == 0) {
+    for (int b = 0; b < 2; b++) {
+      umma::mbar_init(&full_bar[b], 1);
+      umma::mbar_init(&done_bar[b], 1);
+    }
+    umma::mbar_fence_init();
+  }
+  if (warp == 0) umma::tmem_alloc(&tslot, 256);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const u32 tmem = tslot;
+  // signed int8 x signed int8 -> s32, M = N = 128
+  const u32 idesc = umma::idesc_u8(128, PU_POS) | (1u << 7) | (1u << 10);
+  bool bad = false, ok = true;
+  for (u32 c = 0; c < nsteps; c++) {
+    const u32 st = c & 1;
+    uint8_t* stage = smem + st * PU_STAGE;
+    if (c >= 2) ok &= umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1);
+    if (tid == 0) {
+      umma::mbar_expect_tx(&full_bar[st], PU_A);
+      umma::bulk_g2s(stage, Jc + (u64)c * PU_A, PU_A, &full_bar[st]);
+    }
+    // witness step: 128 positions x 128 elements as int8, (k / 16, pos, k % 16)
+    uint8_t* B = stage + PU_A;
+    const u64* src = chunk + (u64)c * PU_KS * d;
+#pragma unroll 4
+    for (u32 x = 0; x < 16; x++) {
+      const u32 t = tid + x * 256;
+      const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
+      const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
+      const u32 k = (k4hi * 4 + k4lo) * 4;
+      u32 packed = 0;
+#pragma unroll
+      for (u32 e = 0; e < 4; e++) {
+        const u64 v = __ldg(src + (u64)(k + e) * d + pos);
+        long long cv = v > half_q ? (long long)v - (long long)q : (long long)v;
+        if (cv < -128 || cv > 127) {
+          bad = true;
+          cv = 0;
+        }
+        packed |= ((u32)cv & 0xffu) << (8 * e);
+      }
+      *(u32*)(B + k4hi * (PU_POS * 16) + pos * 16 + k4lo * 4) = packed;
+    }
+    umma::fence_proxy_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      ok &= umma::mbar_wait(&full_bar[st], (c >> 1) & 1, err, 2);
+#pragma unroll
+      for (u32 h = 0; h < 2; h++)
+#pragma unroll
+        for (u32 ks = 0; ks < PU_KS / 32; ks++) {
+          const uint64_t ad =
+              umma::desc_kmajor(umma::smem_u32(stage + h * (PU_A / 2) + ks * 2 * 128 * 16), 128 * 16, 128);
+          const uint64_t bd = umma::desc_kmajor(umma::smem_u32(B + ks * 2 * PU_POS * 16), PU_POS * 16, 128);
+          umma::mma_i8(tmem + h * 128, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+        }
+      umma::commit(&done_bar[st]);
+    }
+  }
+  ok &= umma::mbar_wait(&done_bar[(nsteps - 1) & 1], ((nsteps - 1) >> 1) & 1, err, 3);
+  ok = __syncthreads_and(ok);
+  if (bad) atomicOr((unsigned long long*)flag, 1ULL);
+  umma::fence_after_sync();
+  if (ok) {
+    const u32 h = warp >> 2, row = (warp & 3) * 32 + lane;
+    u64* dst = out + ((idx * 256) + h * 128 + row) * d + (u64)nblk * PU_POS;
+    for (u32 cb = 0; cb < PU_POS; cb += 16) {
+      uint32_t r[16];
+      umma::tmem_ld16(tmem + (((warp & 3) * 32) << 16) + h * 128 + cb, r);
+      umma::tmem_wait_ld();
+#pragma unroll
+      for (u32 e = 0; e < 16; e += 2) {
+        const int v0 = (int)r[e], v1 = (int)r[e + 1];
+        const u64 a = v0 >= 0 ? (u64)v0 : q - (u64)(-(long long)v0);
+        const u64 b = v1 >= 0 ? (u64)v1 : q - (u64)(-(long long)v1);
+        *(ulonglong2*)(dst + cb + e) = make_ulonglong2(a, b);
+      }
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 256);
+}
+
+int launch_project_umma(RowSet in, u32 rows, u64 nch, u32 d, u64 q, u32 cw, const int8_t* Jc, u64* out, u64* flag,
+                        cudaStream_t st) {
+  const size_t smem = 2 * (size_t)PU_STAGE;
+  cudaError_t e = cudaFuncSetAttribute(project_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "project_umma smem attribute");
+  dim3 g(d / PU_POS, (unsigned)(rows * nch));
+  project_umma_kernel<<<g, 256, smem, st>>>(in, d, q, cw, nch, Jc, out, flag);
+  salsaa_count_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "project_umma launch");
+}
+
 int tc_error_check() {
   u32 h = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&h, g_tc_error, sizeof(u32));

@@ -918,7 +918,7 @@ int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u3
 constexpr u32 PROJ_H = 256;
 
 __global__ void proj_tables_kernel(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask,
-                                   int8_t* J) {
+                                   int8_t* J, int8_t* Jc) {
   const u32 words = cw / 32;
   u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (u64)PROJ_H * words) return;
@@ -932,7 +932,12 @@ __global__ void proj_tables_kernel(const DevState* ds, u32 round, u32 cw, u32* p
       if (sg) pm |= 1u << b;
       else nm |= 1u << b;
     }
-    if (J) J[(u64)k * cw + w * 32 + b] = iz ? 0 : (sg ? 1 : -1);
+    const int8_t v = iz ? 0 : (sg ? 1 : -1);
+    if (J) J[(u64)k * cw + w * 32 + b] = v;
+    if (Jc) {  // (chunk, half, 16-byte slice, row in half, byte)
+      const u32 l = w * 32 + b, cc = l / 128, sl = (l % 128) / 16, h = k / 128, r = k % 128;
+      Jc[((((u64)cc * 2 + h) * 8 + sl) * 128 + r) * 16 + (l % 16)] = v;
+    }
   }
   pos_mask[t] = pm;
   neg_mask[t] = nm;
@@ -951,10 +956,11 @@ __global__ void proj_cj_kernel(u32 cw, const u32* pos_mask, const u32* neg_mask,
 }
 
 int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, int8_t* J, u64* cj,
-                       u64 q, cudaStream_t st) {
+                       u64 q, cudaStream_t st, int8_t* Jc) {
   if (cw % 32) return salsaa_set_error(-2, "project: chunk width must be a multiple of 32");
+  if (Jc && cw % 128) Jc = nullptr;
   u64 tot = (u64)PROJ_H * (cw / 32);
-  proj_tables_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(ds, round, cw, pos_mask, neg_mask, J);
+  proj_tables_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(ds, round, cw, pos_mask, neg_mask, J, Jc);
   int rc = check_launch("proj_tables");
   if (rc) return rc;
   if (cj) {
@@ -1117,7 +1123,7 @@ __global__ void __launch_bounds__(256, 2) project_mma_kernel(RowSet in, u32 d, u
 }
 
 int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_mask, const u32* neg_mask,
-                   const int8_t* J, DevState* ds, u64* out, cudaStream_t st) {
+                   const int8_t* J, DevState* ds, u64* out, cudaStream_t st, const int8_t* Jc) {
   const u32 cw = rows * PROJ_H;
   if (rows == 0 || rows > MAX_WROWS || cw > width || width % cw)
     return salsaa_set_error(-3, "project: chunk width exceeds witness width");
@@ -1125,7 +1131,13 @@ int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_
   const u64 nch = width / cw;
   if ((u64)rows * nch > 65535) return salsaa_set_error(-2, "project: too many chunks");
   const u64* gate = nullptr;
-  if (J && ds && d % PJ_BN == 0 && cw % PJ_KS == 0) {
+  if (Jc && ds && d % 128 == 0 && cw % 128 == 0) {
+    cudaError_t e = cudaMemsetAsync(&ds->proj_flag, 0, sizeof(u64), st);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "project memset");
+    int rc = launch_project_umma(in, rows, nch, d, q, cw, Jc, out, &ds->proj_flag, st);
+    if (rc) return rc;
+    gate = &ds->proj_flag;
+  } else if (J && ds && d % PJ_BN == 0 && cw % PJ_KS == 0) {
     cudaError_t e = cudaMemsetAsync(&ds->proj_flag, 0, sizeof(u64), st);
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "project memset");
     dim3 gm(2 * (d / PJ_BN), (unsigned)(rows * nch));

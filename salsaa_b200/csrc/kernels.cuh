@@ -95,12 +95,17 @@ int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u3
 
 // J as bit masks (CUDA-core path), as an int8 matrix 256 x cw (tensor-core
 // path, optional) and cj[l] = sum_k J[k][l] (optional).
+// Jc (optional): J again, as the tcgen05 A-operand image: for each 128-element
+// chunk, both 128-row halves in the canonical K-major layout (256 x cw bytes).
 int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, int8_t* J, u64* cj,
-                       u64 q, cudaStream_t st);
+                       u64 q, cudaStream_t st, int8_t* Jc = nullptr);
 // Tensor-core path when d is a multiple of 128 and J is given; exact CUDA-core
 // recomputation (chosen on the device) whenever a value does not fit int8.
 int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_mask, const u32* neg_mask,
-                   const int8_t* J, DevState* ds, u64* out, cudaStream_t st);
+                   const int8_t* J, DevState* ds, u64* out, cudaStream_t st, const int8_t* Jc = nullptr);
+// tcgen05 projection over chunks (see ck_umma.cu); Jc from launch_proj_tables.
+int launch_project_umma(RowSet in, u32 rows, u64 nch, u32 d, u64 q, u32 cw, const int8_t* Jc, u64* out, u64* flag,
+                        cudaStream_t st);
 
 int launch_fold_challenge(const DevState* ds, u32 round, u32 rows, u32 d, u64 q, u64* c_coef, cudaStream_t st);
 // pre: scratch of rows x n x 6 words (Shoup constants of the challenges)

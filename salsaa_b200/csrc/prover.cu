@@ -382,6 +382,7 @@ struct salsaa_prover {
   u64* row_cj = nullptr;    // PERIODIC row scalars, rounds x CK_BLOCK
   u32 *pmask = nullptr, *nmask = nullptr;
   int8_t* Jm = nullptr;  // projection challenge as int8, 256 x chunk width
+  int8_t* Jc = nullptr;  // the same in the tcgen05 operand layout
   u64 *c_coef = nullptr, *c_slot = nullptr, *fold_pre = nullptr;
   ScalarRowDesc* sc_desc = nullptr;
   std::vector<int> sc_types;  // host copy of the scalar rows' types (launch tiling)
@@ -418,6 +419,8 @@ extern "C" uint64_t salsaa_workspace_bytes(const salsaa_params* p) {
   words += stmt * CK_BLOCK + stmt * (L / CK_BLOCK + 1);
   words += 2 * stmt * MAX_WROWS * d;
   words += (u64)(S.max_rows + 1) * (L < CK_BLOCK ? L : CK_BLOCK) * d;
+  words += 2 * 256ULL * CK_BLOCK / 8;          // projection J and its tensor-core image (bytes)
+  words += (u64)MAX_WROWS * (d / 2) * 6;       // fold constants
   return words * 8 + (S.proof_words * 8);
 }
 
@@ -460,6 +463,7 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       (rc = m.alloc(&pr->pmask, 256ULL * CK_BLOCK / 32, "pos mask")) ||
       (rc = m.alloc(&pr->nmask, 256ULL * CK_BLOCK / 32, "neg mask")) ||
       (rc = m.alloc(&pr->Jm, 256ULL * CK_BLOCK, "projection J")) ||
+      (rc = m.alloc(&pr->Jc, 256ULL * CK_BLOCK, "projection J (tensor-core layout)")) ||
       (rc = m.alloc(&pr->c_coef, (u64)MAX_WROWS * d, "fold c")) ||
       (rc = m.alloc(&pr->c_slot, (u64)MAX_WROWS * d, "fold c slot")) ||
       (rc = m.alloc(&pr->fold_pre, (u64)MAX_WROWS * (d / 2) * 6, "fold constants")) ||
@@ -681,8 +685,8 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(mark(pr, PH_PROJ));
     const u32 cw = K * 256;
     u64* cj = pr->row_cj + (u64)rd * CK_BLOCK;
-    TRY(launch_proj_tables(pr->ds, rd, cw, pr->pmask, pr->nmask, pr->Jm, cj, q, st));
-    TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Jm, pr->ds, pr->Pc, st));
+    TRY(launch_proj_tables(pr->ds, rd, cw, pr->pmask, pr->nmask, pr->Jm, cj, q, st, pr->Jc));
+    TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Jm, pr->ds, pr->Pc, st, pr->Jc));
     TRY(ntt_launch(pr->Pc, pr->Ps, width, T, true, false, st));
     RowSet Pr = rows_of(pr->Ps, 1, width, d);
     RowSet Prc = rows_of(pr->Pc, 1, width, d);
