@@ -474,6 +474,204 @@ int launch_project_umma(RowSet in, u32 rows, u64 nch, u32 d, u64 q, u32 cw, cons
   return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "project_umma launch");
 }
 
+// ---------------------------------------------------------------------------
+// TENSOR statement rows on tcgen05 (the scalar rows of
+// parallel_dot_series_matrix, src/arithmetic.rs:459-505, whose weights are
+// s(i) = s_hi[i / Bw] s_lo[i % Bw]), over the coefficient-form witness.
+// For one witness row k, one block of Bw elements (one s_hi factor) and 128
+// coefficient positions, sum_i s_lo(i) w(i) is an integer matrix product:
+//   A (M = 128): rows (tensor row r, byte x) of s_lo, unsigned bytes,
+//   B (N = 128): coefficient positions, the centred witness split into three
+//     signed byte limbs (exact for |w| < 2^23), one MMA chain per limb,
+//   D_l[(r,x)][pos] = sum_i byte_x(s_lo(i)) limb_l(w(i, pos)),
+// and the row sum is sum_{x,l} 2^(8(x+l)) D_l mod q.  A CTA that meets a
+// larger value adds nothing and flags itself; sc_exact_kernel then redoes
+// exactly the flagged CTAs on CUDA cores.  The sums land in the coefficient-
+// form accumulators that launch_commit moves to slot form.
+// ---------------------------------------------------------------------------
+constexpr u32 SU_POS = 128, SU_KS = 128, SU_LIMBS = 3;
+constexpr u32 SU_A = 128 * SU_KS;                   // scalar byte tile (16 KiB)
+constexpr u32 SU_B = SU_POS * SU_KS;                // one limb tile (16 KiB)
+constexpr u32 SU_STAGE = SU_A + SU_LIMBS * SU_B;    // 64 KiB
+
+__global__ void sc_img_kernel(const u64* s_lo, u32 Bw, ScRowList tl, uint8_t* img) {
+  const u64 tot = (u64)Bw * 128;  // (chunk, slice, row, byte) = Bw / 128 x 8 x 128 x 16
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u32 b = (u32)(t % 16), row = (u32)((t / 16) % 128), sl = (u32)((t / 2048) % 8), cc = (u32)(t / 16384);
+    uint8_t v = 0;
+    if (row < tl.n * 7) {
+      const u32 r = row / 7, x = row % 7;
+      v = (uint8_t)(s_lo[(u64)tl.idx[r] * Bw + cc * 128 + sl * 16 + b] >> (8 * x));
+    }
+    img[t] = v;
+  }
+}
+
+__global__ void __launch_bounds__(256, 1)
+    sc_umma_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, ScRowList tl, const uint8_t* __restrict__ img,
+                   const u64* s_hi, ModQ M, u64* acc, bool plain, u32* flags) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t full_bar[2], done_bar[2];
+  __shared__ uint32_t tslot;
+  const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const u32 pb = blockIdx.x, hb = blockIdx.y, k = blockIdx.z;
+  const u64 q = M.q, half_q = q >> 1;
+  const u64* src0 = wc.p[k] + ((u64)hb * Bw) * d + (u64)pb * SU_POS;
+  const u32 nsteps = Bw / SU_KS;
+  u32* err = &g_tc_error;
+  if (tid == 0) {
+    for (int b = 0; b < 2; b++) {
+      umma::mbar_init(&full_bar[b], 1);
+      umma::mbar_init(&done_bar[b], 1);
+    }
+    umma::mbar_fence_init();
+  }
+  if (warp == 0) umma::tmem_alloc(&tslot, 512);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const u32 tmem = tslot;
+  // unsigned bytes (A) x signed bytes (B) -> s32, M = N = 128
+  const u32 idesc = umma::idesc_u8(128, SU_POS) | (1u << 10);
+  bool bad = false, ok = true;
+  for (u32 c = 0; c < nsteps; c++) {
+    const u32 st = c & 1;
+    uint8_t* stage = smem + st * SU_STAGE;
+    if (c >= 2) ok &= umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1);
+    if (tid == 0) {
+      umma::mbar_expect_tx(&full_bar[st], SU_A);
+      umma::bulk_g2s(stage, img + (u64)c * SU_A, SU_A, &full_bar[st]);
+    }
+    const u64* src = src0 + (u64)c * SU_KS * d;
+#pragma unroll 2
+    for (u32 x = 0; x < 16; x++) {
+      const u32 t = tid + x * 256;
+      const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
+      const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
+      const u32 e0 = (k4hi * 4 + k4lo) * 4;
+      u32 p0 = 0, p1 = 0, p2 = 0;
+#pragma unroll
+      for (u32 e = 0; e < 4; e++) {
+        const u64 v = __ldg(src + (u64)(e0 + e) * d + pos);
+        const long long cv = v > half_q ? (long long)v - (long long)q : (long long)v;
+        const long long l0 = ((cv + 128) & 255) - 128, c1 = (cv - l0) >> 8;
+        const long long l1 = ((c1 + 128) & 255) - 128;
+        long long l2 = (c1 - l1) >> 8;
+        if (l2 < -128 || l2 > 127) {  // the value needs a fourth limb
+          bad = true;
+          l2 = 0;
+        }
+        p0 |= ((u32)l0 & 0xffu) << (8 * e);
+        p1 |= ((u32)l1 & 0xffu) << (8 * e);
+        p2 |= ((u32)l2 & 0xffu) << (8 * e);
+      }
+      const u32 off = SU_A + k4hi * (SU_POS * 16) + pos * 16 + k4lo * 4;
+      *(u32*)(stage + off) = p0;
+      *(u32*)(stage + off + SU_B) = p1;
+      *(u32*)(stage + off + 2 * SU_B) = p2;
+    }
+    umma::fence_proxy_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      ok &= umma::mbar_wait(&full_bar[st], (c >> 1) & 1, err, 2);
+#pragma unroll
+      for (u32 l = 0; l < SU_LIMBS; l++)
+#pragma unroll
+        for (u32 ks = 0; ks < SU_KS / 32; ks++) {
+          const uint64_t ad = umma::desc_kmajor(umma::smem_u32(stage + ks * 2 * 128 * 16), 128 * 16, 128);
+          const uint64_t bd =
+              umma::desc_kmajor(umma::smem_u32(stage + SU_A + l * SU_B + ks * 2 * SU_POS * 16), SU_POS * 16, 128);
+          umma::mma_i8(tmem + l * 128, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+        }
+      umma::commit(&done_bar[st]);
+    }
+  }
+  ok &= umma::mbar_wait(&done_bar[(nsteps - 1) & 1], ((nsteps - 1) >> 1) & 1, err, 3);
+  ok = __syncthreads_and(ok);
+  bad = __syncthreads_or(bad);
+  umma::fence_after_sync();
+  const u32 cta = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  if (bad && tid == 0) flags[cta] = 1;
+  if (ok && !bad) {
+    // per TMEM lane (row (r, x)), per position: sum_l 2^(8l) D_l, reduced, times 2^(8x)
+    u64* Pm = (u64*)smem;  // 128 rows x 128 positions
+    const u32 row = (warp & 3) * 32 + lane, half = warp >> 2;  // warps 4..7 take positions 64..127
+    const u32 x = row % 7;
+    const u64 pw = ((u64)1 << (8 * x)) % q;
+    const u64 cpos = ((((u64)1 << 62) / q) + 1) * q;
+    for (u32 cb = half * 64; cb < half * 64 + 64; cb += 16) {
+      uint32_t r0[16], r1[16], r2[16];
+      const u32 base = tmem + (((warp & 3) * 32) << 16) + cb;
+      umma::tmem_ld16(base, r0);
+      umma::tmem_ld16(base + 128, r1);
+      umma::tmem_ld16(base + 256, r2);
+      umma::tmem_wait_ld();
+#pragma unroll
+      for (u32 e = 0; e < 16; e++) {
+        const long long v = (long long)(int)r0[e] + ((long long)(int)r1[e] << 8) + ((long long)(int)r2[e] << 16);
+        const u64 red = reduce64(M, v < 0 ? (u64)(v + (long long)cpos) : (u64)v);
+        Pm[(u64)row * 128 + cb + e] = mul_mod(M, red, pw);
+      }
+    }
+  }
+  __syncthreads();
+  if (ok && !bad) {
+    const u64* Pm = (const u64*)smem;
+    for (u32 t = tid; t < tl.n * SU_POS; t += 256) {
+      const u32 r = t / SU_POS, pos = t % SU_POS;
+      u64 v = 0;
+#pragma unroll
+      for (u32 x = 0; x < 7; x++) v = salsaa::add_mod(v, Pm[(u64)(r * 7 + x) * 128 + pos], q);
+      const u32 j = tl.idx[r];
+      v = mul_mod(M, v, s_hi[(u64)j * nhi + hb]);
+      atomic_add_mod(acc + ((u64)j * rows + k) * d + (u64)pb * SU_POS + pos, v, q, plain);
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 512);
+}
+
+// Exact CUDA-core sums for the CTAs sc_umma_kernel flagged (same grid).
+__global__ void sc_exact_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, ScRowList tl, const u64* s_lo,
+                                const u64* s_hi, ModQ M, u64* acc, bool plain, const u32* flags) {
+  const u32 cta = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  if (!flags[cta]) return;
+  const u32 pb = blockIdx.x, hb = blockIdx.y, k = blockIdx.z, pos = threadIdx.x;
+  const u64* src = wc.p[k] + ((u64)hb * Bw) * d + (u64)pb * SU_POS + pos;
+  for (u32 r = 0; r < tl.n; r++) {
+    const u32 j = tl.idx[r];
+    u64 v = 0;
+    for (u32 i = 0; i < Bw; i++) v = salsaa::add_mod(v, mul_mod(M, s_lo[(u64)j * Bw + i], src[(u64)i * d]), M.q);
+    v = mul_mod(M, v, s_hi[(u64)j * nhi + hb]);
+    atomic_add_mod(acc + ((u64)j * rows + k) * d + (u64)pb * SU_POS + pos, v, M.q, plain);
+  }
+}
+
+int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi, const ScRowList& tl,
+                   const u64* s_lo, const u64* s_hi, const ModQ& M, u64* acc, bool plain, uint8_t* img, u32* flags,
+                   cudaStream_t st) {
+  const u64 ctas = (u64)(d / SU_POS) * nhi * rows;
+  cudaError_t e = cudaMemsetAsync(flags, 0, ctas * sizeof(u32), st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sc_umma flags");
+  u64 g = ((u64)Bw * 128 + 255) / 256;
+  sc_img_kernel<<<(unsigned)(g < 4096 ? g : 4096), 256, 0, st>>>(s_lo, Bw, tl, img);
+  salsaa_count_launch();
+  const size_t smem = 2 * (size_t)SU_STAGE;
+  e = cudaFuncSetAttribute(sc_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sc_umma smem attribute");
+  dim3 grid(d / SU_POS, nhi, rows);
+  sc_umma_kernel<<<grid, 256, smem, st>>>(wc, rows, d, Bw, nhi, tl, img, s_hi, M, acc, plain, flags);
+  salsaa_count_launch();
+  sc_exact_kernel<<<grid, SU_POS, 0, st>>>(wc, rows, d, Bw, nhi, tl, s_lo, s_hi, M, acc, plain, flags);
+  salsaa_count_launch();
+  e = cudaGetLastError();
+  (void)width;
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "sc_umma launch");
+}
+
 int tc_error_check() {
   u32 h = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&h, g_tc_error, sizeof(u32));

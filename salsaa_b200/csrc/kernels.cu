@@ -1896,8 +1896,16 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
       if (a.sc_types_host[j] == ROW_TENSOR) tl.idx[tl.n++] = (unsigned char)j;
       else ol.idx[ol.n++] = (unsigned char)j;
     }
-    // TENSOR rows over the witness
-    launch_sc_pass(a, wsrc, a.width, tl, true, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
+    // TENSOR rows over the witness: tensor cores when the coefficient form is
+    // given and the shapes fit, else CUDA cores
+    if (tl.n && a.coef_sc && a.sc_img && a.sc_flags && M.q < (1ULL << 56) && d % 128 == 0 && Bw % 128 == 0 &&
+        tl.n <= SC_UMMA_MAX_ROWS) {
+      rc = launch_sc_umma(wsrc, a.rows, a.width, d, Bw, nhi, tl, a.sc_lo, a.sc_hi, M, acc_sc, plain, a.sc_img,
+                          a.sc_flags, st);
+      if (rc) return rc;
+    } else {
+      launch_sc_pass(a, wsrc, a.width, tl, true, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
+    }
     rc = check_launch("sc_commit (tensor rows)");
     if (rc) return rc;
     // periodic and all-ones rows over the column sums

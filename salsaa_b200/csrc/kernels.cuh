@@ -64,6 +64,12 @@ constexpr u32 CKU_MAX_KEYS = 18, CKU_MAX_WROWS = 9;
 inline u32 ck_tk8_nkp(u32 nck) { return ((nck * 14 + 15) / 16) * 16; }
 inline u64 ck_tk8_bytes(u32 nck, u32 n, u32 bt) { return (u64)bt * n * ck_tk8_nkp(nck); }
 int launch_ck_tk8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* tk8, cudaStream_t st);
+// TENSOR rows on tcgen05 over the coefficient-form witness (see ck_umma.cu).
+constexpr u64 SC_IMG_BYTES = (u64)CK_BLOCK * 128;
+constexpr u32 SC_UMMA_MAX_ROWS = 18;
+int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi, const ScRowList& tl,
+                   const u64* s_lo, const u64* s_hi, const ModQ& M, u64* acc, bool plain, uint8_t* img, u32* flags,
+                   cudaStream_t st);
 // Nonzero (and the last error set) when a tensor-core kernel's bounded wait gave up.
 int tc_error_check();
 int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState* ds, cudaStream_t st);
@@ -128,6 +134,8 @@ struct CommitArgs {
   u32 nsc;           // scalar rows
   const ScalarRowDesc* sc_desc_dev;  // nsc descriptors in device memory
   const int* sc_types_host;          // their types, on the host (required when nsc > 0)
+  uint8_t* sc_img;   // scratch for the tcgen05 TENSOR-row pass (SC_IMG_BYTES), or null
+  u32* sc_flags;     // scratch: one word per CTA of that pass
   const u64* const* sc_base_dev;     // nsc ring bases (slot form) or null (= 1)
   u64* sc_lo;        // scratch nsc x CK_BLOCK
   u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)

@@ -383,6 +383,9 @@ struct salsaa_prover {
   u32 *pmask = nullptr, *nmask = nullptr;
   int8_t* Jm = nullptr;  // projection challenge as int8, 256 x chunk width
   int8_t* Jc = nullptr;  // the same in the tcgen05 operand layout
+  uint8_t* sc_img = nullptr;  // tcgen05 TENSOR-row pass: scalar byte image
+  u32* sc_flags = nullptr;    // and its per-CTA fallback flags
+  u64 sc_flag_words = 0;
   u64 *c_coef = nullptr, *c_slot = nullptr, *fold_pre = nullptr;
   ScalarRowDesc* sc_desc = nullptr;
   std::vector<int> sc_types;  // host copy of the scalar rows' types (launch tiling)
@@ -421,6 +424,7 @@ extern "C" uint64_t salsaa_workspace_bytes(const salsaa_params* p) {
   words += (u64)(S.max_rows + 1) * (L < CK_BLOCK ? L : CK_BLOCK) * d;
   words += 2 * 256ULL * CK_BLOCK / 8;          // projection J and its tensor-core image (bytes)
   words += (u64)MAX_WROWS * (d / 2) * 6;       // fold constants
+  words += SC_IMG_BYTES / 8 + (d / 128 + 1) * (L / CK_BLOCK + 1) * (S.max_rows + 2) / 2;  // scalar-row pass
   return words * 8 + (S.proof_words * 8);
 }
 
@@ -464,6 +468,9 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       (rc = m.alloc(&pr->nmask, 256ULL * CK_BLOCK / 32, "neg mask")) ||
       (rc = m.alloc(&pr->Jm, 256ULL * CK_BLOCK, "projection J")) ||
       (rc = m.alloc(&pr->Jc, 256ULL * CK_BLOCK, "projection J (tensor-core layout)")) ||
+      (rc = m.alloc(&pr->sc_img, SC_IMG_BYTES, "scalar-row byte image")) ||
+      (rc = m.alloc(&pr->sc_flags, pr->sc_flag_words = (u64)(d / 128 + 1) * (L / CK_BLOCK + 1) * (S.max_rows + 2),
+                    "scalar-row flags")) ||
       (rc = m.alloc(&pr->c_coef, (u64)MAX_WROWS * d, "fold c")) ||
       (rc = m.alloc(&pr->c_slot, (u64)MAX_WROWS * d, "fold c slot")) ||
       (rc = m.alloc(&pr->fold_pre, (u64)MAX_WROWS * (d / 2) * 6, "fold constants")) ||
@@ -579,6 +586,10 @@ static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, const RowSet* w
   a.tk8 = c->tk8;
   a.colsum = pr->colsum;
   a.colsum_rows = c->S.max_rows + 1;  // the merged split/projection pass has 2K + 1 rows
+  if ((u64)(c->d / 128) * (width / CK_BLOCK > 0 ? width / CK_BLOCK : 1) * rows <= pr->sc_flag_words) {
+    a.sc_img = pr->sc_img;
+    a.sc_flags = pr->sc_flags;
+  }
   a.out_slot = pr->cout;
   return launch_commit(a, *c->T, c->M, pr->ds, pr->st);
 }
