@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(128) umma_selftest_kernel(const uint8_t* A, co
 // key factor and added into the accumulator as in the CUDA-core path.
 // ---------------------------------------------------------------------------
 constexpr u32 CKU_CHUNK = 128;  // elements per pipeline step (K of 4 MMAs)
-constexpr u32 CKU_THREADS = 256;
+constexpr u32 CKU_THREADS = 512;
 constexpr u32 CKU_ATILE = 128 * CKU_CHUNK;  // witness byte tile of one slot
 
 __global__ void ck_tk8_kernel(const u64* tlo, u32 nck, u32 n, u32 bt, u32 nkp, bool packed, uint8_t* tk8) {
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
       const u32 t = tid + x * CKU_THREADS;
       const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
       const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
-      if (x < kpb && kp < nkpw) {
+      if (t < 256 * kpb && kp < nkpw) {
         const u32 k = kp >> 1, part = kp & 1;
         const u64 e0 = i0 + (u64)c * CKU_CHUNK + (i4hi * 4 + i4lo) * 4;
         const u64* src = w.p[k] + e0 * d + part * n + s0;
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
       const u32 t = tid + x * CKU_THREADS;
       const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
       const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
-      if (x < kpb && kp < nkpw) {
+      if (t < 256 * kpb && kp < nkpw) {
         const u32 i4 = i4hi * 4 + i4lo;  // elements 4 * i4 .. + 3 of the chunk
         const u32 off = (i4 >> 2) * (128 * 16) + (kp * 7) * 16 + (i4 & 3) * 4;
 #pragma unroll
@@ -204,15 +204,18 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
 
   const u32 idesc = umma::idesc_u8(128, nkp);
   bool ok = true;
+  auto copy_keys = [&](u32 c) {  // thread 0: both slots' key tiles of chunk c into stage c & 1
+    const u32 sn = c & 1;
+    umma::mbar_expect_tx(&full_bar[sn], 2 * btile);
+    umma::bulk_g2s(smem + sn * stage_bytes + 2 * CKU_ATILE, tk8 + ((u64)(cc0 + c) * n + s0) * btile, 2 * btile,
+                   &full_bar[sn]);
+  };
+  if (tid == 0) copy_keys(0);
   fetch(0);
   for (u32 c = 0; c < nchunks; c++) {
     const u32 st = c & 1;
     uint8_t* stage = smem + st * stage_bytes;
     if (c >= 2) ok &= umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1);
-    if (tid == 0) {
-      umma::mbar_expect_tx(&full_bar[st], 2 * btile);
-      umma::bulk_g2s(stage + 2 * CKU_ATILE, tk8 + ((u64)(cc0 + c) * n + s0) * btile, 2 * btile, &full_bar[st]);
-    }
     stash(st);
     if (c + 1 < nchunks) fetch(c + 1);
     umma::fence_proxy_async();
@@ -232,6 +235,13 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
           umma::mma_i8(tmem + sg * cs, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
         }
       umma::commit(&done_bar[st]);
+      // key tiles of the next chunk: its stage was last read by the MMAs of
+      // chunk c - 1, which complete before those just issued
+      if (c + 1 < nchunks) {
+        const u32 sn = (c + 1) & 1;
+        if (c >= 1) ok &= umma::mbar_wait(&done_bar[sn], ((c - 1) >> 1) & 1, err, 4);
+        copy_keys(c + 1);
+      }
     }
   }
   // all MMAs done (the last commit covers every earlier MMA of thread 0)
@@ -242,8 +252,8 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
   // ---- epilogue ----
   u64* Pm = (u64*)smem;  // [slot][128 lanes][2 nck] partial sums over x
   const u32 ng = 2 * nck;
-  const u32 sg = warp >> 2, row = (warp & 3) * 32 + lane;
-  if (ok) {
+  const u32 sg = (warp >> 2) & 1, row = (warp & 3) * 32 + lane;
+  if (ok && warp < 8) {
     const bool valid = row < rows * 14;
     const u32 y = row % 7;
     const u64 pw = ((u64)1 << (8 * y)) % M.q;
@@ -507,7 +517,7 @@ __global__ void sc_img_kernel(const u64* s_lo, u32 Bw, ScRowList tl, uint8_t* im
   }
 }
 
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(512, 1)
     sc_umma_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, ScRowList tl, const uint8_t* __restrict__ img,
                    const u64* s_hi, ModQ M, u64* acc, bool plain, u32* flags) {
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -544,8 +554,8 @@ __global__ void __launch_bounds__(256, 1)
     }
     const u64* src = src0 + (u64)c * SU_KS * d;
 #pragma unroll 2
-    for (u32 x = 0; x < 16; x++) {
-      const u32 t = tid + x * 256;
+    for (u32 x = 0; x < 8; x++) {
+      const u32 t = tid + x * 512;
       const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
       const u32 e0 = (k4hi * 4 + k4lo) * 4;
@@ -597,11 +607,11 @@ __global__ void __launch_bounds__(256, 1)
   if (ok && !bad) {
     // per TMEM lane (row (r, x)), per position: sum_l 2^(8l) D_l, reduced, times 2^(8x)
     u64* Pm = (u64*)smem;  // 128 rows x 128 positions
-    const u32 row = (warp & 3) * 32 + lane, half = warp >> 2;  // warps 4..7 take positions 64..127
+    const u32 row = (warp & 3) * 32 + lane, quarter = warp >> 2;  // four groups of 32 positions
     const u32 x = row % 7;
     const u64 pw = ((u64)1 << (8 * x)) % q;
     const u64 cpos = ((((u64)1 << 62) / q) + 1) * q;
-    for (u32 cb = half * 64; cb < half * 64 + 64; cb += 16) {
+    for (u32 cb = quarter * 32; cb < quarter * 32 + 32; cb += 16) {
       uint32_t r0[16], r1[16], r2[16];
       const u32 base = tmem + (((warp & 3) * 32) << 16) + cb;
       umma::tmem_ld16(base, r0);
@@ -619,7 +629,7 @@ __global__ void __launch_bounds__(256, 1)
   __syncthreads();
   if (ok && !bad) {
     const u64* Pm = (const u64*)smem;
-    for (u32 t = tid; t < tl.n * SU_POS; t += 256) {
+    for (u32 t = tid; t < tl.n * SU_POS; t += 512) {
       const u32 r = t / SU_POS, pos = t % SU_POS;
       u64 v = 0;
 #pragma unroll
@@ -663,7 +673,7 @@ int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi
   e = cudaFuncSetAttribute(sc_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sc_umma smem attribute");
   dim3 grid(d / SU_POS, nhi, rows);
-  sc_umma_kernel<<<grid, 256, smem, st>>>(wc, rows, d, Bw, nhi, tl, img, s_hi, M, acc, plain, flags);
+  sc_umma_kernel<<<grid, 512, smem, st>>>(wc, rows, d, Bw, nhi, tl, img, s_hi, M, acc, plain, flags);
   salsaa_count_launch();
   sc_exact_kernel<<<grid, SU_POS, 0, st>>>(wc, rows, d, Bw, nhi, tl, s_lo, s_hi, M, acc, plain, flags);
   salsaa_count_launch();
