@@ -122,6 +122,16 @@ __global__ void ck_tk8_kernel(const u64* tlo, u32 nck, u32 n, u32 bt, u32 nkp, b
 
 __device__ u32 g_tc_error;  // set when a tensor-core wait gave up
 
+// o_i = byte i of a, b, c, d (in that order, a in the low byte)
+__device__ __forceinline__ void transpose4x4(u32 a, u32 b, u32 c, u32 d, u32& o0, u32& o1, u32& o2, u32& o3) {
+  const u32 t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(a, b, 0x7362);
+  const u32 t2 = __byte_perm(c, d, 0x5140), t3 = __byte_perm(c, d, 0x7362);
+  o0 = __byte_perm(t0, t2, 0x5410);
+  o1 = __byte_perm(t0, t2, 0x7632);
+  o2 = __byte_perm(t1, t3, 0x5410);
+  o3 = __byte_perm(t1, t3, 0x7632);
+}
+
 __global__ void __launch_bounds__(CKU_THREADS, 1)
     ck_umma_kernel(const uint8_t* __restrict__ tk8, RowSet w, u32 rows, u32 nck, u32 nkp, u32 n, u32 bt, u32 Bw,
                    const u64* thi, u32 nhi_t, ModQ M, const u64* zeta, u64* acc, bool plain) {
@@ -186,18 +196,21 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
       if (t < 256 * kpb && kp < nkpw) {
         const u32 i4 = i4hi * 4 + i4lo;  // elements 4 * i4 .. + 3 of the chunk
         const u32 off = (i4 >> 2) * (128 * 16) + (kp * 7) * 16 + (i4 & 3) * 4;
+        // byte plane b of the four elements: a 4 x 4 byte transpose of their
+        // low words (planes 0..3) and high words (planes 4..6)
 #pragma unroll
-        for (u32 sg = 0; sg < 2; sg++)
+        for (u32 sg = 0; sg < 2; sg++) {
+          u32 lo[4], hi[4], p[8];
 #pragma unroll
-          for (u32 b = 0; b < 7; b++) {
-            u32 word = 0;
-#pragma unroll
-            for (u32 e = 0; e < 4; e++) {
-              const u64 v = sg ? ((const u64*)&wv[x][e])[1] : ((const u64*)&wv[x][e])[0];
-              word |= ((u32)(v >> (8 * b)) & 0xffu) << (8 * e);
-            }
-            *(u32*)(A + sg * CKU_ATILE + off + b * 16) = word;
+          for (u32 e = 0; e < 4; e++) {
+            lo[e] = sg ? wv[x][e].z : wv[x][e].x;
+            hi[e] = sg ? wv[x][e].w : wv[x][e].y;
           }
+          transpose4x4(lo[0], lo[1], lo[2], lo[3], p[0], p[1], p[2], p[3]);
+          transpose4x4(hi[0], hi[1], hi[2], hi[3], p[4], p[5], p[6], p[7]);
+#pragma unroll
+          for (u32 b = 0; b < 7; b++) *(u32*)(A + sg * CKU_ATILE + off + b * 16) = p[b];
+        }
       }
     }
   };
@@ -252,20 +265,23 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
   // ---- epilogue ----
   u64* Pm = (u64*)smem;  // [slot][128 lanes][2 nck] partial sums over x
   const u32 ng = 2 * nck;
-  const u32 sg = (warp >> 2) & 1, row = (warp & 3) * 32 + lane;
-  if (ok && warp < 8) {
+  // warp w: slot (w >> 2) & 1, TMEM lanes 32 (w & 3) .., and one half of the
+  // 2 nck column groups (w >> 3), split at a group boundary
+  const u32 sg = (warp >> 2) & 1, row = (warp & 3) * 32 + lane, ch = warp >> 3;
+  if (ok) {
     const bool valid = row < rows * 14;
     const u32 y = row % 7;
     const u64 pw = ((u64)1 << (8 * y)) % M.q;
+    const u32 jb = 7 * (ch ? nck : 0), je = 7 * (ch ? 2 * nck : nck);
     u64 hi = 0, lo = 0;
-    for (u32 cb = 0; cb * 16 < nkp; cb++) {
+    for (u32 cb = jb / 16; cb * 16 < je; cb++) {
       uint32_t r[16];
       umma::tmem_ld16(tmem + (((warp & 3) * 32) << 16) + sg * cs + cb * 16, r);
       umma::tmem_wait_ld();
 #pragma unroll
       for (u32 i = 0; i < 16; i++) {
         const u32 j = cb * 16 + i;
-        if (j < nck * 14) {
+        if (j >= jb && j < je) {
           const u32 x = j % 7;
           const u64 v = (u64)r[i];
           const u64 sl = v << (8 * x), sh = x ? (v >> (64 - 8 * x)) : 0;
