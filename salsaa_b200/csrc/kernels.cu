@@ -1896,33 +1896,45 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
       if (a.sc_types_host[j] == ROW_TENSOR) tl.idx[tl.n++] = (unsigned char)j;
       else ol.idx[ol.n++] = (unsigned char)j;
     }
-    // TENSOR rows over the witness: tensor cores when the coefficient form is
-    // given and the shapes fit, else CUDA cores
-    if (tl.n && a.coef_sc && a.sc_img && a.sc_flags && M.q < (1ULL << 56) && d % 128 == 0 && Bw % 128 == 0 &&
-        tl.n <= SC_UMMA_MAX_ROWS) {
-      rc = launch_sc_umma(wsrc, a.rows, a.width, d, Bw, nhi, tl, a.sc_lo, a.sc_hi, M, acc_sc, plain, a.sc_img,
+    // TENSOR rows: one tensor-core pass over the coefficient-form witness when
+    // the shapes fit, else CUDA cores.  Every scalar row weighs element i by
+    // s_hi[i / Bw] s_lo[i % Bw], so when that pass runs anyway the periodic /
+    // all-ones rows ride in it if they fit, and no column sums are needed.
+    const bool tc_ok = a.coef_sc && a.sc_img && a.sc_flags && M.q < (1ULL << 56) && d % 128 == 0 &&
+                       Bw % 128 == 0 && tl.n > 0 && tl.n <= SC_UMMA_MAX_ROWS;
+    bool periodic_done = false;
+    if (tc_ok) {
+      ScRowList gl = tl;
+      if (tl.n + ol.n <= SC_UMMA_MAX_ROWS) {
+        for (u32 i = 0; i < ol.n; i++) gl.idx[gl.n++] = ol.idx[i];
+        periodic_done = true;
+      }
+      rc = launch_sc_umma(wsrc, a.rows, a.width, d, Bw, nhi, gl, a.sc_lo, a.sc_hi, M, acc_sc, plain, a.sc_img,
                           a.sc_flags, st);
       if (rc) return rc;
     } else {
       launch_sc_pass(a, wsrc, a.width, tl, true, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
-    }
-    rc = check_launch("sc_commit (tensor rows)");
-    if (rc) return rc;
-    // periodic and all-ones rows over the column sums
-    RowSet u = wsrc;
-    if (nhi > 1) {
-      if (!a.colsum || a.rows > a.colsum_rows) return salsaa_set_error(-2, "commit: column-sum scratch too small");
-      colsum_kernel<<<grid_1d((u64)a.rows * Bw * d, 256), 256, 0, st>>>(wsrc, a.rows, a.width, Bw, d, M, a.colsum);
-      rc = check_launch("colsum");
+      rc = check_launch("sc_commit (tensor rows)");
       if (rc) return rc;
-      for (u32 k = 0; k < a.rows; k++) u.p[k] = a.colsum + (u64)k * Bw * d;
     }
-    u64 CHu = Bw / 64;
-    if (CHu < 16) CHu = 16;
-    if (CHu > Bw) CHu = Bw;
-    launch_sc_pass(a, u, Bw, ol, false, d, Bw, nhi, (u32)CHu, M, plain, acc_sc, st);
-    rc = check_launch("sc_commit (periodic rows)");
-    if (rc) return rc;
+    if (!periodic_done && ol.n) {
+      // periodic and all-ones rows over the column sums
+      RowSet u = wsrc;
+      if (nhi > 1) {
+        if (!a.colsum || a.rows > a.colsum_rows) return salsaa_set_error(-2, "commit: column-sum scratch too small");
+        colsum_kernel<<<grid_1d((u64)a.rows * Bw * d, 256), 256, 0, st>>>(wsrc, a.rows, a.width, Bw, d, M,
+                                                                         a.colsum);
+        rc = check_launch("colsum");
+        if (rc) return rc;
+        for (u32 k = 0; k < a.rows; k++) u.p[k] = a.colsum + (u64)k * Bw * d;
+      }
+      u64 CHu = Bw / 64;
+      if (CHu < 16) CHu = 16;
+      if (CHu > Bw) CHu = Bw;
+      launch_sc_pass(a, u, Bw, ol, false, d, Bw, nhi, (u32)CHu, M, plain, acc_sc, st);
+      rc = check_launch("sc_commit (periodic rows)");
+      if (rc) return rc;
+    }
     if (a.coef_sc) {
       const u64 cnt = (u64)a.nsc * a.rows;
       reduce_inplace_kernel<<<grid_1d(cnt * d, 256), 256, 0, st>>>(acc_sc, cnt * d, M);
