@@ -4,6 +4,7 @@ sets."""
 import numpy as np
 import pytest
 
+from helpers import rand_mod
 from salsaa_b200 import params as P
 
 pytestmark = pytest.mark.gpu
@@ -45,6 +46,24 @@ def test_explicit_witness(api, oracle):
     rc, want, _ = oracle.prove(p, 1, 2, witness=w)
     assert rc == 0
     got = api.Context(p, crs_seed=1).prove(2, witness=w)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("bound", [0, 1 << 22, 1 << 30])
+def test_large_witness_d128(api, oracle, bound):
+    """Witness values beyond the tensor-core paths' byte limbs (uniform mod q,
+    around 2^22, around 2^30) must still give the oracle's proof bytes: the
+    projection and scalar-row passes fall back to their exact kernels."""
+    p = P.make_params(128, P.Q0, 4, 1 << 13, 2, False)
+    rng = np.random.default_rng(bound + 1)
+    if bound:
+        w = rng.integers(-bound, bound + 1, size=(1, p.wit_len, p.d))
+        w = np.where(w < 0, p.q + w, w).astype(np.uint64)
+    else:
+        w = rand_mod(rng, (1, p.wit_len, p.d), p.q)
+    rc, want, _ = oracle.prove(p, 3, 4, witness=w)
+    assert rc == 0
+    got = api.Context(p, crs_seed=3).prove(4, witness=w)
     assert np.array_equal(got, want)
 
 
