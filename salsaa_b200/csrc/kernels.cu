@@ -109,7 +109,7 @@ __global__ void ck_thi_kernel(const u64* ms, u32 rows, u32 n, u32 B, u32 nhi, Mo
 int launch_ck_tables(const u64* m_slot, u32 rows, const NttDev& T, const ModQ& M, u64 L, u64* tlo, u64* thi,
                      cudaStream_t st) {
   const u32 n = T.n;
-  const u32 B = (u32)(L < CK_BLOCK ? L : CK_BLOCK);
+  const u32 B = (u32)(L < CK_KEY_BLOCK ? L : CK_KEY_BLOCK);
   const u32 nhi = (u32)(L / B);
   u64 tot = (u64)rows * B * n;
   ck_tlo_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(m_slot, rows, n, B, M, T.zeta, tlo);
@@ -1866,8 +1866,11 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
       cudaMemsetAsync(a.acc, 0, (u64)(a.nck + a.nsc) * a.rows * d * sizeof(u64), st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit memset");
   if (a.nck && ck_umma_ok(a, n)) {
-    if (Bw > a.ck_bt) return salsaa_set_error(-2, "commit: witness wider than the key tables");
-    int rc = launch_ck_umma(a, n, Bw, M, T.zeta, plain, st);
+    // element block per CTA: a whole key-table block (one epilogue per block),
+    // halved while the grid would not fill the GPU
+    u32 Bk = (u32)(a.width < a.ck_bt ? a.width : a.ck_bt);
+    while (Bk > CK_BLOCK && (u64)(n / 2) * (a.width / Bk) < 296) Bk /= 2;
+    int rc = launch_ck_umma(a, n, Bk, M, T.zeta, plain, st);
     if (rc) return rc;
   } else if (a.nck && a.tl8 && M.q < (1ULL << 56) && a.width >= CKM_KS && a.rows <= 9 && n <= 512) {
     if (Bw > a.ck_bt) return salsaa_set_error(-2, "commit: witness wider than the key tables");

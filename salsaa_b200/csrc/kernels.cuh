@@ -13,7 +13,10 @@
 namespace salsaa {
 
 constexpr int MAX_WROWS = 16;  // witness rows in one call
-constexpr u32 CK_BLOCK = 2048; // two-level split of commitment-key powers
+constexpr u32 CK_BLOCK = 2048; // block of the scalar-row tables, column sums and projection chunks
+// Two-level split of the commitment-key powers m^(i+1) = thi[i / B] tlo[i % B]:
+// a commitment CTA accumulates up to B elements before its epilogue.
+constexpr u32 CK_KEY_BLOCK = 8192;
 
 struct RowSet {
   const u64* p[MAX_WROWS];
@@ -129,7 +132,7 @@ struct CommitArgs {
   u32 nck;           // commitment-key rows (statement rows 0..nck-1)
   const u64* tlo;    // nck x ck_bt x 3n
   const u64* thi;    // nck x ck_nhi x d
-  u32 ck_bt;         // table block: min(L, CK_BLOCK)
+  u32 ck_bt;         // table block: min(L, CK_KEY_BLOCK)
   u32 ck_nhi;        // L / ck_bt
   u32 nsc;           // scalar rows
   const ScalarRowDesc* sc_desc_dev;  // nsc descriptors in device memory

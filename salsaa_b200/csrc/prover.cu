@@ -343,7 +343,7 @@ extern "C" int salsaa_ctx_create(const salsaa_params* p, uint64_t crs_seed, int 
   c->d = (u32)p->d;
   c->n = c->d / 2;
   c->L = p->wit_len;
-  c->ck_bt = (u32)(c->L < CK_BLOCK ? c->L : CK_BLOCK);
+  c->ck_bt = (u32)(c->L < CK_KEY_BLOCK ? c->L : CK_KEY_BLOCK);
   c->ck_nhi = (u32)(c->L / c->ck_bt);
   c->T = ntt_tables(c->n, p->q);
   if (!c->T) {
