@@ -698,6 +698,291 @@ int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi
   return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "sc_umma launch");
 }
 
+// ---------------------------------------------------------------------------
+// First streaming pass of the norm-check sumcheck on tcgen05
+// (norm_check_1 + the first rounds of sum_check,
+// src/subroutines/fast_norm_check.rs:135-320).  The pass reads groups
+// v_g = (x[g + m ng])_{m < 16} of a witness row and needs, per repetition,
+//   * the sums of rounds 0..3: every value of round t is a fixed linear
+//     combination of v_g (the fold challenges are known up front), so each
+//     sum is a quadratic form of v_g and all of them follow from the 16 x 16
+//     Gram matrix C = sum_g v_g v_g^T (mod q);
+//   * the folded vector v_4[g] = sum_m lambda[m] v_g[m] with
+//     lambda[m] = prod_t (bit_{3-t}(m) ? c_t : 1 - c_t).
+// The witness is small and centred (ternary, or decomposition digits), so
+// each value splits exactly into four signed byte limbs, v = sum_x 2^(8x) l_x.
+// A tile of 256 groups is stored once in shared memory as rows g of 64 bytes
+// (m, x); with 8-group blocks of 8 x 16-byte slices that one image is
+//   * the K-major A operand (M = g, K = (m, x)) of the fold product against
+//     B = the bytes of mu[m, x] = 2^(8x) lambda[m] mod q (N = (rep, byte y)),
+//   * the MN-major A and B operands (M, N = (m, x), K = g) of the Gram
+//     product, accumulated in TMEM over all tiles of the CTA.
+// The fold is sum_y 2^(8y) D[g][rep, y] mod q; C[m1][m2] is
+// sum_{x1,x2} 2^(8(x1+x2)) D[(m1,x1)][(m2,x2)] mod q, added to a per-row
+// accumulator; nc_gram_sums_kernel turns C into the round sums.  A value
+// outside the limb range sets *flag; the CUDA-core pass then runs instead
+// (sc_first_kernel gated on the flag) and the Gram sums are skipped.
+// ---------------------------------------------------------------------------
+constexpr u32 NG_T = 4;                          // rounds covered (groups of 16)
+constexpr u32 NG_TILE = 256;                     // groups per tile (one per thread)
+constexpr u32 NG_GBS = 1024;                     // one 8-group block: 8 slices x 128 B
+constexpr u32 NG_STAGE = NG_TILE / 8 * NG_GBS;   // 32 KiB
+constexpr u32 NG_MAX_TILES = 256;                // per CTA: Gram entries stay below 2^30
+constexpr u32 NG_SMEM = 2 * NG_STAGE + 1024;     // two stages + the fold B table
+
+__device__ __forceinline__ u64 ng_challenge(const DevState* ds, u32 round, u32 rep, u64 j, u64 q) {
+  return uni_mod(prf_at(prf_key(ds->seed, domain_id(DOM_NC, round, rep)), j), q);
+}
+
+__global__ void __launch_bounds__(256, 2)
+    nc_gram_kernel(RowSet w, u32 rows, u64 ng, u32 ntiles, ModQ M, const DevState* ds, u32 round, u64* out,
+                   u64 sout, u64* gram, u32* flag, bool plain) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ uint64_t done_bar[2];
+  __shared__ uint32_t tslot;
+  const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const u32 k = blockIdx.y;
+  const u64 q = M.q, half_q = q >> 1;
+  const u32 t0 = (u32)((u64)blockIdx.x * ntiles / gridDim.x), t1 = (u32)((u64)(blockIdx.x + 1) * ntiles / gridDim.x);
+  const u64* x = w.p[k];
+  u32* err = &g_tc_error;
+  uint8_t* btab = smem + 2 * NG_STAGE;
+
+  // slices 4..7 of every block stay zero: rows 64..127 of the Gram A operand
+  for (u32 v = tid; v < 2 * (NG_TILE / 8) * 32; v += 256)
+    *(uint4*)(smem + (v / 32) * NG_GBS + 512 + (v % 32) * 16) = make_uint4(0, 0, 0, 0);
+  // fold B table (K-major, N = 16 rows (rep, y), K = 64 bytes (m, x)):
+  // offset(n, kk) = (kk / 16) * 256 + (n / 8) * 128 + (n % 8) * 16 + kk % 16
+  if (tid < 128) {
+    const u32 rep = tid >> 6, m = (tid >> 2) & 15, xl = tid & 3;
+    u64 lam = 1 % q;
+#pragma unroll
+    for (u32 t = 0; t < NG_T; t++) {
+      const u64 c = ng_challenge(ds, round, rep, t, q);
+      lam = mul_mod(M, lam, ((m >> (NG_T - 1 - t)) & 1) ? c : salsaa::sub_mod(1 % q, c, q));
+    }
+    const u64 mv = mul_mod(M, lam, ((u64)1 << (8 * xl)) % q);
+    const u32 kk = m * 4 + xl;
+#pragma unroll
+    for (u32 y = 0; y < 8; y++) {
+      const u32 n = rep * 8 + y;
+      btab[(kk / 16) * 256 + (n / 8) * 128 + (n % 8) * 16 + kk % 16] = y < 7 ? (uint8_t)(mv >> (8 * y)) : 0;
+    }
+  }
+  if (tid == 0) {
+    umma::mbar_init(&done_bar[0], 1);
+    umma::mbar_init(&done_bar[1], 1);
+    umma::mbar_fence_init();
+  }
+  if (warp == 0) umma::tmem_alloc(&tslot, 128);
+  umma::fence_proxy_async();
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const u32 tmem = tslot;  // columns 0..63 Gram, 64 + 32 s + 16 h fold of stage s, half h
+  // s8 x s8, both MN-major, M = 128, N = 64
+  const u32 id_gram = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((64u >> 3) << 17) |
+                      ((128u >> 4) << 24);
+  // s8 (limbs) x u8 (mu bytes), both K-major, M = 128, N = 16
+  const u32 id_fold = (2u << 4) | (1u << 7) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+  const u64 w32 = ((u64)1 << 32) % q, w32p = (u64)(((unsigned __int128)w32 << 64) / q);
+  bool bad = false, ok = true;
+
+  u64 v[16];
+  auto load = [&](u32 tile) {
+    const u64* src = x + (u64)tile * NG_TILE + tid;
+#pragma unroll
+    for (u32 m = 0; m < 16; m++) v[m] = __ldg(src + m * ng);
+  };
+  auto epilogue = [&](u32 li, u32 tile) {
+    const u32 se = li & 1;
+    ok &= umma::mbar_wait(&done_bar[se], (li >> 1) & 1, err, 1);
+    umma::fence_after_sync();
+    uint32_t r[16];
+    umma::tmem_ld16(tmem + (((warp & 3) * 32) << 16) + 64 + se * 32 + (warp >> 2) * 16, r);
+    umma::tmem_wait_ld();
+    const u64 g = (u64)tile * NG_TILE + tid;  // TMEM lane (warp & 3) * 32 + lane of half warp >> 2
+#pragma unroll
+    for (u32 rep = 0; rep < 2; rep++) {
+      const int* D = (const int*)r + rep * 8;
+      const long long lo = (long long)D[0] + ((long long)D[1] << 8) + ((long long)D[2] << 16) +
+                           ((long long)D[3] << 24);
+      const long long hi = (long long)D[4] + ((long long)D[5] << 8) + ((long long)D[6] << 16);
+      const u64 loc = lo < 0 ? (u64)(lo + (long long)q) : (u64)lo;  // |lo| < 2^46 < q
+      const u64 hic = hi < 0 ? (u64)(hi + (long long)q) : (u64)hi;  // |hi| < 2^38
+      out[((u64)rep * rows + k) * sout + g] = salsaa::add_mod(mul_shoup(hic, w32, w32p, q), loc, q);
+    }
+  };
+
+  if (t0 < t1) load(t0);
+  for (u32 i = t0; i < t1; i++) {
+    const u32 li = i - t0, s = li & 1;
+    uint8_t* stage = smem + s * NG_STAGE;
+    // stage s was last read by the MMAs of tile li - 2, whose completion the
+    // epilogue of iteration li - 1 waited for
+    uint32_t wd[16];
+#pragma unroll
+    for (u32 m = 0; m < 16; m++) {
+      const u64 t = v[m] + 0x80808080ULL - (v[m] > half_q ? q : 0);  // centred value + limb bias
+      bad |= (t >> 32) != 0;
+      wd[m] = (uint32_t)t ^ 0x80808080u;  // the four signed limbs, byte x = limb x
+    }
+    uint8_t* rowp = stage + (tid >> 3) * NG_GBS + (tid & 7) * 16;
+#pragma unroll
+    for (u32 c = 0; c < 4; c++)
+      *(uint4*)(rowp + c * 128) = make_uint4(wd[4 * c], wd[4 * c + 1], wd[4 * c + 2], wd[4 * c + 3]);
+    if (i + 1 < t1) load(i + 1);
+    umma::fence_proxy_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+      const u32 sa = umma::smem_u32(stage), sb = umma::smem_u32(btab);
+#pragma unroll
+      for (u32 kb = 0; kb < NG_TILE / 32; kb++) {
+        // MN-major: LBO = stride of 8-group K blocks, SBO = stride of 16-byte MN slices
+        const uint64_t dg = umma::desc_kmajor(sa + kb * 4 * NG_GBS, NG_GBS, 128);
+        umma::mma_i8(tmem, dg, dg, id_gram, (li > 0 || kb > 0) ? 1u : 0u);
+      }
+#pragma unroll
+      for (u32 h = 0; h < 2; h++)
+#pragma unroll
+        for (u32 j = 0; j < 2; j++) {
+          const uint64_t ad = umma::desc_kmajor(sa + h * 16 * NG_GBS + j * 256, 128, NG_GBS);
+          const uint64_t bd = umma::desc_kmajor(sb + j * 512, 256, 128);
+          umma::mma_i8(tmem + 64 + s * 32 + h * 16, ad, bd, id_fold, j);
+        }
+      umma::commit(&done_bar[s]);
+    }
+    if (li > 0) epilogue(li - 1, i - 1);
+  }
+  if (t0 < t1) epilogue(t1 - 1 - t0, t1 - 1);
+
+  // Gram epilogue: every MMA of this CTA has completed (the last wait covers them)
+  ok = __syncthreads_and(ok);
+  bad = __syncthreads_or(bad);
+  if (bad && tid == 0) atomicOr(flag, 1u);
+  umma::fence_after_sync();
+  int* Dg = (int*)smem;  // 64 x 64 s32, over stage 0
+  if (warp < 2 && t0 < t1) {
+#pragma unroll
+    for (u32 cb = 0; cb < 4; cb++) {
+      uint32_t r[16];
+      umma::tmem_ld16(tmem + ((warp * 32) << 16) + cb * 16, r);
+      umma::tmem_wait_ld();
+#pragma unroll
+      for (u32 e = 0; e < 16; e++) Dg[(warp * 32 + lane) * 64 + cb * 16 + e] = (int)r[e];
+    }
+  }
+  __syncthreads();
+  if (ok && !bad && t0 < t1) {
+    const u32 m1 = tid >> 4, m2 = tid & 15;
+    u64 acc = 0;
+#pragma unroll
+    for (u32 x1 = 0; x1 < 4; x1++)
+#pragma unroll
+      for (u32 x2 = 0; x2 < 4; x2++) {
+        const long long dv = Dg[(m1 * 4 + x1) * 64 + m2 * 4 + x2];
+        long long rm = dv % (long long)q;
+        if (rm < 0) rm += (long long)q;
+        acc = salsaa::add_mod(acc, mul_mod(M, (u64)rm, ((u64)1 << (8 * (x1 + x2))) % q), q);
+      }
+    atomic_add_mod(gram + (u64)k * 256 + tid, acc, q, plain);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+// Round sums 0..3 of both repetitions from the Gram matrix of each row: with
+// L_t the 2^(4-t) x 16 matrix giving the values of round t from v_g,
+// (sum_g x_t[j] x_t[j']) = L_t[j]^T C L_t[j'].  One CTA per witness row.
+__global__ void __launch_bounds__(256) nc_gram_sums_kernel(const u64* gram, const u32* flag, u32 rows, ModQ M,
+                                                           const DevState* ds, u32 round, u64* sums, u32 nr,
+                                                           bool plain) {
+  if (*flag) return;
+  __shared__ u64 C[256];
+  __shared__ u64 L[2][30][16];  // rows 0..15 round 0, 16..23 round 1, 24..27 round 2, 28..29 round 3
+  __shared__ u64 Y[2][30][16];  // C L
+  __shared__ u64 ch[2][NG_T];
+  const u32 k = blockIdx.x, tid = threadIdx.x;
+  const u64 q = M.q;
+  C[tid] = gram[(u64)k * 256 + tid] % q;
+  if (tid < 2 * NG_T) ch[tid / NG_T][tid % NG_T] = ng_challenge(ds, round, tid / NG_T, tid % NG_T, q);
+  for (u32 e = tid; e < 2 * 256; e += 256) {
+    const u32 rep = e >> 8, j = (e >> 4) & 15, i = e & 15;
+    L[rep][j][i] = (i == j) ? 1 % q : 0;
+  }
+  __syncthreads();
+  u32 off = 0, len = 16;
+  for (u32 t = 0; t + 1 < NG_T; t++) {
+    const u32 h = len / 2;
+    for (u32 e = tid; e < 2 * h * 16; e += 256) {
+      const u32 rep = e / (h * 16), j = (e / 16) % h, i = e % 16;
+      const u64 a = L[rep][off + j][i], b = L[rep][off + j + h][i];
+      L[rep][off + len + j][i] = salsaa::add_mod(a, mul_mod(M, ch[rep][t], salsaa::sub_mod(b, a, q)), q);
+    }
+    __syncthreads();
+    off += len;
+    len = h;
+  }
+  for (u32 e = tid; e < 2 * 30 * 16; e += 256) {
+    const u32 rep = e / 480, r = (e / 16) % 30, i = e % 16;
+    u64 s = 0;
+#pragma unroll
+    for (u32 j = 0; j < 16; j++) s = salsaa::add_mod(s, mul_mod(M, C[i * 16 + j], L[rep][r][j]), q);
+    Y[rep][r][i] = s;
+  }
+  __syncthreads();
+  if (tid < 2 * NG_T * 3) {
+    const u32 rep = tid / (NG_T * 3), t = (tid / 3) % NG_T, a = tid % 3;
+    const u32 o = 32 - (32 >> t), h = 8 >> t;  // first row and half length of round t
+    u64 s = 0;
+    for (u32 j = 0; j < h; j++) {
+      const u32 lrow = o + j + (a == 2 ? h : 0), rrow = o + j + (a == 0 ? 0 : h);
+#pragma unroll
+      for (u32 i = 0; i < 16; i++) s = salsaa::add_mod(s, mul_mod(M, L[rep][lrow][i], Y[rep][rrow][i]), q);
+    }
+    atomic_add_mod(&sums[((rep * (u64)nr + t) * rows + k) * 3 + a], s, q, plain);
+  }
+}
+
+bool nc_gram_ok(u64 nlen, u64 q) {
+  return q > (1ULL << 47) && q < (1ULL << 56) && nlen % (16ULL * NG_TILE) == 0 && nlen / 16 / NG_TILE >= 1;
+}
+
+int launch_nc_gram(const RowSet& w, u32 rows, u64 nlen, const ModQ& M, const DevState* ds, u32 round, u64* out,
+                   u64 sout, u64* gram, bool plain, cudaStream_t st) {
+  const u64 ng = nlen / 16;
+  const u32 ntiles = (u32)(ng / NG_TILE);
+  cudaError_t e = cudaMemsetAsync(gram, 0, ((u64)rows * 256 + 1) * sizeof(u64), st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "nc_gram memset");
+  e = cudaFuncSetAttribute(nc_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NG_SMEM);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "nc_gram smem attribute");
+  u64 nb = (296 + rows - 1) / rows;
+  const u64 need = (ntiles + NG_MAX_TILES - 1) / NG_MAX_TILES;
+  if (nb < need) nb = need;
+  if (nb > ntiles) nb = ntiles;
+  u32* flag = (u32*)(gram + (u64)rows * 256);
+  const bool gplain = plain && nb < (1u << 13);
+  const int tr = salsaa_trace_begin("nc_gram_kernel", st, (double)rows * nlen * 8.0 * (1.0 + 2.0 / 16.0));
+  nc_gram_kernel<<<dim3((unsigned)nb, rows), 256, NG_SMEM, st>>>(w, rows, ng, ntiles, M, ds, round, out, sout, gram,
+                                                                 flag, gplain);
+  salsaa_trace_end(tr, st);
+  salsaa_count_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "nc_gram launch");
+}
+
+int launch_nc_gram_sums(const u64* gram, u32 rows, const ModQ& M, const DevState* ds, u32 round, u64* sums, u32 nr,
+                        bool plain, cudaStream_t st) {
+  const u32* flag = (const u32*)(gram + (u64)rows * 256);
+  nc_gram_sums_kernel<<<rows, 256, 0, st>>>(gram, flag, rows, M, ds, round, sums, nr, plain);
+  salsaa_count_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "nc_gram_sums launch");
+}
+
 int tc_error_check() {
   u32 h = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&h, g_tc_error, sizeof(u32));

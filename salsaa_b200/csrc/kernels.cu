@@ -280,9 +280,10 @@ __device__ __forceinline__ void group_rounds(const ModQ& M, u64 (&x)[1 << T], co
 template <bool LAZY>
 __global__ void __launch_bounds__(256, 2) sc_first_kernel(RowSet w, u32 rows, u64 nlen, ModQ M, const DevState* ds,
                                                           u32 round, u64* out, u64 sout, u64* sums, u32 nr,
-                                                          bool plain) {
+                                                          bool plain, const u32* only_if) {
   constexpr u32 T = SC_T, G = 1u << T;
   __shared__ Sum128 red[SC_T * 3 * 32];
+  if (only_if && *only_if == 0) return;  // the tensor-core pass covered this launch
   const u32 k = blockIdx.y, rep = blockIdx.x & 1, bx = blockIdx.x >> 1, nbx = gridDim.x >> 1;
   const u64* x = w.p[k];
   const u64 q = M.q, ng = nlen / G;
@@ -696,10 +697,17 @@ static int sumcheck_passes(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, c
     return (unsigned)(g < want ? (g ? g : 1) : want);
   };
   if (L > SC_TAIL) {
+    // rounds 0..3 on the tensor cores when the shapes allow; the CUDA-core
+    // pass then runs only if a witness value did not fit the byte limbs
+    const bool tc = B.gram && nc_gram_ok(L, M.q);
+    const u32* flag = tc ? (const u32*)(B.gram + (u64)rows * 256) : nullptr;
+    int rc = 0;
+    if (tc && (rc = launch_nc_gram(w, rows, L, M, ds, round, B.a, sa, B.gram, plain, st))) return rc;
     dim3 g(2 * grid_for(L / (1u << SC_T), 2 * rows), rows);
-    sc_first_kernel<LAZY><<<g, 256, 0, st>>>(w, rows, L, M, ds, round, B.a, sa, B.sums, nr, plain);
-    int rc = check_launch("sc_first");
+    sc_first_kernel<LAZY><<<g, 256, 0, st>>>(w, rows, L, M, ds, round, B.a, sa, B.sums, nr, plain, flag);
+    rc = check_launch("sc_first");
     if (rc) return rc;
+    if (tc && (rc = launch_nc_gram_sums(B.gram, rows, M, ds, round, B.sums, nr, plain, st))) return rc;
     in = B.a;
     sin = sa;
     to_a = false;

@@ -73,6 +73,16 @@ constexpr u32 SC_UMMA_MAX_ROWS = 18;
 int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi, const ScRowList& tl,
                    const u64* s_lo, const u64* s_hi, const ModQ& M, u64* acc, bool plain, uint8_t* img, u32* flags,
                    cudaStream_t st);
+// First sumcheck pass (rounds 0..3 of both repetitions) on tcgen05 through the
+// Gram matrices of 16-element groups (see ck_umma.cu): launch_nc_gram writes
+// the folded vectors and the Gram matrices, or raises the flag word after them
+// when a value does not fit four signed byte limbs; launch_nc_gram_sums adds
+// the round sums unless the flag is raised.
+bool nc_gram_ok(u64 nlen, u64 q);
+int launch_nc_gram(const RowSet& w, u32 rows, u64 nlen, const ModQ& M, const DevState* ds, u32 round, u64* out,
+                   u64 sout, u64* gram, bool plain, cudaStream_t st);
+int launch_nc_gram_sums(const u64* gram, u32 rows, const ModQ& M, const DevState* ds, u32 round, u64* sums, u32 nr,
+                        bool plain, cudaStream_t st);
 // Nonzero (and the last error set) when a tensor-core kernel's bounded wait gave up.
 int tc_error_check();
 int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState* ds, cudaStream_t st);
@@ -87,6 +97,7 @@ struct SumcheckBufs {
   u64* b;     // 2 * rows * nlen/4
   u64* sums;  // 2 * nr * rows * 3 (zeroed by the launcher)
   u64* cap;   // 2 * rows * d: vector after log2(width) rounds
+  u64* gram;  // rows * 256 + 1 (Gram matrices and a flag word) or null: first pass on tcgen05
 };
 int launch_sumcheck(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, const DevState* ds, u32 round,
                     SumcheckBufs B, u64* proof_claims, u64* proof_rep0, u64* proof_rep1, cudaStream_t st);

@@ -417,6 +417,7 @@ extern "C" uint64_t salsaa_workspace_bytes(const salsaa_params* p) {
   words += 4 * S.max_fp_width * d;            // Fc, Fs, Pc, Ps
   words += S.max_nc_rows_width * d;           // sumcheck a
   words += S.max_nc_rows_width * d / 2;       // sumcheck b
+  words += (u64)MAX_WROWS * 256 + 1;          // sumcheck Gram matrices
   words += (u64)S.nsc_total * d + p->nof_rounds * CK_BLOCK;
   const u64 stmt = S.max_stmt + 2;
   words += stmt * CK_BLOCK + stmt * (L / CK_BLOCK + 1);
@@ -462,6 +463,7 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       (rc = m.alloc(&pr->sc.b, S.max_nc_rows_width * d / 2 + 1, "sumcheck b")) ||
       (rc = m.alloc(&pr->sc.sums, 2ULL * 64 * MAX_WROWS * 3, "sumcheck sums")) ||
       (rc = m.alloc(&pr->sc.cap, 2ULL * MAX_WROWS * d, "sumcheck cap")) ||
+      (rc = m.alloc(&pr->sc.gram, (u64)MAX_WROWS * 256 + 1, "sumcheck gram")) ||
       (rc = m.alloc(&pr->row_base, (u64)S.nsc_total * d + 1, "row bases")) ||
       (rc = m.alloc(&pr->row_cj, (c->P.nof_rounds + 1) * (u64)CK_BLOCK, "row cj")) ||
       (rc = m.alloc(&pr->pmask, 256ULL * CK_BLOCK / 32, "pos mask")) ||
@@ -1023,6 +1025,7 @@ extern "C" int salsaa_sumcheck(const uint64_t* d_w, uint64_t rows, uint64_t n, u
   TRY(t.get(&B.b, rows * n / 2));
   TRY(t.get(&B.sums, 2ULL * 64 * rows * 3));
   TRY(t.get(&B.cap, 2ULL * rows * d));
+  TRY(t.get(&B.gram, rows * 256 + 1));
   TRY(t.get(&ds, 1));
   set_seed_kernel<<<1, 1, 0, st>>>(ds, seed);
   const u64 nr = ilog2u(n);

@@ -168,6 +168,48 @@ def test_sumcheck(api, oracle, rows, n, d, q):
             assert np.array_equal(polys[rep, :, k, :], want)
 
 
+def _check_sumcheck(api, oracle, w, d, q, seed=99, rnd=3):
+    from helpers import nc_challenges
+    rows, n = w.shape
+    claims, polys = api.sum_check(api.to_dev(w), d, q, seed, rnd)
+    claims, polys = api.to_host(claims), api.to_host(polys)
+    nr = n.bit_length() - 1
+    for rep in range(2):
+        cs = nc_challenges(seed, rnd, rep, nr, q)
+        for k in range(rows):
+            claim, want, _ = oracle.sumcheck(w[k], q, cs)
+            assert int(claims[k]) == claim
+            assert np.array_equal(polys[rep, :, k, :], want)
+
+
+@pytest.mark.parametrize("rows,n,d,q,bound", [(1, 1 << 15, 128, P.Q0, 1), (3, 1 << 16, 128, P.Q0, 1 << 24),
+                                              (2, 1 << 17, 64, P.Q1, 1 << 30), (1, 1 << 20, 128, P.Q0, 1 << 25)])
+def test_sumcheck_small(api, oracle, rows, n, d, q, bound):
+    """Small centred witnesses (ternary, decomposition digits): the first
+    pass runs on the tensor cores through the groups' Gram matrices."""
+    rng = np.random.default_rng(n + rows + bound)
+    _check_sumcheck(api, oracle, small_signed(rng, (rows, n), bound, q), d, q)
+
+
+@pytest.mark.parametrize("outside", [0, 1, 2])
+def test_sumcheck_limb_edges(api, oracle, outside):
+    """Values at the ends of the four-signed-byte range stay on the tensor
+    cores; one value beyond either end sends the launch to the exact pass."""
+    q, n = P.Q0, 1 << 16
+    rng = np.random.default_rng(5)
+    w = small_signed(rng, (2, n), 3, q)
+    hi, lo = 0x7F7F7F7F, 0x80808080
+    w[0, 17] = hi
+    w[0, 40000] = q - lo
+    w[1, 3] = q - lo
+    w[1, n - 1] = hi
+    if outside == 1:
+        w[1, 1234] = hi + 1
+    elif outside == 2:
+        w[0, 999] = q - lo - 1
+    _check_sumcheck(api, oracle, w, 128, q)
+
+
 @pytest.mark.parametrize("parts", [1, 2, 3])
 def test_decompose(api, oracle, parts):
     q, d = P.Q0, 128
