@@ -560,6 +560,21 @@ __global__ void __launch_bounds__(512, 1)
   // unsigned bytes (A) x signed bytes (B) -> s32, M = N = 128
   const u32 idesc = umma::idesc_u8(128, SU_POS) | (1u << 10);
   bool bad = false, ok = true;
+  // task x of this thread: four consecutive elements e0 .. e0 + 3 at one position
+  u64 vr[8][4];
+  auto load = [&](u32 c) {
+    const u64* src = src0 + (u64)c * SU_KS * d;
+#pragma unroll
+    for (u32 x = 0; x < 8; x++) {
+      const u32 t = tid + x * 512;
+      const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
+      const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
+      const u32 e0 = (k4hi * 4 + k4lo) * 4;
+#pragma unroll
+      for (u32 e = 0; e < 4; e++) vr[x][e] = __ldg(src + (u64)(e0 + e) * d + pos);
+    }
+  };
+  load(0);
   for (u32 c = 0; c < nsteps; c++) {
     const u32 st = c & 1;
     uint8_t* stage = smem + st * SU_STAGE;
@@ -568,34 +583,30 @@ __global__ void __launch_bounds__(512, 1)
       umma::mbar_expect_tx(&full_bar[st], SU_A);
       umma::bulk_g2s(stage, img + (u64)c * SU_A, SU_A, &full_bar[st]);
     }
-    const u64* src = src0 + (u64)c * SU_KS * d;
-#pragma unroll 2
+#pragma unroll
     for (u32 x = 0; x < 8; x++) {
       const u32 t = tid + x * 512;
       const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
-      const u32 e0 = (k4hi * 4 + k4lo) * 4;
-      u32 p0 = 0, p1 = 0, p2 = 0;
+      // centred value + 0x808080: its bytes are the signed limbs + 128 when
+      // the value lies in [-0x808080, 0x7f7f7f] (three balanced base-256 digits)
+      u32 wv[4];
 #pragma unroll
       for (u32 e = 0; e < 4; e++) {
-        const u64 v = __ldg(src + (u64)(e0 + e) * d + pos);
-        const long long cv = v > half_q ? (long long)v - (long long)q : (long long)v;
-        const long long l0 = ((cv + 128) & 255) - 128, c1 = (cv - l0) >> 8;
-        const long long l1 = ((c1 + 128) & 255) - 128;
-        long long l2 = (c1 - l1) >> 8;
-        if (l2 < -128 || l2 > 127) {  // the value needs a fourth limb
-          bad = true;
-          l2 = 0;
-        }
-        p0 |= ((u32)l0 & 0xffu) << (8 * e);
-        p1 |= ((u32)l1 & 0xffu) << (8 * e);
-        p2 |= ((u32)l2 & 0xffu) << (8 * e);
+        const u64 v = vr[x][e];
+        const u64 tb = v + 0x808080ULL - (v > half_q ? q : 0);
+        bad |= (tb >> 24) != 0;  // the value needs a fourth limb
+        wv[e] = (u32)tb ^ 0x808080u;
       }
+      // limb planes of the four elements: byte l of wv[0..3]
+      const u32 lo01 = __byte_perm(wv[0], wv[1], 0x5140), lo23 = __byte_perm(wv[2], wv[3], 0x5140);
+      const u32 hi01 = __byte_perm(wv[0], wv[1], 0x0062), hi23 = __byte_perm(wv[2], wv[3], 0x0062);
       const u32 off = SU_A + k4hi * (SU_POS * 16) + pos * 16 + k4lo * 4;
-      *(u32*)(stage + off) = p0;
-      *(u32*)(stage + off + SU_B) = p1;
-      *(u32*)(stage + off + 2 * SU_B) = p2;
+      *(u32*)(stage + off) = __byte_perm(lo01, lo23, 0x5410);
+      *(u32*)(stage + off + SU_B) = __byte_perm(lo01, lo23, 0x7632);
+      *(u32*)(stage + off + 2 * SU_B) = __byte_perm(hi01, hi23, 0x5410);
     }
+    if (c + 1 < nsteps) load(c + 1);
     umma::fence_proxy_async();
     umma::fence_before_sync();
     __syncthreads();
@@ -926,24 +937,27 @@ __global__ void __launch_bounds__(256) nc_gram_sums_kernel(const u64* gram, cons
     off += len;
     len = h;
   }
+  // dot products as exact 128-bit sums (at most 128 products below 2^112),
+  // one reduction each
   for (u32 e = tid; e < 2 * 30 * 16; e += 256) {
     const u32 rep = e / 480, r = (e / 16) % 30, i = e % 16;
-    u64 s = 0;
+    unsigned __int128 s = 0;
 #pragma unroll
-    for (u32 j = 0; j < 16; j++) s = salsaa::add_mod(s, mul_mod(M, C[i * 16 + j], L[rep][r][j]), q);
-    Y[rep][r][i] = s;
+    for (u32 j = 0; j < 16; j++) s += (unsigned __int128)C[i * 16 + j] * L[rep][r][j];
+    Y[rep][r][i] = reduce128_any(M, (u64)(s >> 64), (u64)s);
   }
   __syncthreads();
   if (tid < 2 * NG_T * 3) {
     const u32 rep = tid / (NG_T * 3), t = (tid / 3) % NG_T, a = tid % 3;
     const u32 o = 32 - (32 >> t), h = 8 >> t;  // first row and half length of round t
-    u64 s = 0;
+    unsigned __int128 s = 0;
     for (u32 j = 0; j < h; j++) {
       const u32 lrow = o + j + (a == 2 ? h : 0), rrow = o + j + (a == 0 ? 0 : h);
 #pragma unroll
-      for (u32 i = 0; i < 16; i++) s = salsaa::add_mod(s, mul_mod(M, L[rep][lrow][i], Y[rep][rrow][i]), q);
+      for (u32 i = 0; i < 16; i++) s += (unsigned __int128)L[rep][lrow][i] * Y[rep][rrow][i];
     }
-    atomic_add_mod(&sums[((rep * (u64)nr + t) * rows + k) * 3 + a], s, q, plain);
+    atomic_add_mod(&sums[((rep * (u64)nr + t) * rows + k) * 3 + a], reduce128_any(M, (u64)(s >> 64), (u64)s), q,
+                   plain);
   }
 }
 

@@ -905,14 +905,17 @@ __global__ void decomp_digits_kernel(RowSet in, u32 rows, u64 per_row, u64 q, u3
 }
 
 int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds, u64* out,
-                     u64* proof_radix, cudaStream_t st) {
+                     u64* proof_radix, cudaStream_t st, bool mag_ready) {
   if (parts < 1 || didx >= 16) return salsaa_set_error(-2, "decompose: bad arguments");
   const u64 per_row = width * d;
-  cudaError_t e = cudaMemsetAsync(&ds->bw_or[didx], 0, sizeof(u64), st);
-  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "decompose memset");
-  decomp_or_kernel<<<grid_1d(per_row, 256), 256, 0, st>>>(in, rows, per_row, q, &ds->bw_or[didx]);
-  int rc = check_launch("decomp_or");
-  if (rc) return rc;
+  int rc = 0;
+  if (!mag_ready) {
+    cudaError_t e = cudaMemsetAsync(&ds->bw_or[didx], 0, sizeof(u64), st);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "decompose memset");
+    decomp_or_kernel<<<grid_1d(per_row, 256), 256, 0, st>>>(in, rows, per_row, q, &ds->bw_or[didx]);
+    rc = check_launch("decomp_or");
+    if (rc) return rc;
+  }
   decomp_digits_kernel<<<grid_1d(per_row, 256), 256, 0, st>>>(in, rows, per_row, q, parts, ds, didx, out,
                                                                 proof_radix);
   return check_launch("decomp_digits");

@@ -110,8 +110,10 @@ int launch_sumcheck_batch(const u64* const* vecs, const u64* lens, u32 count, co
 int launch_norm3(const u64* cap, u32 rows, u32 nr, const NttDev& T, const ModQ& M, const DevState* ds,
                  u32 round, u64* proof_rep0, u64* proof_rep1, u64* base0, u64* base1, cudaStream_t st);
 
+// mag_ready: ds->bw_or[didx] already holds the OR of the inputs' centred
+// magnitudes (accumulated by the transforms that produced or read them).
 int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds,
-                     u64* out, u64* proof_radix, cudaStream_t st);
+                     u64* out, u64* proof_radix, cudaStream_t st, bool mag_ready = false);
 
 // J as bit masks (CUDA-core path), as an int8 matrix 256 x cw (tensor-core
 // path, optional) and cj[l] = sum_k J[k][l] (optional).

@@ -328,9 +328,11 @@ __device__ __forceinline__ u64 nr_canon(u64 a, u64 q, u64 q2, u64 onep) {
 
 // Global side of the last phase: canonical forward output (contiguous), or
 // the inverse output scaled by 1/n (strided).
+__device__ __forceinline__ u64 nr_mag(u64 v, u64 q) { return 2 * v > q ? q - v : v; }
+
 template <int LOGN, bool INC, bool INV, bool RELAX>
 __device__ __forceinline__ void nr_store_global(const u64 (&x)[16], u64* __restrict__ out, u64 ug, u32 tu,
-                                                const NttDev& T, u64 q, u64 q2) {
+                                                const NttDev& T, u64 q, u64 q2, u64* mag = nullptr) {
   constexpr int P = ph_count(LOGN) - 1, S = ph_size(LOGN, P);
   constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
   if (!INV) {
@@ -352,6 +354,7 @@ __device__ __forceinline__ void nr_store_global(const u64 (&x)[16], u64* __restr
         v = v >= q ? v - q : v;
         const u64 g = INC ? (ug >> 1) * (2 * N) + 2 * e + (ug & 1) : ug * N + e;
         out[g] = v;
+        if (mag) *mag |= nr_mag(v, q);
       }
   }
 }
@@ -386,7 +389,7 @@ __device__ __forceinline__ void nr_map(u32 tid, u32& unit, u32& tu) {
 }
 
 template <int LOGN, bool INC, bool INV, bool RELAX>
-__global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u64 units, NttDev T) {
+__global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
   constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
   constexpr int NPH = ph_count(LOGN);
   static_assert(!INC || UPT % 2 == 0, "incomplete mode keeps both halves of an element in one tile");
@@ -396,9 +399,12 @@ __global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u
   const u64 ug = (u64)blockIdx.x * UPT + unit;
   const bool active = ug < units;
   const u64 q = T.q, q2 = 2 * T.q;
-  u64 x[16];
+  u64 x[16], mag = 0;
   if (active) {
     nr_load_global<LOGN, INC, INV>(x, in, ug, tu);
+    if (!INV && mag_or)
+#pragma unroll
+      for (u32 i = 0; i < 16; i++) mag |= nr_mag(x[i], q);
     nr_compute<LOGN, 0, INV, RELAX>(x, tu, T, q, q2);
   }
   if constexpr (NPH > 1) {
@@ -410,7 +416,12 @@ __global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u
       nr_compute<LOGN, NPH - 1, INV, RELAX>(x, tu, T, q, q2);
     }
   }
-  if (active) nr_store_global<LOGN, INC, INV, RELAX>(x, out, ug, tu, T, q, q2);
+  if (active) nr_store_global<LOGN, INC, INV, RELAX>(x, out, ug, tu, T, q, q2, INV && mag_or ? &mag : nullptr);
+  if (mag_or) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
+    if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
+  }
 }
 
 // Fused negacyclic product r = a * b mod (Y^n + 1) for a batch of polynomials:
@@ -510,13 +521,14 @@ int nm_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& T, cu
 }
 
 template <int LOGN>
-int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomplete, bool inverse, cudaStream_t st) {
+int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomplete, bool inverse, cudaStream_t st,
+              u64* mag_or) {
   constexpr u32 UPT = NR_TILE >> LOGN;
   const u64 blocks = (units + UPT - 1) / UPT;
   if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt: batch too large");
   const bool relax = T.q < NR_RELAX_Q;
   auto go = [&](auto kern) -> int {
-    kern<<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T);
+    kern<<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T, mag_or);
     return 0;
   };
   if (incomplete) {
@@ -535,25 +547,29 @@ int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomple
 
 }  // namespace
 
+bool ntt_mag_ok(const u64* in, const u64* out, const NttDev& T, bool incomplete) {
+  const bool aligned = ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
+  return aligned && T.n >= 16 && T.n <= (incomplete ? 2048u : 4096u);
+}
+
 int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incomplete, bool inverse,
-               cudaStream_t st) {
+               cudaStream_t st, u64* mag_or) {
   if (count == 0) return 0;
   const u32 d = incomplete ? 2 * T.n : T.n;
-  const bool aligned = ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
-  if (aligned && T.n >= 16 && T.n <= (incomplete ? 2048u : 4096u)) {
+  if (ntt_mag_ok(in, out, T, incomplete)) {
     const u64 units = incomplete ? 2 * count : count;
     const int tr = salsaa_trace_begin("ntt_kernel", st, 16.0 * (double)count * d);
     int rc = 0;
     switch (T.logn) {
-      case 4: rc = nr_launch<4>(in, out, units, T, incomplete, inverse, st); break;
-      case 5: rc = nr_launch<5>(in, out, units, T, incomplete, inverse, st); break;
-      case 6: rc = nr_launch<6>(in, out, units, T, incomplete, inverse, st); break;
-      case 7: rc = nr_launch<7>(in, out, units, T, incomplete, inverse, st); break;
-      case 8: rc = nr_launch<8>(in, out, units, T, incomplete, inverse, st); break;
-      case 9: rc = nr_launch<9>(in, out, units, T, incomplete, inverse, st); break;
-      case 10: rc = nr_launch<10>(in, out, units, T, incomplete, inverse, st); break;
-      case 11: rc = nr_launch<11>(in, out, units, T, incomplete, inverse, st); break;
-      default: rc = nr_launch<12>(in, out, units, T, incomplete, inverse, st); break;
+      case 4: rc = nr_launch<4>(in, out, units, T, incomplete, inverse, st, mag_or); break;
+      case 5: rc = nr_launch<5>(in, out, units, T, incomplete, inverse, st, mag_or); break;
+      case 6: rc = nr_launch<6>(in, out, units, T, incomplete, inverse, st, mag_or); break;
+      case 7: rc = nr_launch<7>(in, out, units, T, incomplete, inverse, st, mag_or); break;
+      case 8: rc = nr_launch<8>(in, out, units, T, incomplete, inverse, st, mag_or); break;
+      case 9: rc = nr_launch<9>(in, out, units, T, incomplete, inverse, st, mag_or); break;
+      case 10: rc = nr_launch<10>(in, out, units, T, incomplete, inverse, st, mag_or); break;
+      case 11: rc = nr_launch<11>(in, out, units, T, incomplete, inverse, st, mag_or); break;
+      default: rc = nr_launch<12>(in, out, units, T, incomplete, inverse, st, mag_or); break;
     }
     salsaa_trace_end(tr, st);
     if (rc) return rc;
@@ -561,6 +577,7 @@ int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incompl
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ntt launch");
   }
+  if (mag_or) return salsaa_set_error(-2, "ntt: magnitude OR needs the register path");
   // 32 KiB of elements per CTA (at least one element).
   u32 epb = 4096 / d;
   if (epb == 0) epb = 1;

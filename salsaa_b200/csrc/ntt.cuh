@@ -30,8 +30,12 @@ struct NttDev {
 const NttDev* ntt_tables(u32 n, u64 q);
 
 // count units of n (full) or ring elements of 2n (incomplete); in may equal out.
+// With mag_or (register path only, ntt_mag_ok), the bitwise OR of the centred
+// magnitudes min(v, q - v) of the coefficient-form side (the input of a
+// forward, the output of an inverse transform) is OR-ed into *mag_or.
 int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incomplete, bool inverse,
-               cudaStream_t st);
+               cudaStream_t st, u64* mag_or = nullptr);
+bool ntt_mag_ok(const u64* in, const u64* out, const NttDev& T, bool incomplete);
 
 // Fused batched negacyclic product r = a * b mod (Y^n + 1), count polynomials
 // of n words each (r may alias a or b).  Needs 16 <= n <= 4096 and 16-byte

@@ -645,12 +645,14 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
   if (!pending) TRY(commit_rows(pr, Ws, &Wc, K, width, ms, 0, 0, proof + cur));
   cur += (u64)ms * K * d;
   u32 nsc = 0, didx = 0;
+  bool mag_ready = false;  // bw_or[didx] filled by the transforms of the joined witness
   for (u32 rd = 0; rd < P.nof_rounds; rd++) {
     const u32 parts = (u32)P.decomp_parts[rd < 12 ? rd : 11];
     if (!P.folding && parts > 1) {
       // decomp_ell (src/subroutines/decomp.rs:32-67)
       TRY(mark(pr, PH_DECOMP));
-      TRY(launch_decompose(Wc, K, width, d, q, parts, didx++, pr->ds, pr->Dc, proof + cur, st));
+      TRY(launch_decompose(Wc, K, width, d, q, parts, didx++, pr->ds, pr->Dc, proof + cur, st, mag_ready));
+      mag_ready = false;
       cur += 1;
       K *= parts;
       TRY(ntt_launch(pr->Dc, pr->Ds, (u64)K * width, T, true, false, st));
@@ -700,7 +702,18 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     u64* cj = pr->row_cj + (u64)rd * CK_BLOCK;
     TRY(launch_proj_tables(pr->ds, rd, cw, pr->pmask, pr->nmask, pr->Jm, cj, q, st, pr->Jc));
     TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Jm, pr->ds, pr->Pc, st, pr->Jc));
-    TRY(ntt_launch(pr->Pc, pr->Ps, width, T, true, false, st));
+    // the joined witness [folded, projected] is decomposed next: the two
+    // transforms that read P and write the folded row collect the OR of its
+    // centred magnitudes, so the decomposition needs no pass of its own
+    const bool next_decomp =
+        P.folding || (rd + 1 < P.nof_rounds && P.decomp_parts[rd + 1 < 12 ? rd + 1 : 11] > 1);
+    u64* mag = nullptr;
+    if (next_decomp && didx < 16 && ntt_mag_ok(pr->Pc, pr->Ps, T, true) && ntt_mag_ok(pr->Fs, pr->Fc, T, true)) {
+      mag = &pr->ds->bw_or[didx];
+      e = cudaMemsetAsync(mag, 0, sizeof(u64), st);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: magnitude OR");
+    }
+    TRY(ntt_launch(pr->Pc, pr->Ps, width, T, true, false, st, mag));
     RowSet Pr = rows_of(pr->Ps, 1, width, d);
     RowSet Prc = rows_of(pr->Pc, 1, width, d);
     const u32 S = ms + nsc;
@@ -759,7 +772,8 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(launch_fold_challenge(pr->ds, rd, K, d, q, pr->c_coef, st));
     TRY(ntt_launch(pr->c_coef, pr->c_slot, K, T, true, false, st));
     TRY(launch_fold(Ws, K, width, T, M, pr->c_slot, pr->fold_pre, pr->Fs, st));
-    TRY(ntt_launch(pr->Fs, pr->Fc, width, T, true, true, st));
+    TRY(ntt_launch(pr->Fs, pr->Fc, width, T, true, true, st, mag));
+    mag_ready = mag != nullptr;
     // send_cross_terms_before_join (src/subroutines/project.rs:229-245)
     RowSet Fr = rows_of(pr->Fs, 1, width, d), Frc = rows_of(pr->Fc, 1, width, d);
     TRY(commit_rows(pr, Fr, &Frc, 1, width, 0, nsc, 1, proof + cur));  // l0 = <projected_lhs, folded>
@@ -777,7 +791,8 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     Ws.p[1] = pr->Ps;
     if (P.folding) {
       TRY(mark(pr, PH_DECOMP));
-      TRY(launch_decompose(Wc, K, width, d, q, 2, didx++, pr->ds, pr->Dc, proof + cur, st));
+      TRY(launch_decompose(Wc, K, width, d, q, 2, didx++, pr->ds, pr->Dc, proof + cur, st, mag_ready));
+      mag_ready = false;
       cur += 1;
       K *= 2;
       TRY(ntt_launch(pr->Dc, pr->Ds, (u64)K * width, T, true, false, st));
