@@ -421,7 +421,7 @@ extern "C" uint64_t salsaa_workspace_bytes(const salsaa_params* p) {
   words += (u64)S.nsc_total * d + p->nof_rounds * CK_BLOCK;
   const u64 stmt = S.max_stmt + 2;
   words += stmt * CK_BLOCK + stmt * (L / CK_BLOCK + 1);
-  words += 2 * stmt * MAX_WROWS * d;
+  words += 3 * stmt * (MAX_WROWS + 1) * d;      // commitment accumulators and outputs
   words += (u64)(S.max_rows + 1) * (L < CK_BLOCK ? L : CK_BLOCK) * d;
   words += 2 * 256ULL * CK_BLOCK / 8;          // projection J and its tensor-core image (bytes)
   words += (u64)MAX_WROWS * (d / 2) * 6;       // fold constants
@@ -480,10 +480,10 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
       (rc = m.alloc(&pr->sc_base, (u64)S.nsc_total + 1, "row base pointers")) ||
       (rc = m.alloc(&pr->sc_lo, stmt * CK_BLOCK, "commit s_lo")) ||
       (rc = m.alloc(&pr->sc_hi, stmt * (L / CK_BLOCK + 1), "commit s_hi")) ||
-      (rc = m.alloc(&pr->acc, stmt * MAX_WROWS * d, "commit acc")) ||
+      (rc = m.alloc(&pr->acc, stmt * (MAX_WROWS + 1) * d, "commit acc")) ||
       (rc = m.alloc(&pr->colsum, (u64)(S.max_rows + 1) * (L < CK_BLOCK ? L : CK_BLOCK) * d, "commit column sums")) ||
-      (rc = m.alloc(&pr->cout, stmt * MAX_WROWS * d, "commit out")) ||
-      (rc = m.alloc(&pr->cout2, stmt * MAX_WROWS * d, "commit out (coefficients)")))
+      (rc = m.alloc(&pr->cout, stmt * (MAX_WROWS + 1) * d, "commit out")) ||
+      (rc = m.alloc(&pr->cout2, stmt * (MAX_WROWS + 1) * d, "commit out (coefficients)")))
     return fail(rc);
   // Scalar statement rows of the whole proof, in push order: per round
   // TENSOR(rep 0), TENSOR(rep 1), PERIODIC (witness_lhs), ONES (projected_lhs).
@@ -721,12 +721,16 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       // split rhs and projected commitment in one pass over the statement
       // rows: witness columns L_0..L_{K/2-1}, R_0..R_{K/2-1}, P.  The
       // challenges are fixed in advance, so computing P first changes nothing.
+      // The pass also takes this round's witness_lhs (PERIODIC) and
+      // projected_lhs (ONES) rows, statement rows S and S + 1: their products
+      // with the split witness and with P are witness_rhs, projection_rhs and
+      // the cross term l1 of batch_projections / send_cross_terms_before_join.
       TRY(mark(pr, PH_SPLIT));
       RowSet both = Ws, bothc = Wc;
       both.p[K] = pr->Ps;
       bothc.p[K] = pr->Pc;
-      TRY(commit_rows_slot(pr, both, &bothc, K + 1, width, ms, 0, nsc));
-      TRY(ntt_launch(pr->cout, pr->cout2, (u64)S * (K + 1), T, true, true, st));
+      TRY(commit_rows_slot(pr, both, &bothc, K + 1, width, ms, 0, nsc + 2));
+      TRY(ntt_launch(pr->cout, pr->cout2, (u64)(S + 2) * (K + 1), T, true, true, st));
       const size_t row_bytes = (size_t)(K + 1) * d * sizeof(u64);
       e = cudaMemcpy2DAsync(proof + cur, (size_t)K * d * sizeof(u64), pr->cout2, row_bytes,
                             (size_t)K * d * sizeof(u64), S, cudaMemcpyDeviceToDevice, st);
@@ -762,10 +766,21 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       cur += (u64)S * d;
     }
     // batch_projections (src/subroutines/project.rs:131-203): witness_rhs, projection_rhs
-    TRY(commit_rows(pr, Ws, &Wc, K, width, 0, nsc, 1, proof + cur));
-    cur += (u64)K * d;
-    TRY(commit_rows(pr, Pr, &Prc, 1, width, 0, nsc + 1, 1, proof + cur));
-    cur += d;
+    const u64* l1_src = nullptr;  // <witness_lhs, projected> when the merged pass made it
+    if (!P.folding) {
+      const u64* wl = pr->cout2 + (u64)S * (K + 1) * d;  // witness_lhs x [split witness, P]
+      const u64* pl = wl + (u64)(K + 1) * d;             // projected_lhs x [split witness, P]
+      e = cudaMemcpyAsync(proof + cur, wl, (size_t)K * d * sizeof(u64), cudaMemcpyDeviceToDevice, st);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(proof + cur + (u64)K * d, pl + (u64)K * d, (size_t)d * sizeof(u64),
+                            cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: batch projections");
+      l1_src = wl + (u64)K * d;
+    } else {
+      TRY(commit_rows(pr, Ws, &Wc, K, width, 0, nsc, 1, proof + cur));
+      TRY(commit_rows(pr, Pr, &Prc, 1, width, 0, nsc + 1, 1, proof + cur + (u64)K * d));
+    }
+    cur += (u64)K * d + d;
     nsc += 1;  // witness_lhs joins the statement
     // fold (src/subroutines/fold.rs:22-27)
     TRY(mark(pr, PH_FOLD));
@@ -778,7 +793,12 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     RowSet Fr = rows_of(pr->Fs, 1, width, d), Frc = rows_of(pr->Fc, 1, width, d);
     TRY(commit_rows(pr, Fr, &Frc, 1, width, 0, nsc, 1, proof + cur));  // l0 = <projected_lhs, folded>
     cur += d;
-    TRY(commit_rows(pr, Pr, &Prc, 1, width, 0, nsc - 1, 1, proof + cur));  // l1 = <witness_lhs, projected>
+    if (l1_src) {  // l1 = <witness_lhs, projected>
+      e = cudaMemcpyAsync(proof + cur, l1_src, (size_t)d * sizeof(u64), cudaMemcpyDeviceToDevice, st);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: cross term");
+    } else {
+      TRY(commit_rows(pr, Pr, &Prc, 1, width, 0, nsc - 1, 1, proof + cur));
+    }
     cur += d;
     nsc += 1;  // projected_lhs joins the statement
     // join: witness = [folded, projected]
