@@ -921,6 +921,28 @@ int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u3
   return check_launch("decomp_digits");
 }
 
+int launch_decompose_ntt(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds,
+                         u64* out, u64* out_slot, u64* proof_radix, const NttDev& T, cudaStream_t st,
+                         bool mag_ready) {
+  if (parts < 1 || didx >= 16) return salsaa_set_error(-2, "decompose: bad arguments");
+  if (!ntt_digits_ok(out, out_slot, rows, T) || rows > MAX_WROWS || d != 2 * T.n) {
+    const int rc = launch_decompose(in, rows, width, d, q, parts, didx, ds, out, proof_radix, st, mag_ready);
+    if (rc) return rc;
+    return ntt_launch(out, out_slot, (u64)rows * parts * width, T, true, false, st);
+  }
+  if (!mag_ready) {
+    cudaError_t e = cudaMemsetAsync(&ds->bw_or[didx], 0, sizeof(u64), st);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "decompose memset");
+    decomp_or_kernel<<<grid_1d(width * d, 256), 256, 0, st>>>(in, rows, width * d, q, &ds->bw_or[didx]);
+    int rc = check_launch("decomp_or");
+    if (rc) return rc;
+  }
+  NttSrcRows src{};
+  for (u32 k = 0; k < rows; k++) src.p[k] = in.p[k];
+  return ntt_digits_launch(src, rows, width, parts, &ds->bw_or[didx], &ds->rlog[didx], proof_radix, out, out_slot, T,
+                           st);
+}
+
 // ---------------------------------------------------------------------------
 // Projection (src/subroutines/project.rs:26-103).  J is 256 x cw with
 // entries 0 (is_zero), +1 (sign) or -1, drawn from the PRF.  Stored as two
@@ -1239,6 +1261,64 @@ __global__ void fold_kernel(RowSet w, u32 rows, u64 width, u32 logn, ModQ M, con
   }
 }
 
+// The same with two neighbouring slots per thread (16-byte accesses) and the
+// loads of four witness rows issued before their products, so each thread
+// keeps eight independent loads in flight (needs n >= 2 and 16-byte aligned
+// rows and output).
+template <bool LAZY>
+__global__ void __launch_bounds__(256) fold_vec_kernel(RowSet w, u32 rows, u64 width, u32 logn, ModQ M,
+                                                       const u64* __restrict__ pre, u64* out) {
+  const u32 n = 1u << logn, hn = n >> 1;
+  const u64 tot = width << (logn - 1), q = M.q, q2 = 2 * q;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u64 i = t >> (logn - 1);
+    const u32 s = 2 * ((u32)t & (hn - 1));
+    u64 ae[2] = {0, 0}, ao[2] = {0, 0};
+    for (u32 k0 = 0; k0 < rows; k0 += 4) {
+      ulonglong2 E[4], O[4];
+#pragma unroll
+      for (u32 j = 0; j < 4; j++)
+        if (k0 + j < rows) {
+          const u64* x = w.p[k0 + j] + (i << (logn + 1));
+          E[j] = __ldg((const ulonglong2*)(x + s));
+          O[j] = __ldg((const ulonglong2*)(x + n + s));
+        }
+#pragma unroll
+      for (u32 j = 0; j < 4; j++)
+        if (k0 + j < rows) {
+          const u64* pk = pre + ((u64)((k0 + j) << logn) + s) * 6;
+#pragma unroll
+          for (u32 h = 0; h < 2; h++) {
+            const u64* p = pk + 6 * h;
+            const u64 we = h ? E[j].y : E[j].x, wo = h ? O[j].y : O[j].x;
+            u64 e = mul_shoup_lazy(we, __ldg(p), __ldg(p + 1), q) + mul_shoup_lazy(wo, __ldg(p + 4), __ldg(p + 5), q);
+            u64 o = mul_shoup_lazy(we, __ldg(p + 2), __ldg(p + 3), q) + mul_shoup_lazy(wo, __ldg(p), __ldg(p + 1), q);
+            if (LAZY) {
+              ae[h] += e;
+              ao[h] += o;
+            } else {  // e, o < 4q < 2^64
+              e = e >= q2 ? e - q2 : e;
+              e = e >= q ? e - q : e;
+              o = o >= q2 ? o - q2 : o;
+              o = o >= q ? o - q : o;
+              ae[h] = add_mod(ae[h], e, q);
+              ao[h] = add_mod(ao[h], o, q);
+            }
+          }
+        }
+    }
+    if (LAZY) {
+#pragma unroll
+      for (u32 h = 0; h < 2; h++) {
+        ae[h] = reduce64(M, ae[h]);
+        ao[h] = reduce64(M, ao[h]);
+      }
+    }
+    *(ulonglong2*)(out + (i << (logn + 1)) + s) = make_ulonglong2(ae[0], ae[1]);
+    *(ulonglong2*)(out + (i << (logn + 1)) + n + s) = make_ulonglong2(ao[0], ao[1]);
+  }
+}
+
 int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot, u64* pre,
                 u64* out_slot, cudaStream_t st) {
   if (rows == 0 || rows > MAX_WROWS) return salsaa_set_error(-2, "fold: bad row count");
@@ -1246,6 +1326,14 @@ int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ&
   int rc = check_launch("fold_pre");
   if (rc) return rc;
   const bool lazy = M.q < (1ULL << 57);
+  bool vec = T.n >= 2 && (uintptr_t)out_slot % 16 == 0;
+  for (u32 k = 0; k < rows; k++) vec = vec && (uintptr_t)w_slot.p[k] % 16 == 0;
+  if (vec) {
+    const unsigned g = grid_1d(width * T.n / 2, 256);
+    if (lazy) fold_vec_kernel<true><<<g, 256, 0, st>>>(w_slot, rows, width, T.logn, M, pre, out_slot);
+    else fold_vec_kernel<false><<<g, 256, 0, st>>>(w_slot, rows, width, T.logn, M, pre, out_slot);
+    return check_launch("fold");
+  }
   if (lazy)
     fold_kernel<true><<<grid_1d(width * T.n, 256), 256, 0, st>>>(w_slot, rows, width, T.logn, M, pre, out_slot);
   else

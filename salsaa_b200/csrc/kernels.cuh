@@ -114,6 +114,12 @@ int launch_norm3(const u64* cap, u32 rows, u32 nr, const NttDev& T, const ModQ& 
 // magnitudes (accumulated by the transforms that produced or read them).
 int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds,
                      u64* out, u64* proof_radix, cudaStream_t st, bool mag_ready = false);
+// The same, also writing the digits' slot form to out_slot (one fused pass
+// with the forward transform when the shapes allow, else decomposition then
+// transform).
+int launch_decompose_ntt(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds,
+                         u64* out, u64* out_slot, u64* proof_radix, const NttDev& T, cudaStream_t st,
+                         bool mag_ready = false);
 
 // J as bit masks (CUDA-core path), as an int8 matrix 256 x cw (tensor-core
 // path, optional) and cj[l] = sum_k J[k][l] (optional).

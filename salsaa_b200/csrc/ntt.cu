@@ -424,6 +424,73 @@ __global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u
   }
 }
 
+// Digit decomposition (decomp_ell, src/subroutines/decomp.rs:32-67) fused
+// with the forward incomplete transform.  Ring element r of the digit space is
+// (source element (k, i), digit c) with c fastest, so the warps that produce
+// the digits of one source element load the same addresses and HBM sees the
+// source once; digit c = ((pos >> c rlog) & mask) - ((neg >> c rlog) & mask)
+// of the centre-lifted coefficient (pos or neg its magnitude) goes to row
+// k * parts + c of dc, and its transform to the same row of ds.
+template <int LOGN, bool RELAX>
+__global__ void __launch_bounds__(256)
+    ntt_digits_kernel(NttSrcRows src, u64 width, u32 parts, const u64* bw_or, u64* rlog_out, u64* radix_out, u64* dc,
+                      u64* ds, u64 units, NttDev T) {
+  constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N, D = 2 * N;
+  constexpr int NPH = ph_count(LOGN);
+  constexpr int S0 = ph_size(LOGN, 0);
+  constexpr u32 MB = 16 >> S0, KB = 1u << S0;
+  __shared__ u64 sm[NR_TILE + NR_TILE / 16];
+  u32 unit, tu;
+  nr_map<LOGN, true>(threadIdx.x, unit, tu);
+  const u64 ug = (u64)blockIdx.x * UPT + unit;
+  const bool active = ug < units;
+  const u64 q = T.q, q2 = 2 * T.q;
+  const u64 orv = *bw_or;
+  const u32 bw = orv ? 64u - (u32)__clzll((long long)orv) : 0u;
+  const u32 rlog = (bw + parts - 1) / parts;
+  const u64 mask = rlog >= 64 ? ~0ULL : ((1ULL << rlog) - 1);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *rlog_out = rlog;
+    if (radix_out) *radix_out = 1ULL << rlog;
+  }
+  const u64 re = ug >> 1, h = ug & 1;
+  const u32 c = (u32)(re % parts);
+  const u64 se = re / parts;
+  const u32 k = (u32)(se / width);
+  const u64 i = se % width;
+  const u64 dring = ((u64)k * parts + c) * width + i;  // output ring element
+  const u32 sh = rlog * c;
+  u64 x[16];
+  if (active) {
+    const u64* sp = src.p[k] + i * D + h;
+    u64* dco = dc + dring * D + h;
+#pragma unroll
+    for (u32 j = 0; j < MB; j++)
+#pragma unroll
+      for (u32 kk = 0; kk < KB; kk++) {
+        const u32 e = nr_elem<LOGN, 0, false>(tu, j, kk);
+        const u64 v = __ldg(sp + 2 * e);
+        const u64 pos = 2 * v > q ? 0 : v, neg = 2 * v > q ? q - v : 0;
+        const u64 pd = sh >= 64 ? 0 : ((pos >> sh) & mask), nd = sh >= 64 ? 0 : ((neg >> sh) & mask);
+        const u64 dv = pd >= nd ? pd - nd : pd + q - nd;
+        x[j * KB + kk] = dv;
+        dco[2 * e] = dv;
+      }
+    nr_compute<LOGN, 0, false, RELAX>(x, tu, T, q, q2);
+  }
+  if constexpr (NPH > 1) {
+    if (active) nr_store_smem<LOGN, 0, false>(x, sm, unit, tu);
+    __syncthreads();
+    nr_mid<LOGN, 1, NPH - 1, false, RELAX>(x, sm, unit, tu, active, T, q, q2);
+    if (active) {
+      nr_load_smem<LOGN, NPH - 1, false>(x, sm, unit, tu);
+      nr_compute<LOGN, NPH - 1, false, RELAX>(x, tu, T, q, q2);
+    }
+  }
+  // forward output of unit (dring, half h) at ds + (2 dring + h) N
+  if (active) nr_store_global<LOGN, true, false, RELAX>(x, ds, 2 * dring + h, tu, T, q, q2);
+}
+
 // Fused negacyclic product r = a * b mod (Y^n + 1) for a batch of polynomials:
 // forward transforms of a and b, the pointwise product and the inverse
 // transform in one pass over a tile, so HBM sees a and b read once and r
@@ -599,6 +666,50 @@ int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incompl
   };
   if (incomplete) return inverse ? launch(ntt_kernel<true, true>) : launch(ntt_kernel<true, false>);
   return inverse ? launch(ntt_kernel<false, true>) : launch(ntt_kernel<false, false>);
+}
+
+template <int LOGN>
+int nd_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* bw_or, u64* rlog_out,
+              u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st) {
+  constexpr u32 UPT = NR_TILE >> LOGN;
+  const u64 units = 2ULL * rows * parts * width;
+  const u64 blocks = (units + UPT - 1) / UPT;
+  if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt_digits: batch too large");
+  if (T.q < NR_RELAX_Q)
+    ntt_digits_kernel<LOGN, true><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out, radix_out,
+                                                                     dc, ds, units, T);
+  else
+    ntt_digits_kernel<LOGN, false><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out, radix_out,
+                                                                      dc, ds, units, T);
+  return 0;
+}
+
+bool ntt_digits_ok(const u64* dc, const u64* ds, u32 rows, const NttDev& T) {
+  return T.n >= 16 && T.n <= 2048 && rows >= 1 && rows <= 16 && (uintptr_t)dc % 16 == 0 && (uintptr_t)ds % 16 == 0;
+}
+
+int ntt_digits_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* bw_or, u64* rlog_out,
+                      u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st) {
+  if (!ntt_digits_ok(dc, ds, rows, T) || parts == 0 || width == 0)
+    return salsaa_set_error(-2, "ntt_digits: shape or alignment not supported");
+  const double bytes = 8.0 * rows * width * 2.0 * T.n * (1.0 + 2.0 * parts);
+  const int tr = salsaa_trace_begin("ntt_digits_kernel", st, bytes);
+  int rc = 0;
+  switch (T.logn) {
+    case 4: rc = nd_launch<4>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+    case 5: rc = nd_launch<5>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+    case 6: rc = nd_launch<6>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+    case 7: rc = nd_launch<7>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+    case 8: rc = nd_launch<8>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+    case 9: rc = nd_launch<9>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+    case 10: rc = nd_launch<10>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+    default: rc = nd_launch<11>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+  }
+  salsaa_trace_end(tr, st);
+  if (rc) return rc;
+  salsaa_count_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ntt_digits launch");
 }
 
 bool ntt_mul_fused_ok(const u64* a, const u64* b, const u64* r, const NttDev& T) {

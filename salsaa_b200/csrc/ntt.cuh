@@ -37,6 +37,19 @@ int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incompl
                cudaStream_t st, u64* mag_or = nullptr);
 bool ntt_mag_ok(const u64* in, const u64* out, const NttDev& T, bool incomplete);
 
+// Digit decomposition fused with the forward incomplete transform: for rows
+// source rows of width ring elements (2n coefficients, canonical), radix
+// 2^ceil(bw / parts) from the OR of centred magnitudes *bw_or (its log2 goes
+// to *rlog_out, the radix to *radix_out when not null), digit c of row k is
+// written to row k * parts + c of dc (coefficients) and of ds (slot form).
+// Needs 16 <= n <= 2048, rows <= 16 and 16-byte aligned dc and ds.
+struct NttSrcRows {
+  const u64* p[16];
+};
+bool ntt_digits_ok(const u64* dc, const u64* ds, u32 rows, const NttDev& T);
+int ntt_digits_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* bw_or, u64* rlog_out,
+                      u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st);
+
 // Fused batched negacyclic product r = a * b mod (Y^n + 1), count polynomials
 // of n words each (r may alias a or b).  Needs 16 <= n <= 4096 and 16-byte
 // aligned buffers (ntt_mul_fused_ok); the C ABI falls back to three passes.

@@ -651,11 +651,11 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     if (!P.folding && parts > 1) {
       // decomp_ell (src/subroutines/decomp.rs:32-67)
       TRY(mark(pr, PH_DECOMP));
-      TRY(launch_decompose(Wc, K, width, d, q, parts, didx++, pr->ds, pr->Dc, proof + cur, st, mag_ready));
+      TRY(launch_decompose_ntt(Wc, K, width, d, q, parts, didx++, pr->ds, pr->Dc, pr->Ds, proof + cur, T, st,
+                               mag_ready));
       mag_ready = false;
       cur += 1;
       K *= parts;
-      TRY(ntt_launch(pr->Dc, pr->Ds, (u64)K * width, T, true, false, st));
       Wc = rows_of(pr->Dc, K, width, d);
       Ws = rows_of(pr->Ds, K, width, d);
       // decomp rhs: derived after this round's split (see below)
@@ -811,11 +811,11 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     Ws.p[1] = pr->Ps;
     if (P.folding) {
       TRY(mark(pr, PH_DECOMP));
-      TRY(launch_decompose(Wc, K, width, d, q, 2, didx++, pr->ds, pr->Dc, proof + cur, st, mag_ready));
+      TRY(launch_decompose_ntt(Wc, K, width, d, q, 2, didx++, pr->ds, pr->Dc, pr->Ds, proof + cur, T, st,
+                               mag_ready));
       mag_ready = false;
       cur += 1;
       K *= 2;
-      TRY(ntt_launch(pr->Dc, pr->Ds, (u64)K * width, T, true, false, st));
       Ws = rows_of(pr->Ds, K, width, d);
       const RowSet Dcr = rows_of(pr->Dc, K, width, d);
       TRY(commit_rows(pr, Ws, &Dcr, K, width, ms, 0, nsc, proof + cur));

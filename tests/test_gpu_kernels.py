@@ -271,7 +271,8 @@ def test_project_too_narrow_rejected(api):
 
 
 @pytest.mark.parametrize("rows,width,d,q", [(2, 512, 16, P.Q0), (8, 1024, 128, P.Q0), (3, 256, 512, P.Q2),
-                                            (2, 128, 32, P.Q62)])
+                                            (2, 128, 32, P.Q62), (16, 256, 128, P.Q0), (5, 128, 4, P.Q1),
+                                            (7, 64, 64, P.Q62)])
 def test_fold(api, oracle, rows, width, d, q):
     rng = np.random.default_rng(rows + d)
     w = rand_mod(rng, (rows, width, d), q)
