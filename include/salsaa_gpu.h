@@ -166,6 +166,20 @@ int salsaa_prover_timing(salsaa_prover* pr, salsaa_timing* t);
 int salsaa_prove(salsaa_ctx* ctx, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof,
                  uint64_t proof_len);
 
+/* Blocking verification of a proof made with this context's parameters and
+ * CRS and the given seed: the verifier's inline checks of the reference
+ * (verify_decomp src/subroutines/decomp.rs:69-112, verify_norm_check_2/3
+ * src/subroutines/fast_norm_check.rs:352-462, verifier_split
+ * src/subroutines/split.rs:171-221, verify_batching / verifier_fold /
+ * verifier_join src/subroutines/project.rs:205-275, fold.rs:58-67, and the
+ * final check src/protocol.rs:464-472, which the reference runs inside
+ * protocol() with assert!s).  Returns 0 when the check ran, with *verdict 0
+ * for accept or a negative code naming the failed check (-3 header, -5
+ * length, -20/-21 decomposition, -30/-31 sumcheck, -32 norm3, -40/-41 split,
+ * -50 batching, -60 final check); a negative return is an API or CUDA error.
+ * Uses the context's blocking slot, like salsaa_prove. */
+int salsaa_verify(salsaa_ctx* ctx, uint64_t seed, const uint8_t* h_proof, uint64_t proof_len, int* verdict);
+
 /* ---- serving: continuous batching on one GPU ---- */
 /* No reference counterpart (the reference proves one statement per process,
  * src/main.rs:1-11).  A service holds parameter sets, each with a fixed number

@@ -110,6 +110,15 @@ class Context:
         _check(lib().salsaa_prove(self.h, seed, wp, out.ctypes.data_as(ctypes.c_void_p), out.size), "prove")
         return out
 
+    def verify(self, seed, proof):
+        """The reference verifier's checks on proof bytes (GPU-checked final
+        statement); returns 0 for accept, else the code of the failed check."""
+        proof = np.ascontiguousarray(proof, dtype=np.uint8)
+        verdict = ctypes.c_int(0)
+        _check(lib().salsaa_verify(self.h, seed, proof.ctypes.data_as(ctypes.c_void_p), proof.size,
+                                   ctypes.byref(verdict)), "verify")
+        return verdict.value
+
     def parallel_dot_series_matrix(self, w):
         """Commitment-key rows times the witness rows (src/arithmetic.rs:459-505).
         w: CUDA tensor rows x width x d (coefficients) -> module_size x rows x d."""

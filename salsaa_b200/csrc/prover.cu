@@ -939,6 +939,372 @@ extern "C" int salsaa_prove(salsaa_ctx* c, uint64_t seed, const uint64_t* h_witn
   return salsaa_prover_sync(pr);
 }
 
+// ---------------------------------------------------------------------------
+// Verifier.  The checks the reference's verifier makes inline
+// (verify_decomp src/subroutines/decomp.rs:69-112, verify_norm_check_2/3
+// src/subroutines/fast_norm_check.rs:352-462, verifier_split
+// src/subroutines/split.rs:171-221, verify_batching / verifier_fold /
+// verifier_join src/subroutines/project.rs:205-275 and fold.rs:58-67, and the
+// final check src/protocol.rs:464-472) replayed on a proof.  The proof's ring
+// elements move to slot form on the GPU; the scalar and per-element checks run
+// on the host (a few thousand ring elements); the final check, the statement
+// rows against the final witness, is a commitment over the witness and runs on
+// the GPU through the prover's own commitment path.  Verdict codes: 0 accept,
+// -3 header or shape, -5 length, -20 radix, -21 decomposition, -30/-31
+// sumcheck, -32 norm3, -40/-41 split, -50 projection, -60 final check.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct HostSlots {
+  u64 q;
+  u32 n, d;
+  std::vector<u64> zeta;
+  // (a_e + a_o X)(b_e + b_o X) mod (X^2 - zeta_s), slot by slot
+  void mul(const u64* a, const u64* b, u64* r) const {
+    for (u32 s = 0; s < n; s++) {
+      const u64 ae = a[s], ao = a[n + s], be = b[s], bo = b[n + s];
+      const u64 e = host::addmod(host::mulmod(ae, be, q), host::mulmod(host::mulmod(ao, bo, q), zeta[s], q), q);
+      const u64 o = host::addmod(host::mulmod(ae, bo, q), host::mulmod(ao, be, q), q);
+      r[s] = e;
+      r[n + s] = o;
+    }
+  }
+};
+
+// Statement rows as the verifier tracks them: PowerSeries shapes (a base
+// layer of blen elements and K tensor factors).
+struct VRow {
+  int type;             // RowType
+  u32 ck;               // commitment-key row
+  u64 K, blen;
+  std::vector<u64> c;   // TENSOR: the challenges of the K factors (1 - c, c)
+};
+
+u64 nc_chal_host(u64 seed, u64 round, u64 rep, u64 j, u64 q) {
+  return (u64)(((unsigned __int128)prf_at(prf_key(seed, domain_id(DOM_NC, round, rep)), j) * q) >> 64);
+}
+
+// Ring-element segments (word offset, element count) of a proof, in order.
+void proof_segments(const salsaa_params& P, std::vector<std::pair<u64, u64>>& seg) {
+  const u64 d = P.d;
+  u64 pos = 8, S = P.module_size, K = P.init_wit_rep, width = P.wit_len;
+  auto ring = [&](u64 cnt) {
+    seg.push_back({pos, cnt});
+    pos += cnt * d;
+  };
+  ring(S * K);
+  for (u64 rd = 0; rd < P.nof_rounds; rd++) {
+    const u64 parts = P.decomp_parts[rd < 12 ? rd : 11];
+    if (!P.folding && parts > 1) {
+      pos += 1;
+      ring(S * K * parts);
+      K *= parts;
+    }
+    pos += K;
+    const u64 nr = ilog2u(width * d);
+    for (int rep = 0; rep < 2; rep++) {
+      pos += nr * K * 3;
+      ring(K);
+      S += 1;
+    }
+    if (!P.folding) {
+      ring(S * 2 * K);
+      K *= 2;
+      width /= 2;
+    }
+    ring(S);      // projected commitment
+    ring(K);      // witness_rhs
+    ring(1);      // projection_rhs
+    S += 1;
+    ring(2);      // l0, l1
+    S += 1;
+    K = 2;
+    if (P.folding) {
+      pos += 1;
+      ring(S * K * 2);
+      K *= 2;
+      break;
+    }
+  }
+  if (!P.folding) ring(K * width);
+}
+
+}  // namespace
+
+static int verify_impl(salsaa_prover* pr, u64 seed, const u64* proof, int* verdict) {
+  salsaa_ctx* c = pr->ctx;
+  const salsaa_params& P = c->P;
+  const NttDev& T = *c->T;
+  const u64 d = c->d, n = c->n, q = P.q, ms = P.module_size, words = c->S.proof_words, L = c->L;
+  cudaStream_t st = pr->st;
+  *verdict = 0;
+  const u64 hdr[8] = {0x31504141534C4153ULL, P.d, P.q, P.module_size, P.wit_len, P.init_wit_rep, P.nof_rounds,
+                      P.folding};
+  for (int i = 0; i < 8; i++)
+    if (proof[i] != hdr[i]) {
+      *verdict = -3;
+      return 0;
+    }
+  if (words > c->S.max_d_rows_width * d) return salsaa_set_error(-9, "verify: proof larger than the slot's buffers");
+  // the proof in coefficient form (own_proof) and its ring elements in slot form (Ds)
+  cudaError_t e;
+  if (!pr->own_proof && (e = cudaMalloc(&pr->own_proof, words * 8)) != cudaSuccess)
+    return salsaa_set_cuda_error(e, "verify: proof buffer");
+  u64* dcoef = (u64*)pr->own_proof;
+  u64* dslot = pr->Ds;
+  if ((e = cudaMemcpyAsync(dcoef, proof, words * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return salsaa_set_cuda_error(e, "verify: proof upload");
+  set_seed_kernel<<<1, 1, 0, st>>>(pr->ds, seed);  // the challenges drawn on the device
+  salsaa_count_launch();
+  std::vector<std::pair<u64, u64>> seg;
+  proof_segments(P, seg);
+  for (const auto& s : seg) TRY(ntt_launch(dcoef + s.first, dslot + s.first, s.second, T, true, false, st));
+  std::vector<u64> slot(words), mslot((u64)ms * d);
+  HostSlots R{q, (u32)n, (u32)d, std::vector<u64>(n)};
+  if ((e = cudaMemcpyAsync(slot.data(), dslot, words * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(R.zeta.data(), T.zeta, n * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(mslot.data(), c->m_slot, ms * d * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return salsaa_set_cuda_error(e, "verify: slot forms");
+  // m_r^(2^j) for the split checks of the commitment-key rows
+  const u32 logL = (u32)ilog2u(L);
+  std::vector<u64> mpow((u64)ms * (logL + 1) * d);
+  for (u64 r = 0; r < ms; r++) {
+    u64* p = mpow.data() + r * (logL + 1) * d;
+    memcpy(p, mslot.data() + r * d, d * 8);
+    for (u32 j = 1; j <= logL; j++) R.mul(p + (j - 1) * d, p + (j - 1) * d, p + j * d);
+  }
+
+  u64 pos = 8;
+  auto ring = [&](u64 cnt) {
+    const u64* p = slot.data() + pos;
+    pos += cnt * d;
+    return p;
+  };
+  auto word = [&]() { return pos < words ? proof[pos++] : (pos++, 0ULL); };
+  std::vector<VRow> rows;
+  for (u64 r = 0; r < ms; r++) rows.push_back(VRow{ROW_CK, (u32)r, logL, 1, {}});
+  u64 K = P.init_wit_rep, width = L;
+  const u64* v0 = ring(ms * K);
+  std::vector<u64> V(v0, v0 + ms * K * d), tmp(d), tmp2(d);
+  struct RoundRows {
+    u64 rd, nr, cw;
+  };
+  std::vector<RoundRows> rr;
+  int rc = 0;
+  auto compose_check = [&](u64 parts, u64 radix, const u64* Dm) {
+    const u64 S = rows.size(), shift = (u64)__builtin_ctzll(radix);
+    for (u64 j = 0; j < S; j++)
+      for (u64 i = 0; i < K; i++)
+        for (u64 t = 0; t < d; t++) {
+          u64 acc = 0;
+          for (u64 cc = 0; cc < parts; cc++) {
+            const u64 pw = shift * cc < 64 ? ((1ULL << (shift * cc)) % q) : 0;
+            acc = host::addmod(acc, host::mulmod(Dm[((j * K + i) * parts + cc) * d + t], pw, q), q);
+          }
+          if (acc != V[(j * K + i) * d + t]) return false;
+        }
+    return true;
+  };
+
+  for (u64 rd = 0; rd < P.nof_rounds && !rc; rd++) {
+    const u64 parts = P.decomp_parts[rd < 12 ? rd : 11];
+    if (!P.folding && parts > 1) {  // verify_decomp
+      const u64 radix = word();
+      if (!radix || (radix & (radix - 1))) {
+        rc = -20;
+        break;
+      }
+      const u64* Dm = ring(rows.size() * K * parts);
+      if (!compose_check(parts, radix, Dm)) {
+        rc = -21;
+        break;
+      }
+      V.assign(Dm, Dm + rows.size() * K * parts * d);
+      K *= parts;
+    }
+    const u64 nr = ilog2u(width * d);
+    std::vector<u64> claims(K), cs(nr ? nr : 1);
+    for (u64 k = 0; k < K; k++) claims[k] = word();
+    for (u64 rep = 0; rep < 2; rep++) {  // verify_norm_check_2, verify_norm_check_3
+      std::vector<u64> cl = claims;
+      for (u64 j = 0; j < nr; j++) cs[j] = nc_chal_host(seed, rd, rep, j, q);
+      for (u64 j = 0; j < nr; j++)
+        for (u64 k = 0; k < K; k++) {
+          const u64 f0 = word(), f1 = word(), f2 = word();
+          if (f0 >= q || f1 >= q || f2 >= q) rc = rc ? rc : -30;
+          const u64 lhs = host::addmod(host::addmod(host::addmod(f0, f0, q), host::addmod(f1, f1, q), q), f2, q);
+          if (lhs != cl[k]) rc = rc ? rc : -31;
+          const u64 cj = cs[j];
+          cl[k] = host::addmod(host::addmod(f0, host::mulmod(host::addmod(f1, f1, q), cj, q), q),
+                               host::mulmod(host::mulmod(f2, cj, q), cj, q), q);
+        }
+      for (u64 k = 0; k < K; k++) {
+        const u64 c0 = proof[pos];
+        if (host::mulmod(c0, c0, q) != cl[k]) rc = rc ? rc : -32;
+        const u64* rhs = ring(1);
+        V.insert(V.end(), rhs, rhs + d);
+      }
+      const u64 Kr = nr - ilog2u(d);
+      rows.push_back(VRow{ROW_TENSOR, 0, Kr, 1, std::vector<u64>(cs.begin(), cs.begin() + Kr)});
+    }
+    rr.push_back(RoundRows{rd, nr, 0});
+    if (rc) break;
+    if (!P.folding) {  // verifier_split: t0 * L + t1 * R = the unsplit value, row by row
+      const u64 S = rows.size();
+      const u64* SR = ring(S * 2 * K);
+      for (u64 j = 0; j < S && !rc; j++) {
+        const VRow& w = rows[j];
+        if (width % w.blen) {
+          rc = -40;
+          break;
+        }
+        const u64 f = width / w.blen;
+        if (f & (f - 1)) {
+          rc = -40;
+          break;
+        }
+        const u64 jj = ilog2u(f);
+        if (jj == 0 || jj > w.K) {
+          rc = -40;
+          break;
+        }
+        for (u64 k = 0; k < K && !rc; k++) {
+          const u64* a = SR + (j * 2 * K + k) * d;
+          const u64* b = SR + (j * 2 * K + K + k) * d;
+          if (w.type == ROW_CK) {  // t0 = 1, t1 = m^(width / 2)
+            R.mul(mpow.data() + ((u64)w.ck * (logL + 1) + jj - 1) * d, b, tmp.data());
+            for (u64 t = 0; t < d; t++) tmp[t] = host::addmod(tmp[t], a[t], q);
+          } else {  // scalar factors: (1 - c, c) for TENSOR rows, (1, 1) otherwise
+            const u64 ci = w.type == ROW_TENSOR ? w.c[w.K - jj] : 0;
+            const u64 t0 = w.type == ROW_TENSOR ? host::submod(1 % q, ci, q) : 1 % q;
+            const u64 t1 = w.type == ROW_TENSOR ? ci : 1 % q;
+            for (u64 t = 0; t < d; t++) tmp[t] = host::addmod(host::mulmod(a[t], t0, q), host::mulmod(b[t], t1, q), q);
+          }
+          if (memcmp(tmp.data(), V.data() + (j * K + k) * d, d * 8)) rc = -41;
+        }
+      }
+      if (rc) break;
+      V.assign(SR, SR + S * 2 * K * d);
+      K *= 2;
+      width /= 2;
+    }
+    const u64 cw = K * 256;
+    if (cw > width) {
+      rc = -3;
+      break;
+    }
+    rr.back().cw = cw;
+    const u64 Sp = rows.size();
+    const u64* PC = ring(Sp);
+    const u64* wrhs = ring(K);
+    const u64* prhs = ring(1);
+    std::fill(tmp.begin(), tmp.end(), 0);
+    for (u64 k = 0; k < K; k++)
+      for (u64 t = 0; t < d; t++) tmp[t] = host::addmod(tmp[t], wrhs[k * d + t], q);
+    if (memcmp(tmp.data(), prhs, d * 8)) {  // verify_batching
+      rc = -50;
+      break;
+    }
+    V.insert(V.end(), wrhs, wrhs + K * d);
+    rows.push_back(VRow{ROW_PERIODIC, 0, ilog2u(width / cw), cw, {}});
+    // verifier_fold: VF_j = sum_k c_k V_jk with the fold challenges in slot form
+    TRY(launch_fold_challenge(pr->ds, (u32)rd, (u32)K, (u32)d, q, pr->c_coef, st));
+    TRY(ntt_launch(pr->c_coef, pr->c_slot, K, T, true, false, st));
+    std::vector<u64> cslot(K * d);
+    if ((e = cudaMemcpyAsync(cslot.data(), pr->c_slot, K * d * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return salsaa_set_cuda_error(e, "verify: fold challenge");
+    const u64 S = rows.size();
+    std::vector<u64> VF(S * d, 0);
+    for (u64 j = 0; j < S; j++)
+      for (u64 k = 0; k < K; k++) {
+        R.mul(cslot.data() + k * d, V.data() + (j * K + k) * d, tmp.data());
+        for (u64 t = 0; t < d; t++) VF[j * d + t] = host::addmod(VF[j * d + t], tmp[t], q);
+      }
+    const u64* l0 = ring(1);
+    const u64* l1 = ring(1);
+    rows.push_back(VRow{ROW_ONES, 0, ilog2u(width / cw) + ilog2u(K), 256, {}});
+    // verifier_join: new rhs with witness columns [folded, projected]
+    std::vector<u64> NV((Sp + 2) * 2 * d);
+    for (u64 i = 0; i < Sp; i++) {
+      memcpy(NV.data() + (i * 2) * d, VF.data() + i * d, d * 8);
+      memcpy(NV.data() + (i * 2 + 1) * d, PC + i * d, d * 8);
+    }
+    memcpy(NV.data() + (Sp * 2) * d, VF.data() + Sp * d, d * 8);
+    memcpy(NV.data() + (Sp * 2 + 1) * d, l1, d * 8);
+    memcpy(NV.data() + ((Sp + 1) * 2) * d, l0, d * 8);
+    memcpy(NV.data() + ((Sp + 1) * 2 + 1) * d, prhs, d * 8);
+    V.swap(NV);
+    K = 2;
+    if (P.folding) {
+      const u64 radix = word();
+      if (!radix || (radix & (radix - 1))) {
+        rc = -20;
+        break;
+      }
+      const u64* Dm = ring(rows.size() * K * 2);
+      if (!compose_check(2, radix, Dm)) {
+        rc = -21;
+        break;
+      }
+      V.assign(Dm, Dm + rows.size() * K * 2 * d);
+      K *= 2;
+      break;
+    }
+  }
+  if (!rc && !P.folding) {
+    // final check: every statement row against the final witness, on the GPU
+    const u64 fw = K * width * d;
+    if (pos + fw > words || 2 * fw > c->S.max_d_rows_width * d) {
+      rc = -5;
+    } else {
+      u64* wc = pr->Dc;
+      u64* ws = pr->Dc + fw;
+      if ((e = cudaMemcpyAsync(wc, dcoef + pos, fw * 8, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+        return salsaa_set_cuda_error(e, "verify: final witness");
+      pos += fw;
+      TRY(ntt_launch(wc, ws, K * width, T, true, false, st));
+      // the device-side statement rows: norm3 bases and projection sums per round
+      if ((e = cudaMemsetAsync(pr->sc.cap, 0, 2 * d * 8, st)) != cudaSuccess)
+        return salsaa_set_cuda_error(e, "verify: norm3 scratch");
+      for (const RoundRows& x : rr) {
+        TRY(launch_norm3(pr->sc.cap, 1, (u32)x.nr, T, c->M, pr->ds, (u32)x.rd, pr->cout2, pr->cout2 + d,
+                         pr->row_base + (4 * x.rd) * d, pr->row_base + (4 * x.rd + 1) * d, st));
+        TRY(launch_proj_tables(pr->ds, (u32)x.rd, (u32)x.cw, pr->pmask, pr->nmask, pr->Jm,
+                               pr->row_cj + x.rd * CK_BLOCK, q, st, pr->Jc));
+      }
+      const u32 nsc = (u32)(rows.size() - ms);
+      const RowSet fwc = rows_of(wc, (u32)K, width, (u32)d);
+      TRY(commit_rows_slot(pr, rows_of(ws, (u32)K, width, (u32)d), &fwc, (u32)K, width, (u32)ms, 0, nsc));
+      std::vector<u64> out(rows.size() * K * d);
+      if ((e = cudaMemcpyAsync(out.data(), pr->cout, out.size() * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+          (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return salsaa_set_cuda_error(e, "verify: final check");
+      TRY(tc_error_check());
+      if (out != V) rc = -60;
+    }
+  }
+  if (!rc && pos != words) rc = -5;
+  *verdict = rc;
+  return 0;
+}
+
+extern "C" int salsaa_verify(salsaa_ctx* c, uint64_t seed, const uint8_t* h_proof, uint64_t proof_len,
+                             int* verdict) {
+  if (!c || !h_proof || !verdict) return salsaa_set_error(-1, "verify: null argument");
+  if (!c->S.ok) return salsaa_set_error(-1, ("verify: " + c->S.why).c_str());
+  *verdict = -5;
+  if (proof_len != c->S.proof_words * 8) return 0;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "verify: cudaSetDevice");
+  if (!c->blocking) TRY(salsaa_prover_create(c, &c->blocking));
+  std::vector<u64> words(c->S.proof_words);
+  memcpy(words.data(), h_proof, proof_len);
+  return verify_impl(c->blocking, seed, words.data(), verdict);
+}
+
 extern "C" void salsaa_ctx_destroy(salsaa_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
