@@ -380,9 +380,10 @@ int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, const u64*
 // path).  Two stages: the witness of step c + 1 is staged while the MMAs of
 // step c run.
 // ---------------------------------------------------------------------------
-constexpr u32 PU_POS = 128, PU_KS = 128;
-constexpr u32 PU_A = 2 * 128 * PU_KS;  // both J halves of one step (32 KiB)
-constexpr u32 PU_B = PU_POS * PU_KS;   // witness int8 tile (16 KiB)
+constexpr u32 PU_POS = 128, PU_KS = 64;
+constexpr u32 PU_IMG = 2 * 128 * 128;  // Jc: both J halves of one 128-element chunk (32 KiB)
+constexpr u32 PU_A = 2 * 128 * PU_KS;  // both J halves of one step (16 KiB)
+constexpr u32 PU_B = PU_POS * PU_KS;   // witness int8 tile (8 KiB)
 constexpr u32 PU_STAGE = PU_A + PU_B;
 
 __global__ void __launch_bounds__(256, 2)
@@ -415,36 +416,53 @@ __global__ void __launch_bounds__(256, 2)
   // signed int8 x signed int8 -> s32, M = N = 128
   const u32 idesc = umma::idesc_u8(128, PU_POS) | (1u << 7) | (1u << 10);
   bool bad = false, ok = true;
-  for (u32 c = 0; c < nsteps; c++) {
-    const u32 st = c & 1;
-    uint8_t* stage = smem + st * PU_STAGE;
-    if (c >= 2) ok &= umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1);
-    if (tid == 0) {
-      umma::mbar_expect_tx(&full_bar[st], PU_A);
-      umma::bulk_g2s(stage, Jc + (u64)c * PU_A, PU_A, &full_bar[st]);
-    }
-    // witness step: 128 positions x 128 elements as int8, (k / 16, pos, k % 16)
-    uint8_t* B = stage + PU_A;
+  // task x of this thread: four consecutive elements k .. k + 3 at one position;
+  // a step's witness values stay in registers from their loads (issued before
+  // the previous step's barrier) to their conversion
+  u64 vr[8][4];
+  auto load = [&](u32 c) {
     const u64* src = chunk + (u64)c * PU_KS * d;
-#pragma unroll 4
-    for (u32 x = 0; x < 16; x++) {
+#pragma unroll
+    for (u32 x = 0; x < 8; x++) {
       const u32 t = tid + x * 256;
       const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
       const u32 k = (k4hi * 4 + k4lo) * 4;
-      u32 packed = 0;
+#pragma unroll
+      for (u32 e = 0; e < 4; e++) vr[x][e] = __ldg(src + (u64)(k + e) * d + pos);
+    }
+  };
+  load(0);
+  for (u32 c = 0; c < nsteps; c++) {
+    const u32 st = c & 1;
+    uint8_t* stage = smem + st * PU_STAGE;
+    if (c >= 2) ok &= umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1);
+    if (tid == 0) {  // K slices of this step from the chunk's image, one copy per J half
+      umma::mbar_expect_tx(&full_bar[st], PU_A);
+      const int8_t* img = Jc + (u64)(c / 2) * PU_IMG + (c % 2) * (PU_A / 2);
+      umma::bulk_g2s(stage, img, PU_A / 2, &full_bar[st]);
+      umma::bulk_g2s(stage + PU_A / 2, img + PU_IMG / 2, PU_A / 2, &full_bar[st]);
+    }
+    // witness step: 128 positions x 64 elements as int8, (k / 16, pos, k % 16)
+    uint8_t* B = stage + PU_A;
+#pragma unroll
+    for (u32 x = 0; x < 8; x++) {
+      const u32 t = tid + x * 256;
+      const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
+      const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
+      // centred value + 128 is below 256 exactly when the value fits int8
+      u32 packed = 0, hi = 0;
 #pragma unroll
       for (u32 e = 0; e < 4; e++) {
-        const u64 v = __ldg(src + (u64)(k + e) * d + pos);
-        long long cv = v > half_q ? (long long)v - (long long)q : (long long)v;
-        if (cv < -128 || cv > 127) {
-          bad = true;
-          cv = 0;
-        }
-        packed |= ((u32)cv & 0xffu) << (8 * e);
+        const u64 v = vr[x][e];
+        const u64 tb = v + 128 - (v > half_q ? q : 0);
+        hi |= (u32)(tb >> 8) | (u32)(tb >> 40);
+        packed |= ((u32)tb & 0xffu) << (8 * e);
       }
-      *(u32*)(B + k4hi * (PU_POS * 16) + pos * 16 + k4lo * 4) = packed;
+      bad |= hi != 0;
+      *(u32*)(B + k4hi * (PU_POS * 16) + pos * 16 + k4lo * 4) = packed ^ 0x80808080u;
     }
+    if (c + 1 < nsteps) load(c + 1);
     umma::fence_proxy_async();
     umma::fence_before_sync();
     __syncthreads();
