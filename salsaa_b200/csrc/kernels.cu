@@ -1209,18 +1209,20 @@ int launch_fold_challenge(const DevState* ds, u32 round, u32 rows, u32 d, u64 q,
 // Fold constants per (row k, slot s): c_e, c_o and zeta c_o with their Shoup
 // companions, so each slot product is four Shoup multiplications:
 // (c_e + X c_o)(w_e + X w_o) = c_e w_e + (zeta c_o) w_o + X (c_o w_e + c_e w_o).
+// Per (row k, slot s): c_e, c_o, zeta_s c_o and their Shoup companions, as six
+// planes pre[(j * rows + k) * n + s] so that neighbouring slots are adjacent.
 __global__ void fold_pre_kernel(const u64* c, u32 rows, u32 n, ModQ M, const u64* zeta, u64* pre) {
   const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= rows * n) return;
   const u32 k = t / n, s = t % n;
   const u64 ce = c[(u64)k * 2 * n + s], co = c[(u64)k * 2 * n + n + s], zco = mul_mod(M, zeta[s], co);
-  u64* p = pre + (u64)t * 6;
-  p[0] = ce;
-  p[1] = shoup_dev(ce, M.q);
-  p[2] = co;
-  p[3] = shoup_dev(co, M.q);
-  p[4] = zco;
-  p[5] = shoup_dev(zco, M.q);
+  const u64 plane = (u64)rows * n;
+  pre[0 * plane + t] = ce;
+  pre[1 * plane + t] = shoup_dev(ce, M.q);
+  pre[2 * plane + t] = co;
+  pre[3 * plane + t] = shoup_dev(co, M.q);
+  pre[4 * plane + t] = zco;
+  pre[5 * plane + t] = shoup_dev(zco, M.q);
 }
 
 // out = sum_k c_k w_k in slot form.  LAZY (q < 2^57, at most 16 rows): the
@@ -1237,9 +1239,12 @@ __global__ void fold_kernel(RowSet w, u32 rows, u64 width, u32 logn, ModQ M, con
     for (u32 k = 0; k < rows; k++) {
       const u64* x = w.p[k] + (i << (logn + 1));
       const u64 we = x[s], wo = x[n + s];
-      const u64* p = pre + ((u64)(k << logn) + s) * 6;
-      u64 e = mul_shoup_lazy(we, __ldg(p), __ldg(p + 1), q) + mul_shoup_lazy(wo, __ldg(p + 4), __ldg(p + 5), q);
-      u64 o = mul_shoup_lazy(we, __ldg(p + 2), __ldg(p + 3), q) + mul_shoup_lazy(wo, __ldg(p), __ldg(p + 1), q);
+      const u64 plane = (u64)rows << logn;
+      const u64* p = pre + ((u64)(k << logn) + s);
+      const u64 ce = __ldg(p), cep = __ldg(p + plane), co = __ldg(p + 2 * plane), cop = __ldg(p + 3 * plane);
+      const u64 zc = __ldg(p + 4 * plane), zcp = __ldg(p + 5 * plane);
+      u64 e = mul_shoup_lazy(we, ce, cep, q) + mul_shoup_lazy(wo, zc, zcp, q);
+      u64 o = mul_shoup_lazy(we, co, cop, q) + mul_shoup_lazy(wo, ce, cep, q);
       if (LAZY) {
         ae += e;
         ao += o;
@@ -1286,13 +1291,19 @@ __global__ void __launch_bounds__(256) fold_vec_kernel(RowSet w, u32 rows, u64 w
 #pragma unroll
       for (u32 j = 0; j < 4; j++)
         if (k0 + j < rows) {
-          const u64* pk = pre + ((u64)((k0 + j) << logn) + s) * 6;
+          // both slots' constants: one 16-byte load per plane
+          const u64 plane = (u64)rows << logn;
+          const u64* pk = pre + ((u64)((k0 + j) << logn) + s);
+          ulonglong2 C[6];
+#pragma unroll
+          for (u32 g = 0; g < 6; g++) C[g] = __ldg((const ulonglong2*)(pk + g * plane));
 #pragma unroll
           for (u32 h = 0; h < 2; h++) {
-            const u64* p = pk + 6 * h;
             const u64 we = h ? E[j].y : E[j].x, wo = h ? O[j].y : O[j].x;
-            u64 e = mul_shoup_lazy(we, __ldg(p), __ldg(p + 1), q) + mul_shoup_lazy(wo, __ldg(p + 4), __ldg(p + 5), q);
-            u64 o = mul_shoup_lazy(we, __ldg(p + 2), __ldg(p + 3), q) + mul_shoup_lazy(wo, __ldg(p), __ldg(p + 1), q);
+            const u64 ce = h ? C[0].y : C[0].x, cep = h ? C[1].y : C[1].x, co = h ? C[2].y : C[2].x;
+            const u64 cop = h ? C[3].y : C[3].x, zc = h ? C[4].y : C[4].x, zcp = h ? C[5].y : C[5].x;
+            u64 e = mul_shoup_lazy(we, ce, cep, q) + mul_shoup_lazy(wo, zc, zcp, q);
+            u64 o = mul_shoup_lazy(we, co, cop, q) + mul_shoup_lazy(wo, ce, cep, q);
             if (LAZY) {
               ae[h] += e;
               ao[h] += o;
@@ -1326,7 +1337,7 @@ int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ&
   int rc = check_launch("fold_pre");
   if (rc) return rc;
   const bool lazy = M.q < (1ULL << 57);
-  bool vec = T.n >= 2 && (uintptr_t)out_slot % 16 == 0;
+  bool vec = T.n >= 2 && (uintptr_t)out_slot % 16 == 0 && (uintptr_t)pre % 16 == 0 && ((u64)rows * T.n) % 2 == 0;
   for (u32 k = 0; k < rows; k++) vec = vec && (uintptr_t)w_slot.p[k] % 16 == 0;
   if (vec) {
     const unsigned g = grid_1d(width * T.n / 2, 256);
