@@ -361,42 +361,73 @@ __global__ void __launch_bounds__(256) sc_round_kernel(const u64* in, u64 sin, u
 
 // One CTA per (rep,row) finishes rounds j0.. from v_{j0} (length L <= SC_TAIL),
 // reading either a per-pair buffer or (j0 = 0) the witness row itself.
+// T rounds of the tail on the vector v (length cur, shared memory): groups of
+// 2^T values v[g + m ng] per thread, sums of all T rounds in one block
+// reduction, folded values back to v[g] (only thread g touches v[g]).
+template <bool LAZY, u32 T>
+__device__ __forceinline__ void tail_step(u64* v, u64 cur, const ModQ& M, const DevState* ds, u32 round, u32 rep,
+                                          u32 j, u64* sums, u32 nr, u32 rows, u32 k, Sum128* red) {
+  constexpr u32 G = 1u << T;
+  const u64 q = M.q, ng = cur >> T;
+  u64 c[T], cp[T];
+#pragma unroll
+  for (u32 t = 0; t < T; t++) {
+    c[t] = nc_challenge(ds, round, rep, j + t, q);
+    cp[t] = shoup_dev(c[t], q);
+  }
+  ScAcc<LAZY> acc[T][3];
+#pragma unroll
+  for (u32 t = 0; t < T; t++)
+#pragma unroll
+    for (u32 a = 0; a < 3; a++) acc[t][a].zero();
+  for (u64 g = threadIdx.x; g < ng; g += blockDim.x) {
+    u64 x[G];
+#pragma unroll
+    for (u32 m = 0; m < G; m++) x[m] = v[g + m * ng];
+    group_rounds<LAZY, T>(M, x, c, cp, acc, 0);
+    v[g] = x[0];
+  }
+  ScAcc<LAZY> flat[T * 3];
+#pragma unroll
+  for (u32 t = 0; t < T; t++)
+#pragma unroll
+    for (u32 a = 0; a < 3; a++) flat[t * 3 + a] = acc[t][a];
+  const u64 r = block_totals<LAZY, T * 3>(M, flat, red);  // its barriers also publish v
+  if (threadIdx.x < T * 3) sums[((rep * (u64)nr + j + threadIdx.x / 3) * rows + k) * 3 + threadIdx.x % 3] = r;
+}
+
 template <bool LAZY>
-__global__ void __launch_bounds__(1024) sc_tail_kernel(const u64* in, u64 sin, RowSet w0, u64 L, u32 rows, ModQ M,
+__global__ void __launch_bounds__(512) sc_tail_kernel(const u64* in, u64 sin, RowSet w0, u64 L, u32 rows, ModQ M,
                                                        const DevState* ds, u32 round, u32 j0, u64* sums, u32 nr,
                                                        u32 d, u64* cap) {
   extern __shared__ u64 v[];
-  __shared__ Sum128 red[3 * 32];
+  __shared__ Sum128 red[SC_T * 3 * 32];
   const u32 pair = blockIdx.x, rep = pair / rows, k = pair % rows;
-  const u64 q = M.q;
   const u64* x = (j0 == 0) ? w0.p[k] : in + (u64)pair * sin;
   for (u32 i = threadIdx.x; i < L; i += blockDim.x) v[i] = x[i];
   __syncthreads();
   u64 cur = L;
   u32 j = j0;
   while (cur > 1) {
-    if (cur == d)
+    if (cur == d) {
       for (u32 i = threadIdx.x; i < d; i += blockDim.x) cap[(u64)pair * d + i] = v[i];
-    const u64 h = cur / 2;
-    ScAcc<LAZY> a0, a1, a2;
-    a0.zero();
-    a1.zero();
-    a2.zero();
-    for (u32 i = threadIdx.x; i < h; i += blockDim.x) {
-      const u64 p0 = v[i], p1 = v[i + h];
-      a0.mac(M, p0, p0);
-      a1.mac(M, p0, p1);
-      a2.mac(M, p1, p1);
+      __syncthreads();
     }
-    ScAcc<LAZY> tri[3] = {a0, a1, a2};
-    const u64 r = block_totals<LAZY, 3>(M, tri, red);
-    if (threadIdx.x < 3) sums[((rep * (u64)nr + j) * rows + k) * 3 + threadIdx.x] = r;
-    const u64 c = nc_challenge(ds, round, rep, j, q), cp = shoup_dev(c, q);
-    __syncthreads();
-    for (u32 i = threadIdx.x; i < h; i += blockDim.x) v[i] = fold1(v[i], v[i + h], c, cp, q);
-    __syncthreads();
-    cur = h;
-    j++;
+    // up to four rounds per step, stopping at length d (norm_check_3's vector)
+    u32 T = 63u - (u32)__clzll((long long)cur);
+    if (cur > d) {
+      const u32 td = 63u - (u32)__clzll((long long)(cur / d));
+      T = td < T ? td : T;
+    }
+    T = T < SC_T ? T : SC_T;
+    switch (T) {
+      case 4: tail_step<LAZY, 4>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red); break;
+      case 3: tail_step<LAZY, 3>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red); break;
+      case 2: tail_step<LAZY, 2>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red); break;
+      default: tail_step<LAZY, 1>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red); break;
+    }
+    cur >>= T;
+    j += T;
   }
 }
 
@@ -733,7 +764,7 @@ static int sumcheck_passes(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, c
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sc_tail smem attribute");
   }
-  kern<<<2 * rows, 1024, smem, st>>>(in, sin, w, L, rows, M, ds, round, j, B.sums, nr, d, B.cap);
+  kern<<<2 * rows, 512, smem, st>>>(in, sin, w, L, rows, M, ds, round, j, B.sums, nr, d, B.cap);
   return check_launch("sc_tail");
 }
 
