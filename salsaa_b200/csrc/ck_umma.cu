@@ -552,16 +552,18 @@ __global__ void sc_img_kernel(const u64* s_lo, u32 Bw, ScRowList tl, uint8_t* im
 }
 
 __global__ void __launch_bounds__(512, 1)
-    sc_umma_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, ScRowList tl, const uint8_t* __restrict__ img,
-                   const u64* s_hi, ModQ M, u64* acc, bool plain, u32* flags) {
+    sc_umma_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, u32 split, ScRowList tl,
+                   const uint8_t* __restrict__ img, const u64* s_hi, ModQ M, u64* acc, bool plain, u32* flags) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t full_bar[2], done_bar[2];
   __shared__ uint32_t tslot;
   const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const u32 pb = blockIdx.x, hb = blockIdx.y, k = blockIdx.z;
+  // CTA: positions pb, element block hb (one s_hi factor), its part sub of split
+  const u32 pb = blockIdx.x, hb = blockIdx.y / split, sub = blockIdx.y % split, k = blockIdx.z;
   const u64 q = M.q, half_q = q >> 1;
-  const u64* src0 = wc.p[k] + ((u64)hb * Bw) * d + (u64)pb * SU_POS;
-  const u32 nsteps = Bw / SU_KS;
+  const u32 nsteps = Bw / SU_KS / split, c0 = sub * nsteps;
+  const u64* src0 = wc.p[k] + ((u64)hb * Bw + (u64)c0 * SU_KS) * d + (u64)pb * SU_POS;
+  img += (u64)c0 * SU_A;
   u32* err = &g_tc_error;
   if (tid == 0) {
     for (int b = 0; b < 2; b++) {
@@ -690,16 +692,17 @@ __global__ void __launch_bounds__(512, 1)
 }
 
 // Exact CUDA-core sums for the CTAs sc_umma_kernel flagged (same grid).
-__global__ void sc_exact_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, ScRowList tl, const u64* s_lo,
-                                const u64* s_hi, ModQ M, u64* acc, bool plain, const u32* flags) {
+__global__ void sc_exact_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, u32 split, ScRowList tl,
+                                const u64* s_lo, const u64* s_hi, ModQ M, u64* acc, bool plain, const u32* flags) {
   const u32 cta = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   if (!flags[cta]) return;
-  const u32 pb = blockIdx.x, hb = blockIdx.y, k = blockIdx.z, pos = threadIdx.x;
+  const u32 pb = blockIdx.x, hb = blockIdx.y / split, sub = blockIdx.y % split, k = blockIdx.z, pos = threadIdx.x;
+  const u32 i0 = sub * (Bw / split), i1 = i0 + Bw / split;
   const u64* src = wc.p[k] + ((u64)hb * Bw) * d + (u64)pb * SU_POS + pos;
   for (u32 r = 0; r < tl.n; r++) {
     const u32 j = tl.idx[r];
     u64 v = 0;
-    for (u32 i = 0; i < Bw; i++) v = salsaa::add_mod(v, mul_mod(M, s_lo[(u64)j * Bw + i], src[(u64)i * d]), M.q);
+    for (u32 i = i0; i < i1; i++) v = salsaa::add_mod(v, mul_mod(M, s_lo[(u64)j * Bw + i], src[(u64)i * d]), M.q);
     v = mul_mod(M, v, s_hi[(u64)j * nhi + hb]);
     atomic_add_mod(acc + ((u64)j * rows + k) * d + (u64)pb * SU_POS + pos, v, M.q, plain);
   }
@@ -707,8 +710,14 @@ __global__ void sc_exact_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, ScR
 
 int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi, const ScRowList& tl,
                    const u64* s_lo, const u64* s_hi, const ModQ& M, u64* acc, bool plain, uint8_t* img, u32* flags,
-                   cudaStream_t st) {
-  const u64 ctas = (u64)(d / SU_POS) * nhi * rows;
+                   u64 flag_cap, cudaStream_t st) {
+  // short witnesses: split each element block over several CTAs (linear sums)
+  // while the grid stays within one wave (one CTA per SM) and the flag scratch
+  const u64 base = (u64)(d / SU_POS) * nhi * rows;
+  u32 split = 1;
+  while (split * 2 <= Bw / SU_KS && base * split * 2 <= 148 && base * split * 2 <= flag_cap) split *= 2;
+  const u64 ctas = base * split;
+  if (ctas > flag_cap) return salsaa_set_error(-2, "sc_umma: flag scratch too small");
   cudaError_t e = cudaMemsetAsync(flags, 0, ctas * sizeof(u32), st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sc_umma flags");
   u64 g = ((u64)Bw * 128 + 255) / 256;
@@ -717,10 +726,10 @@ int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi
   const size_t smem = 2 * (size_t)SU_STAGE;
   e = cudaFuncSetAttribute(sc_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sc_umma smem attribute");
-  dim3 grid(d / SU_POS, nhi, rows);
-  sc_umma_kernel<<<grid, 512, smem, st>>>(wc, rows, d, Bw, nhi, tl, img, s_hi, M, acc, plain, flags);
+  dim3 grid(d / SU_POS, nhi * split, rows);
+  sc_umma_kernel<<<grid, 512, smem, st>>>(wc, rows, d, Bw, nhi, split, tl, img, s_hi, M, acc, plain, flags);
   salsaa_count_launch();
-  sc_exact_kernel<<<grid, SU_POS, 0, st>>>(wc, rows, d, Bw, nhi, tl, s_lo, s_hi, M, acc, plain, flags);
+  sc_exact_kernel<<<grid, SU_POS, 0, st>>>(wc, rows, d, Bw, nhi, split, tl, s_lo, s_hi, M, acc, plain, flags);
   salsaa_count_launch();
   e = cudaGetLastError();
   (void)width;

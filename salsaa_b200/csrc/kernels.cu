@@ -1007,16 +1007,24 @@ __global__ void proj_tables_kernel(const DevState* ds, u32 round, u32 cw, u32* p
   neg_mask[t] = nm;
 }
 
-__global__ void proj_cj_kernel(u32 cw, const u32* pos_mask, const u32* neg_mask, u64* cj, u64 q) {
-  u32 l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= cw) return;
-  const u32 words = cw / 32;
+// cj[l] = sum_k J[k][l]: one CTA per 32 columns (one mask word), 32 x 32
+// threads, thread (x, y) summing rows y, y + 32, ... of column x.
+__global__ void __launch_bounds__(1024) proj_cj_kernel(u32 cw, const u32* pos_mask, const u32* neg_mask, u64* cj,
+                                                       u64 q) {
+  __shared__ int part[32][33];
+  const u32 x = threadIdx.x & 31, y = threadIdx.x >> 5, wd = blockIdx.x, words = cw / 32;
   int v = 0;
-  for (u32 k = 0; k < PROJ_H; k++) {
-    v += (pos_mask[(u64)k * words + l / 32] >> (l % 32)) & 1;
-    v -= (neg_mask[(u64)k * words + l / 32] >> (l % 32)) & 1;
+  for (u32 k = y; k < PROJ_H; k += 32) {
+    v += (pos_mask[(u64)k * words + wd] >> x) & 1;
+    v -= (neg_mask[(u64)k * words + wd] >> x) & 1;
   }
-  cj[l] = v >= 0 ? (u64)v % q : q - ((u64)(-v) % q);
+  part[y][x] = v;
+  __syncthreads();
+  if (y == 0) {
+    int t = 0;
+    for (u32 r = 0; r < 32; r++) t += part[r][x];
+    cj[wd * 32 + x] = t >= 0 ? (u64)t % q : q - ((u64)(-t) % q);
+  }
 }
 
 int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32* neg_mask, int8_t* J, u64* cj,
@@ -1028,7 +1036,7 @@ int launch_proj_tables(const DevState* ds, u32 round, u32 cw, u32* pos_mask, u32
   int rc = check_launch("proj_tables");
   if (rc) return rc;
   if (cj) {
-    proj_cj_kernel<<<(cw + 255) / 256, 256, 0, st>>>(cw, pos_mask, neg_mask, cj, q);
+    proj_cj_kernel<<<cw / 32, 1024, 0, st>>>(cw, pos_mask, neg_mask, cj, q);
     rc = check_launch("proj_cj");
   }
   return rc;
@@ -2054,7 +2062,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
         periodic_done = true;
       }
       rc = launch_sc_umma(wsrc, a.rows, a.width, d, Bw, nhi, gl, a.sc_lo, a.sc_hi, M, acc_sc, plain, a.sc_img,
-                          a.sc_flags, st);
+                          a.sc_flags, a.sc_flag_cap, st);
       if (rc) return rc;
     } else {
       launch_sc_pass(a, wsrc, a.width, tl, true, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);

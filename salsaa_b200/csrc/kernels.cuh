@@ -72,7 +72,7 @@ constexpr u64 SC_IMG_BYTES = (u64)CK_BLOCK * 128;
 constexpr u32 SC_UMMA_MAX_ROWS = 18;
 int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi, const ScRowList& tl,
                    const u64* s_lo, const u64* s_hi, const ModQ& M, u64* acc, bool plain, uint8_t* img, u32* flags,
-                   cudaStream_t st);
+                   u64 flag_cap, cudaStream_t st);
 // First sumcheck pass (rounds 0..3 of both repetitions) on tcgen05 through the
 // Gram matrices of 16-element groups (see ck_umma.cu): launch_nc_gram writes
 // the folded vectors and the Gram matrices, or raises the flag word after them
@@ -158,6 +158,7 @@ struct CommitArgs {
   const int* sc_types_host;          // their types, on the host (required when nsc > 0)
   uint8_t* sc_img;   // scratch for the tcgen05 TENSOR-row pass (SC_IMG_BYTES), or null
   u32* sc_flags;     // scratch: one word per CTA of that pass
+  u64 sc_flag_cap;   // words of sc_flags
   const u64* const* sc_base_dev;     // nsc ring bases (slot form) or null (= 1)
   u64* sc_lo;        // scratch nsc x CK_BLOCK
   u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)

@@ -591,6 +591,7 @@ static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, const RowSet* w
   if ((u64)(c->d / 128) * (width / CK_BLOCK > 0 ? width / CK_BLOCK : 1) * rows <= pr->sc_flag_words) {
     a.sc_img = pr->sc_img;
     a.sc_flags = pr->sc_flags;
+    a.sc_flag_cap = pr->sc_flag_words;
   }
   a.out_slot = pr->cout;
   return launch_commit(a, *c->T, c->M, pr->ds, pr->st);
