@@ -133,14 +133,19 @@ __device__ __forceinline__ void transpose4x4(u32 a, u32 b, u32 c, u32 d, u32& o0
 }
 
 __global__ void __launch_bounds__(CKU_THREADS, 1)
-    ck_umma_kernel(const uint8_t* __restrict__ tk8, RowSet w, u32 rows, u32 nck, u32 nkp, u32 n, u32 bt, u32 Bw,
-                   const u64* thi, u32 nhi_t, ModQ M, const u64* zeta, u64* acc, bool plain) {
+    ck_umma_kernel(const uint8_t* __restrict__ tk8, RowSet w, u32 rows, u32 G, u32 nck, u32 nkp, u32 n, u32 bt,
+                   u32 Bw, const u64* thi, u32 nhi_t, ModQ M, const u64* zeta, u64* acc, bool plain) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t full_bar[2], done_bar[2];
   __shared__ uint32_t tslot;
   const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const u32 s0 = 2 * blockIdx.x, d = 2 * n;
-  const u64 i0 = (u64)blockIdx.y * Bw;
+  // element blocks g < G of this CTA start at i0 + g bt: the same offsets in
+  // the key block, so they share every key tile; their witness rows stack as
+  // the virtual rows g * rows + k of the MMA's M dimension
+  const u32 lob = bt / Bw, lo_b = blockIdx.y % lob, hg = blockIdx.y / lob;
+  const u64 i0 = (u64)hg * G * bt + (u64)lo_b * Bw;
+  const u32 vrows = rows * G;
   const u32 btile = nkp * CKU_CHUNK;                  // one slot's key tile
   const u32 stage_bytes = 2 * CKU_ATILE + 2 * btile;  // A0 A1 B0 B1
   const u32 nchunks = Bw / CKU_CHUNK;
@@ -168,34 +173,40 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
   umma::fence_after_sync();
   const u32 tmem = tslot;
 
-  // witness task t: (i4lo, kp within a group of 8, kp group, i4hi)
-  const u32 nkpw = 2 * rows, kpb = (nkpw + 7) / 8;
+  // witness task t: (i4lo, kp within a group of 8, kp group, i4hi); kp = (virtual row, part).
+  // A thread's three tasks are the same in every chunk: their source (chunk 0)
+  // and shared-memory offsets are computed once.
+  const u32 nkpw = 2 * vrows, kpb = (nkpw + 7) / 8;
   uint4 wv[3][4];
+  const u64* tsrc[3];
+  u32 toff[3];
+  bool tval[3];
+#pragma unroll
+  for (u32 x = 0; x < 3; x++) {
+    const u32 t = tid + x * CKU_THREADS;
+    const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
+    const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
+    tval[x] = t < 256 * kpb && kp < nkpw;
+    const u32 v = kp >> 1, part = kp & 1, k = tval[x] ? v % rows : 0, g = tval[x] ? v / rows : 0;
+    const u32 i4 = i4hi * 4 + i4lo;  // elements 4 * i4 .. + 3 of the chunk
+    tsrc[x] = w.p[k] + (i0 + (u64)g * bt + i4 * 4) * d + part * n + s0;
+    toff[x] = (i4 >> 2) * (128 * 16) + (kp * 7) * 16 + (i4 & 3) * 4;
+  }
   auto fetch = [&](u32 c) {
 #pragma unroll
-    for (u32 x = 0; x < 3; x++) {
-      const u32 t = tid + x * CKU_THREADS;
-      const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
-      const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
-      if (t < 256 * kpb && kp < nkpw) {
-        const u32 k = kp >> 1, part = kp & 1;
-        const u64 e0 = i0 + (u64)c * CKU_CHUNK + (i4hi * 4 + i4lo) * 4;
-        const u64* src = w.p[k] + e0 * d + part * n + s0;
+    for (u32 x = 0; x < 3; x++)
+      if (tval[x]) {
+        const u64* src = tsrc[x] + (u64)c * CKU_CHUNK * d;
 #pragma unroll
         for (u32 e = 0; e < 4; e++) wv[x][e] = __ldg((const uint4*)(src + (u64)e * d));
       }
-    }
   };
   auto stash = [&](u32 st) {
     uint8_t* A = smem + st * stage_bytes;
 #pragma unroll
-    for (u32 x = 0; x < 3; x++) {
-      const u32 t = tid + x * CKU_THREADS;
-      const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
-      const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
-      if (t < 256 * kpb && kp < nkpw) {
-        const u32 i4 = i4hi * 4 + i4lo;  // elements 4 * i4 .. + 3 of the chunk
-        const u32 off = (i4 >> 2) * (128 * 16) + (kp * 7) * 16 + (i4 & 3) * 4;
+    for (u32 x = 0; x < 3; x++)
+      if (tval[x]) {
+        const u32 off = toff[x];
         // byte plane b of the four elements: a 4 x 4 byte transpose of their
         // low words (planes 0..3) and high words (planes 4..6)
 #pragma unroll
@@ -212,7 +223,6 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
           for (u32 b = 0; b < 7; b++) *(u32*)(A + sg * CKU_ATILE + off + b * 16) = p[b];
         }
       }
-    }
   };
 
   const u32 idesc = umma::idesc_u8(128, nkp);
@@ -269,7 +279,7 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
   // 2 nck column groups (w >> 3), split at a group boundary
   const u32 sg = (warp >> 2) & 1, row = (warp & 3) * 32 + lane, ch = warp >> 3;
   if (ok) {
-    const bool valid = row < rows * 14;
+    const bool valid = row < vrows * 14;
     const u32 y = row % 7;
     const u64 pw = ((u64)1 << (8 * y)) % M.q;
     const u32 jb = 7 * (ch ? nck : 0), je = 7 * (ch ? 2 * nck : nck);
@@ -298,16 +308,16 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
   }
   __syncthreads();
   if (ok) {
-    const u32 hi_t = (u32)(i0 / bt);
-    for (u32 t = tid; t < 2 * rows * nck; t += CKU_THREADS) {
-      const u32 r = t % nck, k = (t / nck) % rows, g2 = t / (nck * rows);
+    for (u32 t = tid; t < 2 * vrows * nck; t += CKU_THREADS) {
+      const u32 r = t % nck, v = (t / nck) % vrows, g2 = t / (nck * vrows);
+      const u32 k = v % rows, hi_t = (u32)(i0 / bt) + v / rows;
       const u32 s = s0 + g2;
       const u64* P = Pm + (u64)g2 * 128 * ng;
       u64 ca = 0, db = 0, cb = 0, da = 0;
 #pragma unroll
       for (u32 y = 0; y < 7; y++) {
-        const u64* pa = P + (u64)((2 * k) * 7 + y) * ng;      // part a rows
-        const u64* pb = P + (u64)((2 * k + 1) * 7 + y) * ng;  // part b rows
+        const u64* pa = P + (u64)((2 * v) * 7 + y) * ng;      // part a rows
+        const u64* pb = P + (u64)((2 * v + 1) * 7 + y) * ng;  // part b rows
         ca = salsaa::add_mod(ca, pa[2 * r], M.q);
         da = salsaa::add_mod(da, pa[2 * r + 1], M.q);
         cb = salsaa::add_mod(cb, pb[2 * r], M.q);
@@ -350,17 +360,21 @@ bool ck_umma_ok(const CommitArgs& a, u32 n) {
   return true;
 }
 
-int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, const u64* zeta, bool plain, cudaStream_t st) {
+int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, u32 G, const ModQ& M, const u64* zeta, bool plain,
+                   cudaStream_t st) {
+  if (G == 0 || a.rows * G > CKU_MAX_WROWS || (G > 1 && (a.width < a.ck_bt || (a.width / a.ck_bt) % G)) ||
+      a.ck_bt % Bw || a.width % ((u64)Bw * G))
+    return salsaa_set_error(-2, "ck_umma: bad block grouping");
   const u32 nkp = ck_tk8_nkp(a.nck);
   const size_t stage = 2 * (size_t)CKU_ATILE + 2 * (size_t)nkp * CKU_CHUNK;
   const size_t epi = 2 * 128 * (size_t)(2 * a.nck) * sizeof(u64);
   const size_t smem = 2 * stage > epi ? 2 * stage : epi;
   cudaError_t e = cudaFuncSetAttribute(ck_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ck_umma smem attribute");
-  dim3 g(n / 2, (unsigned)(a.width / Bw));
+  dim3 g(n / 2, (unsigned)(a.width / Bw / G));
   const int tr = salsaa_trace_begin("ck_umma_kernel", st, 2.0 * 196.0 * a.nck * a.rows * (double)a.width * n);
-  ck_umma_kernel<<<g, CKU_THREADS, smem, st>>>(a.tk8, a.w, a.rows, a.nck, nkp, n, a.ck_bt, Bw, a.thi, a.ck_nhi, M,
-                                               zeta, a.acc, plain);
+  ck_umma_kernel<<<g, CKU_THREADS, smem, st>>>(a.tk8, a.w, a.rows, G, a.nck, nkp, n, a.ck_bt, Bw, a.thi, a.ck_nhi,
+                                               M, zeta, a.acc, plain);
   salsaa_trace_end(tr, st);
   salsaa_count_launch();
   e = cudaGetLastError();

@@ -2019,7 +2019,13 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
     // halved while the grid would not fill the GPU
     u32 Bk = (u32)(a.width < a.ck_bt ? a.width : a.ck_bt);
     while (Bk > CK_BLOCK && (u64)(n / 2) * (a.width / Bk) < 296) Bk /= 2;
-    int rc = launch_ck_umma(a, n, Bk, M, T.zeta, plain, st);
+    // few witness rows: G blocks one key block apart per CTA share the key
+    // tiles (virtual rows g * rows + k), while the grid keeps a full wave
+    u32 G = 1;
+    while (a.width >= a.ck_bt && a.rows * G * 2 <= CKU_MAX_WROWS && (a.width / a.ck_bt) % (G * 2) == 0 &&
+           (u64)(n / 2) * (a.width / Bk) / (G * 2) >= 148)
+      G *= 2;
+    int rc = launch_ck_umma(a, n, Bk, G, M, T.zeta, plain, st);
     if (rc) return rc;
   } else if (a.nck && a.tl8 && M.q < (1ULL << 56) && a.width >= CKM_KS && a.rows <= 9 && n <= 512) {
     if (Bw > a.ck_bt) return salsaa_set_error(-2, "commit: witness wider than the key tables");

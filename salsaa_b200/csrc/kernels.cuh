@@ -172,7 +172,9 @@ struct CommitArgs {
 int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const DevState* ds, cudaStream_t st);
 // Key rows of launch_commit on tcgen05 when ck_umma_ok (see ck_umma.cu).
 bool ck_umma_ok(const CommitArgs& a, u32 n);
-int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, const ModQ& M, const u64* zeta, bool plain, cudaStream_t st);
+// Bw elements per block, G blocks (one key block apart) per CTA.
+int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, u32 G, const ModQ& M, const u64* zeta, bool plain,
+                   cudaStream_t st);
 
 // Commitment of a witness of width w from the commitment of its split halves
 // (slot form): out[j][k] = t0_j * R[j][k] + t1_j * R[j][K + k] for statement
