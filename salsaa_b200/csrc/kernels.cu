@@ -2070,6 +2070,13 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
       rc = launch_sc_umma(wsrc, a.rows, a.width, d, Bw, nhi, gl, a.sc_lo, a.sc_hi, M, acc_sc, plain, a.sc_img,
                           a.sc_flags, a.sc_flag_cap, st);
       if (rc) return rc;
+      if (!periodic_done && ol.n <= SC_UMMA_MAX_ROWS) {
+        // more rows than one pass holds: the periodic / all-ones rows in a second pass
+        rc = launch_sc_umma(wsrc, a.rows, a.width, d, Bw, nhi, ol, a.sc_lo, a.sc_hi, M, acc_sc, plain, a.sc_img,
+                            a.sc_flags, a.sc_flag_cap, st);
+        if (rc) return rc;
+        periodic_done = true;
+      }
     } else {
       launch_sc_pass(a, wsrc, a.width, tl, true, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
       rc = check_launch("sc_commit (tensor rows)");
