@@ -387,7 +387,8 @@ def run_ours(args):
             "sumcheck_batch": scb,
             "serving": serving,
             "roofline": roofline_ck(traced, measured_peaks(tensor=True),
-                                    statistics.mean(plain) * len(plain) if plain else None),
+                                    statistics.mean(plain) * len(plain) if plain else None,
+                                    args.preset == "A0" and not args.wit_log),
             "ntt_roofline": roofline_ntt(ntt, peak, kind),
             "cpu_baseline": cpu,
             "clocks": clk,
@@ -651,11 +652,19 @@ def roofline_ntt(ntt, peak, kind):
 
 # DRAM bytes (read + write) per launch of the commitment kernel are not
 # measured live; the ncu summaries under profiles/ give them for named launches.
-CK_TRAFFIC_NOTE = "DRAM bytes per launch: see the ncu summary of ck_umma_kernel under profiles/"
+# DRAM bytes (read + write) of ck_umma_kernel per launch, mean over the eight
+# launches of one A0 proof, from one ncu capture of those launches
+# (dram__bytes_read.sum + dram__bytes_write.sum; command and per-launch values
+# in profiles/ck_umma_kernel_a0_round0.md).  The witness alone is 400 MB per
+# launch on average; the rest are key tiles that miss L2.
+CK_TRAFFIC_A0 = 653.8e6
+CK_TRAFFIC_NOTE = ("bytes per launch, mean over the 8 launches of one A0 proof (one ncu capture); "
+                   "algorithmic witness bytes 400 MB per launch")
 
 
-def roofline_ck(traced, peak_info, elapsed_ms):
-    # elapsed_ms: summed device time of the traced plain proofs
+def roofline_ck(traced, peak_info, elapsed_ms, a0):
+    # elapsed_ms: summed device time of the traced plain proofs; a0: the
+    # default A0 workload, the one the traffic capture covers
     """Dominant kernel of the prove: the tensor-core commitment product.  Work
     is counted as int8 operations (2 per byte-limb product) and set against
     the measured dense bf16 rate, the only tensor peak measured here."""
@@ -668,7 +677,8 @@ def roofline_ck(traced, peak_info, elapsed_ms):
     return {"kernel": "ck_umma_kernel (exact int8 limb-split commitment, tcgen05.mma kind::i8, TMEM)",
             "bound": "tensor",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_kind": kind, "traffic": None, "traffic_note": CK_TRAFFIC_NOTE,
+            "peak_kind": kind, "traffic": CK_TRAFFIC_A0 if a0 else None,
+            "traffic_note": CK_TRAFFIC_NOTE if a0 else "no capture for this workload",
             "launches": traced["launches"],
             "ms_per_launch": per_ms, "ops_per_launch": work,
             "share_of_plain_prove": traced["ms"] / elapsed_ms if elapsed_ms else None,
