@@ -199,6 +199,8 @@ static Shapes walk(const salsaa_params* p) {
       w += 1 + Sn * K * parts * d;
       K *= parts;
       if (K * width > S.max_d_rows_width) S.max_d_rows_width = K * width;
+    } else if (!p->folding && i > 0 && K * width > S.max_d_rows_width) {
+      S.max_d_rows_width = K * width;  // the joined witness moves to the decomposition buffers
     }
     if (K > MAX_WROWS) {
       S.why = "too many witness rows";
@@ -665,6 +667,20 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       pend_K = K;
       pending = true;
       cur += (u64)(ms + nsc) * K * d;
+    } else if (!P.folding && rd > 0) {
+      // the witness is last round's joined [folded, projected] rows, whose
+      // buffers this round's projection and fold overwrite: move it to the
+      // decomposition buffers, which a round without decomposition leaves free
+      for (u32 k = 0; k < K; k++) {
+        e = cudaMemcpyAsync(pr->Dc + (u64)k * width * d, Wc.p[k], width * d * sizeof(u64), cudaMemcpyDeviceToDevice,
+                            st);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(pr->Ds + (u64)k * width * d, Ws.p[k], width * d * sizeof(u64),
+                              cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: joined witness");
+      }
+      Wc = rows_of(pr->Dc, K, width, d);
+      Ws = rows_of(pr->Ds, K, width, d);
     }
     // norm_check_1 / norm_check_2 (x2) / norm_check_3 (x2), src/protocol.rs:206-259
     TRY(mark(pr, PH_NORM2));

@@ -16,6 +16,10 @@ SMALL = {
     "snark2_d512_q2": P.make_params(512, P.Q2, 3, 1 << 13, 2, False),
     "fold_d16": P.small_folding(d=16, log_len=11),
     "fold_d128": P.make_params(128, P.Q0, 5, 1 << 12, 1, True),
+    # a round without decomposition after a decomposed one: the joined witness
+    # is then read in slot form by the next round
+    "snark3_d128_parts121": P.make_params(128, P.Q0, 3, 1 << 14, 3, False, decomp_parts=[1, 2, 1]),
+    "snark3_d128_parts112": P.make_params(128, P.Q0, 3, 1 << 14, 3, False, decomp_parts=[1, 1, 2]),
 }
 
 
