@@ -229,8 +229,13 @@ static Shapes walk(const salsaa_params* p) {
     }
     if (K > S.max_rows) S.max_rows = (u32)K;
     const u64 cw = K * 256;
-    if (cw > width || width % cw || cw > CK_BLOCK) {
+    if (cw > width || width % cw) {
       S.why = "projection chunk width (rows*256) exceeds the witness width";
+      return S;
+    }
+    if (cw > CK_BLOCK) {
+      S.why = "projection chunk width (rows*256) above 2048: more than 8 witness rows after a split "
+              "(decomposition into more than 2 parts) is not supported";
       return S;
     }
     if (width > S.max_fp_width) S.max_fp_width = width;

@@ -63,6 +63,17 @@ def test_invalid_params_have_no_proof_size(gpu_lib):
     assert gpu_lib.salsaa_proof_size(ctypes.byref(p)) == 0
 
 
+def test_wide_decomposition_rejected(gpu_lib, oracle):
+    """More than two decomposition parts give projection chunks wider than
+    2048 (16 rows x 256 after the split): the library refuses the shape up
+    front (no proof size, no workspace), although the oracle proves it."""
+    p = P.make_params(128, P.Q0, 3, 1 << 15, 2, False, decomp_parts=[1, 4])
+    assert gpu_lib.salsaa_proof_size(ctypes.byref(p)) == 0
+    assert gpu_lib.salsaa_workspace_bytes(ctypes.byref(p)) == 0
+    ok = P.make_params(128, P.Q0, 3, 1 << 15, 2, False)
+    assert gpu_lib.salsaa_proof_size(ctypes.byref(ok)) == oracle.proof_size(ok)
+
+
 def test_host_scalar_symbols(gpu_lib, oracle):
     q = P.Q62
     for a, b in [(12345, 67890), (q - 1, q - 2), (2 ** 61, 3)]:

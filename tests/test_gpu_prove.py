@@ -20,6 +20,10 @@ SMALL = {
     # is then read in slot form by the next round
     "snark3_d128_parts121": P.make_params(128, P.Q0, 3, 1 << 14, 3, False, decomp_parts=[1, 2, 1]),
     "snark3_d128_parts112": P.make_params(128, P.Q0, 3, 1 << 14, 3, False, decomp_parts=[1, 1, 2]),
+    # two initial witness rows; more key rows than the tcgen05 key tiles hold
+    # (mma.sync commitment)
+    "snark2_d128_rep2": P.make_params(128, P.Q0, 3, 1 << 13, 2, False, init_wit_rep=2),
+    "snark2_d128_ms20": P.make_params(128, P.Q0, 20, 1 << 13, 2, False),
 }
 
 
