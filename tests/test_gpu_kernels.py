@@ -183,7 +183,8 @@ def _check_sumcheck(api, oracle, w, d, q, seed=99, rnd=3):
 
 
 @pytest.mark.parametrize("rows,n,d,q,bound", [(1, 1 << 15, 128, P.Q0, 1), (3, 1 << 16, 128, P.Q0, 1 << 24),
-                                              (2, 1 << 17, 64, P.Q1, 1 << 30), (1, 1 << 20, 128, P.Q0, 1 << 25)])
+                                              (2, 1 << 17, 64, P.Q1, 1 << 30), (1, 1 << 20, 128, P.Q0, 1 << 25),
+                                              (16, 1 << 15, 16, P.Q2, 1 << 12)])
 def test_sumcheck_small(api, oracle, rows, n, d, q, bound):
     """Small centred witnesses (ternary, decomposition digits): the first
     pass runs on the tensor cores through the groups' Gram matrices."""
