@@ -296,6 +296,9 @@ def run_ours(args):
     # here, where nothing else shares the GPU, so each launch's events bracket
     # that launch alone.
     plain = []
+    # latency mode: each round's projection runs beside the norm check
+    if args.plain_proofs:
+        slots[0].set_overlap(True)
     for i in range(args.plain_proofs):
         if i == 1:
             torch.cuda.synchronize()

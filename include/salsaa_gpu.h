@@ -155,6 +155,11 @@ int salsaa_prover_enqueue(salsaa_prover* pr, uint64_t seed, const uint64_t* d_wi
  * the slot's workspace, proves, and copies the proof to h_proof, all on the
  * slot's stream.  For overlap the host buffers should be page-locked. */
 int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof);
+/* No reference counterpart.  With on != 0 the slot's later proofs run each
+ * round's projection on a second stream beside the norm-check sumcheck
+ * (results unchanged): lower latency for a proof alone on the GPU, slightly
+ * lower throughput when many slots already fill it.  Off by default. */
+int salsaa_prover_set_overlap(salsaa_prover* pr, int on);
 /* 1 while the last enqueued proof runs, 0 when done, negative on error. */
 int salsaa_prover_query(salsaa_prover* pr);
 int salsaa_prover_sync(salsaa_prover* pr);

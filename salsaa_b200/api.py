@@ -161,6 +161,11 @@ class Prover:
         _check(lib().salsaa_prover_enqueue_host(self.h, seed, wp, ctypes.c_void_p(h_proof.ctypes.data)),
                "prover_enqueue_host")
 
+    def set_overlap(self, on=True):
+        """Run each round's projection beside the norm check (lower latency
+        for a proof alone on the GPU; off by default)."""
+        _check(lib().salsaa_prover_set_overlap(self.h, 1 if on else 0), "prover_set_overlap")
+
     def query(self):
         rc = lib().salsaa_prover_query(self.h)
         if rc < 0:

@@ -381,6 +381,9 @@ constexpr int MAX_EVENTS = 128;
 struct salsaa_prover {
   salsaa_ctx* ctx;
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;  // side stream: the projection runs beside the sumcheck
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool overlap = false;        // use the side stream (salsaa_prover_set_overlap)
   DevBuf mem;
   DevState* ds = nullptr;
   u64 *Dc = nullptr, *Ds = nullptr, *Fc = nullptr, *Fs = nullptr, *Pc = nullptr, *Ps = nullptr;
@@ -449,11 +452,17 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
   const u64 d = c->d, L = c->L;
   auto fail = [&](int rc) {
     pr->mem.release();
+    if (pr->ev_fork) cudaEventDestroy(pr->ev_fork);
+    if (pr->ev_join) cudaEventDestroy(pr->ev_join);
+    if (pr->st2) cudaStreamDestroy(pr->st2);
     if (pr->st) cudaStreamDestroy(pr->st);
     delete pr;
     return rc;
   };
   e = cudaStreamCreateWithFlags(&pr->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&pr->st2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pr->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pr->ev_join, cudaEventDisableTiming);
   if (e != cudaSuccess) return fail(salsaa_set_cuda_error(e, "prover_create: stream"));
   for (int i = 0; i < MAX_EVENTS; i++) {
     e = cudaEventCreate(&pr->ev[i]);
@@ -555,11 +564,20 @@ extern "C" void salsaa_prover_destroy(salsaa_prover* pr) {
   if (pr->own_proof) cudaFree(pr->own_proof);
   if (pr->header_pinned) cudaFreeHost(pr->header_pinned);
   for (int i = 0; i < MAX_EVENTS; i++) cudaEventDestroy(pr->ev[i]);
+  if (pr->ev_fork) cudaEventDestroy(pr->ev_fork);
+  if (pr->ev_join) cudaEventDestroy(pr->ev_join);
+  if (pr->st2) cudaStreamDestroy(pr->st2);
   if (pr->st) cudaStreamDestroy(pr->st);
   delete pr;
 }
 
 extern "C" void* salsaa_prover_stream(salsaa_prover* pr) { return pr ? (void*)pr->st : nullptr; }
+
+extern "C" int salsaa_prover_set_overlap(salsaa_prover* pr, int on) {
+  if (!pr) return salsaa_set_error(-1, "prover_set_overlap: null argument");
+  pr->overlap = on != 0;
+  return 0;
+}
 
 __global__ void set_seed_kernel(DevState* ds, u64 seed) { ds->seed = seed; }
 
@@ -687,6 +705,52 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       Wc = rows_of(pr->Dc, K, width, d);
       Ws = rows_of(pr->Ds, K, width, d);
     }
+    // split (src/subroutines/split.rs:45-76): rows L_0..L_{K-1}, R_0..R_{K-1},
+    // as views; the sumcheck below still reads the unsplit rows
+    RowSet Wc2 = Wc, Ws2 = Ws;
+    u32 K2 = K;
+    u64 width2 = width;
+    if (!P.folding) {
+      const u64 hw = width / 2;
+      for (u32 k = 0; k < K; k++) {
+        Wc2.p[k] = Wc.p[k];
+        Wc2.p[K + k] = Wc.p[k] + hw * d;
+        Ws2.p[k] = Ws.p[k];
+        Ws2.p[K + k] = Ws.p[k] + hw * d;
+      }
+      K2 = 2 * K;
+      width2 = hw;
+    }
+    // project (src/subroutines/project.rs:50-103): it needs the split witness
+    // and its own challenges only, so with overlap on it runs on the side
+    // stream beside the norm check and joins before the merged commitment
+    cudaStream_t ps = pr->overlap ? pr->st2 : st;
+    if (pr->overlap) {
+      e = cudaEventRecord(pr->ev_fork, st);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(pr->st2, pr->ev_fork, 0);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: fork");
+    }
+    {
+      const u32 cw = K2 * 256;
+      u64* cj = pr->row_cj + (u64)rd * CK_BLOCK;
+      TRY(launch_proj_tables(pr->ds, rd, cw, pr->pmask, pr->nmask, pr->Jm, cj, q, ps, pr->Jc));
+      TRY(launch_project(Wc2, K2, width2, d, q, pr->pmask, pr->nmask, pr->Jm, pr->ds, pr->Pc, ps, pr->Jc));
+    }
+    // the joined witness [folded, projected] is decomposed next: the two
+    // transforms that read P and write the folded row collect the OR of its
+    // centred magnitudes, so the decomposition needs no pass of its own
+    const bool next_decomp =
+        P.folding || (rd + 1 < P.nof_rounds && P.decomp_parts[rd + 1 < 12 ? rd + 1 : 11] > 1);
+    u64* mag = nullptr;
+    if (next_decomp && didx < 16 && ntt_mag_ok(pr->Pc, pr->Ps, T, true) && ntt_mag_ok(pr->Fs, pr->Fc, T, true)) {
+      mag = &pr->ds->bw_or[didx];
+      e = cudaMemsetAsync(mag, 0, sizeof(u64), ps);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: magnitude OR");
+    }
+    TRY(ntt_launch(pr->Pc, pr->Ps, width2, T, true, false, ps, mag));
+    if (pr->overlap && (e = cudaEventRecord(pr->ev_join, ps)) != cudaSuccess)
+      return salsaa_set_cuda_error(e, "enqueue: join");
+
     // norm_check_1 / norm_check_2 (x2) / norm_check_3 (x2), src/protocol.rs:206-259
     TRY(mark(pr, PH_NORM2));
     const u64 nr = ilog2u(width * d);
@@ -702,40 +766,13 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     TRY(launch_norm3(pr->sc.cap, K, (u32)nr, T, M, pr->ds, rd, rhs0, rhs1, pr->row_base + (u64)nsc * d,
                      pr->row_base + (u64)(nsc + 1) * d, st));
     nsc += 2;
-    if (!P.folding) {
-      // split (src/subroutines/split.rs:45-76): rows L_0..L_{K-1}, R_0..R_{K-1}
-      TRY(mark(pr, PH_SPLIT));
-      const u64 hw = width / 2;
-      RowSet nc{}, ns{};
-      for (u32 k = 0; k < K; k++) {
-        nc.p[k] = Wc.p[k];
-        nc.p[K + k] = Wc.p[k] + hw * d;
-        ns.p[k] = Ws.p[k];
-        ns.p[K + k] = Ws.p[k] + hw * d;
-      }
-      Wc = nc;
-      Ws = ns;
-      K *= 2;
-      width = hw;
-    }
-    // project (src/subroutines/project.rs:50-103)
-    TRY(mark(pr, PH_PROJ));
-    const u32 cw = K * 256;
-    u64* cj = pr->row_cj + (u64)rd * CK_BLOCK;
-    TRY(launch_proj_tables(pr->ds, rd, cw, pr->pmask, pr->nmask, pr->Jm, cj, q, st, pr->Jc));
-    TRY(launch_project(Wc, K, width, d, q, pr->pmask, pr->nmask, pr->Jm, pr->ds, pr->Pc, st, pr->Jc));
-    // the joined witness [folded, projected] is decomposed next: the two
-    // transforms that read P and write the folded row collect the OR of its
-    // centred magnitudes, so the decomposition needs no pass of its own
-    const bool next_decomp =
-        P.folding || (rd + 1 < P.nof_rounds && P.decomp_parts[rd + 1 < 12 ? rd + 1 : 11] > 1);
-    u64* mag = nullptr;
-    if (next_decomp && didx < 16 && ntt_mag_ok(pr->Pc, pr->Ps, T, true) && ntt_mag_ok(pr->Fs, pr->Fc, T, true)) {
-      mag = &pr->ds->bw_or[didx];
-      e = cudaMemsetAsync(mag, 0, sizeof(u64), st);
-      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "enqueue: magnitude OR");
-    }
-    TRY(ntt_launch(pr->Pc, pr->Ps, width, T, true, false, st, mag));
+    Wc = Wc2;
+    Ws = Ws2;
+    K = K2;
+    width = width2;
+    TRY(mark(pr, P.folding ? PH_PROJ : PH_SPLIT));
+    if (pr->overlap && (e = cudaStreamWaitEvent(st, pr->ev_join, 0)) != cudaSuccess)
+      return salsaa_set_cuda_error(e, "enqueue: join");
     RowSet Pr = rows_of(pr->Ps, 1, width, d);
     RowSet Prc = rows_of(pr->Pc, 1, width, d);
     const u32 S = ms + nsc;

@@ -105,3 +105,19 @@ def test_full_size_proof_verifies(api, oracle, name):
     bad = proof.copy()
     bad[8 * 100] ^= 4
     assert oracle.verify(p, 1, 2, bad) != 0
+
+
+@pytest.mark.parametrize("name", ["snark2_d128", "snark3_d128_parts121", "fold_d128"])
+def test_overlap_slot_matches_oracle(api, oracle, name):
+    """A slot running the projection beside the norm check makes the same bytes."""
+    import torch
+    p = SMALL[name]
+    ctx = api.Context(p, crs_seed=7)
+    pr = api.Prover(ctx)
+    pr.set_overlap(True)
+    buf = torch.empty(ctx.proof_bytes // 8, dtype=torch.int64, device="cuda")
+    for seed in (11, 12):
+        pr.enqueue(seed, buf)
+        pr.sync()
+        assert np.array_equal(api.to_host(buf).view(np.uint8), oracle.prove(p, 7, seed)[1])
+    pr.close()
