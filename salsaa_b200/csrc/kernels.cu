@@ -2014,6 +2014,15 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   cudaError_t e =
       cudaMemsetAsync(a.acc, 0, (u64)(a.nck + a.nsc) * a.rows * d * sizeof(u64), st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit memset");
+  // statement rows: on the side stream when given (they write their own
+  // accumulator rows, after the memset), joined before the finalisation
+  const bool side = a.st2 && a.nck && a.nsc;
+  cudaStream_t ss = side ? a.st2 : st;
+  if (side) {
+    e = cudaEventRecord(a.ev_fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ss, a.ev_fork, 0);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit: fork");
+  }
   if (a.nck && ck_umma_ok(a, n)) {
     // element block per CTA: a whole key-table block (one epilogue per block),
     // halved while the grid would not fill the GPU
@@ -2041,7 +2050,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   }
   if (a.nsc) {
     dim3 gt((Bw + nhi + 255) / 256, a.nsc);
-    sc_tables_kernel<<<gt, 256, 0, st>>>(a.sc_desc_dev, a.nsc, a.width, Bw, nhi, M, ds, a.sc_lo, a.sc_hi);
+    sc_tables_kernel<<<gt, 256, 0, ss>>>(a.sc_desc_dev, a.nsc, a.width, Bw, nhi, M, ds, a.sc_lo, a.sc_hi);
     int rc = check_launch("sc_tables");
     if (rc) return rc;
     u64* acc_sc = a.acc + (u64)a.nck * a.rows * d;
@@ -2068,17 +2077,17 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
         periodic_done = true;
       }
       rc = launch_sc_umma(wsrc, a.rows, a.width, d, Bw, nhi, gl, a.sc_lo, a.sc_hi, M, acc_sc, plain, a.sc_img,
-                          a.sc_flags, a.sc_flag_cap, st);
+                          a.sc_flags, a.sc_flag_cap, ss);
       if (rc) return rc;
       if (!periodic_done && ol.n <= SC_UMMA_MAX_ROWS) {
         // more rows than one pass holds: the periodic / all-ones rows in a second pass
         rc = launch_sc_umma(wsrc, a.rows, a.width, d, Bw, nhi, ol, a.sc_lo, a.sc_hi, M, acc_sc, plain, a.sc_img,
-                            a.sc_flags, a.sc_flag_cap, st);
+                            a.sc_flags, a.sc_flag_cap, ss);
         if (rc) return rc;
         periodic_done = true;
       }
     } else {
-      launch_sc_pass(a, wsrc, a.width, tl, true, d, Bw, nhi, (u32)CH, M, plain, acc_sc, st);
+      launch_sc_pass(a, wsrc, a.width, tl, true, d, Bw, nhi, (u32)CH, M, plain, acc_sc, ss);
       rc = check_launch("sc_commit (tensor rows)");
       if (rc) return rc;
     }
@@ -2087,7 +2096,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
       RowSet u = wsrc;
       if (nhi > 1) {
         if (!a.colsum || a.rows > a.colsum_rows) return salsaa_set_error(-2, "commit: column-sum scratch too small");
-        colsum_kernel<<<grid_1d((u64)a.rows * Bw * d, 256), 256, 0, st>>>(wsrc, a.rows, a.width, Bw, d, M,
+        colsum_kernel<<<grid_1d((u64)a.rows * Bw * d, 256), 256, 0, ss>>>(wsrc, a.rows, a.width, Bw, d, M,
                                                                          a.colsum);
         rc = check_launch("colsum");
         if (rc) return rc;
@@ -2096,18 +2105,23 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
       u64 CHu = Bw / 64;
       if (CHu < 16) CHu = 16;
       if (CHu > Bw) CHu = Bw;
-      launch_sc_pass(a, u, Bw, ol, false, d, Bw, nhi, (u32)CHu, M, plain, acc_sc, st);
+      launch_sc_pass(a, u, Bw, ol, false, d, Bw, nhi, (u32)CHu, M, plain, acc_sc, ss);
       rc = check_launch("sc_commit (periodic rows)");
       if (rc) return rc;
     }
     if (a.coef_sc) {
       const u64 cnt = (u64)a.nsc * a.rows;
-      reduce_inplace_kernel<<<grid_1d(cnt * d, 256), 256, 0, st>>>(acc_sc, cnt * d, M);
+      reduce_inplace_kernel<<<grid_1d(cnt * d, 256), 256, 0, ss>>>(acc_sc, cnt * d, M);
       rc = check_launch("reduce");
       if (rc) return rc;
-      rc = ntt_launch(acc_sc, acc_sc, cnt, T, true, false, st);
+      rc = ntt_launch(acc_sc, acc_sc, cnt, T, true, false, ss);
       if (rc) return rc;
     }
+  }
+  if (side) {
+    e = cudaEventRecord(a.ev_join, ss);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, a.ev_join, 0);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit: join");
   }
   const u64 tot = (u64)(a.nck + a.nsc) * a.rows * n;
   commit_finalize_kernel<<<grid_1d(tot, 256), 256, 0, st>>>(a.acc, a.nck, a.nsc, a.rows, n, M, T.zeta,

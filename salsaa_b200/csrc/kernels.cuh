@@ -159,6 +159,8 @@ struct CommitArgs {
   uint8_t* sc_img;   // scratch for the tcgen05 TENSOR-row pass (SC_IMG_BYTES), or null
   u32* sc_flags;     // scratch: one word per CTA of that pass
   u64 sc_flag_cap;   // words of sc_flags
+  cudaStream_t st2;  // optional: statement rows on this stream beside the key rows
+  cudaEvent_t ev_fork, ev_join;
   const u64* const* sc_base_dev;     // nsc ring bases (slot form) or null (= 1)
   u64* sc_lo;        // scratch nsc x CK_BLOCK
   u64* sc_hi;        // scratch nsc x max(width / CK_BLOCK, 1)

@@ -618,6 +618,11 @@ static int commit_rows_slot(salsaa_prover* pr, const RowSet& ws, const RowSet* w
     a.sc_flags = pr->sc_flags;
     a.sc_flag_cap = pr->sc_flag_words;
   }
+  if (pr->overlap) {
+    a.st2 = pr->st2;
+    a.ev_fork = pr->ev_fork;
+    a.ev_join = pr->ev_join;
+  }
   a.out_slot = pr->cout;
   return launch_commit(a, *c->T, c->M, pr->ds, pr->st);
 }
