@@ -206,6 +206,10 @@ int salsaa_server_limit(salsaa_server* s, uint32_t max_inflight);
 int salsaa_server_progress(salsaa_server* s);
 /* 1 pending, 0 done (latency from submit and from admission, ms), < 0 failed. */
 int salsaa_server_poll(salsaa_server* s, uint64_t ticket, double* latency_ms, double* run_ms);
+/* Withdraw a queued request: 0 = removed (the ticket is forgotten and d_proof
+ * is free again), 1 = already admitted (it runs to completion; poll it as
+ * usual), < 0 = unknown ticket.  Proofs in flight are never interrupted. */
+int salsaa_server_cancel(salsaa_server* s, uint64_t ticket);
 void salsaa_server_destroy(salsaa_server* s);
 
 /* ---- subroutine-level entry points (device pointers, cudaStream_t) ---- */

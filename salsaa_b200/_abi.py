@@ -87,6 +87,7 @@ DEVICE_SYMBOLS = {
     "salsaa_server_limit": (INT, [VP, ctypes.c_uint32]),
     "salsaa_server_progress": (INT, [VP]),
     "salsaa_server_poll": (INT, [VP, U64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "salsaa_server_cancel": (INT, [VP, U64]),
     "salsaa_server_destroy": (None, [VP]),
 }
 

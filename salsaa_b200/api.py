@@ -353,6 +353,13 @@ class Server:
         _check(rc, "server_poll")
         return lat.value, run.value
 
+    def cancel(self, ticket):
+        """True if the queued request was withdrawn, False if it already runs."""
+        rc = lib().salsaa_server_cancel(self.h, ticket)
+        if rc < 0:
+            _check(rc, "server_cancel")
+        return rc == 0
+
     def close(self):
         if self.h:
             lib().salsaa_server_destroy(self.h)

@@ -221,6 +221,25 @@ extern "C" int salsaa_server_poll(salsaa_server* s, uint64_t ticket, double* lat
   return rc;
 }
 
+// Withdraw a request that is still queued: it is forgotten (a later poll
+// reports an unknown ticket) and its proof buffer is the caller's again.
+// A request already admitted keeps running, since its kernels are in flight
+// on the slot's stream; it is reported (1) and completes as usual.
+extern "C" int salsaa_server_cancel(salsaa_server* s, uint64_t ticket) {
+  if (!s) return salsaa_set_error(-1, "server_cancel: null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return salsaa_set_error(-1, "server_cancel: unknown ticket");
+  if (it->second.state != RQ_QUEUED) return 1;
+  for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
+    if (*q == ticket) {
+      s->queue.erase(q);
+      break;
+    }
+  s->reqs.erase(it);
+  return 0;
+}
+
 extern "C" void salsaa_server_destroy(salsaa_server* s) {
   if (!s) return;
   cudaSetDevice(s->device);

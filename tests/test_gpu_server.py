@@ -71,3 +71,37 @@ def test_budget_enforced(api):
     with pytest.raises(SalsaaError):
         srv.register(MIX["snark2_d16"], slots=1)
     srv.close()
+
+
+def test_cancel_queued_request(api, cuda):
+    from salsaa_b200.api import SalsaaError
+    torch = cuda
+    p = MIX["snark2_d16"]
+    srv = api.Server(hbm_budget_bytes=16 << 30)
+    srv.limit(1)
+    sid = srv.register(p, crs_seed=7, slots=1)
+    bufs = [torch.zeros(api.proof_size(p) // 8, dtype=torch.int64, device="cuda") for _ in range(4)]
+    tickets = [srv.submit(sid, 2000 + i, b) for i, b in enumerate(bufs)]
+    assert srv.progress() == 4  # one admitted, three queued
+    assert srv.cancel(tickets[0]) is False  # admitted: runs to completion
+    assert srv.cancel(tickets[2]) is True  # queued: withdrawn and forgotten
+    with pytest.raises(SalsaaError):
+        srv.poll(tickets[2])
+    with pytest.raises(SalsaaError):
+        srv.cancel(tickets[2])
+    left = [t for t in tickets if t != tickets[2]]
+    done = set()
+    while len(done) < len(left):
+        srv.progress()
+        for t in left:
+            if t not in done and srv.poll(t) is not None:
+                done.add(t)
+    torch.cuda.synchronize()
+    alone = api.Context(p, crs_seed=7)
+    for i, b in enumerate(bufs):
+        got = api.to_host(b).view(np.uint8)
+        if i == 2:
+            assert not got.any()  # never written
+        else:
+            assert np.array_equal(got, alone.prove(2000 + i)), i
+    srv.close()
