@@ -19,7 +19,10 @@
  *
  * All arithmetic is exact modulo q (q < 2^62; the protocol moduli are 50-bit).
  * Randomness (CRS, witness, challenges) comes from a counter-based PRF keyed by
- * the caller's seeds; see DESIGN.md for the stream and the proof byte layout.
+ * the caller's seeds, one domain per (kind, round, repetition).  A proof is the
+ * prover's messages in protocol order as canonical little-endian u64 words in
+ * coefficient form, after an 8-word header (magic "SALSAAP1", d, q,
+ * module_size, wit_len, init_wit_rep, nof_rounds, folding).
  */
 #ifndef SALSAA_GPU_H
 #define SALSAA_GPU_H
@@ -155,6 +158,14 @@ int salsaa_prover_enqueue(salsaa_prover* pr, uint64_t seed, const uint64_t* d_wi
  * the slot's workspace, proves, and copies the proof to h_proof, all on the
  * slot's stream.  For overlap the host buffers should be page-locked. */
 int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof);
+/* Short-witness variant of salsaa_prover_enqueue_host: h_witness holds the
+ * init_wit_rep x wit_len x d coefficients as centred signed bytes (value v
+ * stands for v mod q), one byte each instead of eight, so the upload moves an
+ * eighth of the bytes; the slot expands them on the device.  The witness of
+ * the reference's relation is short (random_bounded, ternary in every
+ * parameter set), so it always fits.  Proof bytes equal those of
+ * salsaa_prover_enqueue_host for the same residues. */
+int salsaa_prover_enqueue_host_i8(salsaa_prover* pr, uint64_t seed, const int8_t* h_witness, uint8_t* h_proof);
 /* No reference counterpart.  With on != 0 the slot's later proofs run each
  * round's projection on a second stream beside the norm-check sumcheck
  * (results unchanged): lower latency for a proof alone on the GPU, slightly

@@ -61,6 +61,7 @@ DEVICE_SYMBOLS = {
     "salsaa_prover_stream": (VP, [VP]),
     "salsaa_prover_enqueue": (INT, [VP, U64, VP, VP]),
     "salsaa_prover_enqueue_host": (INT, [VP, U64, VP, VP]),
+    "salsaa_prover_enqueue_host_i8": (INT, [VP, U64, VP, VP]),
     "salsaa_prover_query": (INT, [VP]),
     "salsaa_prover_sync": (INT, [VP]),
     "salsaa_prover_timing": (INT, [VP, ctypes.POINTER(SalsaaTiming)]),

@@ -161,6 +161,15 @@ class Prover:
         _check(lib().salsaa_prover_enqueue_host(self.h, seed, wp, ctypes.c_void_p(h_proof.ctypes.data)),
                "prover_enqueue_host")
 
+    def enqueue_host_i8(self, seed, h_proof, h_witness):
+        """As enqueue_host, with the short witness as centred int8
+        coefficients (one byte each on the bus instead of eight)."""
+        if h_witness.dtype != np.int8:
+            raise TypeError("enqueue_host_i8: witness must be int8")
+        _check(lib().salsaa_prover_enqueue_host_i8(self.h, seed, ctypes.c_void_p(h_witness.ctypes.data),
+                                                   ctypes.c_void_p(h_proof.ctypes.data)),
+               "prover_enqueue_host_i8")
+
     def set_overlap(self, on=True):
         """Run each round's projection beside the norm check (lower latency
         for a proof alone on the GPU; off by default)."""

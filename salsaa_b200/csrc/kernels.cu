@@ -141,6 +141,34 @@ int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState
   return check_launch("gen_witness");
 }
 
+// Short witness sent as centred int8 coefficients: out[i] = in[i] mod q.
+// Four coefficients per thread step (one 4-byte load, two 16-byte stores).
+__global__ void expand_i8_kernel(const int8_t* __restrict__ in, u64 n, u64 q, u64* __restrict__ out) {
+  const u64 stride = (u64)gridDim.x * blockDim.x, n4 = n / 4;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += stride) {
+    const u32 w = __ldg((const u32*)in + t);
+    u64 e[4];
+#pragma unroll
+    for (u32 b = 0; b < 4; b++) {
+      const int s = (int8_t)(w >> (8 * b));
+      e[b] = s < 0 ? q - (u64)(-s) : (u64)s;
+    }
+    ulonglong2* o = (ulonglong2*)(out + 4 * t);
+    o[0] = make_ulonglong2(e[0], e[1]);
+    o[1] = make_ulonglong2(e[2], e[3]);
+  }
+  for (u64 i = 4 * n4 + (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int s = in[i];
+    out[i] = s < 0 ? q - (u64)(-s) : (u64)s;
+  }
+}
+int launch_expand_i8(const int8_t* in, u64 n, u64 q, u64* out, cudaStream_t st) {
+  if (!n) return 0;
+  if ((uintptr_t)in % 4 || (uintptr_t)out % 16) return salsaa_set_error(-2, "expand_i8: misaligned buffers");
+  expand_i8_kernel<<<grid_1d((n + 3) / 4, 256), 256, 0, st>>>(in, n, q, out);
+  return check_launch("expand_i8");
+}
+
 __global__ void fill_kernel(u64* p, u64 n, u64 v) {
   for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (u64)gridDim.x * blockDim.x) p[t] = v;
 }

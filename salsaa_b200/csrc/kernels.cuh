@@ -86,6 +86,7 @@ int launch_nc_gram_sums(const u64* gram, u32 rows, const ModQ& M, const DevState
 // Nonzero (and the last error set) when a tensor-core kernel's bounded wait gave up.
 int tc_error_check();
 int launch_gen_witness(u64* w, u32 rows, u64 width, u32 d, u64 q, const DevState* ds, cudaStream_t st);
+int launch_expand_i8(const int8_t* in, u64 n, u64 q, u64* out, cudaStream_t st);
 int launch_fill(u64* p, u64 n, u64 v, cudaStream_t st);
 // r[i] = r[i] * b[i] mod q (canonical inputs)
 int launch_pointwise_mul(u64* r, const u64* b, u64 n, u64 q, cudaStream_t st);

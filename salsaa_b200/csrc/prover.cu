@@ -935,6 +935,33 @@ extern "C" int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, cons
   return 0;
 }
 
+// The signed bytes are staged in the slot-form witness buffer (an eighth of
+// its size), expanded into the coefficient-form buffer, and overwritten by
+// the proof's first forward transform, all in stream order.
+extern "C" int salsaa_prover_enqueue_host_i8(salsaa_prover* pr, uint64_t seed, const int8_t* h_witness,
+                                             uint8_t* h_proof) {
+  if (!pr || !h_proof || !h_witness) return salsaa_set_error(-1, "prover_enqueue_host_i8: null argument");
+  salsaa_ctx* c = pr->ctx;
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: cudaSetDevice");
+  const u64 need = c->S.proof_words * 8;
+  if (!pr->own_proof) {
+    e = cudaMalloc(&pr->own_proof, need);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: proof buffer");
+  }
+  const u64 n = c->P.init_wit_rep * c->L * c->d;
+  int8_t* stage = (int8_t*)pr->Ds;
+  e = cudaMemcpyAsync(stage, h_witness, n, cudaMemcpyHostToDevice, pr->st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: witness upload");
+  pr->last_rc = launch_expand_i8(stage, n, c->P.q, pr->Dc, pr->st);
+  if (pr->last_rc) return pr->last_rc;
+  pr->last_rc = enqueue_impl(pr, seed, pr->Dc, (u64*)pr->own_proof);
+  if (pr->last_rc) return pr->last_rc;
+  e = cudaMemcpyAsync(h_proof, pr->own_proof, need, cudaMemcpyDeviceToHost, pr->st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: proof download");
+  return 0;
+}
+
 extern "C" int salsaa_prover_query(salsaa_prover* pr) {
   if (!pr) return salsaa_set_error(-1, "prover_query: null argument");
   if (pr->last_rc) return pr->last_rc;

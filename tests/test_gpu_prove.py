@@ -57,6 +57,26 @@ def test_explicit_witness(api, oracle):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("name,lo,hi", [("snark2_d16", -1, 2), ("snark2_d128_rep2", -128, 128),
+                                        ("fold_d16", -128, 128)])
+def test_int8_witness_upload(api, oracle, name, lo, hi):
+    """salsaa_prover_enqueue_host_i8: the witness as centred signed bytes gives
+    the oracle's proof of the same residues."""
+    p = SMALL[name]
+    rng = np.random.default_rng(5)
+    w8 = rng.integers(lo, hi, size=(p.init_wit_rep, p.wit_len, p.d)).astype(np.int8)
+    w = np.where(w8 < 0, p.q + w8.astype(np.int64), w8).astype(np.uint64)
+    rc, want, _ = oracle.prove(p, 3, 4, witness=w)
+    assert rc == 0
+    ctx = api.Context(p, crs_seed=3)
+    pr = api.Prover(ctx)
+    got = np.zeros(ctx.proof_bytes, dtype=np.uint8)
+    pr.enqueue_host_i8(4, got, np.ascontiguousarray(w8.reshape(-1)))
+    pr.sync()
+    assert np.array_equal(got, want)
+    pr.close()
+
+
 @pytest.mark.parametrize("bound", [0, 1 << 22, 1 << 30])
 def test_large_witness_d128(api, oracle, bound):
     """Witness values beyond the tensor-core paths' byte limbs (uniform mod q,
