@@ -156,7 +156,9 @@ int salsaa_prover_enqueue(salsaa_prover* pr, uint64_t seed, const uint64_t* d_wi
 /* Host-buffer variant of salsaa_prover_enqueue, still asynchronous: copies
  * h_witness (init_wit_rep x wit_len x d words; NULL = sample from seed) to
  * the slot's workspace, proves, and copies the proof to h_proof, all on the
- * slot's stream.  For overlap the host buffers should be page-locked. */
+ * slot's stream.  For overlap the host buffers should be page-locked; both
+ * must then stay valid, and the witness unchanged, until salsaa_prover_query
+ * reports the proof done (or salsaa_prover_sync returns). */
 int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, const uint64_t* h_witness, uint8_t* h_proof);
 /* Short-witness variant of salsaa_prover_enqueue_host: h_witness holds the
  * init_wit_rep x wit_len x d coefficients as centred signed bytes (value v
