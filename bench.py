@@ -17,9 +17,10 @@ are independent, so this is replicas with no collective on the data path;
 the timed region is bracketed by barriers and the max over ranks is used.
 
 --impl reference times the CPU implementation of the same workload on this
-host's cores (the C restatement under oracle/, since the Rust + Intel HEXL
-reference cannot be built here) on a bounded sample: the A0 shape with
-WIT_LEN=2^15 and 4 rounds, scaled by 16 (prover work is linear in WIT_LEN).
+host's cores: the C restatement under oracle/ (the Rust + Intel HEXL reference
+cannot be built here).  Every timed step is one full A0 proof with all host
+threads; the warm-up steps prove a small instance of the same shape
+(WIT_LEN=2^13, 2 rounds) so the warm-up does not double the run.
 """
 import argparse
 import json
@@ -36,11 +37,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PRESET = "A0"
-CPU_SAMPLE_LOG_LEN = 15
-CPU_SAMPLE_ROUNDS = 4
-CPU_SCALE = 1 << (19 - CPU_SAMPLE_LOG_LEN)
 WORKLOAD = ("A0 SNARK prove: d=128, q=1125899904679937, module_size=12, wit_len=2^19, 8 rounds, "
             "ternary witness")
+# The statement every arm proves once and compares with the committed oracle
+# digest (tests/golden/proof_digests.json): A0 with CRS seed 1 and seed 2.
+DIGEST_CRS_SEED, DIGEST_SEED = 1, 2
 
 
 def parse():
@@ -84,50 +85,79 @@ def measured_peaks(tensor=False):
 
 
 # ---------------------------------------------------------------------------
-# CPU leg: the oracle port on a bounded sample
+# CPU legs: the oracle port
 # ---------------------------------------------------------------------------
-def cpu_sample_seconds(threads):
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from salsaa_b200 import params as P
-    p = P.make_params(128, P.Q0, 12, 1 << CPU_SAMPLE_LOG_LEN, CPU_SAMPLE_ROUNDS, False)
+    return O
+
+
+def committed_digest(name=PRESET):
+    """(crs_seed, seed, sha256) of the committed oracle proof of preset `name`."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "proof_digests.json")) as f:
+            g = json.load(f)[name]
+        return g["crs_seed"], g["seed"], g["sha256"]
+    except Exception:
+        return None
+
+
+def cpu_prove_seconds(params, seed, threads):
+    """Wall time of one oracle proof (with all `threads`) and its SHA-256."""
+    import hashlib
+    O = _oracle()
     t0 = time.perf_counter()
-    rc, _, _ = O.prove(p, 1, 2, nthreads=threads)
+    rc, proof, _ = O.prove(params, DIGEST_CRS_SEED, seed, nthreads=threads)
     el = time.perf_counter() - t0
     if rc:
         raise RuntimeError("oracle prove failed: %d" % rc)
-    return el
+    return el, hashlib.sha256(proof.tobytes()).hexdigest()
 
 
 def cpu_baseline(threads):
-    el = cpu_sample_seconds(threads)
-    return {"value": 1.0 / (el * CPU_SCALE), "unit": "proofs/s", "cores": threads, "kind": "port",
-            "sample": "A0 shape with wit_len=2^%d and %d rounds (1/%d of the witness), %.2f s, scaled x%d"
-                      % (CPU_SAMPLE_LOG_LEN, CPU_SAMPLE_ROUNDS, CPU_SCALE, el, CPU_SCALE)}
+    """One full A0 proof on the host cores (the same statement as the digest)."""
+    from salsaa_b200 import params as P
+    el, _ = cpu_prove_seconds(P.preset(PRESET), DIGEST_SEED, threads)
+    return {"value": 1.0 / el, "unit": "proofs/s", "cores": threads, "kind": "port",
+            "sample": "one full A0 proof (wit_len=2^19, 8 rounds), %.2f s wall, oracle port with %d threads"
+                      % (el, threads)}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    from salsaa_b200 import params as P
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_sample_seconds(threads)
-    times = [cpu_sample_seconds(threads) for _ in range(args.steps)]
-    tot = sum(times) * CPU_SCALE
-    value = args.steps / tot
+    small = P.make_params(128, P.Q0, 12, 1 << 13, 2, False)
+    for w in range(args.warmup):
+        cpu_prove_seconds(small, 100 + w, threads)
+    full = P.preset(PRESET)
+    times, first_sha = [], None
+    for s in range(args.steps):
+        el, h = cpu_prove_seconds(full, DIGEST_SEED + s, threads)
+        times.append(el)
+        if s == 0:
+            first_sha = h
+    tot = sum(times)
+    value = args.steps / tot if tot else None
+    dg = committed_digest()
     line = {
         "impl": "reference", "metric": "proofs/s", "value": value, "unit": "proofs/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1000.0 * tot / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64 mod q", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "batch": 1, "parallelism": "cpu threads %d" % threads},
+        "config": {"workload": WORKLOAD, "batch": 1, "parallelism": "cpu threads %d" % threads,
+                   "warmup_workload": "A0 shape at wit_len=2^13, 2 rounds"},
         "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port",
-                         "sample": "A0 shape with wit_len=2^%d and %d rounds per step, scaled x%d"
-                                   % (CPU_SAMPLE_LOG_LEN, CPU_SAMPLE_ROUNDS, CPU_SCALE)},
+                         "sample": "each step one full A0 proof (wit_len=2^19, 8 rounds), oracle port, "
+                                   "%d threads" % threads},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "p50_ms": 1000.0 * statistics.median(times) * CPU_SCALE,
-        "p99_ms": 1000.0 * max(times) * CPU_SCALE,
+        "p50_ms": 1000.0 * statistics.median(times) if times else None,
+        "p99_ms": 1000.0 * float(np.percentile(times, 99)) if times else None,
+        "proof_digest": {"crs_seed": DIGEST_CRS_SEED, "seed": DIGEST_SEED, "sha256": first_sha,
+                         "equals_committed": (dg is not None and first_sha == dg[2]) if first_sha else None},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -281,16 +311,24 @@ def run_ours(args):
     value = total / (elapsed_ms / 1000.0)
     timing = slots[0].timing()
 
-    # correctness spot check of the last batch: first proof verifies on the CPU
-    check = None
+    # correctness spot checks after the timed region: the last batch's first
+    # proof verifies on the CPU, and the committed oracle digest's statement
+    # (witness sampled from its seed) gives the same proof bytes here
+    check = digest_check = None
     if rank == 0 and args.steps > 0:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
         try:
-            import oracle as O
+            O = _oracle()
             pb = api.to_host(proofs[0]).view(np.uint8)
             check = O.verify(params, 1, replicas.proof_seed(rank, args.steps - 1, 0, S), pb) == 0
         except Exception as e:  # the checker is optional here; tests own parity
             check = "not run: %s" % e
+        dg = committed_digest()
+        if dg and args.preset == PRESET and not args.wit_log:
+            import hashlib
+            slots[0].enqueue(seed=dg[1], d_proof=proofs[0])
+            slots[0].sync()
+            got = hashlib.sha256(api.to_host(proofs[0]).tobytes()).hexdigest()
+            digest_check = {"crs_seed": dg[0], "seed": dg[1], "sha256": got, "equals_committed": got == dg[2]}
 
     # plain path: one proof at a time on one slot.  First with every kernel on
     # the slot's stream: the per-kernel trace runs there, where nothing else
@@ -314,7 +352,9 @@ def run_ours(args):
         return out
 
     serial = plain_run(False, True)
-    traced = trace_read("ck_umma_kernel") if args.plain_proofs > 1 else None
+    traced = None
+    if args.plain_proofs > 1:
+        traced = {k: trace_read("ck_umma_kernel" + k) for k in ("", ":int8", ":mac")}
     lib().salsaa_trace_enable(0)
     # then latency mode: each round's projection and each commitment's
     # statement rows run on a second stream beside the main chain
@@ -412,13 +452,13 @@ def run_ours(args):
             "commit_dense": dense,
             "sumcheck_batch": scb,
             "serving": serving,
-            "roofline": roofline_ck(traced, measured_peaks(tensor=True),
-                                    sum(serial) if serial else None,
+            "roofline": roofline_ck(traced, sum(serial) if serial else None,
                                     args.preset == "A0" and not args.wit_log),
             "ntt_roofline": roofline_ntt(ntt, peak, kind),
             "cpu_baseline": cpu,
             "clocks": clk,
             "verified": check,
+            "proof_digest": digest_check,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -676,38 +716,53 @@ def roofline_ntt(ntt, peak, kind):
             "algorithmic_bytes_per_launch": 16 * 1024 * (1 << 18)}
 
 
-# DRAM bytes (read + write) per launch of the commitment kernel are not
-# measured live; the ncu summaries under profiles/ give them for named launches.
 # DRAM bytes (read + write) of ck_umma_kernel per launch, mean over the eight
-# launches of one A0 proof, from one ncu capture of those launches
-# (dram__bytes_read.sum + dram__bytes_write.sum; command and per-launch values
-# in profiles/ck_umma_kernel_a0_round0.md).  The witness alone is 400 MB per
-# launch on average; the rest are key tiles that miss L2.
+# launches of one A0 proof (dram__bytes_read.sum + dram__bytes_write.sum), from
+# one ncu capture made by CK_TRAFFIC_CMD; ncu cannot run inside this process,
+# so the figure is carried with the command that measured it.
 CK_TRAFFIC_A0 = 653.8e6
-CK_TRAFFIC_NOTE = ("bytes per launch, mean over the 8 launches of one A0 proof (one ncu capture); "
-                   "algorithmic witness bytes 400 MB per launch")
+CK_TRAFFIC_CMD = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum "
+                  "--clock-control none -k regex:ck_umma -c 8 --csv python bench.py --steps 1 --warmup 1 "
+                  "--slots 1 --plain-proofs 1 --no-e2e --no-ntt --no-serve --no-cpu-baseline --no-dense")
 
 
-def roofline_ck(traced, peak_info, elapsed_ms, a0):
-    # elapsed_ms: summed device time of the traced plain proofs; a0: the
-    # default A0 workload, the one the traffic capture covers
-    """Dominant kernel of the prove: the tensor-core commitment product.  Work
-    is counted as int8 operations (2 per byte-limb product) and set against
-    the measured dense bf16 rate, the only tensor peak measured here."""
-    peak, kind = peak_info
-    if not traced or not traced["launches"]:
+def roofline_ck(traced, elapsed_ms, a0):
+    """Dominant kernel of the prove: the commitment-key rows on the tensor
+    cores.  Its bound is HBM: the algorithmic bytes are the slot-form witness
+    read once and the accumulators written once, against the measured copy
+    bandwidth.  Beside it, the tensor-pipe fraction (int8 operations the
+    tensor cores execute, against NVIDIA's dense int8 rate, which is twice
+    the dense bf16 rate; the bf16 rate is measured here) and the exact mod-q
+    multiply-accumulates per second.  elapsed_ms: summed device time of the
+    traced plain proofs; a0: the default A0 workload, the one the traffic
+    capture covers."""
+    if not traced or not traced[""]["launches"]:
         return None
-    per_ms = traced["ms"] / traced["launches"]
-    work = traced["work"] / traced["launches"]
-    achieved = work / (per_ms * 1e-3) / 1e12
+    t, t8, tm = traced[""], traced[":int8"], traced[":mac"]
+    per_ms = t["ms"] / t["launches"]
+    nbytes = t["work"] / t["launches"]
+    achieved = nbytes / (per_ms * 1e6)
+    hbm, hbm_kind = measured_peaks()
+    bf16, bf16_kind = measured_peaks(tensor=True)
+    int8_peak = 2.0 * bf16
+    ops = t8["work"] / t8["launches"]
+    tops = ops / (per_ms * 1e-3) / 1e12
+    macs = tm["work"] / tm["launches"]
     return {"kernel": "ck_umma_kernel (exact int8 limb-split commitment, tcgen05.mma kind::i8, TMEM)",
-            "bound": "tensor",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_kind": kind, "traffic": CK_TRAFFIC_A0 if a0 else None,
-            "traffic_note": CK_TRAFFIC_NOTE if a0 else "no capture for this workload",
-            "launches": traced["launches"],
-            "ms_per_launch": per_ms, "ops_per_launch": work,
-            "share_of_plain_prove": traced["ms"] / elapsed_ms if elapsed_ms else None,
+            "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_kind": hbm_kind + " copy bandwidth",
+            "traffic": CK_TRAFFIC_A0 if a0 else None,
+            "traffic_note": ("DRAM read+write bytes per launch, mean over the 8 launches of one A0 proof, "
+                             "from one ncu capture (command in traffic_cmd)") if a0
+            else "no capture for this workload",
+            "traffic_cmd": CK_TRAFFIC_CMD if a0 else None,
+            "algorithmic_bytes_per_launch": nbytes,
+            "launches": t["launches"], "ms_per_launch": per_ms,
+            "tensor": {"achieved": tops, "unit": "TOP/s int8", "peak": int8_peak,
+                       "peak_kind": "2 x %s bf16 (dense int8 = 2 x dense bf16 on B200)" % bf16_kind,
+                       "frac": tops / int8_peak, "int8_ops_per_launch": ops},
+            "mac_per_s": macs / (per_ms * 1e-3), "mac_per_launch": macs,
+            "share_of_plain_prove": t["ms"] / elapsed_ms if elapsed_ms else None,
             "measured_on": "plain path (one proof at a time, one stream), CUDA events around each launch"}
 
 

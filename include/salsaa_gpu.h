@@ -123,10 +123,14 @@ uint64_t salsaa_kernel_launches(void);
 /* Device-time trace for measurement (off by default): enable/reset, then read
  * the summed device time (CUDA events on the launching stream), summed
  * algorithmic work and launch count of a traced kernel by name.  Traced:
- * "ck_umma_kernel" and "ck_mma_kernel" (work = 2 x the exact byte-limb
- * products, as int8 operations), "ntt_kernel" (16 bytes per coefficient) and
- * "ntt_mul_kernel" (24 bytes per coefficient).  Reading waits for the traced
- * launches. */
+ * "ck_umma_kernel" (work = algorithmic HBM bytes: the slot-form witness read
+ * once and the accumulators written once), "ck_umma_kernel:int8" (the same
+ * launches; work = int8 operations the tensor cores execute, 2 per byte-limb
+ * product), "ck_umma_kernel:mac" (the same launches; work = exact mod-q
+ * multiply-accumulates of the ring products), "ck_mma_kernel" (int8
+ * operations), "nc_gram_kernel" (bytes), "ntt_kernel" (16 bytes per
+ * coefficient) and "ntt_mul_kernel" (24 bytes per coefficient).  Reading
+ * waits for the traced launches. */
 void salsaa_trace_enable(int on);
 int salsaa_trace_read(const char* name, double* total_ms, double* total_work, uint64_t* launches);
 /* Fill *out with preset "A0".."C2", "F0".."F2" (src/protocol.rs:28-123). */
@@ -310,8 +314,9 @@ int salsaa_project(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t 
  * device allocations.  All scratch lives in a fixed 641 KiB array inside this
  * library (one per GPU, kept until the process exits), so at most 8 rows
  * (chunk width rows*256 <= 2048); larger inputs return -3 with a message.
- * The first call on a device looks up that array's address and should come
- * before any stream capture on that device.  Calls share the array: two calls
+ * The first call on a device (and the first after a device reset, or from
+ * another context of that device) looks up that array's address and should
+ * come before any stream capture on that device.  Calls share the array: two calls
  * whose work overlaps on the GPU race; serialise them on one stream. */
 int salsaa_project_noalloc(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,
                            uint64_t seed, uint64_t round, uint64_t* d_out, void* stream);

@@ -62,6 +62,14 @@ static inline u64 mod_add(u64 a, u64 b, u64 q) {
   return r >= q ? r - q : r;
 }
 static inline u64 mod_sub(u64 a, u64 b, u64 q) { return a >= b ? a - b : a + (q - b); }
+/* Shoup's multiplication by a fixed w < q (V. Shoup, NTL): wp = floor(w 2^64 / q),
+ * x w - floor(x wp / 2^64) q lies in [0, 2q) for any x < 2^64 and q < 2^63. */
+static inline u64 shoup_pre(u64 w, u64 q) { return (u64)(((u128)w << 64) / q); }
+static inline u64 mul_shoup(u64 x, u64 w, u64 wp, u64 q) {
+  const u64 hi = (u64)(((u128)x * wp) >> 64);
+  const u64 r = x * w - hi * q;
+  return r >= q ? r - q : r;
+}
 
 /* hexl_wrapper.cpp:34-36 (MultiplyMod) */
 u64 so_mul_mod(u64 a, u64 b, u64 q) { return (u64)(((u128)a * b) % q); }
@@ -150,6 +158,9 @@ typedef struct NttTab {
   Mod M;
   u64* fwd;
   u64* inv;
+  u64* fwd_p; /* Shoup constants of fwd / inv / n_inv */
+  u64* inv_p;
+  u64 n_inv_p;
   struct NttTab* next;
 } NttTab;
 
@@ -182,6 +193,9 @@ static const NttTab* ntt_tab(u64 n, u64 q) {
     T->n_inv = so_inv_mod(n % q, q);
     T->fwd = (u64*)malloc(n * sizeof(u64));
     T->inv = (u64*)malloc(n * sizeof(u64));
+    T->fwd_p = (u64*)malloc(n * sizeof(u64));
+    T->inv_p = (u64*)malloc(n * sizeof(u64));
+    T->n_inv_p = shoup_pre(T->n_inv, q);
     u64 psi_inv = so_inv_mod(psi, q), p = 1, pi = 1;
     for (u64 i = 0; i < n; i++) {
       u64 j = bitrev(i, T->logn);
@@ -189,6 +203,10 @@ static const NttTab* ntt_tab(u64 n, u64 q) {
       T->inv[j] = pi;
       p = so_mul_mod(p, psi, q);
       pi = so_mul_mod(pi, psi_inv, q);
+    }
+    for (u64 i = 0; i < n; i++) {
+      T->fwd_p[i] = shoup_pre(T->fwd[i], q);
+      T->inv_p[i] = shoup_pre(T->inv[i], q);
     }
     T->next = g_tabs;
     g_tabs = T;
@@ -205,9 +223,9 @@ static void ntt_fwd(const NttTab* T, u64* a) {
   for (u64 m = 1; m < n; m <<= 1) {
     t >>= 1;
     for (u64 i = 0; i < m; i++) {
-      const u64 j1 = 2 * i * t, W = T->fwd[m + i];
+      const u64 j1 = 2 * i * t, W = T->fwd[m + i], Wp = T->fwd_p[m + i];
       for (u64 j = j1; j < j1 + t; j++) {
-        u64 U = a[j], V = mod_mul(&T->M, a[j + t], W);
+        u64 U = a[j], V = mul_shoup(a[j + t], W, Wp, q);
         a[j] = mod_add(U, V, q);
         a[j + t] = mod_sub(U, V, q);
       }
@@ -224,17 +242,17 @@ static void ntt_inv(const NttTab* T, u64* a) {
     u64 j1 = 0;
     const u64 h = m >> 1;
     for (u64 i = 0; i < h; i++) {
-      const u64 W = T->inv[h + i];
+      const u64 W = T->inv[h + i], Wp = T->inv_p[h + i];
       for (u64 j = j1; j < j1 + t; j++) {
         u64 U = a[j], V = a[j + t];
         a[j] = mod_add(U, V, q);
-        a[j + t] = mod_mul(&T->M, mod_sub(U, V, q), W);
+        a[j + t] = mul_shoup(mod_sub(U, V, q), W, Wp, q);
       }
       j1 += 2 * t;
     }
     t <<= 1;
   }
-  for (u64 j = 0; j < n; j++) a[j] = mod_mul(&T->M, a[j], T->n_inv);
+  for (u64 j = 0; j < n; j++) a[j] = mul_shoup(a[j], T->n_inv, T->n_inv_p, q);
 }
 
 int so_ntt_forward(u64* a, u64 n, u64 q) {
@@ -306,8 +324,25 @@ u64 so_sum(const u64* a, u64 n, u64 q) {
   return (u64)(s % q);
 }
 u64 so_sum_sq(const u64* a, u64 n, u64 q) {
+  /* squares of reduced values are below 2^124; 2^3 of them fit a 128-bit sum */
+  const u64 blk = 8;
   u64 s = 0;
-  for (u64 i = 0; i < n; i++) s = so_add_mod(s, so_mul_mod(a[i], a[i], q), q);
+#pragma omp parallel
+  {
+    u64 part = 0;
+#pragma omp for schedule(static)
+    for (long long b = 0; b < (long long)((n + blk - 1) / blk); b++) {
+      const u64 i0 = (u64)b * blk, i1 = i0 + blk < n ? i0 + blk : n;
+      u128 acc = 0;
+      for (u64 i = i0; i < i1; i++) {
+        const u64 x = a[i] % q;
+        acc += (u128)x * x;
+      }
+      part = so_add_mod(part, (u64)(acc % q), q);
+    }
+#pragma omp critical
+    s = so_add_mod(s, part, q);
+  }
   return s;
 }
 
@@ -507,6 +542,35 @@ static void stmt_free(Stmt* S) {
   memset(S, 0, sizeof(*S));
 }
 
+/* A fixed ring element t (slot form) prepared for repeated products t * x:
+ * per slot its even part, odd part and zeta * odd part with their Shoup
+ * constants.  (t_e + X t_o)(x_e + X x_o) = t_e x_e + zeta t_o x_o + X (t_o x_e + t_e x_o),
+ * the product of slot_mul. */
+typedef struct {
+  u64 e[1024], o[1024], z[1024], ep[1024], op[1024], zp[1024];
+} SlotConst;
+static void slot_const_make(const Ring* R, const u64* t, SlotConst* c) {
+  const u64 n = R->n, q = R->q;
+  for (u64 s = 0; s < n; s++) {
+    c->e[s] = t[s];
+    c->o[s] = t[n + s];
+    c->z[s] = mod_mul(&R->M, t[n + s], R->zeta[s]);
+    c->ep[s] = shoup_pre(c->e[s], q);
+    c->op[s] = shoup_pre(c->o[s], q);
+    c->zp[s] = shoup_pre(c->z[s], q);
+  }
+}
+static void slot_mul_const(const Ring* R, const SlotConst* c, const u64* x, u64* r) {
+  const u64 n = R->n, q = R->q;
+  for (u64 s = 0; s < n; s++) {
+    const u64 xe = x[s], xo = x[n + s];
+    const u64 ev = mod_add(mul_shoup(xe, c->e[s], c->ep[s], q), mul_shoup(xo, c->z[s], c->zp[s], q), q);
+    const u64 od = mod_add(mul_shoup(xe, c->o[s], c->op[s], q), mul_shoup(xo, c->e[s], c->ep[s], q), q);
+    r[s] = ev;
+    r[n + s] = od;
+  }
+}
+
 /* The expanded layer whose length is len; -1 when the row has none (the
  * reference panics "No matching layer found", src/arithmetic.rs:474). */
 static int row_layer_index(const Row* row, u64 len, u64* jj) {
@@ -525,14 +589,15 @@ static int row_layer(const Ring* R, const Row* row, u64 len, u64* out) {
   const u64 d = R->d;
   memcpy(out, row->base, row->blen * d * sizeof(u64));
   u64 cur = row->blen;
+  SlotConst c0, c1;
   for (u64 step = 0; step < j; step++) {
     const u64 k = row->K - 1 - step;
-    const u64* t0 = row->tens + (2 * k) * d;
-    const u64* t1 = row->tens + (2 * k + 1) * d;
+    slot_const_make(R, row->tens + (2 * k) * d, &c0);
+    slot_const_make(R, row->tens + (2 * k + 1) * d, &c1);
 #pragma omp parallel for schedule(static)
     for (long long idx = 0; idx < (long long)cur; idx++) {
-      slot_mul(R, t1, out + idx * d, out + (cur + idx) * d);
-      slot_mul(R, t0, out + idx * d, out + idx * d);
+      slot_mul_const(R, &c1, out + idx * d, out + (cur + idx) * d);
+      slot_mul_const(R, &c0, out + idx * d, out + idx * d);
     }
     cur *= 2;
   }
@@ -541,44 +606,53 @@ static int row_layer(const Ring* R, const Row* row, u64 len, u64* out) {
 
 /* out[k] = sum_i E[i] * W_k[i] over slot-form vectors of length len
  * (parallel_dot_series_matrix / parallel_dot_single_series_matrix,
- * src/arithmetic.rs:459-536).  Lazy 128-bit sums, reduced per chunk. */
+ * src/arithmetic.rs:459-536).  Lazy 128-bit sums, reduced per chunk; each
+ * chunk of E is read once for all witness rows, element by element, so the
+ * scan is sequential and the chunk stays in cache across the rows. */
 static void dot_layer(const Ring* R, const u64* E, const u64* Ws, u64 rows, u64 len, u64* out) {
   const u64 n = R->n, d = R->d, q = R->q;
-  const u64 CH = (q < (1ULL << 52)) ? 4096 : 4;
+  const u64 CH = (q < (1ULL << 52)) ? 512 : 4;
   const u64 nch = (len + CH - 1) / CH;
-  for (u64 k = 0; k < rows; k++) {
-    u64* part = (u64*)calloc(nch * 3 * n, sizeof(u64));
-    const u64* W = Ws + k * len * d;
-#pragma omp parallel for schedule(dynamic, 1)
+  u64* part = (u64*)calloc(nch * rows * 3 * n, sizeof(u64));
+#pragma omp parallel
+  {
+    u128* acc = (u128*)malloc(3 * n * sizeof(u128));
+#pragma omp for schedule(dynamic, 4)
     for (long long c = 0; c < (long long)nch; c++) {
-      u64 i0 = (u64)c * CH, i1 = i0 + CH < len ? i0 + CH : len;
-      for (u64 s = 0; s < n; s++) {
-        u128 ee = 0, oo = 0, x = 0;
+      const u64 i0 = (u64)c * CH, i1 = i0 + CH < len ? i0 + CH : len;
+      for (u64 k = 0; k < rows; k++) {
+        const u64* W = Ws + k * len * d;
+        memset(acc, 0, 3 * n * sizeof(u128));
         for (u64 i = i0; i < i1; i++) {
           const u64* e = E + i * d;
           const u64* w = W + i * d;
-          ee += (u128)e[s] * w[s];
-          oo += (u128)e[n + s] * w[n + s];
-          x += (u128)e[n + s] * w[s];
-          x += (u128)e[s] * w[n + s];
+          for (u64 s = 0; s < n; s++) {
+            const u64 es = e[s], eo = e[n + s], ws = w[s], wo = w[n + s];
+            acc[s] += (u128)es * ws;
+            acc[n + s] += (u128)eo * wo;
+            acc[2 * n + s] += (u128)eo * ws + (u128)es * wo;
+          }
         }
-        part[(c * 3 + 0) * n + s] = mod_red_any(&R->M, ee);
-        part[(c * 3 + 1) * n + s] = mod_red_any(&R->M, oo);
-        part[(c * 3 + 2) * n + s] = mod_red_any(&R->M, x);
+        u64* pc = part + ((u64)c * rows + k) * 3 * n;
+        for (u64 t = 0; t < 3 * n; t++) pc[t] = mod_red_any(&R->M, acc[t]);
       }
     }
+    free(acc);
+  }
+  for (u64 k = 0; k < rows; k++) {
     for (u64 s = 0; s < n; s++) {
       u64 ee = 0, oo = 0, x = 0;
       for (u64 c = 0; c < nch; c++) {
-        ee = mod_add(ee, part[(c * 3 + 0) * n + s], q);
-        oo = mod_add(oo, part[(c * 3 + 1) * n + s], q);
-        x = mod_add(x, part[(c * 3 + 2) * n + s], q);
+        const u64* pc = part + (c * rows + k) * 3 * n;
+        ee = mod_add(ee, pc[s], q);
+        oo = mod_add(oo, pc[n + s], q);
+        x = mod_add(x, pc[2 * n + s], q);
       }
       out[k * d + s] = mod_add(ee, mod_mul(&R->M, oo, R->zeta[s]), q);
       out[k * d + n + s] = x;
     }
-    free(part);
   }
+  free(part);
 }
 
 /* Commitment-key row: the power row (m, m^2, ..., m^L) of
@@ -673,7 +747,9 @@ static void sumcheck_rows(const Mod* M, u64** v, u64 rows, u64 len, const u64* c
   const u64 q = M->q;
   u64 cur = len, j = 0;
   while (cur > 1) {
-    const u64 h = cur / 2, c = cs[j];
+    const u64 h = cur / 2, c = cs[j], cp = shoup_pre(cs[j], q);
+    /* products of reduced values are below 2^(2s); this many fit a 128-bit sum */
+    const u64 lazy = M->s <= 52 ? 4096 : 1;
     for (u64 k = 0; k < rows; k++) {
       u64* x = v[k];
       u64 f0 = 0, f1 = 0, f2 = 0;
@@ -681,12 +757,19 @@ static void sumcheck_rows(const Mod* M, u64** v, u64 rows, u64 len, const u64* c
       {
         u64 a0 = 0, a1 = 0, a2 = 0;
 #pragma omp for schedule(static)
-        for (long long i = 0; i < (long long)h; i++) {
-          u64 w0 = x[i], w1 = x[h + i], df = mod_sub(w1, w0, q);
-          a0 = mod_add(a0, mod_mul(M, w0, w0), q);
-          a1 = mod_add(a1, mod_mul(M, w0, df), q);
-          a2 = mod_add(a2, mod_mul(M, df, df), q);
-          x[i] = mod_add(mod_mul(M, df, c), w0, q);
+        for (long long b = 0; b < (long long)((h + lazy - 1) / lazy); b++) {
+          const u64 i0 = (u64)b * lazy, i1 = i0 + lazy < h ? i0 + lazy : h;
+          u128 s0 = 0, s1 = 0, s2 = 0;
+          for (u64 i = i0; i < i1; i++) {
+            const u64 w0 = x[i], w1 = x[h + i], df = mod_sub(w1, w0, q);
+            s0 += (u128)w0 * w0;
+            s1 += (u128)w0 * df;
+            s2 += (u128)df * df;
+            x[i] = mod_add(mul_shoup(df, c, cp, q), w0, q);
+          }
+          a0 = mod_add(a0, (u64)(s0 % q), q);
+          a1 = mod_add(a1, (u64)(s1 % q), q);
+          a2 = mod_add(a2, (u64)(s2 % q), q);
         }
 #pragma omp critical
         {
@@ -769,6 +852,21 @@ static int project_impl(const u64* w, u64 rows, u64 width, u64 d, u64 q, const u
     u64 idx = (u64)o / PROJ_H, k = (u64)o % PROJ_H;
     u64 i = idx / nch, j = idx % nch;
     const u64* chunk = w + (i * width + j * cw) * d;
+    u64* dst = out + (idx * PROJ_H + k) * d;
+    if (q < (1ULL << 52) && cw <= (1ULL << 11)) {
+      /* canonical inputs below 2^52, at most 2^11 of them: the sums stay below 2^63 */
+      u64 pos[2048], neg[2048];
+      memset(pos, 0, d * sizeof(u64));
+      memset(neg, 0, d * sizeof(u64));
+      for (u64 l = 0; l < cw; l++) {
+        if (iz[k * cw + l]) continue;
+        const u64* e = chunk + l * d;
+        u64* acc = sg[k * cw + l] ? pos : neg;
+        for (u64 t = 0; t < d; t++) acc[t] += e[t];
+      }
+      for (u64 t = 0; t < d; t++) dst[t] = mod_sub(pos[t] % q, neg[t] % q, q);
+      continue;
+    }
     u128 pos[4096], neg[4096];
     memset(pos, 0, d * sizeof(u128));
     memset(neg, 0, d * sizeof(u128));
@@ -780,7 +878,6 @@ static int project_impl(const u64* w, u64 rows, u64 width, u64 d, u64 q, const u
       else
         for (u64 t = 0; t < d; t++) neg[t] += e[t];
     }
-    u64* dst = out + (idx * PROJ_H + k) * d;
     for (u64 t = 0; t < d; t++) dst[t] = mod_sub((u64)(pos[t] % q), (u64)(neg[t] % q), q);
   }
   return 0;

@@ -372,7 +372,16 @@ int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, u32 G, const ModQ& M, con
   cudaError_t e = cudaFuncSetAttribute(ck_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ck_umma smem attribute");
   dim3 g(n / 2, (unsigned)(a.width / Bw / G));
-  const int tr = salsaa_trace_begin("ck_umma_kernel", st, 2.0 * 196.0 * a.nck * a.rows * (double)a.width * n);
+  // Traced measures of one launch: algorithmic HBM bytes (the slot-form
+  // witness read once, the accumulators written once), the int8 operations
+  // the tensor cores execute (2 x 14 x 14 byte products per key row, witness
+  // row, element and slot pair half), and the exact mod-q multiply-accumulates
+  // of the ring products (2d per key row, witness row and element).
+  const double wit_bytes = 8.0 * a.rows * (double)a.width * 2 * n;
+  const double out_bytes = 8.0 * a.nck * a.rows * 2 * n;
+  const int tr = salsaa_trace_begin("ck_umma_kernel", st, wit_bytes + out_bytes);
+  salsaa_trace_alias(tr, "ck_umma_kernel:int8", 2.0 * 196.0 * a.nck * a.rows * (double)a.width * n);
+  salsaa_trace_alias(tr, "ck_umma_kernel:mac", (double)a.nck * a.rows * (double)a.width * 2 * n);
   ck_umma_kernel<<<g, CKU_THREADS, smem, st>>>(a.tk8, a.w, a.rows, G, a.nck, nkp, n, a.ck_bt, Bw, a.thi, a.ck_nhi,
                                                M, zeta, a.acc, plain);
   salsaa_trace_end(tr, st);

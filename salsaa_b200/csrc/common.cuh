@@ -156,4 +156,6 @@ void salsaa_count_launch();
 // C ABI): an event pair on the launching stream around each traced launch.
 // `work` is the launch's algorithmic work (bytes or operations, per kernel).
 int salsaa_trace_begin(const char* name, cudaStream_t st, double work);
+// Another measure of the launch that `token` brackets, read under `name`.
+void salsaa_trace_alias(int token, const char* name, double work);
 void salsaa_trace_end(int token, cudaStream_t st);

@@ -35,23 +35,55 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mu;
+// Per device: the CUDA context the address was looked up in, and the address.
+// A device reset (or a caller that switches to another context on the same
+// device) loads this module again, possibly at another address, so the cached
+// address is only reused while the same context is current.
+void* g_noalloc_ctx[NOALLOC_MAX_DEVICES] = {};
 unsigned char* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
 
 __global__ void noalloc_seed_kernel(DevState* ds, u64 seed) { ds->seed = seed; }
 
-// Device address of this device's scratch array, looked up once per device
-// with that device current (host code cannot use the symbol itself).
+// The current driver context, through the runtime's driver entry-point lookup
+// (no link-time dependency on the driver library).
+int noalloc_current_ctx(void** ctx) {
+  if (!g_ctx_get_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &qr);
+    if (e != cudaSuccess || qr != cudaDriverEntryPointSuccess || !fn)
+      return salsaa_set_error(-1, "project_noalloc: cuCtxGetCurrent is not available");
+    g_ctx_get_current = (CtxGetCurrentFn)fn;
+  }
+  *ctx = nullptr;
+  if (g_ctx_get_current(ctx) != 0) return salsaa_set_error(-1, "project_noalloc: cuCtxGetCurrent failed");
+  return 0;
+}
+
+// Device address of this device's scratch array, looked up with that device
+// current the first time a context of it calls here (host code cannot use the
+// symbol itself: in host code its name only stands in for the device array).
 int noalloc_scratch(unsigned char** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "project_noalloc: cudaGetDevice");
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return salsaa_set_error(-1, "project_noalloc: device index out of range");
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  void* ctx = nullptr;
+  int rc = noalloc_current_ctx(&ctx);
+  if (rc) return rc;
+  if (!ctx || !g_noalloc_addr[dev] || g_noalloc_ctx[dev] != ctx) {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);  // makes the primary context current if none was
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "project_noalloc: cudaGetSymbolAddress");
+    rc = noalloc_current_ctx(&ctx);
+    if (rc) return rc;
+    if (!ctx) return salsaa_set_error(-1, "project_noalloc: no current CUDA context");
     g_noalloc_addr[dev] = (unsigned char*)p;
+    g_noalloc_ctx[dev] = ctx;
   }
   *out = g_noalloc_addr[dev];
   return 0;
@@ -62,7 +94,8 @@ int noalloc_scratch(unsigned char** out) {
 extern "C" int salsaa_project_noalloc(const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,
                                       uint64_t seed, uint64_t round, uint64_t* d_out, void* stream) {
   if (!d_w || !d_out) return salsaa_set_error(-1, "project_noalloc: null argument");
-  if (rows == 0 || rows * 256 > NOALLOC_MAX_CW)
+  // rows is bounded before it is multiplied, so the product cannot wrap.
+  if (rows == 0 || rows > NOALLOC_MAX_CW / 256)
     return salsaa_set_error(-3, "project_noalloc: rows * 256 exceeds the 2048-column scratch (at most 8 rows)");
   const u64 cw = rows * 256;
   if (cw > width || width % cw) return salsaa_set_error(-3, "project_noalloc: chunk width exceeds the witness width");

@@ -41,6 +41,7 @@ struct TraceRec {
   cudaEvent_t a, b;
   double work;
   int done;
+  int alias;  // shares the events of record `alias - 1` (another measure of the same launch)
 };
 std::mutex g_trace_mu;
 std::atomic<int> g_trace_on{0};
@@ -51,7 +52,7 @@ int salsaa_trace_begin(const char* name, cudaStream_t st, double work) {
   if (!g_trace_on.load(std::memory_order_relaxed)) return -1;
   std::lock_guard<std::mutex> lk(g_trace_mu);
   if ((int)g_trace.size() >= TRACE_MAX) return -1;
-  TraceRec r{name, nullptr, nullptr, work, 0};
+  TraceRec r{name, nullptr, nullptr, work, 0, 0};
   if (cudaEventCreate(&r.a) != cudaSuccess || cudaEventCreate(&r.b) != cudaSuccess) return -1;
   cudaEventRecord(r.a, st);
   g_trace.push_back(r);
@@ -65,9 +66,20 @@ void salsaa_trace_end(int token, cudaStream_t st) {
     g_trace[token].done = 1;
   }
 }
+void salsaa_trace_alias(int token, const char* name, double work) {
+  if (token < 0) return;
+  std::lock_guard<std::mutex> lk(g_trace_mu);
+  if (token >= (int)g_trace.size() || (int)g_trace.size() >= TRACE_MAX) return;
+  TraceRec r = g_trace[token];
+  r.name = name;
+  r.work = work;
+  r.alias = token + 1;
+  g_trace.push_back(r);
+}
 extern "C" void salsaa_trace_enable(int on) {
   std::lock_guard<std::mutex> lk(g_trace_mu);
   for (TraceRec& r : g_trace) {
+    if (r.alias) continue;
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);
   }
@@ -80,7 +92,8 @@ extern "C" int salsaa_trace_read(const char* name, double* total_ms, double* tot
   double t = 0, wk = 0;
   uint64_t n = 0;
   for (TraceRec& r : g_trace) {
-    if (!r.done || strcmp(r.name, name)) continue;
+    const int done = r.alias ? g_trace[r.alias - 1].done : r.done;
+    if (!done || strcmp(r.name, name)) continue;
     cudaError_t e = cudaEventSynchronize(r.b);
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "trace_read");
     float ms = 0;

@@ -3,9 +3,9 @@
 Each entry restates one deterministic test of lattice-arguments/salsaa with
 its inputs and expected output, and names the file:line it comes from.  The
 reference is Rust + Intel HEXL and cannot be built here, so the vectors are
-taken from the test sources.  When the reference tree is available (path in
-SALSAA_REFERENCE, default /root/reference), `--check` confirms that every
-expected literal still appears at the cited place.
+taken from the test sources.  When the reference tree is available,
+`--check` (which needs its path in the SALSAA_REFERENCE environment variable)
+confirms that every expected literal still appears at the cited place.
 """
 import json
 import os
@@ -78,7 +78,9 @@ def main():
     with open(os.path.join(here, "kats.json"), "w") as f:
         json.dump(KATS, f, indent=1)
     if "--check" in sys.argv:
-        ref = os.environ.get("SALSAA_REFERENCE", "/root/reference")
+        ref = os.environ.get("SALSAA_REFERENCE")
+        if not ref:
+            sys.exit("--check needs SALSAA_REFERENCE set to the reference source tree")
         bad = check(ref)
         print("mismatched literals:", bad)
         sys.exit(1 if bad else 0)

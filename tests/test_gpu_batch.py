@@ -44,6 +44,21 @@ def test_sumcheck_batch_64_instances(api, oracle):
     _check(api, oracle, vecs, q, seed=99, rnd=0)
 
 
+@pytest.mark.slow
+def test_sumcheck_batch_bench_instances(api, oracle, cuda):
+    """The microbench's batch: 64 ternary instances with lengths log-uniform in
+    2^16..2^22 (the same seeded draw), the 50-bit prime."""
+    torch = cuda
+    q = P.Q0
+    rng = np.random.default_rng(2024)
+    logs = np.sort(rng.integers(16, 23, size=64))
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(5)
+    vecs = [api.to_host(torch.randint(-1, 2, (1 << int(k),), dtype=torch.int64, device="cuda", generator=gen) % q)
+            for k in logs]
+    _check(api, oracle, vecs, q, seed=1, rnd=0)
+
+
 def test_sumcheck_batch_wide_modulus(api, oracle):
     """q >= 2^50: exact residues instead of lazy 128-bit sums."""
     q = P.Q62

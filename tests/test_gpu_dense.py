@@ -38,6 +38,32 @@ def test_dense_commit(api, oracle, n, m, d, q, r, digits):
     key.close()
 
 
+@pytest.mark.slow
+@pytest.mark.parametrize("n", [8, 16])
+@pytest.mark.parametrize("r", [1, 8, 32])
+@pytest.mark.parametrize("b", [2, 16])
+def test_dense_commit_full_size(api, oracle, n, r, b):
+    """The microbench shapes: m = 2^16 ring elements of degree 128 at the 50-bit
+    prime, W base-b digits in [-b/2, b/2).  The GPU computes all n x r outputs;
+    the oracle recomputes the first and last key rows against three columns."""
+    import torch
+    q, m, d = P.Q0, 1 << 16, 128
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1000 * n + 10 * r + b)
+    A = torch.randint(0, 1 << 62, (n, m, d), dtype=torch.int64, device="cuda", generator=gen) % q
+    W = torch.randint(-(b // 2), b // 2, (r, m, d), dtype=torch.int64, device="cuda", generator=gen) % q
+    key = api.DenseKey(A, q)
+    got = api.to_host(key.commit(W))
+    key.close()
+    rows = sorted({0, n - 1})
+    cols = sorted({0, r // 2, r - 1})
+    A_s = api.to_host(A[rows])
+    W_s = api.to_host(W[cols])
+    del A, W
+    want = oracle.dense_commit(A_s, W_s, q)
+    assert np.array_equal(got[np.ix_(rows, cols)], want)
+
+
 def test_dense_commit_rejects_bad_shapes(api):
     from salsaa_b200.api import SalsaaError
     with pytest.raises(SalsaaError):

@@ -192,6 +192,15 @@ def test_sumcheck_small(api, oracle, rows, n, d, q, bound):
     _check_sumcheck(api, oracle, small_signed(rng, (rows, n), bound, q), d, q)
 
 
+@pytest.mark.slow
+@pytest.mark.parametrize("logn,bound", [(22, 1), (23, 1 << 12), (24, 1)])
+def test_sumcheck_full_size(api, oracle, logn, bound):
+    """Norm-check sumchecks at 2^22..2^24 coefficients (ternary, and
+    decomposition-digit sized), every round polynomial of both repetitions."""
+    rng = np.random.default_rng(logn)
+    _check_sumcheck(api, oracle, small_signed(rng, (1, 1 << logn), bound, P.Q0), 128, P.Q0)
+
+
 @pytest.mark.parametrize("outside", [0, 1, 2])
 def test_sumcheck_limb_edges(api, oracle, outside):
     """Values at the ends of the four-signed-byte range stay on the tensor

@@ -38,12 +38,25 @@ def test_noalloc_matches_allocating_entry(gpu_lib, cuda):
         assert torch.equal(ref, got)
 
 
-def test_noalloc_rejects_oversize(gpu_lib, cuda):
+@pytest.mark.parametrize("rows,width,d,msg", [
+    (16, 4096, 16, b"2048-column scratch"),          # more rows than the scratch covers
+    (1 << 56, 4096, 16, b"2048-column scratch"),     # rows * 256 would wrap to 0
+    ((1 << 56) + 1, 4096, 16, b"2048-column scratch"),  # rows * 256 would wrap to 256
+    (8, 1024, 16, b"exceeds the witness width"),     # chunk wider than the witness
+    (3, 2048, 16, b"exceeds the witness width"),     # width not a multiple of the chunk
+])
+def test_noalloc_rejects_bad_shapes(gpu_lib, cuda, rows, width, d, msg):
+    """Shapes outside the fixed scratch return -3 before any launch: the
+    output buffer keeps its contents."""
     from salsaa_b200 import api
     torch = cuda
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    w = api.to_dev(np.zeros((16, 4096, 16), dtype=np.uint64))
-    out = api.dev_empty((4096, 16))
-    rc = _call(gpu_lib.salsaa_project_noalloc, w, 16, 4096, 16, P.Q0, 1, 0, out, stream)
+    w = api.to_dev(np.zeros((min(rows, 16), width, d), dtype=np.uint64))
+    out = api.dev_empty((width, d))
+    out.fill_(7)
+    torch.cuda.synchronize()
+    rc = _call(gpu_lib.salsaa_project_noalloc, w, rows, width, d, P.Q0, 1, 0, out, stream)
     assert rc == -3
-    assert b"2048-column scratch" in gpu_lib.salsaa_last_error()
+    assert msg in gpu_lib.salsaa_last_error()
+    torch.cuda.synchronize()
+    assert bool((out == 7).all())
