@@ -68,6 +68,8 @@ def parse():
                     help="profiling: run only the NTT microbench and print its JSON")
     ap.add_argument("--ntt-log-coeffs", type=int, default=28,
                     help="log2 of the coefficients per NTT batch (28 = 2 GiB per buffer)")
+    ap.add_argument("--no-tune-compare", action="store_true",
+                    help="skip the runs with the untuned (default) kernel schedules")
     return ap.parse_args()
 
 
@@ -278,6 +280,27 @@ def run_ours(args):
             done.append(e)
         return done
 
+    # untuned kernel schedules first (the library's defaults), for the
+    # tuned-vs-default comparison; the timed region below runs the tuned table
+    default_value = None
+    if not args.no_tune_compare:
+        set_schedules("default")
+        for w in range(args.warmup):
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(main)
+            batch(-100 - w, ev)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(main)
+        nd = max(1, min(args.steps, 3))
+        for sidx in range(nd):
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(main)
+            batch(-200 - sidx, ev)
+        b.record(main)
+        b.synchronize()
+        default_value = S * nd / (a.elapsed_time(b) / 1000.0)
+    tuned_entries = set_schedules("tuned")
     # warm-up
     for w in range(args.warmup):
         ev = torch.cuda.Event(enable_timing=True)
@@ -422,7 +445,13 @@ def run_ours(args):
     slots = []
     del witnesses, proofs
     torch.cuda.empty_cache()
-    ntt = ntt_bench(torch, api) if rank == 0 and not args.no_ntt else None
+    ntt = ntt_default = None
+    if rank == 0 and not args.no_ntt:
+        if not args.no_tune_compare:
+            set_schedules("default")
+            ntt_default = ntt_bench(torch, api, forward_only=True)
+            set_schedules("tuned")
+        ntt = ntt_bench(torch, api)
     dense = dense_bench(torch, api) if rank == 0 and not args.no_dense else None
     scb = sumcheck_batch_bench(torch, api) if rank == 0 and not args.no_dense else None
     serving = serving_bench(torch, api, args.serve_requests, rank) if not args.no_serve else None
@@ -455,6 +484,11 @@ def run_ours(args):
             "roofline": roofline_ck(traced, sum(serial) if serial else None,
                                     args.preset == "A0" and not args.wit_log),
             "ntt_roofline": roofline_ntt(ntt, peak, kind),
+            "tuning": {"table_entries": tuned_entries,
+                       "value_default_schedules": default_value,
+                       "value_tuned_schedules": value / world,
+                       "tuned_over_default": (value / world) / default_value if default_value else None,
+                       "ntt_default": ntt_default},
             "cpu_baseline": cpu,
             "clocks": clk,
             "verified": check,
@@ -668,7 +702,19 @@ def flush_l2(torch, buf):
     buf.add_(1)
 
 
-def ntt_bench(torch, api, log_coeffs=28):
+def set_schedules(mode):
+    """'default': the library's untuned kernel schedules; 'tuned': reload the
+    tuner's table (tune_table.txt beside the library).  Returns the number of
+    table entries loaded (tuned), or None."""
+    from salsaa_b200 import lib
+    if mode == "default":
+        lib().salsaa_tune_reset()
+        return None
+    n = lib().salsaa_tune_load(None)
+    return n if n >= 0 else 0
+
+
+def ntt_bench(torch, api, log_coeffs=28, forward_only=False):
     """Batched negacyclic NTT microbench (62-bit prime, coefficients uniform in
     [0, q)): forward, inverse and the fused forward-product-inverse for
     n in {64, 128, 256, 1024}, plus the protocol-shaped incomplete transform
@@ -684,11 +730,15 @@ def ntt_bench(torch, api, log_coeffs=28):
         y = torch.randint(0, 1 << 62, (count, n), dtype=torch.int64, device="cuda") % q
         r = torch.empty_like(x)
         row = {"polys": count}
-        for inv in (False, True):
+        for inv in ((False,) if forward_only else (False, True)):
             api.ntt(x, n, q, inverse=inv)
             t = timed_launches(torch, lambda: api.ntt(x, n, q, inverse=inv), "ntt_kernel", reps)
             ms = t["ms"] / t["launches"]
             row["inverse" if inv else "forward"] = {"ms": ms, "GB/s": t["work"] / t["launches"] / (ms * 1e6)}
+        if forward_only:
+            res["n%d" % n] = row
+            del x, y, r
+            continue
         api.poly_mul(x, y, n, q, out=r)
         t = timed_launches(torch, lambda: api.poly_mul(x, y, n, q, out=r), "ntt_mul_kernel", reps)
         ms = t["ms"] / t["launches"]
@@ -708,12 +758,24 @@ def ntt_bench(torch, api, log_coeffs=28):
 
 
 def roofline_ntt(ntt, peak, kind):
+    """The NTT microbench against the measured copy bandwidth: the protocol's
+    incomplete d = 128 transform (50-bit prime) as the headline, every size's
+    forward and inverse fraction beside it."""
     if not ntt:
         return None
-    f = ntt["n1024"]["forward"]
-    return {"kernel": "ntt_reg_kernel (forward, n=1024, 62-bit q, 2^18 polynomials)", "bound": "hbm",
+    f = ntt["incomplete_d128"]
+    per = {}
+    for k, row in ntt.items():
+        if isinstance(row, dict):
+            for direction in ("forward", "inverse"):
+                if direction in row:
+                    per["%s_%s" % (k, direction)] = row[direction]["GB/s"] / peak
+            if "GB/s" in row:
+                per[k] = row["GB/s"] / peak
+    return {"kernel": "register NTT, incomplete d=128 (two 64-point transforms), q=1125899904679937, "
+                      "2^19 ring elements", "bound": "hbm",
             "achieved": f["GB/s"], "peak": peak, "unit": "GB/s", "frac": f["GB/s"] / peak, "peak_kind": kind,
-            "algorithmic_bytes_per_launch": 16 * 1024 * (1 << 18)}
+            "algorithmic_bytes_per_launch": 16 * 128 * f["elements"], "frac_per_size": per}
 
 
 # DRAM bytes (read + write) of ck_umma_kernel per launch, mean over the eight

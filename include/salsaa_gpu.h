@@ -229,11 +229,35 @@ int salsaa_server_poll(salsaa_server* s, uint64_t ticket, double* latency_ms, do
 int salsaa_server_cancel(salsaa_server* s, uint64_t ticket);
 void salsaa_server_destroy(salsaa_server* s);
 
+/* ---- kernel schedules chosen by the autotuner ---- */
+/* No reference counterpart (the reference's HEXL NTT has a fixed schedule).
+ * The register-path NTT (16 <= n <= 4096, 16-byte aligned buffers) runs one
+ * of: variant 0 = one 4096-coefficient tile per CTA; variant 2, 3 or 4 =
+ * persistent CTAs that stage their tiles with bulk copies (cp.async.bulk)
+ * that many tiles ahead; ctas_per_sm caps the resident CTAs per SM (0 = as
+ * many as fit).  The choice is kept per (log2 n, incomplete, inverse,
+ * wide_modulus = q >= 2^50, large = at least 2^22 coefficients in the call);
+ * every variant gives the same outputs.  Untuned default: variant 0.
+ * salsaa_b200/tune.py times the candidates on the GPU and writes a table file
+ * ("ntt <log_n> <incomplete> <inverse> <wide> <large> <variant> <ctas_per_sm>"
+ * per line); the library loads it the first time a
+ * transform launches, from $SALSAA_TUNE_FILE or tune_table.txt beside the
+ * library.  salsaa_tune_load(NULL) reloads that file, salsaa_tune_load(path)
+ * another (returns the entries read, < 0 if unreadable), salsaa_tune_reset()
+ * restores the untuned defaults.  Schedules are process-wide. */
+int salsaa_tune_load(const char* path);
+int salsaa_tune_reset(void);
+int salsaa_ntt_tune_set(uint32_t log_n, int incomplete, int inverse, int wide_modulus, int large, int variant,
+                        int ctas_per_sm);
+int salsaa_ntt_tune_get(uint32_t log_n, int incomplete, int inverse, int wide_modulus, int large, int* variant,
+                        int* ctas_per_sm);
+
 /* ---- subroutine-level entry points (device pointers, cudaStream_t) ---- */
 
 /* Batched negacyclic NTT.  incomplete = 0: `count` polynomials of n
- * coefficients; incomplete = 1: `count` ring elements of d = 2n in the
- * reference's IncompleteNTT layout (src/cyclotomic_ring.rs:484-556).
+ * coefficients; incomplete = 1: `count` ring elements of degree d = n in the
+ * reference's IncompleteNTT layout (two size-n/2 transforms per element,
+ * src/cyclotomic_ring.rs:484-556).
  * d_in may equal d_out. */
 int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uint64_t count, uint64_t q, int inverse,
                int incomplete, void* stream);

@@ -90,6 +90,10 @@ DEVICE_SYMBOLS = {
     "salsaa_server_poll": (INT, [VP, U64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "salsaa_server_cancel": (INT, [VP, U64]),
     "salsaa_server_destroy": (None, [VP]),
+    "salsaa_tune_load": (INT, [ctypes.c_char_p]),
+    "salsaa_tune_reset": (INT, []),
+    "salsaa_ntt_tune_set": (INT, [ctypes.c_uint32, INT, INT, INT, INT, INT, INT]),
+    "salsaa_ntt_tune_get": (INT, [ctypes.c_uint32, INT, INT, INT, INT, ctypes.POINTER(INT), ctypes.POINTER(INT)]),
 }
 
 ALL_SYMBOLS = {**HEXL_SYMBOLS, **DEVICE_SYMBOLS}

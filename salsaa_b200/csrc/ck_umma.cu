@@ -1052,7 +1052,7 @@ int tc_error_check() {
   cudaError_t e = cudaMemcpyFromSymbol(&h, g_tc_error, sizeof(u32));
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "tensor-core status");
   if (h) return salsaa_set_error(-4, "a tensor-core wait timed out; results of that launch are invalid");
-  return 0;
+  return ntt_error_check();
 }
 
 }  // namespace salsaa

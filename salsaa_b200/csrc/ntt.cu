@@ -1,11 +1,18 @@
 // ntt.cu — batched negacyclic NTT / INTT kernels and their twiddle tables.
+#include <dlfcn.h>
+
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
+#include <string>
 #include <tuple>
 #include <vector>
 
+#include "../../include/salsaa_gpu.h"
 #include "host_math.h"
 #include "ntt.cuh"
+#include "umma.cuh"
 
 namespace salsaa {
 
@@ -156,6 +163,99 @@ __global__ void __launch_bounds__(256) ntt_kernel(const u64* in, u64* out, u64 c
     }
     dstp[t] = sm[s];
   }
+}
+
+// ---------------------------------------------------------------------------
+// Kernel schedule of the register-path NTT per (log2 n, incomplete, inverse,
+// q >= 2^50, batch class: large = at least 2^22 coefficients): variant 0 = one 4096-coefficient tile per CTA (ntt_reg_kernel),
+// 2..4 = persistent CTAs with that many bulk-copy stages (ntt_pipe_kernel);
+// ctas_per_sm caps the resident CTAs per SM (0 = as many as fit).  The
+// defaults are variant 0; a table written by the tuner (salsaa_b200/tune.py)
+// replaces them: "ntt <log_n> <incomplete> <inverse> <wide> <large> <variant>
+// <ctas_per_sm>" per line, loaded from SALSAA_TUNE_FILE or from
+// tune_table.txt beside the library the first time a transform launches.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int TUNE_LOGN = 14;
+std::mutex g_tune_mu;
+NttChoice g_tune[TUNE_LOGN][2][2][2][2];
+bool g_tune_loaded = false;
+
+int tune_index_ok(u32 logn) { return logn < (u32)TUNE_LOGN; }
+
+int tune_load_locked(const char* path) {
+  FILE* f = fopen(path, "r");
+  if (!f) return -1;
+  char line[256];
+  int n = 0;
+  while (fgets(line, sizeof line, f)) {
+    unsigned lg, inc, inv, wide, big, var, cps;
+    if (sscanf(line, "ntt %u %u %u %u %u %u %u", &lg, &inc, &inv, &wide, &big, &var, &cps) != 7) continue;
+    if (lg >= (unsigned)TUNE_LOGN || inc > 1 || inv > 1 || wide > 1 || big > 1 ||
+        (var != 0 && (var < 2 || var > 4)) || cps > 8)
+      continue;
+    g_tune[lg][inc][inv][wide][big] = NttChoice{(uint8_t)var, (uint8_t)cps};
+    n++;
+  }
+  fclose(f);
+  return n;
+}
+
+// The library's own directory (for the default table beside it).
+std::string lib_dir() {
+  Dl_info info;
+  if (!dladdr((void*)&lib_dir, &info) || !info.dli_fname) return ".";
+  std::string p = info.dli_fname;
+  const size_t k = p.rfind('/');
+  return k == std::string::npos ? std::string(".") : p.substr(0, k);
+}
+
+void tune_default_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* env = getenv("SALSAA_TUNE_FILE");
+  const std::string path = env && *env ? std::string(env) : lib_dir() + "/tune_table.txt";
+  tune_load_locked(path.c_str());
+}
+}  // namespace
+
+NttChoice ntt_choice(u32 logn, bool incomplete, bool inverse, bool wide, bool large) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_default_locked();
+  if (!tune_index_ok(logn)) return NttChoice{0, 0};
+  return g_tune[logn][incomplete][inverse][wide][large];
+}
+
+int ntt_tune_set(u32 logn, bool incomplete, bool inverse, bool wide, bool large, int variant, int ctas_per_sm) {
+  if (!tune_index_ok(logn) || (variant != 0 && (variant < 2 || variant > 4)) || ctas_per_sm < 0 || ctas_per_sm > 8)
+    return salsaa_set_error(-2, "ntt_tune_set: log_n < 14, variant 0 or 2..4, ctas_per_sm 0..8");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_default_locked();
+  g_tune[logn][incomplete][inverse][wide][large] = NttChoice{(uint8_t)variant, (uint8_t)ctas_per_sm};
+  return 0;
+}
+
+int ntt_tune_load(const char* path) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_loaded = true;
+  if (!path) {
+    const char* env = getenv("SALSAA_TUNE_FILE");
+    const std::string p = env && *env ? std::string(env) : lib_dir() + "/tune_table.txt";
+    const int n = tune_load_locked(p.c_str());
+    return n < 0 ? salsaa_set_error(-1, ("tune_load: cannot read " + p).c_str()) : n;
+  }
+  const int n = tune_load_locked(path);
+  return n < 0 ? salsaa_set_error(-1, "tune_load: cannot read the table file") : n;
+}
+
+void ntt_tune_reset() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_loaded = true;  // defaults, and no automatic load afterwards
+  for (auto& a : g_tune)
+    for (auto& b : a)
+      for (auto& c : b)
+        for (auto& e : c)
+          for (auto& f : e) f = NttChoice{0, 0};
 }
 
 // ---------------------------------------------------------------------------
@@ -424,6 +524,128 @@ __global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u
   }
 }
 
+// ---------------------------------------------------------------------------
+// Bulk-copy staged ("pipe") variant of the register NTT.  The transform is
+// memory-latency bound for short n: one tile per CTA leaves the loads of the
+// next tile waiting behind the butterflies of this one.  Here each CTA is
+// persistent over tiles blockIdx.x, blockIdx.x + gridDim.x, ...; a tile's
+// input is contiguous in global memory (4096 coefficients = 32 KiB, whole
+// units or ring elements), so one thread fetches it with one
+// cp.async.bulk into a ring of STAGES shared-memory buffers, completing on
+// that stage's mbarrier, STAGES tiles ahead of the tile being transformed.
+// The first butterfly phase reads its registers from the staged copy (the
+// same element indices as the global loads of ntt_reg_kernel); the exchange
+// phases and the global stores are those of ntt_reg_kernel.
+//
+// Every mbarrier wait is bounded (umma::SPIN_LIMIT polls).  A CTA whose wait
+// gives up records it in g_ntt_error (read by ntt_error_check), waits
+// (bounded) for the copies it still has in flight and stops.
+// ---------------------------------------------------------------------------
+__device__ u32 g_ntt_error;
+
+template <int LOGN, bool INC, bool INV>
+__device__ __forceinline__ void nr_load_stage(u64 (&x)[16], const u64* stg, u32 unit, u32 tu) {
+  constexpr int S = ph_size(LOGN, 0);
+  constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
+#pragma unroll
+  for (u32 j = 0; j < MB; j++)
+#pragma unroll
+    for (u32 k = 0; k < K; k++) {
+      const u32 e = nr_elem<LOGN, 0, INV>(tu, j, k);
+      const u32 g = (INC && !INV) ? (unit >> 1) * (2 * N) + 2 * e + (unit & 1) : unit * N + e;
+      x[j * K + k] = stg[g];
+    }
+}
+
+constexpr u32 NP_ERR_WAIT = 0x4e54u;  // "NT": a stage's bulk copy did not complete in time
+
+template <int LOGN, bool INC, bool INV, bool RELAX, int STAGES>
+__global__ void __launch_bounds__(256) ntt_pipe_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
+  constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
+  constexpr int NPH = ph_count(LOGN);
+  static_assert(!INC || UPT % 2 == 0, "incomplete mode keeps both halves of an element in one tile");
+  extern __shared__ __align__(128) unsigned char np_smem[];
+  uint64_t* bar = (uint64_t*)np_smem;                                // STAGES mbarriers
+  u64* stg = (u64*)(np_smem + 128);                                  // STAGES x NR_TILE words
+  u64* sm = stg + (size_t)STAGES * NR_TILE;                          // padded exchange tile
+  u32 unit, tu;
+  nr_map<LOGN, INC>(threadIdx.x, unit, tu);
+  const u64 q = T.q, q2 = 2 * T.q;
+  const u64 ntiles = (units + UPT - 1) / UPT;
+  const u64 t0 = blockIdx.x, tstep = gridDim.x;
+  // bytes of tile t (a partial last tile holds whole units)
+  auto tile_bytes = [&](u64 t) -> u32 {
+    const u64 left = units - t * UPT;
+    return (u32)((left < UPT ? left : UPT) * N * sizeof(u64));
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) umma::mbar_init(&bar[s], 1);
+    umma::mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      const u64 t = t0 + (u64)s * tstep;
+      if (t >= ntiles) break;
+      const u32 b = tile_bytes(t);
+      umma::mbar_expect_tx(&bar[s], b);
+      umma::bulk_g2s(stg + (size_t)s * NR_TILE, in + t * NR_TILE, b, &bar[s]);
+    }
+  }
+  u64 mag = 0;
+  u64 i = 0;
+  for (u64 t = t0; t < ntiles; t += tstep, i++) {
+    const int s = (int)(i % STAGES);
+    const u32 par = (u32)((i / STAGES) & 1);
+    const bool ok = umma::mbar_wait(&bar[s], par, nullptr, 0);
+    if (__syncthreads_or(!ok)) {
+      // give up: record it, let the copies issued for later tiles land, stop
+      if (threadIdx.x == 0) {
+        atomicMax(&g_ntt_error, NP_ERR_WAIT);
+        for (u64 j = 0; j < (u64)STAGES && t + j * tstep < ntiles; j++) {
+          const int sj = (int)((i + j) % STAGES);
+          umma::mbar_wait(&bar[sj], (u32)(((i + j) / STAGES) & 1), nullptr, 0);
+        }
+      }
+      break;
+    }
+    const u64 ug = t * UPT + unit;
+    const bool active = ug < units;
+    u64 x[16];
+    if (active) nr_load_stage<LOGN, INC, INV>(x, stg + (size_t)s * NR_TILE, unit, tu);
+    __syncthreads();  // stage s is read: refill it with the tile STAGES ahead
+    if (threadIdx.x == 0) {
+      const u64 tn = t + (u64)STAGES * tstep;
+      if (tn < ntiles) {
+        const u32 b = tile_bytes(tn);
+        umma::mbar_expect_tx(&bar[s], b);
+        umma::bulk_g2s(stg + (size_t)s * NR_TILE, in + tn * NR_TILE, b, &bar[s]);
+      }
+    }
+    if (active) {
+      if (!INV && mag_or)
+#pragma unroll
+        for (u32 k = 0; k < 16; k++) mag |= nr_mag(x[k], q);
+      nr_compute<LOGN, 0, INV, RELAX>(x, tu, T, q, q2);
+    }
+    if constexpr (NPH > 1) {
+      if (active) nr_store_smem<LOGN, 0, INV>(x, sm, unit, tu);
+      __syncthreads();
+      nr_mid<LOGN, 1, NPH - 1, INV, RELAX>(x, sm, unit, tu, active, T, q, q2);
+      if (active) {
+        nr_load_smem<LOGN, NPH - 1, INV>(x, sm, unit, tu);
+        nr_compute<LOGN, NPH - 1, INV, RELAX>(x, tu, T, q, q2);
+      }
+    }
+    if (active) nr_store_global<LOGN, INC, INV, RELAX>(x, out, ug, tu, T, q, q2, INV && mag_or ? &mag : nullptr);
+  }
+  if (mag_or) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
+    if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
+  }
+}
+
 // Digit decomposition (decomp_ell, src/subroutines/decomp.rs:32-67) fused
 // with the forward incomplete transform.  Ring element r of the digit space is
 // (source element (k, i), digit c) with c fastest, so the warps that produce
@@ -587,6 +809,50 @@ int nm_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& T, cu
   return T.q < NR_RELAX_Q ? go(ntt_mul_kernel<LOGN, true>) : go(ntt_mul_kernel<LOGN, false>);
 }
 
+// Persistent bulk-copy pipeline: grid = min(tiles, SMs x resident CTAs),
+// capped at ctas_per_sm CTAs per SM when that is > 0.
+template <int LOGN, bool INC, bool INV, bool RELAX, int STAGES>
+int np_go(const u64* in, u64* out, u64 units, const NttDev& T, cudaStream_t st, u64* mag_or, int ctas_per_sm) {
+  constexpr u32 UPT = NR_TILE >> LOGN;
+  auto kern = ntt_pipe_kernel<LOGN, INC, INV, RELAX, STAGES>;
+  const size_t smem = 128 + ((size_t)STAGES * NR_TILE + NR_TILE + NR_TILE / 16) * sizeof(u64);
+  static int resident_dev[64][2] = {};  // per instantiation and device: attribute set, resident CTAs per SM
+  static std::mutex mu;
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return salsaa_set_error(-1, "ntt pipe: device query");
+  if (dev < 0 || dev >= 64) return salsaa_set_error(-1, "ntt pipe: device index out of range");
+  int* resident = resident_dev[dev];
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!resident[0]) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ntt pipe smem attribute");
+      int r = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, kern, 256, smem);
+      if (e != cudaSuccess || r < 1) return salsaa_set_error(-1, "ntt pipe: kernel does not fit an SM");
+      resident[1] = r;
+      resident[0] = 1;
+    }
+  }
+  const int per_sm = (ctas_per_sm > 0 && ctas_per_sm < resident[1]) ? ctas_per_sm : resident[1];
+  const u64 tiles = (units + UPT - 1) / UPT;
+  const u64 cap = (u64)nsm * (u64)per_sm;
+  const u64 blocks = tiles < cap ? tiles : cap;
+  kern<<<(unsigned)blocks, 256, smem, st>>>(in, out, units, T, mag_or);
+  return 0;
+}
+
+template <int LOGN, bool INC, bool INV, bool RELAX>
+int np_launch(const u64* in, u64* out, u64 units, const NttDev& T, cudaStream_t st, u64* mag_or, int stages,
+              int ctas_per_sm) {
+  switch (stages) {
+    case 2: return np_go<LOGN, INC, INV, RELAX, 2>(in, out, units, T, st, mag_or, ctas_per_sm);
+    case 3: return np_go<LOGN, INC, INV, RELAX, 3>(in, out, units, T, st, mag_or, ctas_per_sm);
+    default: return np_go<LOGN, INC, INV, RELAX, 4>(in, out, units, T, st, mag_or, ctas_per_sm);
+  }
+}
+
 template <int LOGN>
 int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomplete, bool inverse, cudaStream_t st,
               u64* mag_or) {
@@ -594,6 +860,24 @@ int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomple
   const u64 blocks = (units + UPT - 1) / UPT;
   if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt: batch too large");
   const bool relax = T.q < NR_RELAX_Q;
+  const NttChoice ch = ntt_choice(LOGN, incomplete, inverse, !relax, units * (1ULL << LOGN) >= NTT_LARGE_COEFFS);
+  if (ch.variant >= 2 && (!incomplete || UPT >= 2)) {
+    if (incomplete) {
+      if constexpr (UPT >= 2) {
+        if (inverse)
+          return relax ? np_launch<LOGN, true, true, true>(in, out, units, T, st, mag_or, ch.variant, ch.ctas_per_sm)
+                       : np_launch<LOGN, true, true, false>(in, out, units, T, st, mag_or, ch.variant, ch.ctas_per_sm);
+        return relax ? np_launch<LOGN, true, false, true>(in, out, units, T, st, mag_or, ch.variant, ch.ctas_per_sm)
+                     : np_launch<LOGN, true, false, false>(in, out, units, T, st, mag_or, ch.variant, ch.ctas_per_sm);
+      }
+    } else {
+      if (inverse)
+        return relax ? np_launch<LOGN, false, true, true>(in, out, units, T, st, mag_or, ch.variant, ch.ctas_per_sm)
+                     : np_launch<LOGN, false, true, false>(in, out, units, T, st, mag_or, ch.variant, ch.ctas_per_sm);
+      return relax ? np_launch<LOGN, false, false, true>(in, out, units, T, st, mag_or, ch.variant, ch.ctas_per_sm)
+                   : np_launch<LOGN, false, false, false>(in, out, units, T, st, mag_or, ch.variant, ch.ctas_per_sm);
+    }
+  }
   auto go = [&](auto kern) -> int {
     kern<<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T, mag_or);
     return 0;
@@ -740,3 +1024,36 @@ int ntt_mul_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& 
 }
 
 }  // namespace salsaa
+
+namespace salsaa {
+int ntt_error_check() {
+  u32 h = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&h, g_ntt_error, sizeof(u32));
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ntt status");
+  if (h) return salsaa_set_error(-4, "a bulk-copy wait of the NTT timed out; results of that launch are invalid");
+  return 0;
+}
+}  // namespace salsaa
+
+extern "C" int salsaa_tune_load(const char* path) { return salsaa::ntt_tune_load(path); }
+
+extern "C" int salsaa_tune_reset(void) {
+  salsaa::ntt_tune_reset();
+  return 0;
+}
+
+extern "C" int salsaa_ntt_tune_set(uint32_t log_n, int incomplete, int inverse, int wide_modulus, int large,
+                                   int variant, int ctas_per_sm) {
+  return salsaa::ntt_tune_set(log_n, incomplete != 0, inverse != 0, wide_modulus != 0, large != 0, variant,
+                              ctas_per_sm);
+}
+
+extern "C" int salsaa_ntt_tune_get(uint32_t log_n, int incomplete, int inverse, int wide_modulus, int large,
+                                   int* variant, int* ctas_per_sm) {
+  if (!variant || !ctas_per_sm) return salsaa_set_error(-1, "ntt_tune_get: null argument");
+  const salsaa::NttChoice c =
+      salsaa::ntt_choice(log_n, incomplete != 0, inverse != 0, wide_modulus != 0, large != 0);
+  *variant = c.variant;
+  *ctas_per_sm = c.ctas_per_sm;
+  return 0;
+}

@@ -29,6 +29,19 @@ struct NttDev {
 // process lifetime (thread-safe).  Returns nullptr when q has no 2n-th root.
 const NttDev* ntt_tables(u32 n, u64 q);
 
+// Kernel schedule of the register-path transform (see ntt.cu): variant 0 =
+// one tile per CTA, 2..4 = persistent CTAs with that many bulk-copy stages;
+// ctas_per_sm caps resident CTAs per SM (0 = no cap).
+struct NttChoice {
+  uint8_t variant, ctas_per_sm;
+};
+constexpr u64 NTT_LARGE_COEFFS = 1ULL << 22;  // batch class "large": at least this many coefficients per launch
+NttChoice ntt_choice(u32 logn, bool incomplete, bool inverse, bool wide, bool large);
+int ntt_tune_set(u32 logn, bool incomplete, bool inverse, bool wide, bool large, int variant, int ctas_per_sm);
+int ntt_tune_load(const char* path);  // number of entries read, or < 0
+void ntt_tune_reset();
+int ntt_error_check();  // a bounded wait of the pipelined transform gave up
+
 // count units of n (full) or ring elements of 2n (incomplete); in may equal out.
 // With mag_or (register path only, ntt_mag_ok), the bitwise OR of the centred
 // magnitudes min(v, q - v) of the coefficient-form side (the input of a
