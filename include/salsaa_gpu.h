@@ -120,6 +120,11 @@ typedef struct salsaa_timing {
 const char* salsaa_last_error(void);
 /* Kernel launches this library has issued since it was loaded. */
 uint64_t salsaa_kernel_launches(void);
+/* 0 while no bounded wait inside a kernel (tensor-core and bulk-copy
+ * mbarriers of the current device) has given up; -4 with a message once one
+ * has, in which case the results of that launch are invalid.  Call it after
+ * the launches in question have finished (after synchronizing their stream). */
+int salsaa_device_status(void);
 /* Device-time trace for measurement (off by default): enable/reset, then read
  * the summed device time (CUDA events on the launching stream), summed
  * algorithmic work and launch count of a traced kernel by name.  Traced:

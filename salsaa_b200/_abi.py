@@ -48,6 +48,7 @@ PP = ctypes.POINTER(SalsaaParams)
 DEVICE_SYMBOLS = {
     "salsaa_last_error": (ctypes.c_char_p, []),
     "salsaa_kernel_launches": (U64, []),
+    "salsaa_device_status": (INT, []),
     "salsaa_trace_enable": (None, [INT]),
     "salsaa_trace_read": (INT, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                 ctypes.POINTER(U64)]),

@@ -3,6 +3,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <type_traits>
 #include <map>
 #include <mutex>
 #include <string>
@@ -72,7 +73,34 @@ const NttDev* ntt_tables(u32 n, u64 q) {
     cudaFree(d);
     return nullptr;
   }
+  // FP64 companions: exact doubles of the twiddles (w < q < 2^53) and the
+  // correctly rounded quotients w / 2q
+  std::vector<double> hd(4 * (size_t)n);
+  const double q2d = 2.0 * (double)q;
+  for (u64 i = 0; i < n; i++) {
+    hd[i] = (double)fwd[i];
+    hd[n + i] = (double)fwd[i] / q2d;
+    hd[2 * n + i] = (double)inv[i];
+    hd[3 * n + i] = (double)inv[i] / q2d;
+  }
+  double* dd = nullptr;
+  if (cudaMalloc(&dd, hd.size() * sizeof(double)) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  if (cudaMemcpy(dd, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    cudaFree(dd);
+    return nullptr;
+  }
   NttDev* T = new NttDev;
+  T->fwd_d = dd;
+  T->fwd_h = dd + n;
+  T->inv_d = dd + 2 * n;
+  T->inv_h = dd + 3 * n;
+  T->qd = (double)q;
+  T->q2d = q2d;
+  T->qinv = 1.0 / (double)q;
   T->q = q;
   T->n = n;
   T->logn = logn;
@@ -85,6 +113,8 @@ const NttDev* ntt_tables(u32 n, u64 q) {
   T->ninv = host::invmod(n % q, q);
   T->ninvp = shoup_pre(T->ninv, q);
   T->onep = shoup_pre(1, q);
+  T->ninv_d = (double)T->ninv;
+  T->ninv_h = (double)T->ninv / q2d;
   g_tabs[key] = T;
   return T;
 }
@@ -167,7 +197,10 @@ __global__ void __launch_bounds__(256) ntt_kernel(const u64* in, u64* out, u64 c
 
 // ---------------------------------------------------------------------------
 // Kernel schedule of the register-path NTT per (log2 n, incomplete, inverse,
-// q >= 2^50, batch class: large = at least 2^22 coefficients): variant 0 = one 4096-coefficient tile per CTA (ntt_reg_kernel),
+// q >= 2^50, batch class: large = at least 2^22 coefficients): variant 0 =
+// one 4096-coefficient tile per CTA with integer butterflies
+// (ntt_reg_kernel), 1 = the same with FP64 butterflies (ntt_fp_kernel; used
+// only when q < 2^50, and also selecting the digit transform's arithmetic),
 // 2..4 = persistent CTAs with that many bulk-copy stages (ntt_pipe_kernel);
 // ctas_per_sm caps the resident CTAs per SM (0 = as many as fit).  The
 // defaults are variant 0; a table written by the tuner (salsaa_b200/tune.py)
@@ -192,7 +225,7 @@ int tune_load_locked(const char* path) {
     unsigned lg, inc, inv, wide, big, var, cps;
     if (sscanf(line, "ntt %u %u %u %u %u %u %u", &lg, &inc, &inv, &wide, &big, &var, &cps) != 7) continue;
     if (lg >= (unsigned)TUNE_LOGN || inc > 1 || inv > 1 || wide > 1 || big > 1 ||
-        (var != 0 && (var < 2 || var > 4)) || cps > 8)
+        var > 4 || cps > 8)
       continue;
     g_tune[lg][inc][inv][wide][big] = NttChoice{(uint8_t)var, (uint8_t)cps};
     n++;
@@ -227,8 +260,8 @@ NttChoice ntt_choice(u32 logn, bool incomplete, bool inverse, bool wide, bool la
 }
 
 int ntt_tune_set(u32 logn, bool incomplete, bool inverse, bool wide, bool large, int variant, int ctas_per_sm) {
-  if (!tune_index_ok(logn) || (variant != 0 && (variant < 2 || variant > 4)) || ctas_per_sm < 0 || ctas_per_sm > 8)
-    return salsaa_set_error(-2, "ntt_tune_set: log_n < 14, variant 0 or 2..4, ctas_per_sm 0..8");
+  if (!tune_index_ok(logn) || variant < 0 || variant > 4 || ctas_per_sm < 0 || ctas_per_sm > 8)
+    return salsaa_set_error(-2, "ntt_tune_set: log_n < 14, variant 0..4, ctas_per_sm 0..8");
   std::lock_guard<std::mutex> lk(g_tune_mu);
   tune_default_locked();
   g_tune[logn][incomplete][inverse][wide][large] = NttChoice{(uint8_t)variant, (uint8_t)ctas_per_sm};
@@ -367,8 +400,8 @@ __device__ __forceinline__ u32 nr_elem(u32 tu, u32 j, u32 k) {
 
 // Shared-memory exchange: a thread reads and writes the same positions within
 // a phase, so a phase can update the tile in place.
-template <int LOGN, int P, bool INV>
-__device__ __forceinline__ void nr_load_smem(u64 (&x)[16], const u64* sm, u32 unit, u32 tu) {
+template <int LOGN, int P, bool INV, typename W>
+__device__ __forceinline__ void nr_load_smem(W (&x)[16], const W* sm, u32 unit, u32 tu) {
   constexpr int S = ph_size(LOGN, P);
   constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
 #pragma unroll
@@ -376,8 +409,8 @@ __device__ __forceinline__ void nr_load_smem(u64 (&x)[16], const u64* sm, u32 un
 #pragma unroll
     for (u32 k = 0; k < K; k++) x[j * K + k] = sm[npad(unit * N + nr_elem<LOGN, P, INV>(tu, j, k))];
 }
-template <int LOGN, int P, bool INV>
-__device__ __forceinline__ void nr_store_smem(const u64 (&x)[16], u64* sm, u32 unit, u32 tu) {
+template <int LOGN, int P, bool INV, typename W>
+__device__ __forceinline__ void nr_store_smem(const W (&x)[16], W* sm, u32 unit, u32 tu) {
   constexpr int S = ph_size(LOGN, P);
   constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
 #pragma unroll
@@ -612,8 +645,20 @@ __global__ void __launch_bounds__(256) ntt_pipe_kernel(const u64* in, u64* out, 
     const u64 ug = t * UPT + unit;
     const bool active = ug < units;
     u64 x[16];
-    if (active) nr_load_stage<LOGN, INC, INV>(x, stg + (size_t)s * NR_TILE, unit, tu);
-    __syncthreads();  // stage s is read: refill it with the tile STAGES ahead
+    if (active) {
+      nr_load_stage<LOGN, INC, INV>(x, stg + (size_t)s * NR_TILE, unit, tu);
+      if (!INV && mag_or)
+#pragma unroll
+        for (u32 k = 0; k < 16; k++) mag |= nr_mag(x[k], q);
+      nr_compute<LOGN, 0, INV, RELAX>(x, tu, T, q, q2);
+    }
+    // Stage s is refilled with the tile STAGES ahead only after every thread
+    // has consumed its values (the butterflies above use them) and ordered its
+    // generic-proxy reads before the bulk copy's async-proxy writes.
+    umma::fence_proxy_async();
+    if constexpr (NPH > 1)
+      if (active) nr_store_smem<LOGN, 0, INV>(x, sm, unit, tu);
+    __syncthreads();
     if (threadIdx.x == 0) {
       const u64 tn = t + (u64)STAGES * tstep;
       if (tn < ntiles) {
@@ -622,15 +667,7 @@ __global__ void __launch_bounds__(256) ntt_pipe_kernel(const u64* in, u64* out, 
         umma::bulk_g2s(stg + (size_t)s * NR_TILE, in + tn * NR_TILE, b, &bar[s]);
       }
     }
-    if (active) {
-      if (!INV && mag_or)
-#pragma unroll
-        for (u32 k = 0; k < 16; k++) mag |= nr_mag(x[k], q);
-      nr_compute<LOGN, 0, INV, RELAX>(x, tu, T, q, q2);
-    }
     if constexpr (NPH > 1) {
-      if (active) nr_store_smem<LOGN, 0, INV>(x, sm, unit, tu);
-      __syncthreads();
       nr_mid<LOGN, 1, NPH - 1, INV, RELAX>(x, sm, unit, tu, active, T, q, q2);
       if (active) {
         nr_load_smem<LOGN, NPH - 1, INV>(x, sm, unit, tu);
@@ -646,6 +683,191 @@ __global__ void __launch_bounds__(256) ntt_pipe_kernel(const u64* in, u64* out, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 butterflies for q < 2^50 (the protocol's primes).  On B200 the FP64
+// pipe multiplies and adds 53-bit integers exactly at a far higher rate than
+// the 32-bit integer multipliers assemble 64-bit Shoup products, so these
+// kernels keep the coefficients as integer-valued doubles and reduce with
+// error-free transformations (Dekker's exact product via FMA, as used for
+// modular arithmetic in floating point by van der Hoeven, Lecerf and Quintin,
+// "Modular SIMD arithmetic in Mathemagix", ACM TOMS 2016):
+//
+//   x * w mod q, |x| < 2^52, 0 <= w < q:  h = fl(x w), l = x w - h (one FMA,
+//   exact), c = nearest integer to x fl(w / 2q) (one FMA against the
+//   rounding constant 1.5 * 2^52 and one subtraction), r = (h - 2q c) + l.
+//   Since |x w / 2q - c| <= 0.625 the integer x w - 2q c has magnitude at most
+//   1.25 q < 2^51, so the FMA h - 2q c and the addition of l are exact: r is
+//   x w mod q as an integer in [-1.25 q, 1.25 q].
+//
+//   v mod q, |v| < 2^52: c = nearest integer to v fl(1/q), r = v - c q
+//   (exact, in [-q/2 - 1, q/2 + 1]).
+//
+// Forward (Cooley-Tukey): inputs in [0, q); each stage adds at most 1.25 q
+// to a magnitude; all values are reduced after every odd-numbered stage, so
+// magnitudes stay below 4 q < 2^52 and multiplicands below 2.5 q.  Inverse
+// (Gentleman-Sande): the sum a + b is reduced in every stage (magnitudes of
+// sums below 3 q, of differences below 3 q, of products below 1.25 q).  The
+// outputs are reduced once more and shifted into [0, q), so they are the
+// canonical residues, the same words as the integer kernels produce.
+// Conversions between canonical words and doubles go through the exponent
+// bits of 2^52 (v + 2^52 has v in its low 52 mantissa bits), one integer
+// and one FP64 instruction each.
+// ---------------------------------------------------------------------------
+constexpr double FP_MAGIC = 6755399441055744.0;  // 1.5 * 2^52: fl(t + M) - M rounds |t| < 2^51 to an integer
+constexpr double FP_TWO52 = 4503599627370496.0;  // 2^52
+
+__device__ __forceinline__ double fp_mulmod(double x, double w, double wh, double q2d) {
+  const double h = __dmul_rn(x, w);
+  const double l = __fma_rn(x, w, -h);
+  const double c = __dsub_rn(__fma_rn(x, wh, FP_MAGIC), FP_MAGIC);
+  return __dadd_rn(__fma_rn(-c, q2d, h), l);
+}
+__device__ __forceinline__ double fp_reduce(double v, double qinv, double qd) {
+  const double c = __dsub_rn(__fma_rn(v, qinv, FP_MAGIC), FP_MAGIC);
+  return __fma_rn(-c, qd, v);
+}
+// canonical word (< 2^52) -> double, and a reduced-range double -> canonical word
+__device__ __forceinline__ double fp_from_word(u64 v) {
+  return __dsub_rn(__longlong_as_double((long long)(v | 0x4330000000000000ULL)), FP_TWO52);
+}
+__device__ __forceinline__ u64 fp_to_word(double v, double qinv, double qd) {
+  v = fp_reduce(v, qinv, qd);
+  v = v < 0.0 ? __dadd_rn(v, qd) : v;
+  return (u64)__double_as_longlong(__dadd_rn(v, FP_TWO52)) & 0x000FFFFFFFFFFFFFULL;
+}
+
+template <int LOGN, int P, bool INV>
+__device__ __forceinline__ void nf_compute(double (&x)[16], u32 tu, const NttDev& T) {
+  constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
+  constexpr u32 N = 1u << LOGN, TPU = N / 16, MB = 16 >> S, K = 1u << S;
+  constexpr u32 LSTR = INV ? G0 : LOGN - G0 - S;
+  const double q2d = T.q2d, qd = T.qd, qinv = T.qinv;
+#pragma unroll
+  for (u32 j = 0; j < MB; j++) {
+    const u32 mb = tu + j * TPU, blk = mb >> LSTR;
+    double* v = x + j * (1u << S);
+#pragma unroll
+    for (int l = 0; l < S; l++) {
+      const u32 lt = INV ? l : S - 1 - l;
+      const u32 t = 1u << lt;
+      double w = 0, wh = 0;
+#pragma unroll
+      for (u32 p = 0; p < K / 2; p++) {
+        const u32 sb = p >> lt, kk = p & (t - 1), k = (sb << (lt + 1)) + kk;
+        if (kk == 0) {
+          const u32 idx = INV ? (N >> (G0 + l + 1)) + (blk << (S - l - 1)) + sb : (1u << (G0 + l)) + (blk << l) + sb;
+          w = __ldg((INV ? T.inv_d : T.fwd_d) + idx);
+          wh = __ldg((INV ? T.inv_h : T.fwd_h) + idx);
+        }
+        const double a = v[k], b = v[k + t];
+        if (!INV) {
+          const double m = fp_mulmod(b, w, wh, q2d);
+          v[k] = __dadd_rn(a, m);
+          v[k + t] = __dsub_rn(a, m);
+        } else {
+          v[k] = fp_reduce(__dadd_rn(a, b), qinv, qd);
+          v[k + t] = fp_mulmod(__dsub_rn(a, b), w, wh, q2d);
+        }
+      }
+      if (!INV && ((G0 + l) & 1)) {
+#pragma unroll
+        for (u32 i = 0; i < K; i++) v[i] = fp_reduce(v[i], qinv, qd);
+      }
+    }
+  }
+}
+
+// First-phase loads (as nr_load_global) converted to doubles; the OR of the
+// centred magnitudes of the loaded words goes to *mag when mag is not null.
+template <int LOGN, bool INC, bool INV>
+__device__ __forceinline__ void nf_load_global(double (&x)[16], const u64* __restrict__ in, u64 ug, u32 tu,
+                                               u64 q, u64* mag) {
+  u64 w[16];
+  nr_load_global<LOGN, INC, INV>(w, in, ug, tu);
+#pragma unroll
+  for (u32 i = 0; i < 16; i++) {
+    if (mag) *mag |= nr_mag(w[i], q);
+    x[i] = fp_from_word(w[i]);
+  }
+}
+
+// Last-phase stores (as nr_store_global): canonical words, the inverse scaled by 1/n.
+template <int LOGN, bool INC, bool INV>
+__device__ __forceinline__ void nf_store_global(const double (&x)[16], u64* __restrict__ out, u64 ug, u32 tu,
+                                                const NttDev& T, u64* mag) {
+  constexpr int P = ph_count(LOGN) - 1, S = ph_size(LOGN, P);
+  constexpr u32 N = 1u << LOGN, MB = 16 >> S, K = 1u << S;
+  const double qd = T.qd, qinv = T.qinv;
+  if (!INV) {
+#pragma unroll
+    for (u32 j = 0; j < MB; j++) {
+      ulonglong2* dst = (ulonglong2*)(out + ug * N + nr_elem<LOGN, P, INV>(tu, j, 0));
+#pragma unroll
+      for (u32 k = 0; k < K / 2; k++)
+        dst[k] = make_ulonglong2(fp_to_word(x[j * K + 2 * k], qinv, qd), fp_to_word(x[j * K + 2 * k + 1], qinv, qd));
+    }
+  } else {
+#pragma unroll
+    for (u32 j = 0; j < MB; j++)
+#pragma unroll
+      for (u32 k = 0; k < K; k++) {
+        const u32 e = nr_elem<LOGN, P, INV>(tu, j, k);
+        const u64 v = fp_to_word(fp_mulmod(x[j * K + k], T.ninv_d, T.ninv_h, T.q2d), qinv, qd);
+        const u64 g = INC ? (ug >> 1) * (2 * N) + 2 * e + (ug & 1) : ug * N + e;
+        out[g] = v;
+        if (mag) *mag |= nr_mag(v, T.q);
+      }
+  }
+}
+
+template <int LOGN, int P, int PEND, bool INV>
+__device__ __forceinline__ void nf_mid(double (&x)[16], double* sm, u32 unit, u32 tu, bool active, const NttDev& T) {
+  if constexpr (P < PEND) {
+    if (active) {
+      nr_load_smem<LOGN, P, INV>(x, sm, unit, tu);
+      nf_compute<LOGN, P, INV>(x, tu, T);
+      nr_store_smem<LOGN, P, INV>(x, sm, unit, tu);
+    }
+    __syncthreads();
+    nf_mid<LOGN, P + 1, PEND, INV>(x, sm, unit, tu, active, T);
+  }
+}
+
+// The register NTT (ntt_reg_kernel's thread mapping, phases and exchanges)
+// with FP64 butterflies; q < 2^50 and canonical inputs.
+template <int LOGN, bool INC, bool INV>
+__global__ void __launch_bounds__(256) ntt_fp_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
+  constexpr u32 UPT = NR_TILE >> LOGN;
+  constexpr int NPH = ph_count(LOGN);
+  static_assert(!INC || UPT % 2 == 0, "incomplete mode keeps both halves of an element in one tile");
+  __shared__ double sm[NR_TILE + NR_TILE / 16];
+  u32 unit, tu;
+  nr_map<LOGN, INC>(threadIdx.x, unit, tu);
+  const u64 ug = (u64)blockIdx.x * UPT + unit;
+  const bool active = ug < units;
+  double x[16];
+  u64 mag = 0;
+  if (active) {
+    nf_load_global<LOGN, INC, INV>(x, in, ug, tu, T.q, !INV && mag_or ? &mag : nullptr);
+    nf_compute<LOGN, 0, INV>(x, tu, T);
+  }
+  if constexpr (NPH > 1) {
+    if (active) nr_store_smem<LOGN, 0, INV>(x, sm, unit, tu);
+    __syncthreads();
+    nf_mid<LOGN, 1, NPH - 1, INV>(x, sm, unit, tu, active, T);
+    if (active) {
+      nr_load_smem<LOGN, NPH - 1, INV>(x, sm, unit, tu);
+      nf_compute<LOGN, NPH - 1, INV>(x, tu, T);
+    }
+  }
+  if (active) nf_store_global<LOGN, INC, INV>(x, out, ug, tu, T, INV && mag_or ? &mag : nullptr);
+  if (mag_or) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
+    if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
+  }
+}
+
 // Digit decomposition (decomp_ell, src/subroutines/decomp.rs:32-67) fused
 // with the forward incomplete transform.  Ring element r of the digit space is
 // (source element (k, i), digit c) with c fastest, so the warps that produce
@@ -653,15 +875,17 @@ __global__ void __launch_bounds__(256) ntt_pipe_kernel(const u64* in, u64* out, 
 // source once; digit c = ((pos >> c rlog) & mask) - ((neg >> c rlog) & mask)
 // of the centre-lifted coefficient (pos or neg its magnitude) goes to row
 // k * parts + c of dc, and its transform to the same row of ds.
-template <int LOGN, bool RELAX>
+template <int LOGN, bool RELAX, bool FP>
 __global__ void __launch_bounds__(256)
     ntt_digits_kernel(NttSrcRows src, u64 width, u32 parts, const u64* bw_or, u64* rlog_out, u64* radix_out, u64* dc,
                       u64* ds, u64 units, NttDev T) {
+  // FP: the FP64 butterflies (q < 2^50), else the integer ones
+  using Wd = typename std::conditional<FP, double, u64>::type;
   constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N, D = 2 * N;
   constexpr int NPH = ph_count(LOGN);
   constexpr int S0 = ph_size(LOGN, 0);
   constexpr u32 MB = 16 >> S0, KB = 1u << S0;
-  __shared__ u64 sm[NR_TILE + NR_TILE / 16];
+  __shared__ Wd sm[NR_TILE + NR_TILE / 16];
   u32 unit, tu;
   nr_map<LOGN, true>(threadIdx.x, unit, tu);
   const u64 ug = (u64)blockIdx.x * UPT + unit;
@@ -682,7 +906,7 @@ __global__ void __launch_bounds__(256)
   const u64 i = se % width;
   const u64 dring = ((u64)k * parts + c) * width + i;  // output ring element
   const u32 sh = rlog * c;
-  u64 x[16];
+  Wd x[16];
   if (active) {
     const u64* sp = src.p[k] + i * D + h;
     u64* dco = dc + dring * D + h;
@@ -695,22 +919,39 @@ __global__ void __launch_bounds__(256)
         const u64 pos = 2 * v > q ? 0 : v, neg = 2 * v > q ? q - v : 0;
         const u64 pd = sh >= 64 ? 0 : ((pos >> sh) & mask), nd = sh >= 64 ? 0 : ((neg >> sh) & mask);
         const u64 dv = pd >= nd ? pd - nd : pd + q - nd;
-        x[j * KB + kk] = dv;
+        if constexpr (FP)
+          x[j * KB + kk] = fp_from_word(dv);
+        else
+          x[j * KB + kk] = dv;
         dco[2 * e] = dv;
       }
-    nr_compute<LOGN, 0, false, RELAX>(x, tu, T, q, q2);
+    if constexpr (FP)
+      nf_compute<LOGN, 0, false>(x, tu, T);
+    else
+      nr_compute<LOGN, 0, false, RELAX>(x, tu, T, q, q2);
   }
   if constexpr (NPH > 1) {
     if (active) nr_store_smem<LOGN, 0, false>(x, sm, unit, tu);
     __syncthreads();
-    nr_mid<LOGN, 1, NPH - 1, false, RELAX>(x, sm, unit, tu, active, T, q, q2);
+    if constexpr (FP)
+      nf_mid<LOGN, 1, NPH - 1, false>(x, sm, unit, tu, active, T);
+    else
+      nr_mid<LOGN, 1, NPH - 1, false, RELAX>(x, sm, unit, tu, active, T, q, q2);
     if (active) {
       nr_load_smem<LOGN, NPH - 1, false>(x, sm, unit, tu);
-      nr_compute<LOGN, NPH - 1, false, RELAX>(x, tu, T, q, q2);
+      if constexpr (FP)
+        nf_compute<LOGN, NPH - 1, false>(x, tu, T);
+      else
+        nr_compute<LOGN, NPH - 1, false, RELAX>(x, tu, T, q, q2);
     }
   }
   // forward output of unit (dring, half h) at ds + (2 dring + h) N
-  if (active) nr_store_global<LOGN, true, false, RELAX>(x, ds, 2 * dring + h, tu, T, q, q2);
+  if (active) {
+    if constexpr (FP)
+      nf_store_global<LOGN, true, false>(x, ds, 2 * dring + h, tu, T, nullptr);
+    else
+      nr_store_global<LOGN, true, false, RELAX>(x, ds, 2 * dring + h, tu, T, q, q2);
+  }
 }
 
 // Fused negacyclic product r = a * b mod (Y^n + 1) for a batch of polynomials:
@@ -861,6 +1102,18 @@ int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomple
   if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt: batch too large");
   const bool relax = T.q < NR_RELAX_Q;
   const NttChoice ch = ntt_choice(LOGN, incomplete, inverse, !relax, units * (1ULL << LOGN) >= NTT_LARGE_COEFFS);
+  if (ch.variant == 1 && relax) {  // FP64 butterflies
+    auto gof = [&](auto kern) -> int {
+      kern<<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T, mag_or);
+      return 0;
+    };
+    if (incomplete) {
+      if constexpr (UPT >= 2)
+        return inverse ? gof(ntt_fp_kernel<LOGN, true, true>) : gof(ntt_fp_kernel<LOGN, true, false>);
+    } else {
+      return inverse ? gof(ntt_fp_kernel<LOGN, false, true>) : gof(ntt_fp_kernel<LOGN, false, false>);
+    }
+  }
   if (ch.variant >= 2 && (!incomplete || UPT >= 2)) {
     if (incomplete) {
       if constexpr (UPT >= 2) {
@@ -959,12 +1212,18 @@ int nd_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* 
   const u64 units = 2ULL * rows * parts * width;
   const u64 blocks = (units + UPT - 1) / UPT;
   if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt_digits: batch too large");
-  if (T.q < NR_RELAX_Q)
-    ntt_digits_kernel<LOGN, true><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out, radix_out,
-                                                                     dc, ds, units, T);
+  // the forward incomplete transform's schedule decides the arithmetic
+  const bool relax = T.q < NR_RELAX_Q;
+  const bool fp = relax && ntt_choice(LOGN, true, false, false, units * (1ULL << LOGN) >= NTT_LARGE_COEFFS).variant == 1;
+  if (fp)
+    ntt_digits_kernel<LOGN, true, true><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
+                                                                           radix_out, dc, ds, units, T);
+  else if (relax)
+    ntt_digits_kernel<LOGN, true, false><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
+                                                                            radix_out, dc, ds, units, T);
   else
-    ntt_digits_kernel<LOGN, false><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out, radix_out,
-                                                                      dc, ds, units, T);
+    ntt_digits_kernel<LOGN, false, false><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
+                                                                             radix_out, dc, ds, units, T);
   return 0;
 }
 

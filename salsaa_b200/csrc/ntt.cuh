@@ -23,6 +23,13 @@ struct NttDev {
   u64 onep;         // Shoup companion of 1: floor(2^64 / q), for reductions
   const u64* zeta;  // shift factors NTT_n(Y) (slot order), for ring products
   const u64* zetap;
+  // FP64 form of the tables for q < 2^50 (the FP64 butterflies in ntt.cu):
+  // each twiddle w as a double and fl(w / 2q); q, 2q and fl(1/q).
+  const double* fwd_d;
+  const double* fwd_h;
+  const double* inv_d;
+  const double* inv_h;
+  double qd, q2d, qinv, ninv_d, ninv_h;
 };
 
 // Tables for (n, q) on the current device, built once and kept for the

@@ -112,6 +112,7 @@ extern "C" int salsaa_trace_read(const char* name, double* total_ms, double* tot
 static std::atomic<uint64_t> g_launches{0};
 void salsaa_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 extern "C" uint64_t salsaa_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+extern "C" int salsaa_device_status(void) { return salsaa::tc_error_check(); }
 
 #define TRY(x)            \
   do {                    \

@@ -2,11 +2,12 @@
 
 The register-path negacyclic NTT (salsaa_ntt and every transform inside the
 prover) has several kernel schedules that give identical outputs: one
-4096-coefficient tile per CTA, or persistent CTAs that stage tiles through
-shared memory with bulk copies 2, 3 or 4 tiles ahead, optionally capped at one
-CTA per SM.  Which is fastest depends on the transform size, the direction,
-the modulus width and the batch size, so this script times every candidate on
-the GPU for each key (log2 n, incomplete, inverse, q >= 2^50, large batch),
+4096-coefficient tile per CTA with integer (64-bit Shoup) butterflies, the
+same with FP64 butterflies (for the protocol's primes below 2^50), or
+persistent CTAs that stage tiles through shared memory with bulk copies 2, 3
+or 4 tiles ahead, optionally capped at one CTA per SM.  Which is fastest
+depends on the transform size, the direction, the modulus width and the batch
+size, so this script times every candidate on the GPU for each key (log2 n, incomplete, inverse, q >= 2^50, large batch),
 checks that each candidate's output equals the default schedule's bit for bit,
 and writes the winners to a table the library loads at its first transform
 (tune_table.txt beside the library, or $SALSAA_TUNE_FILE).
@@ -25,8 +26,9 @@ from .params import Q0, Q1, Q2, Q62
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_TABLE = os.path.join(HERE, "tune_table.txt")
 
-# (variant, ctas_per_sm): 0 = one tile per CTA; 2..4 = bulk-copy stages ahead
-CANDIDATES = [(0, 0), (2, 0), (2, 1), (3, 0), (4, 0)]
+# (variant, ctas_per_sm): 0 = one tile per CTA, integer butterflies; 1 = the
+# same with FP64 butterflies (q < 2^50 only); 2..4 = bulk-copy stages ahead
+CANDIDATES = [(0, 0), (1, 0), (2, 0), (2, 1), (3, 0), (4, 0)]
 SMALL_COEFFS = 1 << 20  # a "small" call (below the library's 2^22 large-batch class)
 LARGE_COEFFS = 1 << 27  # a "large" call: 1 GiB of coefficients, far above L2
 
@@ -93,6 +95,8 @@ def tune(reps=10, quick=False, verbose=True):
                 key = _key(n_arg, incomplete, q, inverse, large)
                 times = {}
                 for var, cps in CANDIDATES:
+                    if var == 1 and q >= (1 << 50):
+                        continue
                     _check(L.salsaa_ntt_tune_set(key[0], key[1], key[2], key[3], key[4], var, cps), "tune_set")
                     ms = time_schedule(torch, x, out, n_arg, incomplete, q, inverse, reps)
                     if (var, cps) == (0, 0):
