@@ -245,7 +245,7 @@ void salsaa_server_destroy(salsaa_server* s);
  * every variant gives the same outputs.  Untuned default: variant 0.
  * salsaa_b200/tune.py times the candidates on the GPU and writes a table file
  * ("ntt <log_n> <incomplete> <inverse> <wide> <large> <variant> <ctas_per_sm>"
- * per line); the library loads it the first time a
+ * per line, and the "fold" line below); the library loads it the first time a
  * transform launches, from $SALSAA_TUNE_FILE or tune_table.txt beside the
  * library.  salsaa_tune_load(NULL) reloads that file, salsaa_tune_load(path)
  * another (returns the entries read, < 0 if unreadable), salsaa_tune_reset()
@@ -256,6 +256,11 @@ int salsaa_ntt_tune_set(uint32_t log_n, int incomplete, int inverse, int wide_mo
                         int ctas_per_sm);
 int salsaa_ntt_tune_get(uint32_t log_n, int incomplete, int inverse, int wide_modulus, int large, int* variant,
                         int* ctas_per_sm);
+/* The fold's ring products (salsaa_fold and the prover's fold): variant 0 =
+ * integer Shoup products, 1 = FP64 products (used only when q < 2^50); the
+ * same outputs.  Table line: "fold <variant>".  _get returns the variant. */
+int salsaa_fold_tune_set(int variant);
+int salsaa_fold_tune_get(void);
 
 /* ---- subroutine-level entry points (device pointers, cudaStream_t) ---- */
 

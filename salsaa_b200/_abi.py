@@ -93,6 +93,8 @@ DEVICE_SYMBOLS = {
     "salsaa_server_destroy": (None, [VP]),
     "salsaa_tune_load": (INT, [ctypes.c_char_p]),
     "salsaa_tune_reset": (INT, []),
+    "salsaa_fold_tune_set": (INT, [INT]),
+    "salsaa_fold_tune_get": (INT, []),
     "salsaa_ntt_tune_set": (INT, [ctypes.c_uint32, INT, INT, INT, INT, INT, INT]),
     "salsaa_ntt_tune_get": (INT, [ctypes.c_uint32, INT, INT, INT, INT, ctypes.POINTER(INT), ctypes.POINTER(INT)]),
 }

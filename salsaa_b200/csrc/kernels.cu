@@ -1278,18 +1278,81 @@ int launch_fold_challenge(const DevState* ds, u32 round, u32 rows, u32 d, u64 q,
 // (c_e + X c_o)(w_e + X w_o) = c_e w_e + (zeta c_o) w_o + X (c_o w_e + c_e w_o).
 // Per (row k, slot s): c_e, c_o, zeta_s c_o and their Shoup companions, as six
 // planes pre[(j * rows + k) * n + s] so that neighbouring slots are adjacent.
-__global__ void fold_pre_kernel(const u64* c, u32 rows, u32 n, ModQ M, const u64* zeta, u64* pre) {
+// FP: the same six planes for the FP64 products (q < 2^50): each constant as
+// a double and its quotient fl(c / 2q), stored as the doubles' bits.
+__global__ void fold_pre_kernel(const u64* c, u32 rows, u32 n, ModQ M, const u64* zeta, u64* pre, bool fp) {
   const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= rows * n) return;
   const u32 k = t / n, s = t % n;
   const u64 ce = c[(u64)k * 2 * n + s], co = c[(u64)k * 2 * n + n + s], zco = mul_mod(M, zeta[s], co);
   const u64 plane = (u64)rows * n;
+  if (fp) {
+    const double q2d = 2.0 * (double)M.q;
+    const u64 v[3] = {ce, co, zco};
+    for (int j = 0; j < 3; j++) {
+      pre[(2 * j) * plane + t] = (u64)__double_as_longlong((double)v[j]);
+      pre[(2 * j + 1) * plane + t] = (u64)__double_as_longlong(__ddiv_rn((double)v[j], q2d));
+    }
+    return;
+  }
   pre[0 * plane + t] = ce;
   pre[1 * plane + t] = shoup_dev(ce, M.q);
   pre[2 * plane + t] = co;
   pre[3 * plane + t] = shoup_dev(co, M.q);
   pre[4 * plane + t] = zco;
   pre[5 * plane + t] = shoup_dev(zco, M.q);
+}
+
+// fold_vec_kernel with FP64 products (q < 2^50, canonical slot-form rows):
+// per row the two products of each output are at most 1.25 q each, and the
+// running sum is reduced after every row, so every value stays below 4 q.
+__global__ void __launch_bounds__(256) fold_fp_kernel(RowSet w, u32 rows, u64 width, u32 logn, ModQ M,
+                                                      const u64* __restrict__ pre, u64* out) {
+  const u32 n = 1u << logn, hn = n >> 1;
+  const u64 tot = width << (logn - 1);
+  const double qd = (double)M.q, q2d = 2.0 * qd, qinv = 1.0 / qd;
+  for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
+    const u64 i = t >> (logn - 1);
+    const u32 s = 2 * ((u32)t & (hn - 1));
+    double ae[2] = {0, 0}, ao[2] = {0, 0};
+    for (u32 k0 = 0; k0 < rows; k0 += 4) {
+      ulonglong2 E[4], O[4];
+#pragma unroll
+      for (u32 j = 0; j < 4; j++)
+        if (k0 + j < rows) {
+          const u64* x = w.p[k0 + j] + (i << (logn + 1));
+          E[j] = __ldg((const ulonglong2*)(x + s));
+          O[j] = __ldg((const ulonglong2*)(x + n + s));
+        }
+#pragma unroll
+      for (u32 j = 0; j < 4; j++)
+        if (k0 + j < rows) {
+          const u64 plane = (u64)rows << logn;
+          const u64* pk = pre + ((u64)((k0 + j) << logn) + s);
+          ulonglong2 C[6];
+#pragma unroll
+          for (u32 g = 0; g < 6; g++) C[g] = __ldg((const ulonglong2*)(pk + g * plane));
+#pragma unroll
+          for (u32 h = 0; h < 2; h++) {
+            const double we = fp_from_word(h ? E[j].y : E[j].x), wo = fp_from_word(h ? O[j].y : O[j].x);
+            const double ce = __longlong_as_double((long long)(h ? C[0].y : C[0].x));
+            const double ceh = __longlong_as_double((long long)(h ? C[1].y : C[1].x));
+            const double co = __longlong_as_double((long long)(h ? C[2].y : C[2].x));
+            const double coh = __longlong_as_double((long long)(h ? C[3].y : C[3].x));
+            const double zc = __longlong_as_double((long long)(h ? C[4].y : C[4].x));
+            const double zch = __longlong_as_double((long long)(h ? C[5].y : C[5].x));
+            const double e = __dadd_rn(fp_mulmod(we, ce, ceh, q2d), fp_mulmod(wo, zc, zch, q2d));
+            const double o = __dadd_rn(fp_mulmod(we, co, coh, q2d), fp_mulmod(wo, ce, ceh, q2d));
+            ae[h] = fp_reduce(__dadd_rn(ae[h], e), qinv, qd);
+            ao[h] = fp_reduce(__dadd_rn(ao[h], o), qinv, qd);
+          }
+        }
+    }
+    *(ulonglong2*)(out + (i << (logn + 1)) + s) =
+        make_ulonglong2(fp_to_word(ae[0], qinv, qd), fp_to_word(ae[1], qinv, qd));
+    *(ulonglong2*)(out + (i << (logn + 1)) + n + s) =
+        make_ulonglong2(fp_to_word(ao[0], qinv, qd), fp_to_word(ao[1], qinv, qd));
+  }
 }
 
 // out = sum_k c_k w_k in slot form.  LAZY (q < 2^57, at most 16 rows): the
@@ -1400,12 +1463,17 @@ __global__ void __launch_bounds__(256) fold_vec_kernel(RowSet w, u32 rows, u64 w
 int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot, u64* pre,
                 u64* out_slot, cudaStream_t st) {
   if (rows == 0 || rows > MAX_WROWS) return salsaa_set_error(-2, "fold: bad row count");
-  fold_pre_kernel<<<(rows * T.n + 127) / 128, 128, 0, st>>>(c_slot, rows, T.n, M, T.zeta, pre);
-  int rc = check_launch("fold_pre");
-  if (rc) return rc;
   const bool lazy = M.q < (1ULL << 57);
   bool vec = T.n >= 2 && (uintptr_t)out_slot % 16 == 0 && (uintptr_t)pre % 16 == 0 && ((u64)rows * T.n) % 2 == 0;
   for (u32 k = 0; k < rows; k++) vec = vec && (uintptr_t)w_slot.p[k] % 16 == 0;
+  const bool fp = vec && M.q < (1ULL << 50) && fold_choice() == 1;
+  fold_pre_kernel<<<(rows * T.n + 127) / 128, 128, 0, st>>>(c_slot, rows, T.n, M, T.zeta, pre, fp);
+  int rc = check_launch("fold_pre");
+  if (rc) return rc;
+  if (fp) {
+    fold_fp_kernel<<<grid_1d(width * T.n / 2, 256), 256, 0, st>>>(w_slot, rows, width, T.logn, M, pre, out_slot);
+    return check_launch("fold");
+  }
   if (vec) {
     const unsigned g = grid_1d(width * T.n / 2, 256);
     if (lazy) fold_vec_kernel<true><<<g, 256, 0, st>>>(w_slot, rows, width, T.logn, M, pre, out_slot);

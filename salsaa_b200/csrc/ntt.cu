@@ -212,6 +212,7 @@ namespace {
 constexpr int TUNE_LOGN = 14;
 std::mutex g_tune_mu;
 NttChoice g_tune[TUNE_LOGN][2][2][2][2];
+int g_fold_variant = 0;  // fold products: 0 = integer (Shoup), 1 = FP64 (q < 2^50)
 bool g_tune_loaded = false;
 
 int tune_index_ok(u32 logn) { return logn < (u32)TUNE_LOGN; }
@@ -222,6 +223,14 @@ int tune_load_locked(const char* path) {
   char line[256];
   int n = 0;
   while (fgets(line, sizeof line, f)) {
+    unsigned fv;
+    if (sscanf(line, "fold %u", &fv) == 1) {
+      if (fv <= 1) {
+        g_fold_variant = (int)fv;
+        n++;
+      }
+      continue;
+    }
     unsigned lg, inc, inv, wide, big, var, cps;
     if (sscanf(line, "ntt %u %u %u %u %u %u %u", &lg, &inc, &inv, &wide, &big, &var, &cps) != 7) continue;
     if (lg >= (unsigned)TUNE_LOGN || inc > 1 || inv > 1 || wide > 1 || big > 1 ||
@@ -281,9 +290,24 @@ int ntt_tune_load(const char* path) {
   return n < 0 ? salsaa_set_error(-1, "tune_load: cannot read the table file") : n;
 }
 
+int fold_choice() {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_default_locked();
+  return g_fold_variant;
+}
+
+int fold_tune_set(int variant) {
+  if (variant < 0 || variant > 1) return salsaa_set_error(-2, "fold_tune_set: variant 0 or 1");
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_default_locked();
+  g_fold_variant = variant;
+  return 0;
+}
+
 void ntt_tune_reset() {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_loaded = true;  // defaults, and no automatic load afterwards
+  g_fold_variant = 0;
   for (auto& a : g_tune)
     for (auto& b : a)
       for (auto& c : b)
@@ -713,29 +737,6 @@ __global__ void __launch_bounds__(256) ntt_pipe_kernel(const u64* in, u64* out, 
 // bits of 2^52 (v + 2^52 has v in its low 52 mantissa bits), one integer
 // and one FP64 instruction each.
 // ---------------------------------------------------------------------------
-constexpr double FP_MAGIC = 6755399441055744.0;  // 1.5 * 2^52: fl(t + M) - M rounds |t| < 2^51 to an integer
-constexpr double FP_TWO52 = 4503599627370496.0;  // 2^52
-
-__device__ __forceinline__ double fp_mulmod(double x, double w, double wh, double q2d) {
-  const double h = __dmul_rn(x, w);
-  const double l = __fma_rn(x, w, -h);
-  const double c = __dsub_rn(__fma_rn(x, wh, FP_MAGIC), FP_MAGIC);
-  return __dadd_rn(__fma_rn(-c, q2d, h), l);
-}
-__device__ __forceinline__ double fp_reduce(double v, double qinv, double qd) {
-  const double c = __dsub_rn(__fma_rn(v, qinv, FP_MAGIC), FP_MAGIC);
-  return __fma_rn(-c, qd, v);
-}
-// canonical word (< 2^52) -> double, and a reduced-range double -> canonical word
-__device__ __forceinline__ double fp_from_word(u64 v) {
-  return __dsub_rn(__longlong_as_double((long long)(v | 0x4330000000000000ULL)), FP_TWO52);
-}
-__device__ __forceinline__ u64 fp_to_word(double v, double qinv, double qd) {
-  v = fp_reduce(v, qinv, qd);
-  v = v < 0.0 ? __dadd_rn(v, qd) : v;
-  return (u64)__double_as_longlong(__dadd_rn(v, FP_TWO52)) & 0x000FFFFFFFFFFFFFULL;
-}
-
 template <int LOGN, int P, bool INV>
 __device__ __forceinline__ void nf_compute(double (&x)[16], u32 tu, const NttDev& T) {
   constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
@@ -1306,6 +1307,9 @@ extern "C" int salsaa_ntt_tune_set(uint32_t log_n, int incomplete, int inverse, 
   return salsaa::ntt_tune_set(log_n, incomplete != 0, inverse != 0, wide_modulus != 0, large != 0, variant,
                               ctas_per_sm);
 }
+
+extern "C" int salsaa_fold_tune_set(int variant) { return salsaa::fold_tune_set(variant); }
+extern "C" int salsaa_fold_tune_get(void) { return salsaa::fold_choice(); }
 
 extern "C" int salsaa_ntt_tune_get(uint32_t log_n, int incomplete, int inverse, int wide_modulus, int large,
                                    int* variant, int* ctas_per_sm) {

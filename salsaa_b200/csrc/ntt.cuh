@@ -47,6 +47,9 @@ NttChoice ntt_choice(u32 logn, bool incomplete, bool inverse, bool wide, bool la
 int ntt_tune_set(u32 logn, bool incomplete, bool inverse, bool wide, bool large, int variant, int ctas_per_sm);
 int ntt_tune_load(const char* path);  // number of entries read, or < 0
 void ntt_tune_reset();
+// Fold products (launch_fold): 0 = integer Shoup products, 1 = FP64 (q < 2^50).
+int fold_choice();
+int fold_tune_set(int variant);
 int ntt_error_check();  // a bounded wait of the pipelined transform gave up
 
 // count units of n (full) or ring elements of 2n (incomplete); in may equal out.
@@ -75,6 +78,31 @@ int ntt_digits_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, con
 // aligned buffers (ntt_mul_fused_ok); the C ABI falls back to three passes.
 bool ntt_mul_fused_ok(const u64* a, const u64* b, const u64* r, const NttDev& T);
 int ntt_mul_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& T, cudaStream_t st);
+
+// ---- FP64 modular arithmetic for q < 2^50 (exactness argument in ntt.cu) ----
+constexpr double FP_MAGIC = 6755399441055744.0;  // 1.5 * 2^52: fl(t + M) - M rounds |t| < 2^51 to an integer
+constexpr double FP_TWO52 = 4503599627370496.0;  // 2^52
+
+__device__ __forceinline__ double fp_mulmod(double x, double w, double wh, double q2d) {
+  const double h = __dmul_rn(x, w);
+  const double l = __fma_rn(x, w, -h);
+  const double c = __dsub_rn(__fma_rn(x, wh, FP_MAGIC), FP_MAGIC);
+  return __dadd_rn(__fma_rn(-c, q2d, h), l);
+}
+__device__ __forceinline__ double fp_reduce(double v, double qinv, double qd) {
+  const double c = __dsub_rn(__fma_rn(v, qinv, FP_MAGIC), FP_MAGIC);
+  return __fma_rn(-c, qd, v);
+}
+// canonical word (< 2^52) -> double, and a reduced-range double -> canonical word
+__device__ __forceinline__ double fp_from_word(u64 v) {
+  return __dsub_rn(__longlong_as_double((long long)(v | 0x4330000000000000ULL)), FP_TWO52);
+}
+__device__ __forceinline__ u64 fp_to_word(double v, double qinv, double qd) {
+  v = fp_reduce(v, qinv, qd);
+  v = v < 0.0 ? __dadd_rn(v, qd) : v;
+  return (u64)__double_as_longlong(__dadd_rn(v, FP_TWO52)) & 0x000FFFFFFFFFFFFFULL;
+}
+
 
 // ---- ring helpers in slot form, used by several kernels ----
 // (a_e + X a_o)(b_e + X b_o) = a_e b_e + zeta a_o b_o + X (a_o b_e + a_e b_o)

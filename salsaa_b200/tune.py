@@ -120,10 +120,55 @@ def tune(reps=10, quick=False, verbose=True):
     return results
 
 
-def write_table(results, path):
+def tune_fold(reps=10, verbose=True):
+    """Times the fold (salsaa_fold: two rows of 2^18 ring elements, d = 128,
+    the 50-bit prime) with integer and FP64 products, checks that both give
+    the same words, and leaves the faster set.  Returns the timing record."""
+    import torch
+    L = lib()
+    q, d, rows, width = Q0, 128, 2, 1 << 18
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(12)
+    w = torch.randint(0, 1 << 62, (rows, width, d), dtype=torch.int64, device="cuda", generator=gen) % q
+    c = torch.randint(0, 1 << 62, (rows, d), dtype=torch.int64, device="cuda", generator=gen) % q
+    out = torch.empty((width, d), dtype=torch.int64, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def call():
+        _check(L.salsaa_fold(ctypes.c_void_p(w.data_ptr()), rows, width, d, q, ctypes.c_void_p(c.data_ptr()),
+                             ctypes.c_void_p(out.data_ptr()), st), "salsaa_fold")
+
+    times, ref = {}, None
+    for var in (0, 1):
+        _check(L.salsaa_fold_tune_set(var), "fold_tune_set")
+        call()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            call()
+        b.record()
+        b.synchronize()
+        times[var] = a.elapsed_time(b) / reps
+        if ref is None:
+            ref = out.clone()
+        elif not torch.equal(out, ref):
+            raise RuntimeError("fold variant %d differs from the integer products" % var)
+    best = min(times, key=times.get)
+    _check(L.salsaa_fold_tune_set(best), "fold_tune_set")
+    if verbose:
+        print("fold (salsaa_fold, 2 x 2^18 x 128)  int %.3f ms  fp64 %.3f ms  best %d" % (times[0], times[1], best),
+              flush=True)
+    return {"target": "fold", "ms": {str(k): v for k, v in times.items()}, "best": best}
+
+
+def write_table(results, path, fold=None):
     with open(path, "w") as f:
         f.write("# NTT kernel schedules chosen by salsaa_b200/tune.py on %s\n" % _device_name())
         f.write("# ntt <log_n> <incomplete> <inverse> <wide_modulus> <large_batch> <variant> <ctas_per_sm>\n")
+        if fold is not None:
+            f.write("fold %d   # fold products: int %.4f ms, fp64 %.4f ms\n"
+                    % (fold["best"], fold["ms"]["0"], fold["ms"]["1"]))
         for r in results:
             k, b = r["key"], r["best"]
             f.write("ntt %d %d %d %d %d %d %d   # %s %s %s: default %.4f ms, best %.4f ms\n"
@@ -147,10 +192,11 @@ def main(argv=None):
     ap.add_argument("--json", default=None, help="also write the timing records here")
     a = ap.parse_args(argv)
     res = tune(a.reps, a.quick)
-    write_table(res, a.out)
+    fold = tune_fold(a.reps)
+    write_table(res, a.out, fold)
     if a.json:
         with open(a.json, "w") as f:
-            json.dump(res, f, indent=1)
+            json.dump({"ntt": res, "fold": fold}, f, indent=1)
     print("wrote", a.out)
     return 0
 

@@ -38,8 +38,10 @@ def test_tune_table_roundtrip(gpu_lib, tmp_path):
                      "ntt 10 0 1 1 0 2 1\n"
                      "ntt 6 1 1 0 1 7 0   # variant 7 does not exist: ignored\n"
                      "ntt 7 1 0 0 1 1 0   # FP64 butterflies\n"
+                     "fold 1\n"
                      "garbage line\n")
-    assert L.salsaa_tune_load(str(table).encode()) == 3
+    assert L.salsaa_tune_load(str(table).encode()) == 4
+    assert L.salsaa_fold_tune_get() == 1
     assert _get(L, (6, 1, 0, 0, 1)) == (3, 0)
     assert _get(L, (10, 0, 1, 1, 0)) == (2, 1)
     assert _get(L, (6, 1, 1, 0, 1)) == (0, 0)
@@ -48,8 +50,10 @@ def test_tune_table_roundtrip(gpu_lib, tmp_path):
     assert L.salsaa_ntt_tune_set(6, 1, 0, 0, 1, 5, 0) < 0  # no variant 5
     assert L.salsaa_ntt_tune_set(6, 1, 0, 0, 1, -1, 0) < 0
     assert L.salsaa_ntt_tune_set(14, 1, 0, 0, 1, 2, 0) < 0  # log n out of range
+    assert L.salsaa_fold_tune_set(2) < 0
     assert L.salsaa_tune_reset() == 0
     assert _get(L, (6, 1, 0, 0, 1)) == (0, 0)
+    assert L.salsaa_fold_tune_get() == 0
 
 
 @pytest.mark.gpu
@@ -99,7 +103,31 @@ def test_proofs_under_each_schedule(gpu_lib, oracle, var, cps):
     assert rc == 0
     try:
         _set_all(L, var, cps)
+        assert L.salsaa_fold_tune_set(1 if var == 1 else 0) == 0
         got = api.Context(p, crs_seed=7).prove(11)
     finally:
         L.salsaa_tune_reset()
     assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows,width,d,q", [(2, 1 << 12, 128, P.Q0), (5, 300, 256, P.Q1), (16, 64, 512, P.Q2),
+                                            (3, 100, 64, P.Q62)])
+def test_fold_variants(gpu_lib, oracle, rows, width, d, q):
+    """The fold with integer and with FP64 products (q < 2^50; wider moduli
+    keep the integer products) equals the oracle's fold."""
+    from helpers import fold_challenge
+    from salsaa_b200 import api
+    L = gpu_lib
+    rng = np.random.default_rng(rows * width)
+    w = rand_mod(rng, (rows, width, d), q)
+    c = fold_challenge(3, 1, rows, d, q)
+    want = oracle.fold(w, q, c)
+    try:
+        for var in (0, 1):
+            assert L.salsaa_fold_tune_set(var) == 0
+            assert L.salsaa_fold_tune_get() == var
+            got = api.to_host(api.fold(api.to_dev(w), q, api.to_dev(c)))
+            assert np.array_equal(got, want), var
+    finally:
+        L.salsaa_tune_reset()
