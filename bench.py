@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ntt", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--serve-only", action="store_true", help="run only the serving sweep and print its JSON")
+    ap.add_argument("--serve-requests", type=int, default=96)
     ap.add_argument("--preset", default=PRESET, help="parameter set (profiling; the metric is quoted on A0)")
     ap.add_argument("--wit-log", type=int, default=0,
                     help="profiling: shrink WIT_LEN to 2^L (SNARK rounds L-11), keeping d, q and the rows")
@@ -454,6 +455,7 @@ def run_ours(args):
         ntt = ntt_bench(torch, api)
     dense = dense_bench(torch, api) if rank == 0 and not args.no_dense else None
     scb = sumcheck_batch_bench(torch, api) if rank == 0 and not args.no_dense else None
+    multi = batched_launch_bench(torch, api) if rank == 0 and not args.no_dense else None
     serving = serving_bench(torch, api, args.serve_requests, rank) if not args.no_serve else None
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -480,6 +482,7 @@ def run_ours(args):
             "ntt": ntt,
             "commit_dense": dense,
             "sumcheck_batch": scb,
+            "batched_launches": multi,
             "serving": serving,
             "roofline": roofline_ck(traced, sum(serial) if serial else None,
                                     args.preset == "A0" and not args.wit_log),
@@ -503,22 +506,35 @@ def run_ours(args):
 
 SERVE_SLOTS = {"A0": 4, "A1": 4, "A2": 4, "F0": 4, "F1": 2, "F2": 1}
 SERVE_BUDGET = 140 << 30
-SERVE_MAX_INFLIGHT = 3  # proofs running at once in the served path (2: fewer proofs/s, 4: higher p50/p99)
+SERVE_MAX_INFLIGHT = 4  # proofs running at once in the served path
+SERVE_LOADS = (0.5, 1.0, 1.5, 2.0, 3.0)  # offered load as multiples of the plain path's capacity
+SERVE_SLO_MS = (100.0, 200.0, 400.0, 800.0)  # p99 targets for the equal-p99 comparison
 
 
 def serving_bench(torch, api, nreq, rank):
-    """Poisson arrivals of A0/A1/A2 SNARK proves and F0/F1/F2 folding
-    steps (size classes 0/1/2 drawn 40/30/30, SNARK or folding 50/50), each with
-    its own seed and a witness sampled on the GPU.  The same stream is run
-    through the continuous-batching server and through the plain path (one
-    proof at a time, in arrival order); latency counts from arrival."""
+    """Serving stream: Poisson arrivals of A0/A1/A2 SNARK proves and F0/F1/F2
+    folding steps (size classes 0/1/2 drawn 40/30/30, SNARK or folding 50/50),
+    each with its own seed and a witness sampled on the GPU.  The same request
+    stream (names, seeds, arrival pattern) is offered at several loads, as
+    multiples of the plain path's capacity (1 / mean service time), through
+    the plain path (one proof at a time, in arrival order) and through the
+    continuous-batching server; latency counts from arrival.  At each p99
+    target the throughput each path sustains within it is compared (the
+    highest completed rate over the loads whose p99 meets the target)."""
     import time as _t
     rng = np.random.default_rng(4242 + rank)
     cls = rng.choice(3, size=nreq, p=[0.4, 0.3, 0.3])
     kind = rng.integers(0, 2, size=nreq)
     names = [("A%d" if k == 0 else "F%d") % c for c, k in zip(cls, kind)]
+    gaps = rng.exponential(1.0, size=nreq)  # unit-rate gaps, scaled per load
+    seeds = [10 ** 7 + rank * 10 ** 5 + i for i in range(nreq)]
     params = {nm: api.params_preset(nm) for nm in SERVE_SLOTS}
-    # plain path first: one slot per set, proofs strictly one after another
+
+    def stats(lat, span):
+        return {"proofs_per_s": nreq / span, "p50_ms": 1e3 * float(np.median(lat)),
+                "p99_ms": 1e3 * float(np.percentile(lat, 99))}
+
+    # plain path: one slot per set, proofs strictly one after another
     ctxs = {nm: api.Context(params[nm], crs_seed=3) for nm in SERVE_SLOTS}
     provers = {nm: api.Prover(ctxs[nm]) for nm in SERVE_SLOTS}
     bufs = {nm: torch.empty(ctxs[nm].proof_bytes // 8, dtype=torch.int64, device="cuda") for nm in SERVE_SLOTS}
@@ -530,19 +546,19 @@ def serving_bench(torch, api, nreq, rank):
         provers[nm].enqueue(2, bufs[nm])
         provers[nm].sync()
         service[nm] = _t.perf_counter() - t0
-    mean_service = float(np.mean([service[nm] for nm in names]))
-    rate = 1.5 / mean_service  # offered load 1.5x the plain path's capacity
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=nreq))
-    seeds = [10 ** 7 + rank * 10 ** 5 + i for i in range(nreq)]
-    plain_lat = []
-    t0 = _t.perf_counter()
-    for i, nm in enumerate(names):
-        while _t.perf_counter() - t0 < arrivals[i]:
-            pass
-        provers[nm].enqueue(seeds[i], bufs[nm])
-        provers[nm].sync()
-        plain_lat.append(_t.perf_counter() - t0 - arrivals[i])
-    plain_span = _t.perf_counter() - t0
+    capacity = 1.0 / float(np.mean([service[nm] for nm in names]))
+    plain_runs = {}
+    for load in SERVE_LOADS:
+        arrivals = np.cumsum(gaps) / (load * capacity)
+        lat = []
+        t0 = _t.perf_counter()
+        for i, nm in enumerate(names):
+            while _t.perf_counter() - t0 < arrivals[i]:
+                pass
+            provers[nm].enqueue(seeds[i], bufs[nm])
+            provers[nm].sync()
+            lat.append(_t.perf_counter() - t0 - arrivals[i])
+        plain_runs[load] = stats(lat, _t.perf_counter() - t0)
     for nm in SERVE_SLOTS:
         provers[nm].close()
         ctxs[nm].close()
@@ -559,32 +575,44 @@ def serving_bench(torch, api, nreq, rank):
         pass
     for t in warm:
         srv.poll(t)
-    tickets = [None] * nreq
-    done = {}
-    nsub = 0
-    t0 = _t.perf_counter()
-    while len(done) < nreq:
-        now = _t.perf_counter() - t0
-        while nsub < nreq and arrivals[nsub] <= now:
-            tickets[nsub] = srv.submit(sets[names[nsub]], seeds[nsub], outs[nsub])
-            nsub += 1
-        srv.progress()
-        for i in range(nsub):
-            if i not in done:
-                r = srv.poll(tickets[i])
-                if r is not None:
-                    done[i] = _t.perf_counter() - t0 - arrivals[i]
-    span = _t.perf_counter() - t0
+    served_runs = {}
+    for load in SERVE_LOADS:
+        arrivals = np.cumsum(gaps) / (load * capacity)
+        tickets = [None] * nreq
+        done = {}
+        nsub = 0
+        t0 = _t.perf_counter()
+        while len(done) < nreq:
+            now = _t.perf_counter() - t0
+            while nsub < nreq and arrivals[nsub] <= now:
+                tickets[nsub] = srv.submit(sets[names[nsub]], seeds[nsub], outs[nsub])
+                nsub += 1
+            srv.progress()
+            for i in range(nsub):
+                if i not in done:
+                    r = srv.poll(tickets[i])
+                    if r is not None:
+                        done[i] = _t.perf_counter() - t0 - arrivals[i]
+        served_runs[load] = stats([done[i] for i in range(nreq)], _t.perf_counter() - t0)
     srv.close()
-    lat = [done[i] for i in range(nreq)]
-    served = {"proofs_per_s": nreq / span, "p50_ms": 1e3 * float(np.median(lat)),
-              "p99_ms": 1e3 * float(np.percentile(lat, 99))}
-    plain = {"proofs_per_s": nreq / plain_span, "p50_ms": 1e3 * float(np.median(plain_lat)),
-             "p99_ms": 1e3 * float(np.percentile(plain_lat, 99))}
-    return {"requests": nreq, "offered_per_s": rate, "mix": {nm: names.count(nm) for nm in SERVE_SLOTS},
-            "slots": SERVE_SLOTS, "max_in_flight": SERVE_MAX_INFLIGHT, "served": served, "plain": plain,
-            "served_over_plain": served["proofs_per_s"] / plain["proofs_per_s"],
-            "service_ms_alone": {nm: 1e3 * v for nm, v in service.items()}}
+    sweep = [{"offered_x_plain_capacity": load, "offered_per_s": load * capacity, "plain": plain_runs[load],
+              "served": served_runs[load]} for load in SERVE_LOADS]
+
+    def best_within(runs, slo):
+        ok = [r["proofs_per_s"] for r in runs.values() if r["p99_ms"] <= slo]
+        return max(ok) if ok else None
+
+    equal_p99 = []
+    for slo in SERVE_SLO_MS:
+        a, b = best_within(plain_runs, slo), best_within(served_runs, slo)
+        equal_p99.append({"p99_target_ms": slo, "plain_proofs_per_s": a, "served_proofs_per_s": b,
+                          "served_over_plain": (b / a) if (a and b) else None})
+    return {"requests": nreq, "mix": {nm: names.count(nm) for nm in SERVE_SLOTS}, "slots": SERVE_SLOTS,
+            "max_in_flight": SERVE_MAX_INFLIGHT, "plain_capacity_per_s": capacity,
+            "service_ms_alone": {nm: 1e3 * v for nm, v in service.items()}, "sweep": sweep,
+            "at_equal_p99": equal_p99,
+            "served_over_plain_peak": max(r["proofs_per_s"] for r in served_runs.values())
+            / max(r["proofs_per_s"] for r in plain_runs.values())}
 
 
 def dense_bench(torch, api):
@@ -672,6 +700,56 @@ def sumcheck_batch_bench(torch, api):
     del vecs
     torch.cuda.empty_cache()
     return res
+
+
+def batched_launch_bench(torch, api):
+    """Uneven instances in one launch against one launch each: 64 batches of
+    incomplete d = 128 transforms (log-uniform 2^8..2^14 ring elements, the
+    50-bit prime, salsaa_ntt_multi) and the A0 commitment-key rows over 8
+    witnesses of uneven shapes (salsaa_commit_multi).  CUDA events around 5
+    repetitions of each form on the current stream."""
+    from salsaa_b200 import params as P
+    reps = 5
+    rng = np.random.default_rng(99)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(9)
+
+    def timed(fn):
+        fn()
+        a = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        e.synchronize()
+        return a.elapsed_time(e) / reps
+
+    q, d = P.Q0, 128
+    logs = np.sort(rng.integers(8, 15, size=64))
+    xs = [torch.randint(0, 1 << 50, (1 << int(k), d), dtype=torch.int64, device="cuda", generator=gen) % q
+          for k in logs]
+    outs = [torch.empty_like(x) for x in xs]
+    one = timed(lambda: api.ntt_multi(xs, d, q, incomplete=True, outs=outs))
+    each = timed(lambda: [api.ntt(x, d, q, incomplete=True, out=o) for x, o in zip(xs, outs)])
+    coeffs = sum(x.numel() for x in xs)
+    ntt = {"instances": len(xs), "elements_log2": [int(k) for k in logs], "one_launch_ms": one,
+           "one_launch_each_ms": each, "speedup": each / one, "one_launch_GB/s": 16.0 * coeffs / (one * 1e6)}
+    del xs, outs
+    params = api.params_preset("A0")
+    ctx = api.Context(params, crs_seed=1)
+    shapes = [(1, 1 << 19), (3, 1 << 16), (9, 1 << 12), (2, 1 << 18), (1, 1 << 14), (5, 1 << 15), (4, 1 << 11),
+              (2, 1 << 17)]
+    ws = [torch.randint(-1, 2, (r, w, params.d), dtype=torch.int64, device="cuda", generator=gen) % params.q
+          for r, w in shapes]
+    one = timed(lambda: ctx.parallel_dot_series_matrix_multi(ws))
+    each = timed(lambda: [ctx.parallel_dot_series_matrix(w) for w in ws])
+    commit = {"witnesses": [list(sh) for sh in shapes], "one_launch_ms": one, "one_launch_each_ms": each,
+              "speedup": each / one}
+    del ws
+    ctx.close()
+    torch.cuda.empty_cache()
+    return {"ntt": ntt, "commit": commit}
 
 
 def trace_read(name):
@@ -836,7 +914,13 @@ def main():
         import torch
         from salsaa_b200 import api
         print(json.dumps({"commit_dense": dense_bench(torch, api),
-                          "sumcheck_batch": sumcheck_batch_bench(torch, api)}), flush=True)
+                          "sumcheck_batch": sumcheck_batch_bench(torch, api),
+                          "batched_launches": batched_launch_bench(torch, api)}), flush=True)
+        return 0
+    if args.serve_only:
+        import torch
+        from salsaa_b200 import api
+        print(json.dumps({"serving": serving_bench(torch, api, args.serve_requests, 0)}), flush=True)
         return 0
     if args.ntt_only:
         import torch

@@ -272,6 +272,17 @@ int salsaa_fold_tune_get(void);
 int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uint64_t count, uint64_t q, int inverse,
                int incomplete, void* stream);
 
+/* Many uneven batches of one transform in ONE launch: the batched form of
+ * salsaa_ntt (ntt_forward_in_place / ntt_inverse_in_place,
+ * hexl-bindings/hexl_wrapper.cpp:213-229, and the IncompleteNTT conversions,
+ * src/cyclotomic_ring.rs:484-556) for `ninst` <= 64 batches, batch i being
+ * counts[i] units at d_in[i] -> d_out[i] (host arrays of device pointers;
+ * d_in[i] may equal d_out[i]).  n and incomplete mean what they mean for
+ * salsaa_ntt; needs 16 <= n <= 4096 (register path) and 16-byte aligned
+ * buffers.  Outputs equal salsaa_ntt on each batch. */
+int salsaa_ntt_multi(const uint64_t* const* d_in, uint64_t* const* d_out, const uint64_t* counts, uint32_t ninst,
+                     uint64_t n, uint64_t q, int inverse, int incomplete, void* stream);
+
 /* Many independent norm-check sumchecks in a few launches: the batched form
  * of norm_check_1 + sum_check (src/subroutines/fast_norm_check.rs:135-320) for
  * `count` <= 64 vectors of uneven power-of-two lengths (2..2^30), one
@@ -324,6 +335,18 @@ int salsaa_poly_mul(const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_r, uin
  * d_out receives module_size x rows ring elements (coefficient form). */
 int salsaa_commit(salsaa_ctx* ctx, const uint64_t* d_w, uint64_t rows, uint64_t width, uint64_t* d_out,
                   void* stream);
+
+/* Several parallel_dot_series_matrix calls (src/arithmetic.rs:459-505) with
+ * the commitment-key rows of ctx, for `ninst` <= 8 witnesses of uneven shapes,
+ * in one launch of each step (one transform to slot form for all witnesses,
+ * ONE tensor-core launch over all witnesses' element blocks, one
+ * finalisation, one inverse transform): witness i is rows[i] (<= 9) x
+ * widths[i] (a power of two, 128 .. WIT_LEN) x d coefficients at d_w[i], its
+ * commitment (module_size x rows[i] ring elements, coefficient form) goes to
+ * d_out[i]; 16-byte aligned buffers; q < 2^56 and module_size <= 18 (the
+ * tensor-core path).  Outputs equal salsaa_commit on each witness. */
+int salsaa_commit_multi(salsaa_ctx* ctx, const uint64_t* const* d_w, const uint64_t* rows, const uint64_t* widths,
+                        uint32_t ninst, uint64_t* const* d_out, void* stream);
 
 /* norm_check_1 + sum_check (src/subroutines/fast_norm_check.rs:135-199,282-320)
  * of each row of d_w (rows x n coefficients, n a power of two >= 4) with the

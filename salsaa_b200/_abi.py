@@ -71,6 +71,8 @@ DEVICE_SYMBOLS = {
     "salsaa_prover_set_overlap": (INT, [VP, INT]),
     "salsaa_ntt": (INT, [VP, VP, U64, U64, U64, INT, INT, VP]),
     "salsaa_poly_mul": (INT, [VP, VP, VP, U64, U64, U64, VP]),
+    "salsaa_ntt_multi": (INT, [ctypes.POINTER(VP), ctypes.POINTER(VP), ctypes.POINTER(U64), ctypes.c_uint32, U64,
+                               U64, INT, INT, VP]),
     "salsaa_sumcheck_batch": (INT, [ctypes.POINTER(VP), ctypes.POINTER(U64), ctypes.c_uint32, U64, U64, U64, VP,
                                     VP, VP]),
     "salsaa_dense_key_create": (INT, [VP, U64, U64, U64, U64, VP, ctypes.POINTER(VP)]),
@@ -78,6 +80,8 @@ DEVICE_SYMBOLS = {
     "salsaa_dense_commit": (INT, [VP, VP, U64, VP, VP, VP]),
     "salsaa_selftest_umma_i8": (INT, [VP, VP, ctypes.c_uint32, ctypes.c_uint32, VP, VP]),
     "salsaa_commit": (INT, [VP, VP, U64, U64, VP, VP]),
+    "salsaa_commit_multi": (INT, [VP, ctypes.POINTER(VP), ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.c_uint32,
+                                  ctypes.POINTER(VP), VP]),
     "salsaa_sumcheck": (INT, [VP, U64, U64, U64, U64, U64, U64, VP, VP, VP]),
     "salsaa_decompose": (INT, [VP, U64, U64, U64, U64, U64, VP, VP, VP]),
     "salsaa_project": (INT, [VP, U64, U64, U64, U64, U64, U64, VP, VP]),

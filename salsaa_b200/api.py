@@ -127,6 +127,18 @@ class Context:
         _check(lib().salsaa_commit(self.h, _p(w), rows, width, _p(out), _stream()), "commit")
         return out
 
+    def parallel_dot_series_matrix_multi(self, ws):
+        """The same for several witnesses of uneven shapes in one launch of
+        each step (salsaa_commit_multi); returns one output per witness."""
+        k = len(ws)
+        outs = [dev_empty((self.params.module_size, w.shape[0], w.shape[2])) for w in ws]
+        wp = (ctypes.c_void_p * k)(*[w.data_ptr() for w in ws])
+        op = (ctypes.c_void_p * k)(*[o.data_ptr() for o in outs])
+        rows = (ctypes.c_uint64 * k)(*[w.shape[0] for w in ws])
+        widths = (ctypes.c_uint64 * k)(*[w.shape[1] for w in ws])
+        _check(lib().salsaa_commit_multi(self.h, wp, rows, widths, k, op, _stream()), "commit_multi")
+        return outs
+
 
 class Prover:
     """One proof slot (device workspace + private stream) of a Context."""
@@ -197,6 +209,18 @@ def ntt(x, n, q, inverse=False, incomplete=False, out=None):
     out = x if out is None else out
     _check(lib().salsaa_ntt(_p(x), _p(out), n, count, q, int(inverse), int(incomplete), _stream()), "ntt")
     return out
+
+
+def ntt_multi(xs, n, q, inverse=False, incomplete=False, outs=None):
+    """Several uneven batches (CUDA tensors whose last axis has n, or d,
+    words) transformed in one launch; in place unless outs is given."""
+    outs = list(xs) if outs is None else list(outs)
+    k = len(xs)
+    ins = (ctypes.c_void_p * k)(*[x.data_ptr() for x in xs])
+    ous = (ctypes.c_void_p * k)(*[o.data_ptr() for o in outs])
+    counts = (ctypes.c_uint64 * k)(*[x.numel() // n for x in xs])
+    _check(lib().salsaa_ntt_multi(ins, ous, counts, k, n, q, int(inverse), int(incomplete), _stream()), "ntt_multi")
+    return outs
 
 
 def poly_mul(a, b, n, q, out=None):

@@ -132,9 +132,12 @@ __device__ __forceinline__ void transpose4x4(u32 a, u32 b, u32 c, u32 d, u32& o0
   o3 = __byte_perm(t1, t3, 0x7632);
 }
 
-__global__ void __launch_bounds__(CKU_THREADS, 1)
-    ck_umma_kernel(const uint8_t* __restrict__ tk8, RowSet w, u32 rows, u32 G, u32 nck, u32 nkp, u32 n, u32 bt,
-                   u32 Bw, const u64* thi, u32 nhi_t, ModQ M, const u64* zeta, u64* acc, bool plain) {
+// One CTA of the key-row product: element-block group `by` of the witness w
+// (rows x width, slot form); its sums go to acc rows (r * acc_rows + koff + k).
+__device__ __forceinline__ void ck_umma_body(const uint8_t* __restrict__ tk8, const RowSet& w, u32 rows, u32 G,
+                                             u32 nck, u32 nkp, u32 n, u32 bt, u32 Bw, const u64* thi, u32 nhi_t,
+                                             const ModQ& M, const u64* zeta, u64* acc, u32 acc_rows, u32 koff,
+                                             bool plain, u32 by) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t full_bar[2], done_bar[2];
   __shared__ uint32_t tslot;
@@ -143,7 +146,7 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
   // element blocks g < G of this CTA start at i0 + g bt: the same offsets in
   // the key block, so they share every key tile; their witness rows stack as
   // the virtual rows g * rows + k of the MMA's M dimension
-  const u32 lob = bt / Bw, lo_b = blockIdx.y % lob, hg = blockIdx.y / lob;
+  const u32 lob = bt / Bw, lo_b = by % lob, hg = by / lob;
   const u64 i0 = (u64)hg * G * bt + (u64)lo_b * Bw;
   const u32 vrows = rows * G;
   const u32 btile = nkp * CKU_CHUNK;                  // one slot's key tile
@@ -327,7 +330,7 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
       u64 im = salsaa::add_mod(cb, da, M.q);
       const u64* th = thi + ((u64)r * nhi_t + hi_t) * d;
       slot_mul(M, re, im, th[s], th[n + s], zeta[s], re, im);
-      u64* dst = acc + ((u64)r * rows + k) * d;
+      u64* dst = acc + ((u64)r * acc_rows + koff + k) * d;
       atomic_add_mod(dst + s, re, M.q, plain);
       atomic_add_mod(dst + n + s, im, M.q, plain);
     }
@@ -335,6 +338,33 @@ __global__ void __launch_bounds__(CKU_THREADS, 1)
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_dealloc(tmem, 2 * cs);
+}
+
+__global__ void __launch_bounds__(CKU_THREADS, 1)
+    ck_umma_kernel(const uint8_t* __restrict__ tk8, RowSet w, u32 rows, u32 G, u32 nck, u32 nkp, u32 n, u32 bt,
+                   u32 Bw, const u64* thi, u32 nhi_t, ModQ M, const u64* zeta, u64* acc, bool plain) {
+  ck_umma_body(tk8, w, rows, G, nck, nkp, n, bt, Bw, thi, nhi_t, M, zeta, acc, rows, 0, plain, blockIdx.y);
+}
+
+// Several witnesses (uneven widths and row counts) against the same key rows
+// in one launch: witness i owns the grid rows [ystart[i], ystart[i+1]) and
+// its own accumulator acc[i] (nck x rows[i] ring elements).
+struct CkMulti {
+  RowSet w[CKU_MULTI_MAX];
+  u64* acc[CKU_MULTI_MAX];
+  u32 rows[CKU_MULTI_MAX], G[CKU_MULTI_MAX], Bw[CKU_MULTI_MAX];
+  u32 ystart[CKU_MULTI_MAX + 1];
+  uint8_t plain[CKU_MULTI_MAX];
+  u32 count;
+};
+
+__global__ void __launch_bounds__(CKU_THREADS, 1)
+    ck_umma_multi_kernel(const uint8_t* __restrict__ tk8, CkMulti m, u32 nck, u32 nkp, u32 n, u32 bt,
+                         const u64* thi, u32 nhi_t, ModQ M, const u64* zeta) {
+  u32 i = 0;
+  while (i + 1 < m.count && m.ystart[i + 1] <= blockIdx.y) i++;
+  ck_umma_body(tk8, m.w[i], m.rows[i], m.G[i], nck, nkp, n, bt, m.Bw[i], thi, nhi_t, M, zeta, m.acc[i], m.rows[i],
+               0, m.plain[i] != 0, blockIdx.y - m.ystart[i]);
 }
 
 }  // namespace
@@ -358,6 +388,70 @@ bool ck_umma_ok(const CommitArgs& a, u32 n) {
   for (u32 k = 0; k < a.rows; k++)
     if ((uintptr_t)a.w.p[k] % 16) return false;
   return true;
+}
+
+void ck_umma_shape(u64 width, u32 rows, u32 n, u32 ck_bt, u32* Bk_out, u32* G_out) {
+  // element block per CTA: a whole key-table block (one epilogue per block),
+  // halved while the grid would not fill the GPU
+  u32 Bk = (u32)(width < ck_bt ? width : ck_bt);
+  while (Bk > CK_BLOCK && (u64)(n / 2) * (width / Bk) < 296) Bk /= 2;
+  // few witness rows: G blocks one key block apart per CTA share the key
+  // tiles (virtual rows g * rows + k), while the grid keeps a full wave
+  u32 G = 1;
+  while (width >= ck_bt && rows * G * 2 <= CKU_MAX_WROWS && (width / ck_bt) % (G * 2) == 0 &&
+         (u64)(n / 2) * (width / Bk) / (G * 2) >= 148)
+    G *= 2;
+  *Bk_out = Bk;
+  *G_out = G;
+}
+
+int launch_ck_umma_multi(const CommitArgs* a, u32 ninst, u32 n, const ModQ& M, const u64* zeta, cudaStream_t st) {
+  if (ninst == 0 || ninst > CKU_MULTI_MAX) return salsaa_set_error(-2, "ck_umma_multi: 1..8 witnesses per launch");
+  CkMulti m{};
+  u32 y = 0;
+  double wit_bytes = 0, out_bytes = 0, ops = 0, macs = 0;
+  for (u32 i = 0; i < ninst; i++) {
+    const CommitArgs& c = a[i];
+    if (!ck_umma_ok(c, n) || c.nck != a[0].nck || c.tk8 != a[0].tk8)
+      return salsaa_set_error(-2, "ck_umma_multi: a witness does not fit the tensor-core key-row product");
+    u32 Bk, G;
+    ck_umma_shape(c.width, c.rows, n, c.ck_bt, &Bk, &G);
+    if (c.rows * G > CKU_MAX_WROWS || c.ck_bt % Bk || c.width % ((u64)Bk * G))
+      return salsaa_set_error(-2, "ck_umma_multi: bad block grouping");
+    u64 CH = c.width / 512;
+    if (CH < 128) CH = 128;
+    if (CH > Bk) CH = Bk;
+    m.w[i] = c.w;
+    m.rows[i] = c.rows;
+    m.G[i] = G;
+    m.Bw[i] = Bk;
+    m.acc[i] = c.acc;
+    m.plain[i] = (M.q < (1ULL << 50) && (c.width / CH) < (1ULL << 13)) ? 1 : 0;
+    m.ystart[i] = y;
+    y += (u32)(c.width / Bk / G);
+    wit_bytes += 8.0 * c.rows * (double)c.width * 2 * n;
+    out_bytes += 8.0 * c.nck * c.rows * 2 * n;
+    ops += 2.0 * 196.0 * c.nck * c.rows * (double)c.width * n;
+    macs += (double)c.nck * c.rows * (double)c.width * 2 * n;
+  }
+  m.ystart[ninst] = y;
+  m.count = ninst;
+  const u32 nck = a[0].nck, nkp = ck_tk8_nkp(nck);
+  const size_t stage = 2 * (size_t)CKU_ATILE + 2 * (size_t)nkp * CKU_CHUNK;
+  const size_t epi = 2 * 128 * (size_t)(2 * nck) * sizeof(u64);
+  const size_t smem = 2 * stage > epi ? 2 * stage : epi;
+  cudaError_t e =
+      cudaFuncSetAttribute(ck_umma_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ck_umma_multi smem attribute");
+  const int tr = salsaa_trace_begin("ck_umma_kernel", st, wit_bytes + out_bytes);
+  salsaa_trace_alias(tr, "ck_umma_kernel:int8", ops);
+  salsaa_trace_alias(tr, "ck_umma_kernel:mac", macs);
+  ck_umma_multi_kernel<<<dim3(n / 2, y), CKU_THREADS, smem, st>>>(a[0].tk8, m, nck, nkp, n, a[0].ck_bt, a[0].thi,
+                                                                   a[0].ck_nhi, M, zeta);
+  salsaa_trace_end(tr, st);
+  salsaa_count_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ck_umma_multi launch");
 }
 
 int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, u32 G, const ModQ& M, const u64* zeta, bool plain,

@@ -2120,16 +2120,8 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit: fork");
   }
   if (a.nck && ck_umma_ok(a, n)) {
-    // element block per CTA: a whole key-table block (one epilogue per block),
-    // halved while the grid would not fill the GPU
-    u32 Bk = (u32)(a.width < a.ck_bt ? a.width : a.ck_bt);
-    while (Bk > CK_BLOCK && (u64)(n / 2) * (a.width / Bk) < 296) Bk /= 2;
-    // few witness rows: G blocks one key block apart per CTA share the key
-    // tiles (virtual rows g * rows + k), while the grid keeps a full wave
-    u32 G = 1;
-    while (a.width >= a.ck_bt && a.rows * G * 2 <= CKU_MAX_WROWS && (a.width / a.ck_bt) % (G * 2) == 0 &&
-           (u64)(n / 2) * (a.width / Bk) / (G * 2) >= 148)
-      G *= 2;
+    u32 Bk, G;
+    ck_umma_shape(a.width, a.rows, n, a.ck_bt, &Bk, &G);
     int rc = launch_ck_umma(a, n, Bk, G, M, T.zeta, plain, st);
     if (rc) return rc;
   } else if (a.nck && a.tl8 && M.q < (1ULL << 56) && a.width >= CKM_KS && a.rows <= 9 && n <= 512) {
@@ -2222,6 +2214,13 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   const u64 tot = (u64)(a.nck + a.nsc) * a.rows * n;
   commit_finalize_kernel<<<grid_1d(tot, 256), 256, 0, st>>>(a.acc, a.nck, a.nsc, a.rows, n, M, T.zeta,
                                                           a.sc_base_dev, a.out_slot);
+  return check_launch("commit_finalize");
+}
+
+int launch_commit_finalize(const u64* acc, u32 nck, u32 rows, const NttDev& T, const ModQ& M, u64* out,
+                           cudaStream_t st) {
+  const u64 tot = (u64)nck * rows * T.n;
+  commit_finalize_kernel<<<grid_1d(tot, 256), 256, 0, st>>>(acc, nck, 0, rows, T.n, M, T.zeta, nullptr, out);
   return check_launch("commit_finalize");
 }
 

@@ -64,6 +64,7 @@ int launch_ck_tl8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* 
 // byte image of the B operand (rows (key row, comp c|d, byte), padded to nkp)
 // in the canonical K-major shared-memory layout; q < 2^56, nck <= 18.
 constexpr u32 CKU_MAX_KEYS = 18, CKU_MAX_WROWS = 9;
+constexpr u32 CKU_MULTI_MAX = 8;  // witnesses per launch of the multi-witness key-row product
 inline u32 ck_tk8_nkp(u32 nck) { return ((nck * 14 + 15) / 16) * 16; }
 inline u64 ck_tk8_bytes(u32 nck, u32 n, u32 bt) { return (u64)bt * n * ck_tk8_nkp(nck); }
 int launch_ck_tk8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* tk8, cudaStream_t st);
@@ -178,6 +179,15 @@ bool ck_umma_ok(const CommitArgs& a, u32 n);
 // Bw elements per block, G blocks (one key block apart) per CTA.
 int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, u32 G, const ModQ& M, const u64* zeta, bool plain,
                    cudaStream_t st);
+// The block width and grouping launch_commit uses for a witness of this shape.
+void ck_umma_shape(u64 width, u32 rows, u32 n, u32 ck_bt, u32* Bk, u32* G);
+// Key rows of several witnesses (a[i].w, a[i].rows, a[i].width; the same
+// context tables) in one launch; witness i's sums go to a[i].acc (nck x
+// a[i].rows ring elements, zeroed by the caller).
+int launch_ck_umma_multi(const CommitArgs* a, u32 ninst, u32 n, const ModQ& M, const u64* zeta, cudaStream_t st);
+// The finalisation of launch_commit (key rows only): acc -> slot-form outputs.
+int launch_commit_finalize(const u64* acc, u32 nck, u32 rows, const NttDev& T, const ModQ& M, u64* out,
+                           cudaStream_t st);
 
 // Commitment of a witness of width w from the commitment of its split halves
 // (slot form): out[j][k] = t0_j * R[j][k] + t1_j * R[j][K + k] for statement

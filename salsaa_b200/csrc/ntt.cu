@@ -545,15 +545,18 @@ __device__ __forceinline__ void nr_map(u32 tid, u32& unit, u32& tu) {
   }
 }
 
+// One 4096-coefficient tile (tile index blk) of a batch of `units` units;
+// sm is the CTA's padded exchange tile.  Called by the single-batch kernel
+// with blk = blockIdx.x and by the multi-batch kernel with its local tile.
 template <int LOGN, bool INC, bool INV, bool RELAX>
-__global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
+__device__ __forceinline__ void nr_tile(const u64* in, u64* out, u64 units, u64 blk, const NttDev& T, u64* mag_or,
+                                        u64* sm) {
   constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
   constexpr int NPH = ph_count(LOGN);
   static_assert(!INC || UPT % 2 == 0, "incomplete mode keeps both halves of an element in one tile");
-  __shared__ u64 sm[NR_TILE + NR_TILE / 16];
   u32 unit, tu;
   nr_map<LOGN, INC>(threadIdx.x, unit, tu);
-  const u64 ug = (u64)blockIdx.x * UPT + unit;
+  const u64 ug = blk * UPT + unit;
   const bool active = ug < units;
   const u64 q = T.q, q2 = 2 * T.q;
   u64 x[16], mag = 0;
@@ -579,6 +582,12 @@ __global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u
     for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
     if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
   }
+}
+
+template <int LOGN, bool INC, bool INV, bool RELAX>
+__global__ void __launch_bounds__(256) ntt_reg_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
+  __shared__ u64 sm[NR_TILE + NR_TILE / 16];
+  nr_tile<LOGN, INC, INV, RELAX>(in, out, units, blockIdx.x, T, mag_or, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -837,14 +846,14 @@ __device__ __forceinline__ void nf_mid(double (&x)[16], double* sm, u32 unit, u3
 // The register NTT (ntt_reg_kernel's thread mapping, phases and exchanges)
 // with FP64 butterflies; q < 2^50 and canonical inputs.
 template <int LOGN, bool INC, bool INV>
-__global__ void __launch_bounds__(256) ntt_fp_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
+__device__ __forceinline__ void nf_tile(const u64* in, u64* out, u64 units, u64 blk, const NttDev& T, u64* mag_or,
+                                        double* sm) {
   constexpr u32 UPT = NR_TILE >> LOGN;
   constexpr int NPH = ph_count(LOGN);
   static_assert(!INC || UPT % 2 == 0, "incomplete mode keeps both halves of an element in one tile");
-  __shared__ double sm[NR_TILE + NR_TILE / 16];
   u32 unit, tu;
   nr_map<LOGN, INC>(threadIdx.x, unit, tu);
-  const u64 ug = (u64)blockIdx.x * UPT + unit;
+  const u64 ug = blk * UPT + unit;
   const bool active = ug < units;
   double x[16];
   u64 mag = 0;
@@ -867,6 +876,41 @@ __global__ void __launch_bounds__(256) ntt_fp_kernel(const u64* in, u64* out, u6
     for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
     if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
   }
+}
+
+template <int LOGN, bool INC, bool INV>
+__global__ void __launch_bounds__(256) ntt_fp_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
+  __shared__ double sm[NR_TILE + NR_TILE / 16];
+  nf_tile<LOGN, INC, INV>(in, out, units, blockIdx.x, T, mag_or, sm);
+}
+
+// ---------------------------------------------------------------------------
+// Many uneven batches of one transform shape in one launch (the batched form
+// used by salsaa_ntt_multi): batch i owns the CTAs [bstart[i], bstart[i+1]),
+// one 4096-coefficient tile each, found by a binary search over bstart.
+// ---------------------------------------------------------------------------
+struct NttMulti {
+  const u64* in[NTT_MULTI_MAX];
+  u64* out[NTT_MULTI_MAX];
+  u64 units[NTT_MULTI_MAX];
+  u64 bstart[NTT_MULTI_MAX + 1];
+  u32 count;
+};
+
+template <int LOGN, bool INC, bool INV, bool RELAX, bool FP>
+__global__ void __launch_bounds__(256) ntt_multi_kernel(NttMulti m, NttDev T) {
+  __shared__ u64 sm[NR_TILE + NR_TILE / 16];
+  const u64 b = blockIdx.x;
+  u32 lo = 0, hi = m.count;  // invariant: bstart[lo] <= b < bstart[hi]
+  while (hi - lo > 1) {
+    const u32 mid = (lo + hi) / 2;
+    if (m.bstart[mid] <= b) lo = mid;
+    else hi = mid;
+  }
+  if constexpr (FP)
+    nf_tile<LOGN, INC, INV>(m.in[lo], m.out[lo], m.units[lo], b - m.bstart[lo], T, nullptr, (double*)sm);
+  else
+    nr_tile<LOGN, INC, INV, RELAX>(m.in[lo], m.out[lo], m.units[lo], b - m.bstart[lo], T, nullptr, sm);
 }
 
 // Digit decomposition (decomp_ell, src/subroutines/decomp.rs:32-67) fused
@@ -1152,6 +1196,36 @@ int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomple
 
 }  // namespace
 
+template <int LOGN>
+int nm_multi_go(const NttMulti& m, u64 blocks, const NttDev& T, bool incomplete, bool inverse, cudaStream_t st,
+                bool large) {
+  const bool relax = T.q < NR_RELAX_Q;
+  const bool fp = relax && ntt_choice(LOGN, incomplete, inverse, false, large).variant == 1;
+  auto go = [&](auto kern) -> int {
+    kern<<<(unsigned)blocks, 256, 0, st>>>(m, T);
+    return 0;
+  };
+  if (incomplete) {
+    if constexpr ((NR_TILE >> LOGN) >= 2) {
+      if (inverse)
+        return fp ? go(ntt_multi_kernel<LOGN, true, true, true, true>)
+                  : relax ? go(ntt_multi_kernel<LOGN, true, true, true, false>)
+                          : go(ntt_multi_kernel<LOGN, true, true, false, false>);
+      return fp ? go(ntt_multi_kernel<LOGN, true, false, true, true>)
+                : relax ? go(ntt_multi_kernel<LOGN, true, false, true, false>)
+                        : go(ntt_multi_kernel<LOGN, true, false, false, false>);
+    }
+    return salsaa_set_error(-2, "ntt_multi: incomplete transforms need d <= 4096");
+  }
+  if (inverse)
+    return fp ? go(ntt_multi_kernel<LOGN, false, true, true, true>)
+              : relax ? go(ntt_multi_kernel<LOGN, false, true, true, false>)
+                      : go(ntt_multi_kernel<LOGN, false, true, false, false>);
+  return fp ? go(ntt_multi_kernel<LOGN, false, false, true, true>)
+            : relax ? go(ntt_multi_kernel<LOGN, false, false, true, false>)
+                    : go(ntt_multi_kernel<LOGN, false, false, false, false>);
+}
+
 bool ntt_mag_ok(const u64* in, const u64* out, const NttDev& T, bool incomplete) {
   const bool aligned = ((uintptr_t)in % 16 == 0) && ((uintptr_t)out % 16 == 0);
   return aligned && T.n >= 16 && T.n <= (incomplete ? 2048u : 4096u);
@@ -1204,6 +1278,53 @@ int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incompl
   };
   if (incomplete) return inverse ? launch(ntt_kernel<true, true>) : launch(ntt_kernel<true, false>);
   return inverse ? launch(ntt_kernel<false, true>) : launch(ntt_kernel<false, false>);
+}
+
+int ntt_multi_launch(const u64* const* in, u64* const* out, const u64* count, u32 ninst, const NttDev& T,
+                     bool incomplete, bool inverse, cudaStream_t st) {
+  if (ninst > (u32)NTT_MULTI_MAX) return salsaa_set_error(-2, "ntt_multi: at most 64 batches per launch");
+  if (T.n < 16 || T.n > (incomplete ? 2048u : 4096u))
+    return salsaa_set_error(-2, "ntt_multi: needs 16 <= n <= 4096 (2048 in incomplete mode)");
+  NttMulti m{};
+  const u32 upt = NR_TILE >> T.logn;
+  u64 blocks = 0, coeffs = 0;
+  u32 k = 0;
+  for (u32 i = 0; i < ninst; i++) {
+    if (!count[i]) continue;
+    if (!in[i] || !out[i]) return salsaa_set_error(-1, "ntt_multi: null buffer");
+    if ((uintptr_t)in[i] % 16 || (uintptr_t)out[i] % 16) return salsaa_set_error(-2, "ntt_multi: buffers must be 16-byte aligned");
+    const u64 units = incomplete ? 2 * count[i] : count[i];
+    m.in[k] = in[i];
+    m.out[k] = out[i];
+    m.units[k] = units;
+    m.bstart[k] = blocks;
+    blocks += (units + upt - 1) / upt;
+    coeffs += units * T.n;
+    k++;
+  }
+  if (k == 0) return 0;
+  m.bstart[k] = blocks;
+  m.count = k;
+  if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt_multi: batch too large");
+  const bool large = coeffs >= NTT_LARGE_COEFFS;
+  const int tr = salsaa_trace_begin("ntt_kernel", st, 16.0 * (double)coeffs);
+  int rc = 0;
+  switch (T.logn) {
+    case 4: rc = nm_multi_go<4>(m, blocks, T, incomplete, inverse, st, large); break;
+    case 5: rc = nm_multi_go<5>(m, blocks, T, incomplete, inverse, st, large); break;
+    case 6: rc = nm_multi_go<6>(m, blocks, T, incomplete, inverse, st, large); break;
+    case 7: rc = nm_multi_go<7>(m, blocks, T, incomplete, inverse, st, large); break;
+    case 8: rc = nm_multi_go<8>(m, blocks, T, incomplete, inverse, st, large); break;
+    case 9: rc = nm_multi_go<9>(m, blocks, T, incomplete, inverse, st, large); break;
+    case 10: rc = nm_multi_go<10>(m, blocks, T, incomplete, inverse, st, large); break;
+    case 11: rc = nm_multi_go<11>(m, blocks, T, incomplete, inverse, st, large); break;
+    default: rc = nm_multi_go<12>(m, blocks, T, incomplete, inverse, st, large); break;
+  }
+  salsaa_trace_end(tr, st);
+  if (rc) return rc;
+  salsaa_count_launch();
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ntt_multi launch");
 }
 
 template <int LOGN>

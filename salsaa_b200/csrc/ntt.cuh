@@ -60,6 +60,13 @@ int ntt_launch(const u64* in, u64* out, u64 count, const NttDev& T, bool incompl
                cudaStream_t st, u64* mag_or = nullptr);
 bool ntt_mag_ok(const u64* in, const u64* out, const NttDev& T, bool incomplete);
 
+// Up to NTT_MULTI_MAX batches (count[i] units of n, or ring elements of 2n in
+// incomplete mode) of one (n, q) transformed in one launch; every buffer
+// 16-byte aligned and 16 <= n <= 4096 (2048 incomplete).  in[i] may equal out[i].
+constexpr int NTT_MULTI_MAX = 64;
+int ntt_multi_launch(const u64* const* in, u64* const* out, const u64* count, u32 ninst, const NttDev& T,
+                     bool incomplete, bool inverse, cudaStream_t st);
+
 // Digit decomposition fused with the forward incomplete transform: for rows
 // source rows of width ring elements (2n coefficients, canonical), radix
 // 2^ceil(bw / parts) from the OR of centred magnitudes *bw_or (its log2 goes

@@ -1457,6 +1457,16 @@ extern "C" int salsaa_ntt(const uint64_t* d_in, uint64_t* d_out, uint64_t n, uin
   return ntt_launch(d_in, d_out, count, *T, incomplete != 0, inverse != 0, (cudaStream_t)stream);
 }
 
+extern "C" int salsaa_ntt_multi(const uint64_t* const* d_in, uint64_t* const* d_out, const uint64_t* counts,
+                                uint32_t ninst, uint64_t n, uint64_t q, int inverse, int incomplete, void* stream) {
+  if (!d_in || !d_out || !counts) return salsaa_set_error(-1, "ntt_multi: null argument");
+  const u64 nn = incomplete ? n / 2 : n;
+  if (incomplete && (n < 4 || n % 2)) return salsaa_set_error(-1, "ntt_multi: incomplete mode needs even d >= 4");
+  const NttDev* T = ntt_tables((u32)nn, q);
+  if (!T || nn > 8192) return salsaa_set_error(-1, "ntt_multi: no NTT for (n, q)");
+  return ntt_multi_launch(d_in, d_out, counts, ninst, *T, incomplete != 0, inverse != 0, (cudaStream_t)stream);
+}
+
 extern "C" int salsaa_poly_mul(const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_r, uint64_t n,
                                uint64_t count, uint64_t q, void* stream) {
   if (!d_a || !d_b || !d_r) return salsaa_set_error(-1, "poly_mul: null pointer");
@@ -1514,6 +1524,69 @@ extern "C" int salsaa_commit(salsaa_ctx* c, const uint64_t* d_w, uint64_t rows, 
   a.out_slot = cout;
   TRY(launch_commit(a, *c->T, c->M, ds, st));
   return ntt_launch(cout, d_out, (u64)ms * rows, *c->T, true, true, st);
+}
+
+extern "C" int salsaa_commit_multi(salsaa_ctx* c, const uint64_t* const* d_w, const uint64_t* rows,
+                                   const uint64_t* widths, uint32_t ninst, uint64_t* const* d_out, void* stream) {
+  if (!c || !d_w || !rows || !widths || !d_out) return salsaa_set_error(-1, "commit_multi: null argument");
+  if (ninst == 0 || ninst > CKU_MULTI_MAX) return salsaa_set_error(-2, "commit_multi: 1..8 witnesses per call");
+  cudaStream_t st = (cudaStream_t)stream;
+  const u32 d = c->d, ms = (u32)c->P.module_size;
+  u64 wtot = 0, etot = 0;
+  for (u32 i = 0; i < ninst; i++) {
+    if (!d_w[i] || !d_out[i]) return salsaa_set_error(-1, "commit_multi: null buffer");
+    if (rows[i] == 0 || rows[i] > CKU_MAX_WROWS || widths[i] < 128 || widths[i] > c->L ||
+        (widths[i] & (widths[i] - 1)) || (uintptr_t)d_w[i] % 16 || (uintptr_t)d_out[i] % 16)
+      return salsaa_set_error(-2, "commit_multi: witness shape or alignment outside the one-launch path");
+    wtot += rows[i] * widths[i] * d;
+    etot += (u64)ms * rows[i] * d;
+  }
+  Tmp t(st);
+  u64 *ws, *acc, *cout;
+  TRY(t.get(&ws, wtot));
+  TRY(t.get(&acc, etot));
+  TRY(t.get(&cout, etot));
+  // every witness to slot form in one launch
+  const u64* ins[CKU_MULTI_MAX];
+  u64* outs[CKU_MULTI_MAX];
+  u64 cnt[CKU_MULTI_MAX];
+  CommitArgs a[CKU_MULTI_MAX];
+  u64 wo = 0, eo = 0;
+  for (u32 i = 0; i < ninst; i++) {
+    ins[i] = d_w[i];
+    outs[i] = ws + wo;
+    cnt[i] = rows[i] * widths[i];
+    a[i] = CommitArgs{};
+    a[i].tl8 = c->tl8;
+    a[i].tk8 = c->tk8;
+    a[i].w = rows_of(ws + wo, (u32)rows[i], widths[i], d);
+    a[i].rows = (u32)rows[i];
+    a[i].width = widths[i];
+    a[i].nck = ms;
+    a[i].tlo = c->tlo;
+    a[i].thi = c->thi;
+    a[i].ck_bt = c->ck_bt;
+    a[i].ck_nhi = c->ck_nhi;
+    a[i].acc = acc + eo;
+    wo += cnt[i] * d;
+    eo += (u64)ms * rows[i] * d;
+  }
+  TRY(ntt_multi_launch(ins, outs, cnt, ninst, *c->T, true, false, st));
+  cudaError_t e = cudaMemsetAsync(acc, 0, etot * sizeof(u64), st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "commit_multi: memset");
+  // the key rows of every witness in one launch, then one finalisation over
+  // all accumulators and one inverse transform into the callers' buffers
+  TRY(launch_ck_umma_multi(a, ninst, c->T->n, c->M, c->T->zeta, st));
+  TRY(launch_commit_finalize(acc, 1, (u32)(etot / d), *c->T, c->M, cout, st));
+  const u64* cin[CKU_MULTI_MAX];
+  u64 ecnt[CKU_MULTI_MAX];
+  eo = 0;
+  for (u32 i = 0; i < ninst; i++) {
+    cin[i] = cout + eo;
+    ecnt[i] = (u64)ms * rows[i];
+    eo += ecnt[i] * d;
+  }
+  return ntt_multi_launch(cin, d_out, ecnt, ninst, *c->T, true, true, st);
 }
 
 extern "C" int salsaa_sumcheck(const uint64_t* d_w, uint64_t rows, uint64_t n, uint64_t d, uint64_t q,

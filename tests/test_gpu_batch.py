@@ -82,3 +82,62 @@ def test_sumcheck_batch_rejects_bad_lengths(api):
     from salsaa_b200.api import SalsaaError
     with pytest.raises(SalsaaError):
         api.sum_check_batch([api.to_dev(np.zeros(100, dtype=np.uint64))], P.Q0, 1, 0)
+
+
+@pytest.mark.parametrize("n_arg,incomplete,q", [(128, True, P.Q0), (256, True, P.Q1), (512, True, P.Q2),
+                                                (64, False, P.Q62), (1024, False, P.Q62), (16, False, P.Q0)])
+def test_ntt_multi_uneven(api, oracle, cuda, n_arg, incomplete, q):
+    """64 uneven batches (some empty, some not a whole tile) in one launch,
+    forward then inverse, equal one salsaa_ntt call per batch and the oracle."""
+    torch = cuda
+    rng = np.random.default_rng(n_arg)
+    counts = [int(c) for c in rng.integers(0, 300, size=64)]
+    counts[5] = 0
+    counts[7] = 1
+    xs = [rand_mod(rng, (c, n_arg), q) for c in counts]
+    dev = [api.to_dev(x) for x in xs]
+    fwd = api.ntt_multi(dev, n_arg, q, incomplete=incomplete, outs=[api.dev_empty(d.shape) for d in dev])
+    single = [api.ntt(d, n_arg, q, incomplete=incomplete, out=api.dev_empty(d.shape)) for d in dev]
+    back = api.ntt_multi([f.clone() for f in fwd], n_arg, q, inverse=True, incomplete=incomplete)  # in place
+    torch.cuda.synchronize()
+    for i, c in enumerate(counts):
+        f = api.to_host(fwd[i])
+        assert np.array_equal(f, api.to_host(single[i])), i
+        assert np.array_equal(api.to_host(back[i]), xs[i]), i
+    i = 8
+    want = oracle.ring_to_slot(xs[i][:3], q) if incomplete else oracle.ntt_forward(xs[i][:3], q)
+    assert np.array_equal(api.to_host(fwd[i])[:3], want)
+
+
+def test_ntt_multi_rejects(api):
+    from salsaa_b200.api import SalsaaError
+    with pytest.raises(SalsaaError):  # n = 8 is below the register path
+        api.ntt_multi([api.to_dev(np.zeros((4, 8), dtype=np.uint64))], 8, P.Q0)
+
+
+def test_commit_multi_uneven(api, oracle):
+    """Eight witnesses of uneven widths and row counts against one context's
+    key rows in one tensor-core launch equal one salsaa_commit each and the
+    oracle's parallel_dot_series_matrix."""
+    p = P.make_params(128, P.Q0, 12, 1 << 15, 2, False)
+    ctx = api.Context(p, crs_seed=4)
+    rng = np.random.default_rng(17)
+    shapes = [(1, 1 << 15), (3, 1 << 12), (9, 1 << 7), (2, 1 << 14), (1, 1 << 10), (5, 1 << 13), (4, 1 << 8),
+              (2, 1 << 15)]
+    ws = [small_signed(rng, (r, w, p.d), 3, p.q) for r, w in shapes]
+    got = ctx.parallel_dot_series_matrix_multi([api.to_dev(w) for w in ws])
+    for i, w in enumerate(ws):
+        single = api.to_host(ctx.parallel_dot_series_matrix(api.to_dev(w)))
+        assert np.array_equal(api.to_host(got[i]), single), i
+    for i in (1, 2, 6):
+        assert np.array_equal(api.to_host(got[i]), oracle.commit_ck(p, 4, ws[i])), i
+    ctx.close()
+
+
+def test_commit_multi_rejects(api):
+    from salsaa_b200.api import SalsaaError
+    p = P.make_params(128, P.Q0, 12, 1 << 12, 1, False)
+    ctx = api.Context(p, crs_seed=4)
+    with pytest.raises(SalsaaError):  # width below one 128-element chunk
+        ctx.parallel_dot_series_matrix_multi([api.to_dev(np.zeros((1, 64, 128), dtype=np.uint64))])
+    ctx.close()
