@@ -514,7 +514,8 @@ __global__ void __launch_bounds__(256, 2)
   const u64 idx = blockIdx.y;
   const u32 i = (u32)(idx / nch);
   const u64 j = idx % nch;
-  const u64* chunk = in.p[i] + (j * cw) * d + (u64)nblk * PU_POS;
+  const bool nar = (in.narrow >> i) & 1;
+  const u64* chunk = row_advance(in.p[i], nar, (j * cw) * d + (u64)nblk * PU_POS);
   const u64 half_q = q >> 1;
   const u32 nsteps = cw / PU_KS;
   u32* err = &g_tc_error;
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(256, 2)
   // the previous step's barrier) to their conversion
   u64 vr[8][4];
   auto load = [&](u32 c) {
-    const u64* src = chunk + (u64)c * PU_KS * d;
+    const u64* src = row_advance(chunk, nar, (u64)c * PU_KS * d);
 #pragma unroll
     for (u32 x = 0; x < 8; x++) {
       const u32 t = tid + x * 256;
@@ -546,7 +547,7 @@ __global__ void __launch_bounds__(256, 2)
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
       const u32 k = (k4hi * 4 + k4lo) * 4;
 #pragma unroll
-      for (u32 e = 0; e < 4; e++) vr[x][e] = __ldg(src + (u64)(k + e) * d + pos);
+      for (u32 e = 0; e < 4; e++) vr[x][e] = wres(src, nar, (u64)(k + e) * d + pos, q);
     }
   };
   load(0);
@@ -679,7 +680,8 @@ __global__ void __launch_bounds__(512, 1)
   const u32 pb = blockIdx.x, hb = blockIdx.y / split, sub = blockIdx.y % split, k = blockIdx.z;
   const u64 q = M.q, half_q = q >> 1;
   const u32 nsteps = Bw / SU_KS / split, c0 = sub * nsteps;
-  const u64* src0 = wc.p[k] + ((u64)hb * Bw + (u64)c0 * SU_KS) * d + (u64)pb * SU_POS;
+  const bool nar = (wc.narrow >> k) & 1;
+  const u64* src0 = row_advance(wc.p[k], nar, ((u64)hb * Bw + (u64)c0 * SU_KS) * d + (u64)pb * SU_POS);
   img += (u64)c0 * SU_A;
   u32* err = &g_tc_error;
   if (tid == 0) {
@@ -700,7 +702,7 @@ __global__ void __launch_bounds__(512, 1)
   // task x of this thread: four consecutive elements e0 .. e0 + 3 at one position
   u64 vr[8][4];
   auto load = [&](u32 c) {
-    const u64* src = src0 + (u64)c * SU_KS * d;
+    const u64* src = row_advance(src0, nar, (u64)c * SU_KS * d);
 #pragma unroll
     for (u32 x = 0; x < 8; x++) {
       const u32 t = tid + x * 512;
@@ -708,7 +710,7 @@ __global__ void __launch_bounds__(512, 1)
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
       const u32 e0 = (k4hi * 4 + k4lo) * 4;
 #pragma unroll
-      for (u32 e = 0; e < 4; e++) vr[x][e] = __ldg(src + (u64)(e0 + e) * d + pos);
+      for (u32 e = 0; e < 4; e++) vr[x][e] = wres(src, nar, (u64)(e0 + e) * d + pos, q);
     }
   };
   load(0);
@@ -815,11 +817,13 @@ __global__ void sc_exact_kernel(RowSet wc, u32 rows, u32 d, u32 Bw, u32 nhi, u32
   if (!flags[cta]) return;
   const u32 pb = blockIdx.x, hb = blockIdx.y / split, sub = blockIdx.y % split, k = blockIdx.z, pos = threadIdx.x;
   const u32 i0 = sub * (Bw / split), i1 = i0 + Bw / split;
-  const u64* src = wc.p[k] + ((u64)hb * Bw) * d + (u64)pb * SU_POS + pos;
+  const bool nar = (wc.narrow >> k) & 1;
+  const u64* src = row_advance(wc.p[k], nar, ((u64)hb * Bw) * d + (u64)pb * SU_POS + pos);
   for (u32 r = 0; r < tl.n; r++) {
     const u32 j = tl.idx[r];
     u64 v = 0;
-    for (u32 i = i0; i < i1; i++) v = salsaa::add_mod(v, mul_mod(M, s_lo[(u64)j * Bw + i], src[(u64)i * d]), M.q);
+    for (u32 i = i0; i < i1; i++)
+      v = salsaa::add_mod(v, mul_mod(M, s_lo[(u64)j * Bw + i], wres(src, nar, (u64)i * d, M.q)), M.q);
     v = mul_mod(M, v, s_hi[(u64)j * nhi + hb]);
     atomic_add_mod(acc + ((u64)j * rows + k) * d + (u64)pb * SU_POS + pos, v, M.q, plain);
   }
@@ -900,6 +904,7 @@ __global__ void __launch_bounds__(256, 2)
   const u64 q = M.q, half_q = q >> 1;
   const u32 t0 = (u32)((u64)blockIdx.x * ntiles / gridDim.x), t1 = (u32)((u64)(blockIdx.x + 1) * ntiles / gridDim.x);
   const u64* x = w.p[k];
+  const bool nar = (w.narrow >> k) & 1;
   u32* err = &g_tc_error;
   uint8_t* btab = smem + 2 * NG_STAGE;
 
@@ -945,9 +950,9 @@ __global__ void __launch_bounds__(256, 2)
 
   u64 v[16];
   auto load = [&](u32 tile) {
-    const u64* src = x + (u64)tile * NG_TILE + tid;
+    const u64 o = (u64)tile * NG_TILE + tid;
 #pragma unroll
-    for (u32 m = 0; m < 16; m++) v[m] = __ldg(src + m * ng);
+    for (u32 m = 0; m < 16; m++) v[m] = wres(x, nar, o + m * ng, q);
   };
   auto epilogue = [&](u32 li, u32 tile) {
     const u32 se = li & 1;

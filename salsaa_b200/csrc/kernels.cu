@@ -314,6 +314,7 @@ __global__ void __launch_bounds__(256, 2) sc_first_kernel(RowSet w, u32 rows, u6
   if (only_if && *only_if == 0) return;  // the tensor-core pass covered this launch
   const u32 k = blockIdx.y, rep = blockIdx.x & 1, bx = blockIdx.x >> 1, nbx = gridDim.x >> 1;
   const u64* x = w.p[k];
+  const bool nar = (w.narrow >> k) & 1;
   const u64 q = M.q, ng = nlen / G;
   u64 c[T], cp[T];
 #pragma unroll
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(256, 2) sc_first_kernel(RowSet w, u32 rows, u6
   for (u64 g = (u64)bx * blockDim.x + threadIdx.x; g < ng; g += (u64)nbx * blockDim.x) {
     u64 v[G];
 #pragma unroll
-    for (u32 m = 0; m < G; m++) v[m] = __ldg(x + g + m * ng);
+    for (u32 m = 0; m < G; m++) v[m] = wres(x, nar, g + m * ng, q);
     group_rounds<LAZY, T>(M, v, c, cp, acc, rep == 0 ? 0 : 1);
     out[((u64)rep * rows + k) * sout + g] = v[0];
   }
@@ -432,7 +433,8 @@ __global__ void __launch_bounds__(512) sc_tail_kernel(const u64* in, u64 sin, Ro
   __shared__ Sum128 red[SC_T * 3 * 32];
   const u32 pair = blockIdx.x, rep = pair / rows, k = pair % rows;
   const u64* x = (j0 == 0) ? w0.p[k] : in + (u64)pair * sin;
-  for (u32 i = threadIdx.x; i < L; i += blockDim.x) v[i] = x[i];
+  const bool nar = j0 == 0 && ((w0.narrow >> k) & 1);
+  for (u32 i = threadIdx.x; i < L; i += blockDim.x) v[i] = wres(x, nar, i, M.q);
   __syncthreads();
   u64 cur = L;
   u32 j = j0;
@@ -966,6 +968,7 @@ __global__ void decomp_digits_kernel(RowSet in, u32 rows, u64 per_row, u64 q, u3
 int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds, u64* out,
                      u64* proof_radix, cudaStream_t st, bool mag_ready) {
   if (parts < 1 || didx >= 16) return salsaa_set_error(-2, "decompose: bad arguments");
+  if (in.narrow) return salsaa_set_error(-2, "decompose: source rows must be canonical words");
   const u64 per_row = width * d;
   int rc = 0;
   if (!mag_ready) {
@@ -982,8 +985,10 @@ int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u3
 
 int launch_decompose_ntt(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds,
                          u64* out, u64* out_slot, u64* proof_radix, const NttDev& T, cudaStream_t st,
-                         bool mag_ready) {
+                         bool mag_ready, bool* narrow_out) {
   if (parts < 1 || didx >= 16) return salsaa_set_error(-2, "decompose: bad arguments");
+  if (in.narrow) return salsaa_set_error(-2, "decompose: source rows must be canonical words");
+  if (narrow_out) *narrow_out = false;
   if (!ntt_digits_ok(out, out_slot, rows, T) || rows > MAX_WROWS || d != 2 * T.n) {
     const int rc = launch_decompose(in, rows, width, d, q, parts, didx, ds, out, proof_radix, st, mag_ready);
     if (rc) return rc;
@@ -998,8 +1003,12 @@ int launch_decompose_ntt(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts
   }
   NttSrcRows src{};
   for (u32 k = 0; k < rows; k++) src.p[k] = in.p[k];
-  return ntt_digits_launch(src, rows, width, parts, &ds->bw_or[didx], &ds->rlog[didx], proof_radix, out, out_slot, T,
-                           st);
+  // with two or more parts the digits are below 2^25: coefficient form as int32
+  const bool narrow = narrow_out != nullptr && parts >= 2;
+  const int rc = ntt_digits_launch(src, rows, width, parts, &ds->bw_or[didx], &ds->rlog[didx], proof_radix, out,
+                                   out_slot, T, st, narrow);
+  if (!rc && narrow_out) *narrow_out = narrow;
+  return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -1091,7 +1100,8 @@ __global__ void project_kernel(RowSet in, u64 width, u32 d, u64 q, u32 cw, u64 n
   __syncthreads();
   const u32 pos = threadIdx.x;
   if (pos >= d) return;
-  const u64* chunk = in.p[i] + (j * cw) * d;
+  const bool nar = (in.narrow >> i) & 1;
+  const u64* chunk = row_advance(in.p[i], nar, (j * cw) * d);
   u64 acc[KT];
 #pragma unroll
   for (int kk = 0; kk < KT; kk++) acc[kk] = 0;
@@ -1103,7 +1113,7 @@ __global__ void project_kernel(RowSet in, u64 width, u32 d, u64 q, u32 cw, u64 n
       nm[kk] = msk[KT * words + kk * words + w];
     }
     for (u32 b = 0; b < 32; b++) {
-      const u64 x = chunk[(u64)(w * 32 + b) * d + pos];
+      const u64 x = wres(chunk, nar, (u64)(w * 32 + b) * d + pos, q);
       const u64 nx = x ? q - x : 0;
 #pragma unroll
       for (int kk = 0; kk < KT; kk++) {
@@ -1147,7 +1157,8 @@ __global__ void __launch_bounds__(256, 2) project_mma_kernel(RowSet in, u32 d, u
   const u64 idx = blockIdx.y;
   const u32 i = (u32)(idx / nch);
   const u64 j = idx % nch;
-  const u64* chunk = in.p[i] + (j * cw) * d + (u64)nblk * PJ_BN;
+  const bool nar = (in.narrow >> i) & 1;
+  const u64* chunk = row_advance(in.p[i], nar, (j * cw) * d + (u64)nblk * PJ_BN);
   const u32 k0 = mhalf * PJ_BM;
   const u64 half_q = q >> 1;
   int acc[2][8][4];
@@ -1168,7 +1179,7 @@ __global__ void __launch_bounds__(256, 2) project_mma_kernel(RowSet in, u32 d, u
       u32 packed = 0;
 #pragma unroll
       for (u32 e = 0; e < 4; e++) {
-        const u64 v = chunk[(u64)(l0 + l4 * 4 + e) * d + pos];
+        const u64 v = wres(chunk, nar, (u64)(l0 + l4 * 4 + e) * d + pos, q);
         long long c = v > half_q ? (long long)v - (long long)q : (long long)v;
         if (c < -128 || c > 127) {
           bad = true;
@@ -1463,6 +1474,7 @@ __global__ void __launch_bounds__(256) fold_vec_kernel(RowSet w, u32 rows, u64 w
 int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ& M, const u64* c_slot, u64* pre,
                 u64* out_slot, cudaStream_t st) {
   if (rows == 0 || rows > MAX_WROWS) return salsaa_set_error(-2, "fold: bad row count");
+  if (w_slot.narrow) return salsaa_set_error(-2, "fold: slot-form rows must be canonical words");
   const bool lazy = M.q < (1ULL << 57);
   bool vec = T.n >= 2 && (uintptr_t)out_slot % 16 == 0 && (uintptr_t)pre % 16 == 0 && ((u64)rows * T.n) % 2 == 0;
   for (u32 k = 0; k < rows; k++) vec = vec && (uintptr_t)w_slot.p[k] % 16 == 0;
@@ -1644,21 +1656,27 @@ __global__ void __launch_bounds__(512) sc_commit_kernel(RowSet w, u32 rows, ScRo
       g[a][b] = 0;
     }
   const u64* wp[KT];
+  bool wn[KT];
+  const u64 wo = i0 * d + p;
 #pragma unroll
-  for (int b = 0; b < KT; b++) wp[b] = ((k0 + b < rows) ? w.p[k0 + b] : w.p[k0]) + i0 * d + p;
+  for (int b = 0; b < KT; b++) {
+    const u32 kk = (k0 + b < rows) ? k0 + b : k0;
+    wp[b] = w.p[kk];
+    wn[b] = (w.narrow >> kk) & 1;
+  }
   const u64* sp[RT];
 #pragma unroll
   for (int a = 0; a < RT; a++) sp[a] = s_lo + (u64)row[a] * Bw + lo0;
   u64 x[KT], sv[RT];
 #pragma unroll
-  for (int b = 0; b < KT; b++) x[b] = __ldg(wp[b]);
+  for (int b = 0; b < KT; b++) x[b] = wres(wp[b], wn[b], wo, q);
 #pragma unroll
   for (int a = 0; a < RT; a++) sv[a] = __ldg(sp[a]);
   for (u32 e = 0; e < CH; e++) {
     const u32 en = (e + 1 < CH) ? e + 1 : e;
     u64 nx[KT], ns[RT];
 #pragma unroll
-    for (int b = 0; b < KT; b++) nx[b] = __ldg(wp[b] + (u64)en * d);
+    for (int b = 0; b < KT; b++) nx[b] = wres(wp[b], wn[b], wo + (u64)en * d, q);
 #pragma unroll
     for (int a = 0; a < RT; a++) ns[a] = __ldg(sp[a] + en);
     if (LIMB) {
@@ -1741,13 +1759,14 @@ __global__ void colsum_kernel(RowSet w, u32 rows, u64 width, u32 Bw, u32 d, ModQ
   const bool lazy = M.q < (1ULL << 50) && nhi <= 4096;
   for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
     const u64 k = t / per, r = t % per;
-    const u64* x = w.p[k] + r;
+    const u64* x = w.p[k];
+    const bool nar = (w.narrow >> k) & 1;
     u64 sacc = 0;
     if (lazy) {
-      for (u64 h = 0; h < nhi; h++) sacc += __ldg(x + h * per);
+      for (u64 h = 0; h < nhi; h++) sacc += wres(x, nar, r + h * per, M.q);
       sacc %= M.q;
     } else {
-      for (u64 h = 0; h < nhi; h++) sacc = add_mod(sacc, __ldg(x + h * per), M.q);
+      for (u64 h = 0; h < nhi; h++) sacc = add_mod(sacc, wres(x, nar, r + h * per, M.q), M.q);
     }
     out[t] = sacc;
   }
@@ -2099,6 +2118,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
   if (a.rows == 0 || a.rows > MAX_WROWS || a.width == 0 || (a.width & (a.width - 1)))
     return salsaa_set_error(-2, "commit: bad witness shape");
   if (d > 512) return salsaa_set_error(-2, "commit: ring degree above 512");
+  if (a.w.narrow) return salsaa_set_error(-2, "commit: slot-form rows must be canonical words");
   const u32 Bw = (u32)(a.width < CK_BLOCK ? a.width : CK_BLOCK);
   const u32 nhi = (u32)(a.width / Bw);
   // chunk: >= 128 elements (each thread's lazy sums are reduced once per
@@ -2189,6 +2209,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
         rc = check_launch("colsum");
         if (rc) return rc;
         for (u32 k = 0; k < a.rows; k++) u.p[k] = a.colsum + (u64)k * Bw * d;
+        u.narrow = 0;  // the column sums are canonical words
       }
       u64 CHu = Bw / 64;
       if (CHu < 16) CHu = 16;

@@ -20,7 +20,24 @@ constexpr u32 CK_KEY_BLOCK = 8192;
 
 struct RowSet {
   const u64* p[MAX_WROWS];
+  // bit k set: row k holds centred int32 values (decomposition digits, whose
+  // magnitudes stay below the radix <= 2^25) instead of canonical u64 words;
+  // p[k] then points at int32 data and element offsets count int32 values
+  u32 narrow;
 };
+
+// Row pointer advanced by `elems` elements of the row's type.
+__host__ __device__ inline const u64* row_advance(const u64* p, bool narrow, u64 elems) {
+  return narrow ? (const u64*)((const int*)p + elems) : p + elems;
+}
+// Element i of a coefficient-form row as a canonical residue mod q.
+__device__ __forceinline__ u64 wres(const u64* p, bool narrow, u64 i, u64 q) {
+  if (narrow) {
+    const long long v = __ldg((const int*)p + i);
+    return v < 0 ? (u64)(v + (long long)q) : (u64)v;
+  }
+  return __ldg(p + i);
+}
 
 // Per-proof device state that data-dependent steps write and later kernels read.
 struct DevState {
@@ -118,10 +135,11 @@ int launch_decompose(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u3
                      u64* out, u64* proof_radix, cudaStream_t st, bool mag_ready = false);
 // The same, also writing the digits' slot form to out_slot (one fused pass
 // with the forward transform when the shapes allow, else decomposition then
-// transform).
+// transform).  With narrow_out given, the fused pass with parts >= 2 writes
+// the coefficient-form digits as centred int32 values and sets *narrow_out.
 int launch_decompose_ntt(RowSet in, u32 rows, u64 width, u32 d, u64 q, u32 parts, u32 didx, DevState* ds,
                          u64* out, u64* out_slot, u64* proof_radix, const NttDev& T, cudaStream_t st,
-                         bool mag_ready = false);
+                         bool mag_ready = false, bool* narrow_out = nullptr);
 
 // J as bit masks (CUDA-core path), as an int8 matrix 256 x cw (tensor-core
 // path, optional) and cj[l] = sum_k J[k][l] (optional).

@@ -923,8 +923,10 @@ __global__ void __launch_bounds__(256) ntt_multi_kernel(NttMulti m, NttDev T) {
 template <int LOGN, bool RELAX, bool FP>
 __global__ void __launch_bounds__(256)
     ntt_digits_kernel(NttSrcRows src, u64 width, u32 parts, const u64* bw_or, u64* rlog_out, u64* radix_out, u64* dc,
-                      u64* ds, u64 units, NttDev T) {
-  // FP: the FP64 butterflies (q < 2^50), else the integer ones
+                      u64* ds, u64 units, NttDev T, bool narrow) {
+  // FP: the FP64 butterflies (q < 2^50), else the integer ones.  narrow: the
+  // coefficient-form digits go to dc as centred int32 values (parts >= 2, so
+  // |digit| < radix <= 2^25), else as canonical words.
   using Wd = typename std::conditional<FP, double, u64>::type;
   constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N, D = 2 * N;
   constexpr int NPH = ph_count(LOGN);
@@ -955,6 +957,7 @@ __global__ void __launch_bounds__(256)
   if (active) {
     const u64* sp = src.p[k] + i * D + h;
     u64* dco = dc + dring * D + h;
+    int* dcn = (int*)dc + dring * D + h;
 #pragma unroll
     for (u32 j = 0; j < MB; j++)
 #pragma unroll
@@ -968,7 +971,10 @@ __global__ void __launch_bounds__(256)
           x[j * KB + kk] = fp_from_word(dv);
         else
           x[j * KB + kk] = dv;
-        dco[2 * e] = dv;
+        if (narrow)
+          dcn[2 * e] = (int)((long long)pd - (long long)nd);
+        else
+          dco[2 * e] = dv;
       }
     if constexpr (FP)
       nf_compute<LOGN, 0, false>(x, tu, T);
@@ -1329,7 +1335,7 @@ int ntt_multi_launch(const u64* const* in, u64* const* out, const u64* count, u3
 
 template <int LOGN>
 int nd_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* bw_or, u64* rlog_out,
-              u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st) {
+              u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st, bool narrow) {
   constexpr u32 UPT = NR_TILE >> LOGN;
   const u64 units = 2ULL * rows * parts * width;
   const u64 blocks = (units + UPT - 1) / UPT;
@@ -1339,13 +1345,13 @@ int nd_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* 
   const bool fp = relax && ntt_choice(LOGN, true, false, false, units * (1ULL << LOGN) >= NTT_LARGE_COEFFS).variant == 1;
   if (fp)
     ntt_digits_kernel<LOGN, true, true><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
-                                                                           radix_out, dc, ds, units, T);
+                                                                           radix_out, dc, ds, units, T, narrow);
   else if (relax)
     ntt_digits_kernel<LOGN, true, false><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
-                                                                            radix_out, dc, ds, units, T);
+                                                                            radix_out, dc, ds, units, T, narrow);
   else
     ntt_digits_kernel<LOGN, false, false><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
-                                                                             radix_out, dc, ds, units, T);
+                                                                             radix_out, dc, ds, units, T, narrow);
   return 0;
 }
 
@@ -1354,21 +1360,21 @@ bool ntt_digits_ok(const u64* dc, const u64* ds, u32 rows, const NttDev& T) {
 }
 
 int ntt_digits_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* bw_or, u64* rlog_out,
-                      u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st) {
-  if (!ntt_digits_ok(dc, ds, rows, T) || parts == 0 || width == 0)
+                      u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st, bool narrow) {
+  if (!ntt_digits_ok(dc, ds, rows, T) || parts == 0 || width == 0 || (narrow && parts < 2))
     return salsaa_set_error(-2, "ntt_digits: shape or alignment not supported");
-  const double bytes = 8.0 * rows * width * 2.0 * T.n * (1.0 + 2.0 * parts);
+  const double bytes = 8.0 * rows * width * 2.0 * T.n * (1.0 + (narrow ? 1.5 : 2.0) * parts);
   const int tr = salsaa_trace_begin("ntt_digits_kernel", st, bytes);
   int rc = 0;
   switch (T.logn) {
-    case 4: rc = nd_launch<4>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
-    case 5: rc = nd_launch<5>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
-    case 6: rc = nd_launch<6>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
-    case 7: rc = nd_launch<7>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
-    case 8: rc = nd_launch<8>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
-    case 9: rc = nd_launch<9>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
-    case 10: rc = nd_launch<10>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
-    default: rc = nd_launch<11>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st); break;
+    case 4: rc = nd_launch<4>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st, narrow); break;
+    case 5: rc = nd_launch<5>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st, narrow); break;
+    case 6: rc = nd_launch<6>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st, narrow); break;
+    case 7: rc = nd_launch<7>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st, narrow); break;
+    case 8: rc = nd_launch<8>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st, narrow); break;
+    case 9: rc = nd_launch<9>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st, narrow); break;
+    case 10: rc = nd_launch<10>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st, narrow); break;
+    default: rc = nd_launch<11>(src, rows, width, parts, bw_or, rlog_out, radix_out, dc, ds, T, st, narrow); break;
   }
   salsaa_trace_end(tr, st);
   if (rc) return rc;

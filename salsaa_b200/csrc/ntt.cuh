@@ -77,8 +77,9 @@ struct NttSrcRows {
   const u64* p[16];
 };
 bool ntt_digits_ok(const u64* dc, const u64* ds, u32 rows, const NttDev& T);
+// narrow: the coefficient-form digits as centred int32 values (parts >= 2).
 int ntt_digits_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* bw_or, u64* rlog_out,
-                      u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st);
+                      u64* radix_out, u64* dc, u64* ds, const NttDev& T, cudaStream_t st, bool narrow = false);
 
 // Fused batched negacyclic product r = a * b mod (Y^n + 1), count polynomials
 // of n words each (r may alias a or b).  Needs 16 <= n <= 4096 and 16-byte

@@ -653,6 +653,13 @@ static RowSet rows_of(const u64* base, u32 rows, u64 width, u32 d) {
   for (u32 k = 0; k < rows; k++) r.p[k] = base + (u64)k * width * d;
   return r;
 }
+// The same rows stored as centred int32 values (decomposition digits).
+static RowSet rows_of_narrow(const u64* base, u32 rows, u64 width, u32 d) {
+  RowSet r{};
+  for (u32 k = 0; k < rows; k++) r.p[k] = (const u64*)((const int*)base + (u64)k * width * d);
+  r.narrow = rows >= 32 ? ~0u : ((1u << rows) - 1);
+  return r;
+}
 
 static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* proof) {
   salsaa_ctx* c = pr->ctx;
@@ -696,12 +703,13 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     if (!P.folding && parts > 1) {
       // decomp_ell (src/subroutines/decomp.rs:32-67)
       TRY(mark(pr, PH_DECOMP));
+      bool narrow = false;
       TRY(launch_decompose_ntt(Wc, K, width, d, q, parts, didx++, pr->ds, pr->Dc, pr->Ds, proof + cur, T, st,
-                               mag_ready));
+                               mag_ready, &narrow));
       mag_ready = false;
       cur += 1;
       K *= parts;
-      Wc = rows_of(pr->Dc, K, width, d);
+      Wc = narrow ? rows_of_narrow(pr->Dc, K, width, d) : rows_of(pr->Dc, K, width, d);
       Ws = rows_of(pr->Ds, K, width, d);
       // decomp rhs: derived after this round's split (see below)
       pend_off = cur;
@@ -733,10 +741,11 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
       const u64 hw = width / 2;
       for (u32 k = 0; k < K; k++) {
         Wc2.p[k] = Wc.p[k];
-        Wc2.p[K + k] = Wc.p[k] + hw * d;
+        Wc2.p[K + k] = row_advance(Wc.p[k], (Wc.narrow >> k) & 1, hw * d);
         Ws2.p[k] = Ws.p[k];
         Ws2.p[K + k] = Ws.p[k] + hw * d;
       }
+      Wc2.narrow = Wc.narrow | (Wc.narrow << K);
       K2 = 2 * K;
       width2 = hw;
     }
@@ -889,13 +898,14 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
     Ws.p[1] = pr->Ps;
     if (P.folding) {
       TRY(mark(pr, PH_DECOMP));
+      bool narrow = false;
       TRY(launch_decompose_ntt(Wc, K, width, d, q, 2, didx++, pr->ds, pr->Dc, pr->Ds, proof + cur, T, st,
-                               mag_ready));
+                               mag_ready, &narrow));
       mag_ready = false;
       cur += 1;
       K *= 2;
       Ws = rows_of(pr->Ds, K, width, d);
-      const RowSet Dcr = rows_of(pr->Dc, K, width, d);
+      const RowSet Dcr = narrow ? rows_of_narrow(pr->Dc, K, width, d) : rows_of(pr->Dc, K, width, d);
       TRY(commit_rows(pr, Ws, &Dcr, K, width, ms, 0, nsc, proof + cur));
       cur += (u64)(ms + nsc) * K * d;
       break;
