@@ -295,6 +295,19 @@ int salsaa_ntt_multi(const uint64_t* const* d_in, uint64_t* const* d_out, const 
 int salsaa_sumcheck_batch(const uint64_t* const* d_vecs, const uint64_t* lens, uint32_t count, uint64_t q,
                           uint64_t seed, uint64_t round, uint64_t* d_claims, uint64_t* d_polys, void* stream);
 
+/* The same norm-check sumcheck over the quadratic extension F_{q^2} =
+ * F_q[X]/(X^2 - s), with the QuadraticExtension product of
+ * src/quadratic_extension.rs:30-58 and s = salsaa_fq2_shift(q), the smallest
+ * quadratic non-residue mod q (so the extension is a field): challenges and
+ * folded values in F_{q^2}, inputs in F_q.  Instance i draws challenge j as
+ * two PRF words (indices 2j, 2j + 1) of the domain (6, round, i).  d_claims:
+ * count sums of squares (F_q); d_polys: per instance log2(len) x 3 extension
+ * elements (f0, f1, f2), each as (re, im) words.  One launch per round level
+ * covers every instance that still has rounds. */
+uint64_t salsaa_fq2_shift(uint64_t q);
+int salsaa_sumcheck_fq2_batch(const uint64_t* const* d_vecs, const uint64_t* lens, uint32_t count, uint64_t q,
+                              uint64_t seed, uint64_t round, uint64_t* d_claims, uint64_t* d_polys, void* stream);
+
 /* Dense ring-matrix commitment C = A * W over R_q: parallel_dot_matrix_matrix
  * (src/arithmetic.rs:429-457) in the Ajtai shape, C[j][c] = sum_i A[j][i] W[c][i].
  * The key holds A (n x m ring elements of degree d, coefficient form, given

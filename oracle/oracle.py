@@ -81,6 +81,10 @@ def lib():
         L.so_tensor.argtypes = [U64P, U64P, U64, U64]
         L.so_sumcheck.restype = ctypes.c_int
         L.so_sumcheck.argtypes = [U64P, U64, U64, U64P, U64P, U64P, U64P]
+        L.so_qnr.restype = U64
+        L.so_qnr.argtypes = [U64]
+        L.so_sumcheck_fq2.restype = ctypes.c_int
+        L.so_sumcheck_fq2.argtypes = [U64P, U64, U64, U64, U64P, U64P, U64P, U64P]
         L.so_decompose.restype = ctypes.c_int
         L.so_decompose.argtypes = [U64P, U64, U64, U64, U64, U64, U64P, U64P]
         L.so_project.restype = ctypes.c_int
@@ -277,6 +281,22 @@ def sumcheck(w, q, cs):
     polys = np.zeros((max(nr, 1), 3), dtype=np.uint64)
     assert lib().so_sumcheck(_p(w), n, q, _p(cs), ctypes.byref(claim), _p(polys), ctypes.byref(final)) == 0
     return int(claim.value), polys[:nr], int(final.value)
+
+
+def qnr(q):
+    return lib().so_qnr(q)
+
+
+def sumcheck_fq2(w, q, shift, cs):
+    """cs: log2(n) x 2 challenges (re, im) -> (claim, polys log2(n) x 3 x 2, final (re, im))."""
+    w, cs = u64(w), u64(cs)
+    n = w.size
+    nr = n.bit_length() - 1
+    claim = U64(0)
+    final = np.zeros(2, dtype=np.uint64)
+    polys = np.zeros((max(nr, 1), 3, 2), dtype=np.uint64)
+    assert lib().so_sumcheck_fq2(_p(w), n, q, shift, _p(cs), ctypes.byref(claim), _p(polys), _p(final)) == 0
+    return int(claim.value), polys[:nr], (int(final[0]), int(final[1]))
 
 
 def decompose(w, q, parts):

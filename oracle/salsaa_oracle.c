@@ -799,6 +799,71 @@ int so_sumcheck(const u64* w, u64 n, u64 q, const u64* cs, u64* claim, u64* poly
   return 0;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Norm-check sumcheck over F_{q^2} = F_q[X]/(X^2 - s), s the smallest        */
+/* quadratic non-residue mod q: the QuadraticExtension of                    */
+/* src/quadratic_extension.rs:30-58 ((a + bX)(c + dX) = ac + s bd + (ad + bc)X */
+/* ) with a non-residue shift, so the extension is a field.  Same rounds as  */
+/* sum_check (src/subroutines/fast_norm_check.rs:135-199) with the           */
+/* challenges and the folded vector in F_{q^2}: round polynomial              */
+/* (f0, f1, f2) = (sum v0^2, sum v0 (v1 - v0), sum (v1 - v0)^2), fold           */
+/* v <- v0 + c (v1 - v0).  The input vector has F_q entries.                 */
+/* ------------------------------------------------------------------------ */
+u64 so_qnr(u64 q) {
+  for (u64 s = 2; s < q; s++)
+    if (so_pow_mod(s, (q - 1) / 2, q) == q - 1) return s;
+  return 0;
+}
+static inline void qe_mul(const Mod* M, u64 s, u64 a0, u64 a1, u64 b0, u64 b1, u64* r0, u64* r1) {
+  const u64 q = M->q;
+  const u64 t0 = mod_add(mod_mul(M, a0, b0), mod_mul(M, s, mod_mul(M, a1, b1)), q);
+  const u64 t1 = mod_add(mod_mul(M, a0, b1), mod_mul(M, a1, b0), q);
+  *r0 = t0;
+  *r1 = t1;
+}
+int so_sumcheck_fq2(const u64* w, u64 n, u64 q, u64 shift, const u64* cs, u64* claim, u64* polys,
+                    u64* final_v) {
+  if (n == 0 || (n & (n - 1))) return -1;
+  Mod M = mod_make(q);
+  u64* v = (u64*)malloc(2 * n * sizeof(u64));
+  for (u64 i = 0; i < n; i++) {
+    v[2 * i] = w[i] % q;
+    v[2 * i + 1] = 0;
+  }
+  *claim = so_sum_sq(w, n, q);
+  u64 cur = n, j = 0;
+  while (cur > 1) {
+    const u64 h = cur / 2, c0 = cs[2 * j], c1 = cs[2 * j + 1];
+    u64 f[6] = {0, 0, 0, 0, 0, 0};
+    for (u64 i = 0; i < h; i++) {
+      const u64 a0 = v[2 * i], a1 = v[2 * i + 1];
+      const u64 e0 = mod_sub(v[2 * (h + i)], a0, q), e1 = mod_sub(v[2 * (h + i) + 1], a1, q);
+      u64 r0, r1;
+      qe_mul(&M, shift, a0, a1, a0, a1, &r0, &r1);
+      f[0] = mod_add(f[0], r0, q);
+      f[1] = mod_add(f[1], r1, q);
+      qe_mul(&M, shift, a0, a1, e0, e1, &r0, &r1);
+      f[2] = mod_add(f[2], r0, q);
+      f[3] = mod_add(f[3], r1, q);
+      qe_mul(&M, shift, e0, e1, e0, e1, &r0, &r1);
+      f[4] = mod_add(f[4], r0, q);
+      f[5] = mod_add(f[5], r1, q);
+      qe_mul(&M, shift, c0, c1, e0, e1, &r0, &r1);
+      v[2 * i] = mod_add(a0, r0, q);
+      v[2 * i + 1] = mod_add(a1, r1, q);
+    }
+    memcpy(polys + 6 * j, f, sizeof(f));
+    cur = h;
+    j++;
+  }
+  if (final_v) {
+    final_v[0] = v[0];
+    final_v[1] = v[1];
+  }
+  free(v);
+  return 0;
+}
+
 /* decompose_matrix_by_chunks (src/arithmetic.rs:1461-1593): centre-lift into
  * positive/negative parts, global bit width, radix 2^ceil(bw/parts), digits
  * pos_k - neg_k; new row index = row*parts + k. */

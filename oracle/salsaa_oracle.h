@@ -77,6 +77,13 @@ void so_tensor(uint64_t* out, const uint64_t* cs, uint64_t k, uint64_t q);
 /* flattened witness row -> sum of squares and sumcheck transcript. */
 int so_sumcheck(const uint64_t* w, uint64_t n, uint64_t q, const uint64_t* cs,
                 uint64_t* claim, uint64_t* polys /* log2(n) x 3 */, uint64_t* final_v);
+/* smallest quadratic non-residue mod q (the F_{q^2} shift below) */
+uint64_t so_qnr(uint64_t q);
+/* the same sumcheck over F_{q^2} = F_q[X]/(X^2 - shift): cs holds log2(n)
+ * challenges as (re, im) pairs, polys log2(n) x 3 extension elements (re, im),
+ * final_v the last folded value (re, im); the input has F_q entries. */
+int so_sumcheck_fq2(const uint64_t* w, uint64_t n, uint64_t q, uint64_t shift, const uint64_t* cs,
+                    uint64_t* claim, uint64_t* polys, uint64_t* final_v);
 /* decompose_matrix_by_chunks: rows x width x d coef -> (rows*parts) x width x d */
 int so_decompose(const uint64_t* w, uint64_t rows, uint64_t width, uint64_t d, uint64_t q,
                  uint64_t parts, uint64_t* out, uint64_t* radix);

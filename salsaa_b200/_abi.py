@@ -75,6 +75,9 @@ DEVICE_SYMBOLS = {
                                U64, INT, INT, VP]),
     "salsaa_sumcheck_batch": (INT, [ctypes.POINTER(VP), ctypes.POINTER(U64), ctypes.c_uint32, U64, U64, U64, VP,
                                     VP, VP]),
+    "salsaa_fq2_shift": (U64, [U64]),
+    "salsaa_sumcheck_fq2_batch": (INT, [ctypes.POINTER(VP), ctypes.POINTER(U64), ctypes.c_uint32, U64, U64, U64,
+                                        VP, VP, VP]),
     "salsaa_dense_key_create": (INT, [VP, U64, U64, U64, U64, VP, ctypes.POINTER(VP)]),
     "salsaa_dense_key_destroy": (None, [VP]),
     "salsaa_dense_commit": (INT, [VP, VP, U64, VP, VP, VP]),

@@ -251,6 +251,30 @@ def sum_check_batch(vecs, q, seed, round_):
     return claims, out
 
 
+
+def fq2_shift(q):
+    """The non-residue s of F_{q^2} = F_q[X]/(X^2 - s) used by sum_check_fq2_batch."""
+    return int(lib().salsaa_fq2_shift(q))
+
+
+def sum_check_fq2_batch(vecs, q, seed, round_):
+    """The sumcheck over F_{q^2} of a list of CUDA vectors (F_q entries,
+    power-of-two lengths) -> (claims[count], [polys_i of shape (log2 len_i, 3, 2)])."""
+    count = len(vecs)
+    ptrs = (ctypes.c_void_p * count)(*[v.data_ptr() for v in vecs])
+    lens = (ctypes.c_uint64 * count)(*[v.numel() for v in vecs])
+    nrs = [v.numel().bit_length() - 1 for v in vecs]
+    claims = dev_empty((count,))
+    polys = dev_empty((max(sum(nrs), 1), 3, 2))
+    _check(lib().salsaa_sumcheck_fq2_batch(ptrs, lens, count, q, seed, round_, _p(claims), _p(polys), _stream()),
+           "sumcheck_fq2_batch")
+    out, o = [], 0
+    for nr in nrs:
+        out.append(polys[o:o + nr])
+        o += nr
+    return claims, out
+
+
 class DenseKey:
     """Ajtai commitment key A (n x m ring elements, coefficient form) for
     C = A * W (parallel_dot_matrix_matrix, src/arithmetic.rs:429-457)."""

@@ -585,6 +585,176 @@ __global__ void sb_finalize_kernel(const u64* sums, const u32* nrs, const u64* o
   if (j == 0) claims[i] = add_mod(s00, s11, q);
 }
 
+// ---------------------------------------------------------------------------
+// Norm-check sumcheck over F_{q^2} = F_q[X]/(X^2 - s) (s a quadratic
+// non-residue; the QuadraticExtension product of
+// src/quadratic_extension.rs:30-58), batched over uneven instances: one
+// launch per round level covers every instance that still has rounds, each
+// thread folding pairs (v0, v1) -> v0 + c (v1 - v0) with the level's
+// challenge while it accumulates the round sums (v0^2, v0 (v1 - v0),
+// (v1 - v0)^2); warp shuffles and a shared-memory pass reduce the six words
+// per block, which are added to the instance's sums in global memory.
+// Round 0 reads the instance's F_q vector; later rounds the pairs written by
+// the previous level.  Challenge j of instance i: two PRF words of the
+// domain (6, round, i), indices 2j and 2j + 1.
+// ---------------------------------------------------------------------------
+constexpr u64 DOM_NC2 = 6;
+
+struct Fq2Level {
+  const u64* in[SB_MAX_INST];  // level input: F_q words (round 0) or (re, im) pairs
+  u64* out[SB_MAX_INST];       // folded (re, im) pairs, half the length
+  u64 half[SB_MAX_INST];       // pairs of this level
+  u64 start[SB_MAX_INST + 1];  // prefix sums of half
+  u32 id[SB_MAX_INST], j[SB_MAX_INST];
+  u32 first[SB_MAX_INST];      // 1: input is F_q words
+  u32 count;
+};
+
+__device__ __forceinline__ void qe_mul_dev(const ModQ& M, u64 s, u64 a0, u64 a1, u64 b0, u64 b1, u64& r0, u64& r1) {
+  const u64 t0 = add_mod(mul_mod(M, a0, b0), mul_mod(M, s, mul_mod(M, a1, b1)), M.q);
+  const u64 t1 = add_mod(mul_mod(M, a0, b1), mul_mod(M, a1, b0), M.q);
+  r0 = t0;
+  r1 = t1;
+}
+
+__global__ void __launch_bounds__(256) fq2_level_kernel(Fq2Level L, ModQ M, u64 shift, u64 seed, u32 round,
+                                                        u64* sums, u32 nrmax) {
+  __shared__ u64 red[6][8];
+  const u64 q = M.q;
+  const u64 total = L.start[L.count];
+  // each block works on one instance's contiguous range of pairs
+  for (u64 base = (u64)blockIdx.x * blockDim.x; base < total; base += (u64)gridDim.x * blockDim.x) {
+    u32 lo = 0, hi = L.count;  // start[lo] <= base < start[hi]
+    while (hi - lo > 1) {
+      const u32 mid = (lo + hi) / 2;
+      if (L.start[mid] <= base) lo = mid;
+      else hi = mid;
+    }
+    const u32 inst = lo;
+    const u64 h = L.half[inst];
+    const u64 key = prf_key(seed, domain_id(DOM_NC2, round, L.id[inst]));
+    const u64 c0 = uni_mod(prf_at(key, 2 * (u64)L.j[inst]), q), c1 = uni_mod(prf_at(key, 2 * (u64)L.j[inst] + 1), q);
+    const u64 i = base - L.start[inst] + threadIdx.x;
+    u64 f[6] = {0, 0, 0, 0, 0, 0};
+    // the block's threads past its instance's end (a block never spans two
+    // instances: start[] is a multiple of the block size) add nothing
+    if (base - L.start[inst] + threadIdx.x < h) {
+      u64 a0, a1, b0, b1;
+      if (L.first[inst]) {
+        a0 = L.in[inst][i] % q;
+        a1 = 0;
+        b0 = L.in[inst][h + i] % q;
+        b1 = 0;
+      } else {
+        a0 = L.in[inst][2 * i];
+        a1 = L.in[inst][2 * i + 1];
+        b0 = L.in[inst][2 * (h + i)];
+        b1 = L.in[inst][2 * (h + i) + 1];
+      }
+      const u64 e0 = sub_mod(b0, a0, q), e1 = sub_mod(b1, a1, q);
+      qe_mul_dev(M, shift, a0, a1, a0, a1, f[0], f[1]);
+      qe_mul_dev(M, shift, a0, a1, e0, e1, f[2], f[3]);
+      qe_mul_dev(M, shift, e0, e1, e0, e1, f[4], f[5]);
+      u64 r0, r1;
+      qe_mul_dev(M, shift, c0, c1, e0, e1, r0, r1);
+      L.out[inst][2 * i] = add_mod(a0, r0, q);
+      L.out[inst][2 * i + 1] = add_mod(a1, r1, q);
+    }
+#pragma unroll
+    for (u32 t = 0; t < 6; t++)
+      for (int o = 16; o > 0; o >>= 1) f[t] = add_mod(f[t], __shfl_xor_sync(0xffffffffu, f[t], o), q);
+    const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+      for (u32 t = 0; t < 6; t++) red[t][warp] = f[t];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      u64 acc = 0;
+      for (u32 w = 0; w < blockDim.x / 32; w++) acc = add_mod(acc, red[threadIdx.x][w], q);
+      if (acc) atomic_add_mod(&sums[((u64)L.id[inst] * nrmax + L.j[inst]) * 6 + threadIdx.x], acc, q, false);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void fq2_claims_kernel(const u64* sums, u32 count, u32 nrmax, u64 q, u64* claims) {
+  const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const u64* f = sums + (u64)i * nrmax * 6;  // round 0: real parts f0, f1, f2 at 0, 2, 4
+  u64 c = add_mod(f[0], f[0], q);
+  c = add_mod(c, add_mod(f[2], f[2], q), q);
+  claims[i] = add_mod(c, f[4], q);
+}
+
+int launch_sumcheck_fq2_batch(const u64* const* vecs, const u64* lens, u32 count, const ModQ& M, u64 shift,
+                              u64 seed, u32 round, u64* claims, u64* polys, u64* scratch, cudaStream_t st) {
+  if (count == 0 || count > SB_MAX_INST) return salsaa_set_error(-2, "sumcheck_fq2: 1..64 instances");
+  u32 nrmax = 0;
+  u64 scr = 0;
+  for (u32 i = 0; i < count; i++) {
+    if (lens[i] < 2 || (lens[i] & (lens[i] - 1)) || lens[i] > (1ULL << 30) || !vecs[i])
+      return salsaa_set_error(-2, "sumcheck_fq2: lengths must be powers of two in 2..2^30");
+    const u32 nr = 63u - (u32)__builtin_clzll(lens[i]);
+    if (nr > nrmax) nrmax = nr;
+    scr += lens[i];  // ping (n/2 pairs) + pong (n/4 pairs): n + n/2 words <= 2n
+  }
+  (void)scr;
+  // sums[(i, j)] : 6 words each, zeroed; polys are written per instance at the end
+  u64* sums = scratch;
+  cudaError_t e = cudaMemsetAsync(sums, 0, (u64)count * nrmax * 6 * sizeof(u64), st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sumcheck_fq2: memset");
+  u64* pool = sums + (u64)count * nrmax * 6;
+  // per instance: buffer A (len pairs / 2 = len words) and buffer B (len / 2 words)
+  std::vector<u64*> bufA(count), bufB(count);
+  {
+    u64 off = 0;
+    for (u32 i = 0; i < count; i++) {
+      bufA[i] = pool + off;
+      off += lens[i];
+      bufB[i] = pool + off;
+      off += lens[i] / 2;
+    }
+  }
+  const u32 BS = 256;
+  for (u32 j = 0; j < nrmax; j++) {
+    Fq2Level L{};
+    u64 start = 0;
+    u32 k = 0;
+    for (u32 i = 0; i < count; i++) {
+      const u32 nr = 63u - (u32)__builtin_clzll(lens[i]);
+      if (j >= nr) continue;
+      const u64 half = lens[i] >> (j + 1);
+      L.in[k] = j == 0 ? vecs[i] : ((j & 1) ? bufA[i] : bufB[i]);
+      L.out[k] = (j & 1) ? bufB[i] : bufA[i];
+      L.half[k] = half;
+      L.start[k] = start;
+      L.id[k] = i;
+      L.j[k] = j;
+      L.first[k] = j == 0;
+      start += (half + BS - 1) / BS * BS;  // block-aligned ranges
+      k++;
+    }
+    L.start[k] = start;
+    L.count = k;
+    u64 blocks = start / BS;
+    if (blocks > 148ULL * 16) blocks = 148ULL * 16;
+    fq2_level_kernel<<<(unsigned)blocks, BS, 0, st>>>(L, M, shift, seed, round, sums, nrmax);
+    int rc = check_launch("sumcheck_fq2 level");
+    if (rc) return rc;
+  }
+  // claims (2 f0 + 2 f1 + f2 of round 0, real) and the polynomials in order
+  u64 po = 0;
+  for (u32 i = 0; i < count; i++) {
+    const u32 nr = 63u - (u32)__builtin_clzll(lens[i]);
+    e = cudaMemcpyAsync(polys + po, sums + (u64)i * nrmax * 6, (u64)nr * 6 * sizeof(u64), cudaMemcpyDeviceToDevice,
+                        st);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "sumcheck_fq2: polys");
+    po += (u64)nr * 6;
+  }
+  fq2_claims_kernel<<<(count + 63) / 64, 64, 0, st>>>(sums, count, nrmax, M.q, claims);
+  return check_launch("sumcheck_fq2 claims");
+}
+
 int launch_sumcheck_batch(const u64* const* vecs, const u64* lens, u32 count, const ModQ& M, u64 seed, u32 round,
                           u64* claims, u64* polys, cudaStream_t st) {
   if (count == 0) return 0;

@@ -123,6 +123,11 @@ int launch_sumcheck(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, const De
 // Independent sumchecks of `count` <= 64 vectors of power-of-two lengths (one
 // repetition each; instance i uses the norm-check challenges of (round, i)):
 // claims[i] and the round polynomials of instance i at polys + 3 * sum_{i'<i} log2 len.
+// The sumcheck over F_{q^2} = F_q[X]/(X^2 - shift) for count <= 64 vectors of
+// uneven power-of-two lengths; scratch holds count * max_rounds * 6 +
+// 1.5 * sum(lens) words.  polys: per instance log2(len) x 3 x (re, im).
+int launch_sumcheck_fq2_batch(const u64* const* vecs, const u64* lens, u32 count, const ModQ& M, u64 shift,
+                              u64 seed, u32 round, u64* claims, u64* polys, u64* scratch, cudaStream_t st);
 int launch_sumcheck_batch(const u64* const* vecs, const u64* lens, u32 count, const ModQ& M, u64 seed, u32 round,
                           u64* claims, u64* polys, cudaStream_t st);
 // norm_check_3 outputs: rhs (coef, into proof) and each repetition's ring base (slot).

@@ -1495,6 +1495,37 @@ extern "C" int salsaa_poly_mul(const uint64_t* d_a, const uint64_t* d_b, uint64_
   return ntt_launch(d_r, d_r, count, *T, false, true, st);
 }
 
+extern "C" uint64_t salsaa_fq2_shift(uint64_t q) {
+  if (q < 3 || q >= (1ULL << 62) || !(q & 1)) return 0;
+  for (u64 s = 2; s < q && s < (1ULL << 20); s++)
+    if (host::powmod(s, (q - 1) / 2, q) == q - 1) return s;
+  return 0;
+}
+
+extern "C" int salsaa_sumcheck_fq2_batch(const uint64_t* const* d_vecs, const uint64_t* lens, uint32_t count,
+                                         uint64_t q, uint64_t seed, uint64_t round, uint64_t* d_claims,
+                                         uint64_t* d_polys, void* stream) {
+  if (!d_vecs || !lens || !d_claims || !d_polys) return salsaa_set_error(-1, "sumcheck_fq2: null argument");
+  if (q < 3 || q >= (1ULL << 62)) return salsaa_set_error(-1, "sumcheck_fq2: modulus must be in [3, 2^62)");
+  const u64 shift = salsaa_fq2_shift(q);
+  if (!shift) return salsaa_set_error(-1, "sumcheck_fq2: no quadratic non-residue found");
+  if (count == 0 || count > 64) return salsaa_set_error(-2, "sumcheck_fq2: 1..64 instances");
+  u64 words = 0, nrmax = 0;
+  for (u32 i = 0; i < count; i++) {
+    if (lens[i] < 2 || (lens[i] & (lens[i] - 1)) || lens[i] > (1ULL << 30))
+      return salsaa_set_error(-2, "sumcheck_fq2: lengths must be powers of two in 2..2^30");
+    words += lens[i] + lens[i] / 2;
+    const u64 nr = ilog2u(lens[i]);
+    if (nr > nrmax) nrmax = nr;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  Tmp t(st);
+  u64* scratch;
+  TRY(t.get(&scratch, words + (u64)count * nrmax * 6));
+  return launch_sumcheck_fq2_batch(d_vecs, lens, count, make_modq(q), shift, seed, (u32)round, d_claims, d_polys,
+                                   scratch, st);
+}
+
 extern "C" int salsaa_sumcheck_batch(const uint64_t* const* d_vecs, const uint64_t* lens, uint32_t count, uint64_t q,
                                      uint64_t seed, uint64_t round, uint64_t* d_claims, uint64_t* d_polys,
                                      void* stream) {

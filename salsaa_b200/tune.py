@@ -7,10 +7,12 @@ same with FP64 butterflies (for the protocol's primes below 2^50), or
 persistent CTAs that stage tiles through shared memory with bulk copies 2, 3
 or 4 tiles ahead, optionally capped at one CTA per SM.  Which is fastest
 depends on the transform size, the direction, the modulus width and the batch
-size, so this script times every candidate on the GPU for each key (log2 n, incomplete, inverse, q >= 2^50, large batch),
-checks that each candidate's output equals the default schedule's bit for bit,
-and writes the winners to a table the library loads at its first transform
-(tune_table.txt beside the library, or $SALSAA_TUNE_FILE).
+size, so this script times every candidate on the GPU for each key (log2 n,
+incomplete, inverse, q >= 2^50, large batch), checks that each candidate's
+output equals the default schedule's bit for bit, and writes the winners to a
+table the library loads at its first transform (tune_table.txt beside the
+library, or $SALSAA_TUNE_FILE).  It also times the fold with integer and with
+FP64 products.
 
 Usage: python -m salsaa_b200.tune [--out PATH] [--reps K] [--quick]
 """

@@ -97,7 +97,8 @@ def test_ntt_multi_uneven(api, oracle, cuda, n_arg, incomplete, q):
     xs = [rand_mod(rng, (c, n_arg), q) for c in counts]
     dev = [api.to_dev(x) for x in xs]
     fwd = api.ntt_multi(dev, n_arg, q, incomplete=incomplete, outs=[api.dev_empty(d.shape) for d in dev])
-    single = [api.ntt(d, n_arg, q, incomplete=incomplete, out=api.dev_empty(d.shape)) for d in dev]
+    single = [api.ntt(d, n_arg, q, incomplete=incomplete, out=api.dev_empty(d.shape)) if d.numel() else d
+              for d in dev]
     back = api.ntt_multi([f.clone() for f in fwd], n_arg, q, inverse=True, incomplete=incomplete)  # in place
     torch.cuda.synchronize()
     for i, c in enumerate(counts):
@@ -141,3 +142,49 @@ def test_commit_multi_rejects(api):
     with pytest.raises(SalsaaError):  # width below one 128-element chunk
         ctx.parallel_dot_series_matrix_multi([api.to_dev(np.zeros((1, 64, 128), dtype=np.uint64))])
     ctx.close()
+
+
+def _fq2_challenges(seed, rnd, inst, nr, q):
+    from helpers import domain, prf_np
+    r = prf_np(seed, domain(6, rnd, inst), np.arange(2 * nr, dtype=np.uint64))
+    return np.array([(int(x) * q) >> 64 for x in r], dtype=np.uint64).reshape(nr, 2)
+
+
+@pytest.mark.parametrize("q", [P.Q0, P.Q62])
+def test_sumcheck_fq2_batch(api, oracle, q):
+    """The F_{q^2} norm-check sumcheck of uneven instances (one launch per
+    round level) equals the oracle's restatement, every round polynomial."""
+    rng = np.random.default_rng(23)
+    logs = [1, 5, 10, 12, 13, 9, 16]
+    vecs = [small_signed(rng, 1 << k, 1, q) for k in logs]
+    shift = api.fq2_shift(q)
+    assert shift == oracle.qnr(q)
+    claims, polys = api.sum_check_fq2_batch([api.to_dev(v) for v in vecs], q, 31, 2)
+    claims = api.to_host(claims)
+    for i, v in enumerate(vecs):
+        nr = v.size.bit_length() - 1
+        cs = _fq2_challenges(31, 2, i, nr, q)
+        claim, want, _ = oracle.sumcheck_fq2(v, q, shift, cs)
+        assert int(claims[i]) == claim, i
+        assert np.array_equal(api.to_host(polys[i]), want), i
+
+
+@pytest.mark.slow
+def test_sumcheck_fq2_bench_instances(api, oracle, cuda):
+    """The microbench's batch (64 ternary instances, 2^16..2^22) over F_{q^2}."""
+    torch = cuda
+    q = P.Q0
+    rng = np.random.default_rng(2024)
+    logs = np.sort(rng.integers(16, 23, size=64))
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(5)
+    dev = [torch.randint(-1, 2, (1 << int(k),), dtype=torch.int64, device="cuda", generator=gen) % q for k in logs]
+    shift = api.fq2_shift(q)
+    claims, polys = api.sum_check_fq2_batch(dev, q, 1, 0)
+    claims = api.to_host(claims)
+    for i in (0, 31, 63):
+        v = api.to_host(dev[i])
+        cs = _fq2_challenges(1, 0, i, v.size.bit_length() - 1, q)
+        claim, want, _ = oracle.sumcheck_fq2(v, q, shift, cs)
+        assert int(claims[i]) == claim
+        assert np.array_equal(api.to_host(polys[i]), want)

@@ -255,3 +255,41 @@ def test_dense_commit_matches_ring_products(oracle):
                 pr = oracle.ring_mul(A[j, i], W[c, i], q)
                 acc = [(x + int(y)) % q for x, y in zip(acc, pr)]
             assert [int(v) for v in C[j, c]] == acc
+
+
+def _qe(O, a, b, s, q):
+    return _quad_mul(O, a, b, s, q)
+
+
+@pytest.mark.parametrize("q", [P.Q0, 1000003])
+def test_sumcheck_fq2_verifier_identities(oracle, q):
+    """The F_{q^2} sumcheck restatement satisfies the verifier's round checks
+    (verify_norm_check_2, src/subroutines/fast_norm_check.rs:352-399, with
+    values in the extension): g(0) + g(1) = 2 f0 + 2 f1 + f2 equals the running
+    claim, which becomes f0 + 2 f1 c + f2 c^2, and ends at the square of the
+    last folded value; with real challenges it equals the F_q sumcheck."""
+    O = oracle
+    s = O.qnr(q)
+    assert O.pow_mod(s, (q - 1) // 2, q) == q - 1
+    rng = np.random.default_rng(3)
+    w = small_signed(rng, 1 << 9, 1, q)
+    nr = 9
+    cs = rand_mod(rng, (nr, 2), q)
+    claim, polys, final = O.sumcheck_fq2(w, q, s, cs)
+    cur = [claim, 0]
+    for j in range(nr):
+        f0, f1, f2 = ([int(x) for x in polys[j, t]] for t in range(3))
+        tot = [(2 * f0[k] + 2 * f1[k] + f2[k]) % q for k in range(2)]
+        assert tot == cur, j
+        c = [int(cs[j, 0]), int(cs[j, 1])]
+        c2 = _qe(O, c, c, s, q)
+        t1 = _qe(O, f1, c, s, q)
+        t2 = _qe(O, f2, c2, s, q)
+        cur = [(f0[k] + 2 * t1[k] + t2[k]) % q for k in range(2)]
+    assert cur == _qe(O, list(final), list(final), s, q)
+    # real challenges: the F_q sumcheck
+    cr = np.stack([cs[:, 0], np.zeros(nr, dtype=np.uint64)], axis=1)
+    claim2, polys2, _ = O.sumcheck_fq2(w, q, s, cr)
+    c1, p1, _ = O.sumcheck(w, q, cs[:, 0])
+    assert claim2 == c1
+    assert np.array_equal(polys2[:, :, 0], p1) and not polys2[:, :, 1].any()
