@@ -237,10 +237,11 @@ void salsaa_server_destroy(salsaa_server* s);
 /* ---- kernel schedules chosen by the autotuner ---- */
 /* No reference counterpart (the reference's HEXL NTT has a fixed schedule).
  * The register-path NTT (16 <= n <= 4096, 16-byte aligned buffers) runs one
- * of: variant 0 = one 4096-coefficient tile per CTA; variant 2, 3 or 4 =
- * persistent CTAs that stage their tiles with bulk copies (cp.async.bulk)
- * that many tiles ahead; ctas_per_sm caps the resident CTAs per SM (0 = as
- * many as fit).  The choice is kept per (log2 n, incomplete, inverse,
+ * of: variant 0 = one 4096-coefficient tile per CTA; 1 = the same with FP64
+ * butterflies (q < 2^50); variant 2, 3 or 4 = persistent CTAs that stage their
+ * tiles with bulk copies (cp.async.bulk) that many tiles ahead; 5, 6, 7 = the
+ * same with FP64 butterflies (q < 2^50); ctas_per_sm caps the resident CTAs
+ * per SM (0 = as many as fit).  The choice is kept per (log2 n, incomplete, inverse,
  * wide_modulus = q >= 2^50, large = at least 2^22 coefficients in the call);
  * every variant gives the same outputs.  Untuned default: variant 0.
  * salsaa_b200/tune.py times the candidates on the GPU and writes a table file

@@ -201,7 +201,8 @@ __global__ void __launch_bounds__(256) ntt_kernel(const u64* in, u64* out, u64 c
 // one 4096-coefficient tile per CTA with integer butterflies
 // (ntt_reg_kernel), 1 = the same with FP64 butterflies (ntt_fp_kernel; used
 // only when q < 2^50, and also selecting the digit transform's arithmetic),
-// 2..4 = persistent CTAs with that many bulk-copy stages (ntt_pipe_kernel);
+// 2..4 = persistent CTAs with that many bulk-copy stages (ntt_pipe_kernel),
+// 5..7 = the same with FP64 butterflies (q < 2^50; else as 2..4);
 // ctas_per_sm caps the resident CTAs per SM (0 = as many as fit).  The
 // defaults are variant 0; a table written by the tuner (salsaa_b200/tune.py)
 // replaces them: "ntt <log_n> <incomplete> <inverse> <wide> <large> <variant>
@@ -234,7 +235,7 @@ int tune_load_locked(const char* path) {
     unsigned lg, inc, inv, wide, big, var, cps;
     if (sscanf(line, "ntt %u %u %u %u %u %u %u", &lg, &inc, &inv, &wide, &big, &var, &cps) != 7) continue;
     if (lg >= (unsigned)TUNE_LOGN || inc > 1 || inv > 1 || wide > 1 || big > 1 ||
-        var > 4 || cps > 8)
+        var > 7 || cps > 8)
       continue;
     g_tune[lg][inc][inv][wide][big] = NttChoice{(uint8_t)var, (uint8_t)cps};
     n++;
@@ -269,8 +270,8 @@ NttChoice ntt_choice(u32 logn, bool incomplete, bool inverse, bool wide, bool la
 }
 
 int ntt_tune_set(u32 logn, bool incomplete, bool inverse, bool wide, bool large, int variant, int ctas_per_sm) {
-  if (!tune_index_ok(logn) || variant < 0 || variant > 4 || ctas_per_sm < 0 || ctas_per_sm > 8)
-    return salsaa_set_error(-2, "ntt_tune_set: log_n < 14, variant 0..4, ctas_per_sm 0..8");
+  if (!tune_index_ok(logn) || variant < 0 || variant > 7 || ctas_per_sm < 0 || ctas_per_sm > 8)
+    return salsaa_set_error(-2, "ntt_tune_set: log_n < 14, variant 0..7, ctas_per_sm 0..8");
   std::lock_guard<std::mutex> lk(g_tune_mu);
   tune_default_locked();
   g_tune[logn][incomplete][inverse][wide][large] = NttChoice{(uint8_t)variant, (uint8_t)ctas_per_sm};
@@ -625,97 +626,6 @@ __device__ __forceinline__ void nr_load_stage(u64 (&x)[16], const u64* stg, u32 
 
 constexpr u32 NP_ERR_WAIT = 0x4e54u;  // "NT": a stage's bulk copy did not complete in time
 
-template <int LOGN, bool INC, bool INV, bool RELAX, int STAGES>
-__global__ void __launch_bounds__(256) ntt_pipe_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
-  constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
-  constexpr int NPH = ph_count(LOGN);
-  static_assert(!INC || UPT % 2 == 0, "incomplete mode keeps both halves of an element in one tile");
-  extern __shared__ __align__(128) unsigned char np_smem[];
-  uint64_t* bar = (uint64_t*)np_smem;                                // STAGES mbarriers
-  u64* stg = (u64*)(np_smem + 128);                                  // STAGES x NR_TILE words
-  u64* sm = stg + (size_t)STAGES * NR_TILE;                          // padded exchange tile
-  u32 unit, tu;
-  nr_map<LOGN, INC>(threadIdx.x, unit, tu);
-  const u64 q = T.q, q2 = 2 * T.q;
-  const u64 ntiles = (units + UPT - 1) / UPT;
-  const u64 t0 = blockIdx.x, tstep = gridDim.x;
-  // bytes of tile t (a partial last tile holds whole units)
-  auto tile_bytes = [&](u64 t) -> u32 {
-    const u64 left = units - t * UPT;
-    return (u32)((left < UPT ? left : UPT) * N * sizeof(u64));
-  };
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; s++) umma::mbar_init(&bar[s], 1);
-    umma::mbar_fence_init();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; s++) {
-      const u64 t = t0 + (u64)s * tstep;
-      if (t >= ntiles) break;
-      const u32 b = tile_bytes(t);
-      umma::mbar_expect_tx(&bar[s], b);
-      umma::bulk_g2s(stg + (size_t)s * NR_TILE, in + t * NR_TILE, b, &bar[s]);
-    }
-  }
-  u64 mag = 0;
-  u64 i = 0;
-  for (u64 t = t0; t < ntiles; t += tstep, i++) {
-    const int s = (int)(i % STAGES);
-    const u32 par = (u32)((i / STAGES) & 1);
-    const bool ok = umma::mbar_wait(&bar[s], par, nullptr, 0);
-    if (__syncthreads_or(!ok)) {
-      // give up: record it, let the copies issued for later tiles land, stop
-      if (threadIdx.x == 0) {
-        atomicMax(&g_ntt_error, NP_ERR_WAIT);
-        for (u64 j = 0; j < (u64)STAGES && t + j * tstep < ntiles; j++) {
-          const int sj = (int)((i + j) % STAGES);
-          umma::mbar_wait(&bar[sj], (u32)(((i + j) / STAGES) & 1), nullptr, 0);
-        }
-      }
-      break;
-    }
-    const u64 ug = t * UPT + unit;
-    const bool active = ug < units;
-    u64 x[16];
-    if (active) {
-      nr_load_stage<LOGN, INC, INV>(x, stg + (size_t)s * NR_TILE, unit, tu);
-      if (!INV && mag_or)
-#pragma unroll
-        for (u32 k = 0; k < 16; k++) mag |= nr_mag(x[k], q);
-      nr_compute<LOGN, 0, INV, RELAX>(x, tu, T, q, q2);
-    }
-    // Stage s is refilled with the tile STAGES ahead only after every thread
-    // has consumed its values (the butterflies above use them) and ordered its
-    // generic-proxy reads before the bulk copy's async-proxy writes.
-    umma::fence_proxy_async();
-    if constexpr (NPH > 1)
-      if (active) nr_store_smem<LOGN, 0, INV>(x, sm, unit, tu);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const u64 tn = t + (u64)STAGES * tstep;
-      if (tn < ntiles) {
-        const u32 b = tile_bytes(tn);
-        umma::mbar_expect_tx(&bar[s], b);
-        umma::bulk_g2s(stg + (size_t)s * NR_TILE, in + tn * NR_TILE, b, &bar[s]);
-      }
-    }
-    if constexpr (NPH > 1) {
-      nr_mid<LOGN, 1, NPH - 1, INV, RELAX>(x, sm, unit, tu, active, T, q, q2);
-      if (active) {
-        nr_load_smem<LOGN, NPH - 1, INV>(x, sm, unit, tu);
-        nr_compute<LOGN, NPH - 1, INV, RELAX>(x, tu, T, q, q2);
-      }
-    }
-    if (active) nr_store_global<LOGN, INC, INV, RELAX>(x, out, ug, tu, T, q, q2, INV && mag_or ? &mag : nullptr);
-  }
-  if (mag_or) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
-    if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
-  }
-}
-
 // ---------------------------------------------------------------------------
 // FP64 butterflies for q < 2^50 (the protocol's primes).  On B200 the FP64
 // pipe multiplies and adds 53-bit integers exactly at a far higher rate than
@@ -882,6 +792,119 @@ template <int LOGN, bool INC, bool INV>
 __global__ void __launch_bounds__(256) ntt_fp_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
   __shared__ double sm[NR_TILE + NR_TILE / 16];
   nf_tile<LOGN, INC, INV>(in, out, units, blockIdx.x, T, mag_or, sm);
+}
+
+// FP: FP64 butterflies (q < 2^50, the nf_* code), else the integer ones.
+template <int LOGN, bool INC, bool INV, bool RELAX, int STAGES, bool FP>
+__global__ void __launch_bounds__(256) ntt_pipe_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
+  using Wd = typename std::conditional<FP, double, u64>::type;
+  constexpr u32 N = 1u << LOGN, UPT = NR_TILE / N;
+  constexpr int NPH = ph_count(LOGN);
+  static_assert(!INC || UPT % 2 == 0, "incomplete mode keeps both halves of an element in one tile");
+  extern __shared__ __align__(128) unsigned char np_smem[];
+  uint64_t* bar = (uint64_t*)np_smem;                                // STAGES mbarriers
+  u64* stg = (u64*)(np_smem + 128);                                  // STAGES x NR_TILE words
+  Wd* sm = (Wd*)(stg + (size_t)STAGES * NR_TILE);                    // padded exchange tile
+  u32 unit, tu;
+  nr_map<LOGN, INC>(threadIdx.x, unit, tu);
+  const u64 q = T.q, q2 = 2 * T.q;
+  const u64 ntiles = (units + UPT - 1) / UPT;
+  const u64 t0 = blockIdx.x, tstep = gridDim.x;
+  // bytes of tile t (a partial last tile holds whole units)
+  auto tile_bytes = [&](u64 t) -> u32 {
+    const u64 left = units - t * UPT;
+    return (u32)((left < UPT ? left : UPT) * N * sizeof(u64));
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) umma::mbar_init(&bar[s], 1);
+    umma::mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      const u64 t = t0 + (u64)s * tstep;
+      if (t >= ntiles) break;
+      const u32 b = tile_bytes(t);
+      umma::mbar_expect_tx(&bar[s], b);
+      umma::bulk_g2s(stg + (size_t)s * NR_TILE, in + t * NR_TILE, b, &bar[s]);
+    }
+  }
+  u64 mag = 0;
+  u64 i = 0;
+  for (u64 t = t0; t < ntiles; t += tstep, i++) {
+    const int s = (int)(i % STAGES);
+    const u32 par = (u32)((i / STAGES) & 1);
+    const bool ok = umma::mbar_wait(&bar[s], par, nullptr, 0);
+    if (__syncthreads_or(!ok)) {
+      // give up: record it, let the copies issued for later tiles land, stop
+      if (threadIdx.x == 0) {
+        atomicMax(&g_ntt_error, NP_ERR_WAIT);
+        for (u64 j = 0; j < (u64)STAGES && t + j * tstep < ntiles; j++) {
+          const int sj = (int)((i + j) % STAGES);
+          umma::mbar_wait(&bar[sj], (u32)(((i + j) / STAGES) & 1), nullptr, 0);
+        }
+      }
+      break;
+    }
+    const u64 ug = t * UPT + unit;
+    const bool active = ug < units;
+    Wd x[16];
+    if (active) {
+      u64 wv[16];
+      nr_load_stage<LOGN, INC, INV>(wv, stg + (size_t)s * NR_TILE, unit, tu);
+      if (!INV && mag_or)
+#pragma unroll
+        for (u32 k = 0; k < 16; k++) mag |= nr_mag(wv[k], q);
+      if constexpr (FP) {
+#pragma unroll
+        for (u32 k = 0; k < 16; k++) x[k] = fp_from_word(wv[k]);
+        nf_compute<LOGN, 0, INV>(x, tu, T);
+      } else {
+#pragma unroll
+        for (u32 k = 0; k < 16; k++) x[k] = wv[k];
+        nr_compute<LOGN, 0, INV, RELAX>(x, tu, T, q, q2);
+      }
+    }
+    // Stage s is refilled with the tile STAGES ahead only after every thread
+    // has consumed its values (the butterflies above use them) and ordered its
+    // generic-proxy reads before the bulk copy's async-proxy writes.
+    umma::fence_proxy_async();
+    if constexpr (NPH > 1)
+      if (active) nr_store_smem<LOGN, 0, INV>(x, sm, unit, tu);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const u64 tn = t + (u64)STAGES * tstep;
+      if (tn < ntiles) {
+        const u32 b = tile_bytes(tn);
+        umma::mbar_expect_tx(&bar[s], b);
+        umma::bulk_g2s(stg + (size_t)s * NR_TILE, in + tn * NR_TILE, b, &bar[s]);
+      }
+    }
+    if constexpr (NPH > 1) {
+      if constexpr (FP)
+        nf_mid<LOGN, 1, NPH - 1, INV>(x, sm, unit, tu, active, T);
+      else
+        nr_mid<LOGN, 1, NPH - 1, INV, RELAX>(x, sm, unit, tu, active, T, q, q2);
+      if (active) {
+        nr_load_smem<LOGN, NPH - 1, INV>(x, sm, unit, tu);
+        if constexpr (FP)
+          nf_compute<LOGN, NPH - 1, INV>(x, tu, T);
+        else
+          nr_compute<LOGN, NPH - 1, INV, RELAX>(x, tu, T, q, q2);
+      }
+    }
+    if (active) {
+      if constexpr (FP)
+        nf_store_global<LOGN, INC, INV>(x, out, ug, tu, T, INV && mag_or ? &mag : nullptr);
+      else
+        nr_store_global<LOGN, INC, INV, RELAX>(x, out, ug, tu, T, q, q2, INV && mag_or ? &mag : nullptr);
+    }
+  }
+  if (mag_or) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
+    if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1103,10 +1126,10 @@ int nm_launch(const u64* a, const u64* b, u64* r, u64 count, const NttDev& T, cu
 
 // Persistent bulk-copy pipeline: grid = min(tiles, SMs x resident CTAs),
 // capped at ctas_per_sm CTAs per SM when that is > 0.
-template <int LOGN, bool INC, bool INV, bool RELAX, int STAGES>
+template <int LOGN, bool INC, bool INV, bool RELAX, int STAGES, bool FP>
 int np_go(const u64* in, u64* out, u64 units, const NttDev& T, cudaStream_t st, u64* mag_or, int ctas_per_sm) {
   constexpr u32 UPT = NR_TILE >> LOGN;
-  auto kern = ntt_pipe_kernel<LOGN, INC, INV, RELAX, STAGES>;
+  auto kern = ntt_pipe_kernel<LOGN, INC, INV, RELAX, STAGES, FP>;
   const size_t smem = 128 + ((size_t)STAGES * NR_TILE + NR_TILE + NR_TILE / 16) * sizeof(u64);
   static int resident_dev[64][2] = {};  // per instantiation and device: attribute set, resident CTAs per SM
   static std::mutex mu;
@@ -1135,13 +1158,23 @@ int np_go(const u64* in, u64* out, u64 units, const NttDev& T, cudaStream_t st, 
   return 0;
 }
 
+// variant 2..4: integer butterflies with that many stages; 5..7: FP64 ones
+// (q < 2^50 only) with 2..4 stages.
 template <int LOGN, bool INC, bool INV, bool RELAX>
-int np_launch(const u64* in, u64* out, u64 units, const NttDev& T, cudaStream_t st, u64* mag_or, int stages,
+int np_launch(const u64* in, u64* out, u64 units, const NttDev& T, cudaStream_t st, u64* mag_or, int variant,
               int ctas_per_sm) {
-  switch (stages) {
-    case 2: return np_go<LOGN, INC, INV, RELAX, 2>(in, out, units, T, st, mag_or, ctas_per_sm);
-    case 3: return np_go<LOGN, INC, INV, RELAX, 3>(in, out, units, T, st, mag_or, ctas_per_sm);
-    default: return np_go<LOGN, INC, INV, RELAX, 4>(in, out, units, T, st, mag_or, ctas_per_sm);
+  if constexpr (RELAX) {
+    switch (variant) {
+      case 5: return np_go<LOGN, INC, INV, RELAX, 2, true>(in, out, units, T, st, mag_or, ctas_per_sm);
+      case 6: return np_go<LOGN, INC, INV, RELAX, 3, true>(in, out, units, T, st, mag_or, ctas_per_sm);
+      case 7: return np_go<LOGN, INC, INV, RELAX, 4, true>(in, out, units, T, st, mag_or, ctas_per_sm);
+      default: break;
+    }
+  }
+  switch (variant) {
+    case 2: return np_go<LOGN, INC, INV, RELAX, 2, false>(in, out, units, T, st, mag_or, ctas_per_sm);
+    case 3: return np_go<LOGN, INC, INV, RELAX, 3, false>(in, out, units, T, st, mag_or, ctas_per_sm);
+    default: return np_go<LOGN, INC, INV, RELAX, 4, false>(in, out, units, T, st, mag_or, ctas_per_sm);
   }
 }
 
@@ -1206,7 +1239,7 @@ template <int LOGN>
 int nm_multi_go(const NttMulti& m, u64 blocks, const NttDev& T, bool incomplete, bool inverse, cudaStream_t st,
                 bool large) {
   const bool relax = T.q < NR_RELAX_Q;
-  const bool fp = relax && ntt_choice(LOGN, incomplete, inverse, false, large).variant == 1;
+  const bool fp = relax && ntt_choice(LOGN, incomplete, inverse, false, large).fp64();
   auto go = [&](auto kern) -> int {
     kern<<<(unsigned)blocks, 256, 0, st>>>(m, T);
     return 0;
@@ -1342,7 +1375,7 @@ int nd_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* 
   if (blocks > 0x7fffffffULL) return salsaa_set_error(-2, "ntt_digits: batch too large");
   // the forward incomplete transform's schedule decides the arithmetic
   const bool relax = T.q < NR_RELAX_Q;
-  const bool fp = relax && ntt_choice(LOGN, true, false, false, units * (1ULL << LOGN) >= NTT_LARGE_COEFFS).variant == 1;
+  const bool fp = relax && ntt_choice(LOGN, true, false, false, units * (1ULL << LOGN) >= NTT_LARGE_COEFFS).fp64();
   if (fp)
     ntt_digits_kernel<LOGN, true, true><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
                                                                            radix_out, dc, ds, units, T, narrow);

@@ -41,6 +41,8 @@ const NttDev* ntt_tables(u32 n, u64 q);
 // ctas_per_sm caps resident CTAs per SM (0 = no cap).
 struct NttChoice {
   uint8_t variant, ctas_per_sm;
+  // the schedule's arithmetic: FP64 butterflies (variants 1 and 5..7)
+  __host__ __device__ bool fp64() const { return variant == 1 || variant >= 5; }
 };
 constexpr u64 NTT_LARGE_COEFFS = 1ULL << 22;  // batch class "large": at least this many coefficients per launch
 NttChoice ntt_choice(u32 logn, bool incomplete, bool inverse, bool wide, bool large);

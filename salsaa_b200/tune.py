@@ -29,8 +29,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_TABLE = os.path.join(HERE, "tune_table.txt")
 
 # (variant, ctas_per_sm): 0 = one tile per CTA, integer butterflies; 1 = the
-# same with FP64 butterflies (q < 2^50 only); 2..4 = bulk-copy stages ahead
-CANDIDATES = [(0, 0), (1, 0), (2, 0), (2, 1), (3, 0), (4, 0)]
+# same with FP64 butterflies (q < 2^50 only); 2..4 = bulk-copy stages ahead;
+# 5..7 = bulk-copy stages 2..4 with FP64 butterflies (q < 2^50 only)
+CANDIDATES = [(0, 0), (1, 0), (2, 0), (2, 1), (3, 0), (4, 0), (5, 0), (6, 0), (7, 0)]
 SMALL_COEFFS = 1 << 20  # a "small" call (below the library's 2^22 large-batch class)
 LARGE_COEFFS = 1 << 27  # a "large" call: 1 GiB of coefficients, far above L2
 
@@ -97,7 +98,7 @@ def tune(reps=10, quick=False, verbose=True):
                 key = _key(n_arg, incomplete, q, inverse, large)
                 times = {}
                 for var, cps in CANDIDATES:
-                    if var == 1 and q >= (1 << 50):
+                    if var in (1, 5, 6, 7) and q >= (1 << 50):
                         continue
                     _check(L.salsaa_ntt_tune_set(key[0], key[1], key[2], key[3], key[4], var, cps), "tune_set")
                     ms = time_schedule(torch, x, out, n_arg, incomplete, q, inverse, reps)

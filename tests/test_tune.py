@@ -10,7 +10,7 @@ import pytest
 from helpers import rand_mod
 from salsaa_b200 import params as P
 
-CANDIDATES = [(0, 0), (1, 0), (2, 0), (2, 1), (3, 0), (4, 0)]  # variant 1: FP64, q < 2^50 only
+CANDIDATES = [(0, 0), (1, 0), (2, 0), (2, 1), (3, 0), (4, 0), (5, 0), (6, 0), (7, 1)]  # 1, 5-7: FP64 when q < 2^50
 
 
 def _get(L, key):
@@ -36,7 +36,7 @@ def test_tune_table_roundtrip(gpu_lib, tmp_path):
     table.write_text("# comment\n"
                      "ntt 6 1 0 0 1 3 0   # incomplete d=128 forward, large\n"
                      "ntt 10 0 1 1 0 2 1\n"
-                     "ntt 6 1 1 0 1 7 0   # variant 7 does not exist: ignored\n"
+                     "ntt 6 1 1 0 1 9 0   # variant 9 does not exist: ignored\n"
                      "ntt 7 1 0 0 1 1 0   # FP64 butterflies\n"
                      "fold 1\n"
                      "garbage line\n")
@@ -47,7 +47,7 @@ def test_tune_table_roundtrip(gpu_lib, tmp_path):
     assert _get(L, (6, 1, 1, 0, 1)) == (0, 0)
     assert _get(L, (7, 1, 0, 0, 1)) == (1, 0)
     assert L.salsaa_tune_load(str(tmp_path / "missing.txt").encode()) < 0
-    assert L.salsaa_ntt_tune_set(6, 1, 0, 0, 1, 5, 0) < 0  # no variant 5
+    assert L.salsaa_ntt_tune_set(6, 1, 0, 0, 1, 8, 0) < 0  # no variant 8
     assert L.salsaa_ntt_tune_set(6, 1, 0, 0, 1, -1, 0) < 0
     assert L.salsaa_ntt_tune_set(14, 1, 0, 0, 1, 2, 0) < 0  # log n out of range
     assert L.salsaa_fold_tune_set(2) < 0
@@ -93,7 +93,7 @@ def test_schedules_equal_default(gpu_lib, cuda, oracle, n_arg, incomplete, q, co
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("var,cps", [(1, 0), (2, 0), (3, 0), (4, 0), (2, 1)])
+@pytest.mark.parametrize("var,cps", [(1, 0), (2, 0), (3, 0), (4, 0), (2, 1), (5, 0), (7, 0)])
 def test_proofs_under_each_schedule(gpu_lib, oracle, var, cps):
     """Whole proofs with every transform on a pipelined schedule equal the oracle's."""
     from salsaa_b200 import api
@@ -103,7 +103,7 @@ def test_proofs_under_each_schedule(gpu_lib, oracle, var, cps):
     assert rc == 0
     try:
         _set_all(L, var, cps)
-        assert L.salsaa_fold_tune_set(1 if var == 1 else 0) == 0
+        assert L.salsaa_fold_tune_set(1 if var in (1, 5, 6, 7) else 0) == 0
         got = api.Context(p, crs_seed=7).prove(11)
     finally:
         L.salsaa_tune_reset()
