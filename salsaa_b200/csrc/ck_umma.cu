@@ -548,9 +548,7 @@ __global__ void __launch_bounds__(256, 2)
       const u32 k = (k4hi * 4 + k4lo) * 4;
 #pragma unroll
       for (u32 e = 0; e < 4; e++) vr[x][e] = wres(src, nar, (u64)(k + e) * d + pos, q);
-      if (c + 1 < nsteps)  // the next step's values: into L2 while this step is converted
-#pragma unroll
-        for (u32 e = 0; e < 4; e++) wprefetch(src, nar, (u64)PU_KS * d + (u64)(k + e) * d + pos);
+
     }
   };
   load(0);
@@ -714,9 +712,6 @@ __global__ void __launch_bounds__(512, 1)
       const u32 e0 = (k4hi * 4 + k4lo) * 4;
 #pragma unroll
       for (u32 e = 0; e < 4; e++) vr[x][e] = wres(src, nar, (u64)(e0 + e) * d + pos, q);
-      if (c + 1 < nsteps)  // the next step's values: into L2 while this step is converted
-#pragma unroll
-        for (u32 e = 0; e < 4; e++) wprefetch(src, nar, (u64)SU_KS * d + (u64)(e0 + e) * d + pos);
     }
   };
   load(0);
@@ -959,11 +954,6 @@ __global__ void __launch_bounds__(256, 2)
     const u64 o = (u64)tile * NG_TILE + tid;
 #pragma unroll
     for (u32 m = 0; m < 16; m++) v[m] = wres(x, nar, o + m * ng, q);
-    if (tile + 1 < t1) {  // the tile after this one: into L2 while this one is converted
-      const u64 o2 = o + NG_TILE;
-#pragma unroll
-      for (u32 m = 0; m < 16; m++) wprefetch(x, nar, o2 + m * ng);
-    }
   };
   auto epilogue = [&](u32 li, u32 tile) {
     const u32 se = li & 1;

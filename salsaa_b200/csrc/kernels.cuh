@@ -30,13 +30,6 @@ struct RowSet {
 __host__ __device__ inline const u64* row_advance(const u64* p, bool narrow, u64 elems) {
   return narrow ? (const u64*)((const int*)p + elems) : p + elems;
 }
-// Hint that element i of a coefficient-form row will be read soon: an L2
-// prefetch (no register, no wait), so a pass that keeps one step of loads in
-// registers has the step after it in flight as well.  i must lie in the row.
-__device__ __forceinline__ void wprefetch(const u64* p, bool narrow, u64 i) {
-  const void* a = narrow ? (const void*)((const int*)p + i) : (const void*)(p + i);
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
-}
 // Element i of a coefficient-form row as a canonical residue mod q.
 __device__ __forceinline__ u64 wres(const u64* p, bool narrow, u64 i, u64 q) {
   if (narrow) {
