@@ -538,8 +538,19 @@ __global__ void __launch_bounds__(256, 2)
   // a step's witness values stay in registers from their loads (issued before
   // the previous step's barrier) to their conversion
   u64 vr[8][4];
+  // narrow (int32) rows: 16 consecutive elements x 2 positions per thread,
+  // one 8-byte load per element, so a load moves as many bytes as a word
+  // row's; the 16 bytes of one position are one 16-byte store to the tile
+  int2 nv[16];
+  const u32 nkq = tid >> 6, np2 = tid & 63;
   auto load = [&](u32 c) {
-    const u64* src = row_advance(chunk, nar, (u64)c * PU_KS * d);
+    if (nar) {
+      const int* src = (const int*)chunk + (u64)c * PU_KS * d;
+#pragma unroll
+      for (u32 e = 0; e < 16; e++) nv[e] = __ldg((const int2*)(src + (u64)(16 * nkq + e) * d + 2 * np2));
+      return;
+    }
+    const u64* src = chunk + (u64)c * PU_KS * d;
 #pragma unroll
     for (u32 x = 0; x < 8; x++) {
       const u32 t = tid + x * 256;
@@ -547,8 +558,7 @@ __global__ void __launch_bounds__(256, 2)
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
       const u32 k = (k4hi * 4 + k4lo) * 4;
 #pragma unroll
-      for (u32 e = 0; e < 4; e++) vr[x][e] = wres(src, nar, (u64)(k + e) * d + pos, q);
-
+      for (u32 e = 0; e < 4; e++) vr[x][e] = __ldg(src + (u64)(k + e) * d + pos);
     }
   };
   load(0);
@@ -564,8 +574,27 @@ __global__ void __launch_bounds__(256, 2)
     }
     // witness step: 128 positions x 64 elements as int8, (k / 16, pos, k % 16)
     uint8_t* B = stage + PU_A;
+    if (nar) {
 #pragma unroll
-    for (u32 x = 0; x < 8; x++) {
+      for (u32 p = 0; p < 2; p++) {
+        u32 w4[4];
+#pragma unroll
+        for (u32 g = 0; g < 4; g++) {
+          u32 packed = 0;
+#pragma unroll
+          for (u32 e = 0; e < 4; e++) {
+            const u32 tb = (u32)((p ? nv[4 * g + e].y : nv[4 * g + e].x) + 128);  // below 256 iff it fits int8
+            bad |= tb > 255u;
+            packed |= (tb & 0xffu) << (8 * e);
+          }
+          w4[g] = packed ^ 0x80808080u;
+        }
+        *(uint4*)(B + nkq * (PU_POS * 16) + (2 * np2 + p) * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+      }
+    }
+    if (!nar)
+#pragma unroll
+      for (u32 x = 0; x < 8; x++) {
       const u32 t = tid + x * 256;
       const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
@@ -702,8 +731,18 @@ __global__ void __launch_bounds__(512, 1)
   bool bad = false, ok = true;
   // task x of this thread: four consecutive elements e0 .. e0 + 3 at one position
   u64 vr[8][4];
+  // narrow (int32) rows: 16 consecutive elements x 2 positions per thread,
+  // one 8-byte load per element; one 16-byte store per limb plane and position
+  int2 nv[16];
+  const u32 nkq = tid >> 6, np2 = tid & 63;
   auto load = [&](u32 c) {
-    const u64* src = row_advance(src0, nar, (u64)c * SU_KS * d);
+    if (nar) {
+      const int* src = (const int*)src0 + (u64)c * SU_KS * d;
+#pragma unroll
+      for (u32 e = 0; e < 16; e++) nv[e] = __ldg((const int2*)(src + (u64)(16 * nkq + e) * d + 2 * np2));
+      return;
+    }
+    const u64* src = src0 + (u64)c * SU_KS * d;
 #pragma unroll
     for (u32 x = 0; x < 8; x++) {
       const u32 t = tid + x * 512;
@@ -711,7 +750,7 @@ __global__ void __launch_bounds__(512, 1)
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
       const u32 e0 = (k4hi * 4 + k4lo) * 4;
 #pragma unroll
-      for (u32 e = 0; e < 4; e++) vr[x][e] = wres(src, nar, (u64)(e0 + e) * d + pos, q);
+      for (u32 e = 0; e < 4; e++) vr[x][e] = __ldg(src + (u64)(e0 + e) * d + pos);
     }
   };
   load(0);
@@ -723,8 +762,36 @@ __global__ void __launch_bounds__(512, 1)
       umma::mbar_expect_tx(&full_bar[st], SU_A);
       umma::bulk_g2s(stage, img + (u64)c * SU_A, SU_A, &full_bar[st]);
     }
+    if (nar) {
 #pragma unroll
-    for (u32 x = 0; x < 8; x++) {
+      for (u32 p = 0; p < 2; p++) {
+        u32 l0[4], l1[4], l2[4];
+#pragma unroll
+        for (u32 g = 0; g < 4; g++) {
+          u32 a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+          for (u32 e = 0; e < 4; e++) {
+            // centred value + 0x808080: three balanced base-256 digits + 128 when it fits
+            const u32 tb = (u32)((p ? nv[4 * g + e].y : nv[4 * g + e].x) + 0x808080);
+            bad |= tb >= 0x1000000u;
+            const u32 w = tb ^ 0x808080u;
+            a0 |= (w & 0xffu) << (8 * e);
+            a1 |= ((w >> 8) & 0xffu) << (8 * e);
+            a2 |= ((w >> 16) & 0xffu) << (8 * e);
+          }
+          l0[g] = a0;
+          l1[g] = a1;
+          l2[g] = a2;
+        }
+        const u32 off = SU_A + nkq * (SU_POS * 16) + (2 * np2 + p) * 16;
+        *(uint4*)(stage + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+        *(uint4*)(stage + off + SU_B) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+        *(uint4*)(stage + off + 2 * SU_B) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+      }
+    }
+    if (!nar)
+#pragma unroll
+      for (u32 x = 0; x < 8; x++) {
       const u32 t = tid + x * 512;
       const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
       const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
