@@ -27,16 +27,29 @@ def _stale():
 
 
 def build(force=False, verbose=False, extra=()):
+    """Compiles every source (in parallel, one nvcc per file) and links the library."""
     if not force and not _stale():
         return LIB
-    objs = []
+    from concurrent.futures import ThreadPoolExecutor
+    objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmds.append([NVCC, *ARCH, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj])
+        objs.append(obj)
+
+    def run(cmd):
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(run, cmds))
+    for cmd, r in zip(cmds, results):
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+            sys.stdout.write(r.stdout)
+            sys.stdout.write(r.stderr)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise subprocess.CalledProcessError(r.returncode, cmd)
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
     for o in objs:

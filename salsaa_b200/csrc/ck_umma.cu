@@ -534,31 +534,23 @@ __global__ void __launch_bounds__(256, 2)
   // signed int8 x signed int8 -> s32, M = N = 128
   const u32 idesc = umma::idesc_u8(128, PU_POS) | (1u << 7) | (1u << 10);
   bool bad = false, ok = true;
-  // task x of this thread: four consecutive elements k .. k + 3 at one position;
-  // a step's witness values stay in registers from their loads (issued before
-  // the previous step's barrier) to their conversion
-  u64 vr[8][4];
-  // narrow (int32) rows: 16 consecutive elements x 2 positions per thread,
-  // one 8-byte load per element, so a load moves as many bytes as a word
-  // row's; the 16 bytes of one position are one 16-byte store to the tile
-  int2 nv[16];
+  // task of this thread: 16 consecutive elements x 2 neighbouring positions,
+  // one 16-byte load per element for word rows (two u64 values) and one
+  // 8-byte load for narrow rows (two int32 values, kept in wv[e].x); a
+  // step's values stay in registers from their loads (issued before the
+  // previous step's barrier) to their conversion
+  ulonglong2 wv[16];
   const u32 nkq = tid >> 6, np2 = tid & 63;
   auto load = [&](u32 c) {
     if (nar) {
       const int* src = (const int*)chunk + (u64)c * PU_KS * d;
 #pragma unroll
-      for (u32 e = 0; e < 16; e++) nv[e] = __ldg((const int2*)(src + (u64)(16 * nkq + e) * d + 2 * np2));
-      return;
-    }
-    const u64* src = chunk + (u64)c * PU_KS * d;
+      for (u32 e = 0; e < 16; e++)
+        wv[e].x = (u64)__ldg((const long long*)(src + (u64)(16 * nkq + e) * d + 2 * np2));
+    } else {
+      const u64* src = chunk + (u64)c * PU_KS * d;
 #pragma unroll
-    for (u32 x = 0; x < 8; x++) {
-      const u32 t = tid + x * 256;
-      const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
-      const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
-      const u32 k = (k4hi * 4 + k4lo) * 4;
-#pragma unroll
-      for (u32 e = 0; e < 4; e++) vr[x][e] = __ldg(src + (u64)(k + e) * d + pos);
+      for (u32 e = 0; e < 16; e++) wv[e] = __ldg((const ulonglong2*)(src + (u64)(16 * nkq + e) * d + 2 * np2));
     }
   };
   load(0);
@@ -572,43 +564,32 @@ __global__ void __launch_bounds__(256, 2)
       umma::bulk_g2s(stage, img, PU_A / 2, &full_bar[st]);
       umma::bulk_g2s(stage + PU_A / 2, img + PU_IMG / 2, PU_A / 2, &full_bar[st]);
     }
-    // witness step: 128 positions x 64 elements as int8, (k / 16, pos, k % 16)
+    // witness step: 128 positions x 64 elements as int8, (k / 16, pos, k % 16):
+    // the 16 bytes of one position are one 16-byte store
     uint8_t* B = stage + PU_A;
-    if (nar) {
 #pragma unroll
-      for (u32 p = 0; p < 2; p++) {
-        u32 w4[4];
+    for (u32 p = 0; p < 2; p++) {
+      u32 w4[4];
 #pragma unroll
-        for (u32 g = 0; g < 4; g++) {
-          u32 packed = 0;
+      for (u32 g = 0; g < 4; g++) {
+        u32 packed = 0;
 #pragma unroll
-          for (u32 e = 0; e < 4; e++) {
-            const u32 tb = (u32)((p ? nv[4 * g + e].y : nv[4 * g + e].x) + 128);  // below 256 iff it fits int8
-            bad |= tb > 255u;
-            packed |= (tb & 0xffu) << (8 * e);
+        for (u32 e = 0; e < 4; e++) {
+          const ulonglong2 v2 = wv[4 * g + e];
+          long long cv;  // centred value
+          if (nar) {
+            cv = (long long)(int)(u32)(p ? (v2.x >> 32) : v2.x);
+          } else {
+            const u64 v = p ? v2.y : v2.x;
+            cv = v > half_q ? (long long)v - (long long)q : (long long)v;
           }
-          w4[g] = packed ^ 0x80808080u;
+          const unsigned long long tb = (unsigned long long)(cv + 128);  // below 256 iff it fits int8
+          bad |= tb > 255ULL;
+          packed |= ((u32)tb & 0xffu) << (8 * e);
         }
-        *(uint4*)(B + nkq * (PU_POS * 16) + (2 * np2 + p) * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        w4[g] = packed ^ 0x80808080u;
       }
-    }
-    if (!nar)
-#pragma unroll
-      for (u32 x = 0; x < 8; x++) {
-      const u32 t = tid + x * 256;
-      const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
-      const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
-      // centred value + 128 is below 256 exactly when the value fits int8
-      u32 packed = 0, hi = 0;
-#pragma unroll
-      for (u32 e = 0; e < 4; e++) {
-        const u64 v = vr[x][e];
-        const u64 tb = v + 128 - (v > half_q ? q : 0);
-        hi |= (u32)(tb >> 8) | (u32)(tb >> 40);
-        packed |= ((u32)tb & 0xffu) << (8 * e);
-      }
-      bad |= hi != 0;
-      *(u32*)(B + k4hi * (PU_POS * 16) + pos * 16 + k4lo * 4) = packed ^ 0x80808080u;
+      *(uint4*)(B + nkq * (PU_POS * 16) + (2 * np2 + p) * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
     }
     if (c + 1 < nsteps) load(c + 1);
     umma::fence_proxy_async();
@@ -729,28 +710,22 @@ __global__ void __launch_bounds__(512, 1)
   // unsigned bytes (A) x signed bytes (B) -> s32, M = N = 128
   const u32 idesc = umma::idesc_u8(128, SU_POS) | (1u << 10);
   bool bad = false, ok = true;
-  // task x of this thread: four consecutive elements e0 .. e0 + 3 at one position
-  u64 vr[8][4];
-  // narrow (int32) rows: 16 consecutive elements x 2 positions per thread,
-  // one 8-byte load per element; one 16-byte store per limb plane and position
-  int2 nv[16];
+  // task of this thread: 16 consecutive elements x 2 neighbouring positions,
+  // one 16-byte load per element for word rows (two u64 values) and one
+  // 8-byte load for narrow rows (two int32 values, kept in wv[e].x); one
+  // 16-byte store per limb plane and position
+  ulonglong2 wv[16];
   const u32 nkq = tid >> 6, np2 = tid & 63;
   auto load = [&](u32 c) {
     if (nar) {
       const int* src = (const int*)src0 + (u64)c * SU_KS * d;
 #pragma unroll
-      for (u32 e = 0; e < 16; e++) nv[e] = __ldg((const int2*)(src + (u64)(16 * nkq + e) * d + 2 * np2));
-      return;
-    }
-    const u64* src = src0 + (u64)c * SU_KS * d;
+      for (u32 e = 0; e < 16; e++)
+        wv[e].x = (u64)__ldg((const long long*)(src + (u64)(16 * nkq + e) * d + 2 * np2));
+    } else {
+      const u64* src = src0 + (u64)c * SU_KS * d;
 #pragma unroll
-    for (u32 x = 0; x < 8; x++) {
-      const u32 t = tid + x * 512;
-      const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
-      const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
-      const u32 e0 = (k4hi * 4 + k4lo) * 4;
-#pragma unroll
-      for (u32 e = 0; e < 4; e++) vr[x][e] = __ldg(src + (u64)(e0 + e) * d + pos);
+      for (u32 e = 0; e < 16; e++) wv[e] = __ldg((const ulonglong2*)(src + (u64)(16 * nkq + e) * d + 2 * np2));
     }
   };
   load(0);
@@ -762,56 +737,38 @@ __global__ void __launch_bounds__(512, 1)
       umma::mbar_expect_tx(&full_bar[st], SU_A);
       umma::bulk_g2s(stage, img + (u64)c * SU_A, SU_A, &full_bar[st]);
     }
-    if (nar) {
 #pragma unroll
-      for (u32 p = 0; p < 2; p++) {
-        u32 l0[4], l1[4], l2[4];
+    for (u32 p = 0; p < 2; p++) {
+      u32 l0[4], l1[4], l2[4];
 #pragma unroll
-        for (u32 g = 0; g < 4; g++) {
-          u32 a0 = 0, a1 = 0, a2 = 0;
+      for (u32 g = 0; g < 4; g++) {
+        u32 a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
-          for (u32 e = 0; e < 4; e++) {
-            // centred value + 0x808080: three balanced base-256 digits + 128 when it fits
-            const u32 tb = (u32)((p ? nv[4 * g + e].y : nv[4 * g + e].x) + 0x808080);
-            bad |= tb >= 0x1000000u;
-            const u32 w = tb ^ 0x808080u;
-            a0 |= (w & 0xffu) << (8 * e);
-            a1 |= ((w >> 8) & 0xffu) << (8 * e);
-            a2 |= ((w >> 16) & 0xffu) << (8 * e);
+        for (u32 e = 0; e < 4; e++) {
+          const ulonglong2 v2 = wv[4 * g + e];
+          // centred value + 0x808080: its bytes are the signed limbs + 128 when
+          // the value lies in [-0x808080, 0x7f7f7f] (three balanced base-256 digits)
+          u64 tb;
+          if (nar) {
+            tb = (u64)((long long)(int)(u32)(p ? (v2.x >> 32) : v2.x) + 0x808080LL);
+          } else {
+            const u64 v = p ? v2.y : v2.x;
+            tb = v + 0x808080ULL - (v > half_q ? q : 0);
           }
-          l0[g] = a0;
-          l1[g] = a1;
-          l2[g] = a2;
+          bad |= (tb >> 24) != 0;  // the value needs a fourth limb
+          const u32 w = (u32)tb ^ 0x808080u;
+          a0 |= (w & 0xffu) << (8 * e);
+          a1 |= ((w >> 8) & 0xffu) << (8 * e);
+          a2 |= ((w >> 16) & 0xffu) << (8 * e);
         }
-        const u32 off = SU_A + nkq * (SU_POS * 16) + (2 * np2 + p) * 16;
-        *(uint4*)(stage + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
-        *(uint4*)(stage + off + SU_B) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
-        *(uint4*)(stage + off + 2 * SU_B) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+        l0[g] = a0;
+        l1[g] = a1;
+        l2[g] = a2;
       }
-    }
-    if (!nar)
-#pragma unroll
-      for (u32 x = 0; x < 8; x++) {
-      const u32 t = tid + x * 512;
-      const u32 k4lo = t & 3, posl = (t >> 2) & 7, rest = t >> 5;
-      const u32 pos = (rest & 15) * 8 + posl, k4hi = rest >> 4;
-      // centred value + 0x808080: its bytes are the signed limbs + 128 when
-      // the value lies in [-0x808080, 0x7f7f7f] (three balanced base-256 digits)
-      u32 wv[4];
-#pragma unroll
-      for (u32 e = 0; e < 4; e++) {
-        const u64 v = vr[x][e];
-        const u64 tb = v + 0x808080ULL - (v > half_q ? q : 0);
-        bad |= (tb >> 24) != 0;  // the value needs a fourth limb
-        wv[e] = (u32)tb ^ 0x808080u;
-      }
-      // limb planes of the four elements: byte l of wv[0..3]
-      const u32 lo01 = __byte_perm(wv[0], wv[1], 0x5140), lo23 = __byte_perm(wv[2], wv[3], 0x5140);
-      const u32 hi01 = __byte_perm(wv[0], wv[1], 0x0062), hi23 = __byte_perm(wv[2], wv[3], 0x0062);
-      const u32 off = SU_A + k4hi * (SU_POS * 16) + pos * 16 + k4lo * 4;
-      *(u32*)(stage + off) = __byte_perm(lo01, lo23, 0x5410);
-      *(u32*)(stage + off + SU_B) = __byte_perm(lo01, lo23, 0x7632);
-      *(u32*)(stage + off + 2 * SU_B) = __byte_perm(hi01, hi23, 0x5410);
+      const u32 off = SU_A + nkq * (SU_POS * 16) + (2 * np2 + p) * 16;
+      *(uint4*)(stage + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+      *(uint4*)(stage + off + SU_B) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+      *(uint4*)(stage + off + 2 * SU_B) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
     }
     if (c + 1 < nsteps) load(c + 1);
     umma::fence_proxy_async();
@@ -1016,11 +973,29 @@ __global__ void __launch_bounds__(256, 2)
   const u64 w32 = ((u64)1 << 32) % q, w32p = (u64)(((unsigned __int128)w32 << 64) / q);
   bool bad = false, ok = true;
 
-  u64 v[16];
+  // loads of this thread: 4 consecutive groups g0 .. g0 + 3 (g0 = 4 (tid % 64))
+  // x the 4 values m = 4 (tid / 64) .. + 3 of each, so one value index is
+  // one 16-byte load for narrow rows (four int32 in wv[2 mm]) and two for
+  // word rows (u64 pairs in wv[2 mm], wv[2 mm + 1]); the 16 limb bytes of
+  // one group's four values are one 16-byte store to the tile
+  ulonglong2 wv[8];
+  const u32 g0 = 4 * (tid & 63), mq = tid >> 6;
+  // stores of the four groups in the order rot, rot + 1, .. (mod 4): the 8
+  // lanes of a store phase then hit 8 distinct 16-byte bank groups
+  const u32 rot = (lane >> 1) & 3;
   auto load = [&](u32 tile) {
-    const u64 o = (u64)tile * NG_TILE + tid;
+    const u64 o = (u64)tile * NG_TILE + g0;
+    if (nar) {
+      const int* xs = (const int*)x + o;
 #pragma unroll
-    for (u32 m = 0; m < 16; m++) v[m] = wres(x, nar, o + m * ng, q);
+      for (u32 mm = 0; mm < 4; mm++) wv[2 * mm] = __ldg((const ulonglong2*)(xs + (u64)(4 * mq + mm) * ng));
+    } else {
+#pragma unroll
+      for (u32 mm = 0; mm < 4; mm++)
+#pragma unroll
+        for (u32 h = 0; h < 2; h++)
+          wv[2 * mm + h] = __ldg((const ulonglong2*)(x + o + (u64)(4 * mq + mm) * ng + 2 * h));
+    }
   };
   auto epilogue = [&](u32 li, u32 tile) {
     const u32 se = li & 1;
@@ -1048,17 +1023,49 @@ __global__ void __launch_bounds__(256, 2)
     uint8_t* stage = smem + s * NG_STAGE;
     // stage s was last read by the MMAs of tile li - 2, whose completion the
     // epilogue of iteration li - 1 waited for
-    uint32_t wd[16];
+    uint32_t wd[4][4];  // [group][value]: the four signed limbs, byte x = limb x
 #pragma unroll
-    for (u32 m = 0; m < 16; m++) {
-      const u64 t = v[m] + 0x80808080ULL - (v[m] > half_q ? q : 0);  // centred value + limb bias
-      bad |= (t >> 32) != 0;
-      wd[m] = (uint32_t)t ^ 0x80808080u;  // the four signed limbs, byte x = limb x
+    for (u32 gi = 0; gi < 4; gi++)
+#pragma unroll
+      for (u32 mm = 0; mm < 4; mm++) {
+        if (nar) {
+          const u64 pr = (gi & 2) ? wv[2 * mm].y : wv[2 * mm].x;
+          const int cv = (int)(u32)((gi & 1) ? pr >> 32 : pr);  // centred value
+          bad |= cv > 0x7f7f7f7f;  // below -0x80808080 is out of int32 range
+          wd[gi][mm] = ((u32)cv + 0x80808080u) ^ 0x80808080u;
+        } else {
+          const ulonglong2 pr = wv[2 * mm + (gi >> 1)];
+          const u64 v = (gi & 1) ? pr.y : pr.x;
+          const u64 t = v + 0x80808080ULL - (v > half_q ? q : 0);  // centred value + limb bias
+          bad |= (t >> 32) != 0;
+          wd[gi][mm] = (uint32_t)t ^ 0x80808080u;
+        }
+      }
+    // rotate the groups by rot (selects on a lane-uniform-per-pair value)
+#pragma unroll
+    for (u32 mm = 0; mm < 4; mm++) {
+      if (rot & 1) {
+        const u32 t0 = wd[0][mm];
+        wd[0][mm] = wd[1][mm];
+        wd[1][mm] = wd[2][mm];
+        wd[2][mm] = wd[3][mm];
+        wd[3][mm] = t0;
+      }
+      if (rot & 2) {
+        u32 t0 = wd[0][mm];
+        wd[0][mm] = wd[2][mm];
+        wd[2][mm] = t0;
+        t0 = wd[1][mm];
+        wd[1][mm] = wd[3][mm];
+        wd[3][mm] = t0;
+      }
     }
-    uint8_t* rowp = stage + (tid >> 3) * NG_GBS + (tid & 7) * 16;
 #pragma unroll
-    for (u32 c = 0; c < 4; c++)
-      *(uint4*)(rowp + c * 128) = make_uint4(wd[4 * c], wd[4 * c + 1], wd[4 * c + 2], wd[4 * c + 3]);
+    for (u32 sidx = 0; sidx < 4; sidx++) {
+      const u32 g = g0 + ((sidx + rot) & 3);
+      *(uint4*)(stage + (g >> 3) * NG_GBS + (g & 7) * 16 + mq * 128) =
+          make_uint4(wd[sidx][0], wd[sidx][1], wd[sidx][2], wd[sidx][3]);
+    }
     if (i + 1 < t1) load(i + 1);
     umma::fence_proxy_async();
     umma::fence_before_sync();
@@ -1178,8 +1185,9 @@ __global__ void __launch_bounds__(256) nc_gram_sums_kernel(const u64* gram, cons
   }
 }
 
-bool nc_gram_ok(u64 nlen, u64 q) {
-  return q > (1ULL << 47) && q < (1ULL << 56) && nlen % (16ULL * NG_TILE) == 0 && nlen / 16 / NG_TILE >= 1;
+bool nc_gram_ok(const RowSet& w, u32 rows, u64 nlen, u64 q) {
+  return q > (1ULL << 47) && q < (1ULL << 56) && nlen % (16ULL * NG_TILE) == 0 && nlen / 16 / NG_TILE >= 1 &&
+         rowset_aligned(w, rows, 16, 16);
 }
 
 int launch_nc_gram(const RowSet& w, u32 rows, u64 nlen, const ModQ& M, const DevState* ds, u32 round, u64* out,

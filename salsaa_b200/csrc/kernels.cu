@@ -930,7 +930,7 @@ static int sumcheck_passes(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, c
   if (L > SC_TAIL) {
     // rounds 0..3 on the tensor cores when the shapes allow; the CUDA-core
     // pass then runs only if a witness value did not fit the byte limbs
-    const bool tc = B.gram && nc_gram_ok(L, M.q);
+    const bool tc = B.gram && nc_gram_ok(w, rows, L, M.q);
     const u32* flag = tc ? (const u32*)(B.gram + (u64)rows * 256) : nullptr;
     int rc = 0;
     if (tc && (rc = launch_nc_gram(w, rows, L, M, ds, round, B.a, sa, B.gram, plain, st))) return rc;
@@ -1412,7 +1412,7 @@ int launch_project(RowSet in, u32 rows, u64 width, u32 d, u64 q, const u32* pos_
   const u64 nch = width / cw;
   if ((u64)rows * nch > 65535) return salsaa_set_error(-2, "project: too many chunks");
   const u64* gate = nullptr;
-  if (Jc && ds && d % 128 == 0 && cw % 128 == 0) {
+  if (Jc && ds && d % 128 == 0 && cw % 128 == 0 && rowset_aligned(in, rows, 16, 8)) {
     cudaError_t e = cudaMemsetAsync(&ds->proj_flag, 0, sizeof(u64), st);
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "project memset");
     int rc = launch_project_umma(in, rows, nch, d, q, cw, Jc, out, &ds->proj_flag, st);
@@ -2346,7 +2346,7 @@ int launch_commit(const CommitArgs& a, const NttDev& T, const ModQ& M, const Dev
     // s_hi[i / Bw] s_lo[i % Bw], so when that pass runs anyway the periodic /
     // all-ones rows ride in it if they fit, and no column sums are needed.
     const bool tc_ok = a.coef_sc && a.sc_img && a.sc_flags && M.q < (1ULL << 56) && d % 128 == 0 &&
-                       Bw % 128 == 0 && tl.n > 0 && tl.n <= SC_UMMA_MAX_ROWS;
+                       Bw % 128 == 0 && tl.n > 0 && tl.n <= SC_UMMA_MAX_ROWS && rowset_aligned(wsrc, a.rows, 16, 8);
     bool periodic_done = false;
     if (tc_ok) {
       ScRowList gl = tl;

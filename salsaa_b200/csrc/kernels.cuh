@@ -30,6 +30,16 @@ struct RowSet {
 __host__ __device__ inline const u64* row_advance(const u64* p, bool narrow, u64 elems) {
   return narrow ? (const u64*)((const int*)p + elems) : p + elems;
 }
+// True when rows 0 .. rows-1 start on word_bytes boundaries (u64 rows) or
+// narrow_bytes boundaries (narrow rows): the tensor-core passes load several
+// neighbouring elements of a row at a time.
+inline bool rowset_aligned(const RowSet& rs, u32 rows, u32 word_bytes, u32 narrow_bytes) {
+  for (u32 k = 0; k < rows && k < MAX_WROWS; k++) {
+    const uintptr_t a = (uintptr_t)rs.p[k];
+    if (a % (((rs.narrow >> k) & 1) ? narrow_bytes : word_bytes)) return false;
+  }
+  return true;
+}
 // Element i of a coefficient-form row as a canonical residue mod q.
 __device__ __forceinline__ u64 wres(const u64* p, bool narrow, u64 i, u64 q) {
   if (narrow) {
@@ -96,7 +106,7 @@ int launch_sc_umma(const RowSet& wc, u32 rows, u64 width, u32 d, u32 Bw, u32 nhi
 // the folded vectors and the Gram matrices, or raises the flag word after them
 // when a value does not fit four signed byte limbs; launch_nc_gram_sums adds
 // the round sums unless the flag is raised.
-bool nc_gram_ok(u64 nlen, u64 q);
+bool nc_gram_ok(const RowSet& w, u32 rows, u64 nlen, u64 q);
 int launch_nc_gram(const RowSet& w, u32 rows, u64 nlen, const ModQ& M, const DevState* ds, u32 round, u64* out,
                    u64 sout, u64* gram, bool plain, cudaStream_t st);
 int launch_nc_gram_sums(const u64* gram, u32 rows, const ModQ& M, const DevState* ds, u32 round, u64* sums, u32 nr,
