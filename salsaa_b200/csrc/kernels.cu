@@ -1487,52 +1487,66 @@ __global__ void fold_pre_kernel(const u64* c, u32 rows, u32 n, ModQ M, const u64
 // fold_vec_kernel with FP64 products (q < 2^50, canonical slot-form rows):
 // per row the two products of each output are at most 1.25 q each, and the
 // running sum is reduced after every row, so every value stays below 4 q.
+// A thread folds one slot pair of FOLD_EL consecutive elements, so each
+// row's six constant planes are loaded once for FOLD_EL elements (the
+// constants were three quarters of the load requests with one element per
+// thread); a warp's loads of one element stay 512 contiguous bytes.
+constexpr u32 FOLD_EL = 4;
+
 __global__ void __launch_bounds__(256) fold_fp_kernel(RowSet w, u32 rows, u64 width, u32 logn, ModQ M,
                                                       const u64* __restrict__ pre, u64* out) {
   const u32 n = 1u << logn, hn = n >> 1;
-  const u64 tot = width << (logn - 1);
+  const u64 groups = (width + FOLD_EL - 1) / FOLD_EL;
+  const u64 tot = groups << (logn - 1);
+  const u64 plane = (u64)rows << logn;
   const double qd = (double)M.q, q2d = 2.0 * qd, qinv = 1.0 / qd;
   for (u64 t = (u64)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (u64)gridDim.x * blockDim.x) {
-    const u64 i = t >> (logn - 1);
+    const u64 i0 = (t >> (logn - 1)) * FOLD_EL;
     const u32 s = 2 * ((u32)t & (hn - 1));
-    double ae[2] = {0, 0}, ao[2] = {0, 0};
-    for (u32 k0 = 0; k0 < rows; k0 += 4) {
-      ulonglong2 E[4], O[4];
+    const u32 nel = width - i0 < FOLD_EL ? (u32)(width - i0) : FOLD_EL;
+    double ae[FOLD_EL][2], ao[FOLD_EL][2];
 #pragma unroll
-      for (u32 j = 0; j < 4; j++)
-        if (k0 + j < rows) {
-          const u64* x = w.p[k0 + j] + (i << (logn + 1));
-          E[j] = __ldg((const ulonglong2*)(x + s));
-          O[j] = __ldg((const ulonglong2*)(x + n + s));
+    for (u32 j = 0; j < FOLD_EL; j++) ae[j][0] = ae[j][1] = ao[j][0] = ao[j][1] = 0.0;
+#pragma unroll 2
+    for (u32 k = 0; k < rows; k++) {
+      const u64* pk = pre + ((u64)k << logn) + s;
+      ulonglong2 C[6], E[FOLD_EL], O[FOLD_EL];
+#pragma unroll
+      for (u32 g = 0; g < 6; g++) C[g] = __ldg((const ulonglong2*)(pk + g * plane));
+      const u64* x = w.p[k] + (i0 << (logn + 1));
+#pragma unroll
+      for (u32 j = 0; j < FOLD_EL; j++)
+        if (j < nel) {
+          E[j] = __ldg((const ulonglong2*)(x + ((u64)j << (logn + 1)) + s));
+          O[j] = __ldg((const ulonglong2*)(x + ((u64)j << (logn + 1)) + n + s));
         }
 #pragma unroll
-      for (u32 j = 0; j < 4; j++)
-        if (k0 + j < rows) {
-          const u64 plane = (u64)rows << logn;
-          const u64* pk = pre + ((u64)((k0 + j) << logn) + s);
-          ulonglong2 C[6];
+      for (u32 h = 0; h < 2; h++) {
+        const double ce = __longlong_as_double((long long)(h ? C[0].y : C[0].x));
+        const double ceh = __longlong_as_double((long long)(h ? C[1].y : C[1].x));
+        const double co = __longlong_as_double((long long)(h ? C[2].y : C[2].x));
+        const double coh = __longlong_as_double((long long)(h ? C[3].y : C[3].x));
+        const double zc = __longlong_as_double((long long)(h ? C[4].y : C[4].x));
+        const double zch = __longlong_as_double((long long)(h ? C[5].y : C[5].x));
 #pragma unroll
-          for (u32 g = 0; g < 6; g++) C[g] = __ldg((const ulonglong2*)(pk + g * plane));
-#pragma unroll
-          for (u32 h = 0; h < 2; h++) {
+        for (u32 j = 0; j < FOLD_EL; j++)
+          if (j < nel) {
             const double we = fp_from_word(h ? E[j].y : E[j].x), wo = fp_from_word(h ? O[j].y : O[j].x);
-            const double ce = __longlong_as_double((long long)(h ? C[0].y : C[0].x));
-            const double ceh = __longlong_as_double((long long)(h ? C[1].y : C[1].x));
-            const double co = __longlong_as_double((long long)(h ? C[2].y : C[2].x));
-            const double coh = __longlong_as_double((long long)(h ? C[3].y : C[3].x));
-            const double zc = __longlong_as_double((long long)(h ? C[4].y : C[4].x));
-            const double zch = __longlong_as_double((long long)(h ? C[5].y : C[5].x));
             const double e = __dadd_rn(fp_mulmod(we, ce, ceh, q2d), fp_mulmod(wo, zc, zch, q2d));
             const double o = __dadd_rn(fp_mulmod(we, co, coh, q2d), fp_mulmod(wo, ce, ceh, q2d));
-            ae[h] = fp_reduce(__dadd_rn(ae[h], e), qinv, qd);
-            ao[h] = fp_reduce(__dadd_rn(ao[h], o), qinv, qd);
+            ae[j][h] = fp_reduce(__dadd_rn(ae[j][h], e), qinv, qd);
+            ao[j][h] = fp_reduce(__dadd_rn(ao[j][h], o), qinv, qd);
           }
-        }
+      }
     }
-    *(ulonglong2*)(out + (i << (logn + 1)) + s) =
-        make_ulonglong2(fp_to_word(ae[0], qinv, qd), fp_to_word(ae[1], qinv, qd));
-    *(ulonglong2*)(out + (i << (logn + 1)) + n + s) =
-        make_ulonglong2(fp_to_word(ao[0], qinv, qd), fp_to_word(ao[1], qinv, qd));
+#pragma unroll
+    for (u32 j = 0; j < FOLD_EL; j++)
+      if (j < nel) {
+        u64* dst = out + ((i0 + j) << (logn + 1));
+        *(ulonglong2*)(dst + s) = make_ulonglong2(fp_to_word(ae[j][0], qinv, qd), fp_to_word(ae[j][1], qinv, qd));
+        *(ulonglong2*)(dst + n + s) =
+            make_ulonglong2(fp_to_word(ao[j][0], qinv, qd), fp_to_word(ao[j][1], qinv, qd));
+      }
   }
 }
 
@@ -1653,7 +1667,8 @@ int launch_fold(RowSet w_slot, u32 rows, u64 width, const NttDev& T, const ModQ&
   int rc = check_launch("fold_pre");
   if (rc) return rc;
   if (fp) {
-    fold_fp_kernel<<<grid_1d(width * T.n / 2, 256), 256, 0, st>>>(w_slot, rows, width, T.logn, M, pre, out_slot);
+    fold_fp_kernel<<<grid_1d((width + FOLD_EL - 1) / FOLD_EL * T.n / 2, 256), 256, 0, st>>>(w_slot, rows, width,
+                                                                                            T.logn, M, pre, out_slot);
     return check_launch("fold");
   }
   if (vec) {

@@ -656,45 +656,49 @@ constexpr u32 NP_ERR_WAIT = 0x4e54u;  // "NT": a stage's bulk copy did not compl
 // bits of 2^52 (v + 2^52 has v in its low 52 mantissa bits), one integer
 // and one FP64 instruction each.
 // ---------------------------------------------------------------------------
+// Butterflies of phase P on one mini-block v[0 .. 2^S) with block index blk.
+template <int LOGN, int P, bool INV>
+__device__ __forceinline__ void nf_block(double* v, u32 blk, const NttDev& T) {
+  constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
+  constexpr u32 N = 1u << LOGN, K = 1u << S;
+  const double q2d = T.q2d, qd = T.qd, qinv = T.qinv;
+#pragma unroll
+  for (int l = 0; l < S; l++) {
+    const u32 lt = INV ? l : S - 1 - l;
+    const u32 t = 1u << lt;
+    double w = 0, wh = 0;
+#pragma unroll
+    for (u32 p = 0; p < K / 2; p++) {
+      const u32 sb = p >> lt, kk = p & (t - 1), k = (sb << (lt + 1)) + kk;
+      if (kk == 0) {
+        const u32 idx = INV ? (N >> (G0 + l + 1)) + (blk << (S - l - 1)) + sb : (1u << (G0 + l)) + (blk << l) + sb;
+        w = __ldg((INV ? T.inv_d : T.fwd_d) + idx);
+        wh = __ldg((INV ? T.inv_h : T.fwd_h) + idx);
+      }
+      const double a = v[k], b = v[k + t];
+      if (!INV) {
+        const double m = fp_mulmod(b, w, wh, q2d);
+        v[k] = __dadd_rn(a, m);
+        v[k + t] = __dsub_rn(a, m);
+      } else {
+        v[k] = fp_reduce(__dadd_rn(a, b), qinv, qd);
+        v[k + t] = fp_mulmod(__dsub_rn(a, b), w, wh, q2d);
+      }
+    }
+    if (!INV && ((G0 + l) & 1)) {
+#pragma unroll
+      for (u32 i = 0; i < K; i++) v[i] = fp_reduce(v[i], qinv, qd);
+    }
+  }
+}
+
 template <int LOGN, int P, bool INV>
 __device__ __forceinline__ void nf_compute(double (&x)[16], u32 tu, const NttDev& T) {
   constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
-  constexpr u32 N = 1u << LOGN, TPU = N / 16, MB = 16 >> S, K = 1u << S;
+  constexpr u32 N = 1u << LOGN, TPU = N / 16, MB = 16 >> S;
   constexpr u32 LSTR = INV ? G0 : LOGN - G0 - S;
-  const double q2d = T.q2d, qd = T.qd, qinv = T.qinv;
 #pragma unroll
-  for (u32 j = 0; j < MB; j++) {
-    const u32 mb = tu + j * TPU, blk = mb >> LSTR;
-    double* v = x + j * (1u << S);
-#pragma unroll
-    for (int l = 0; l < S; l++) {
-      const u32 lt = INV ? l : S - 1 - l;
-      const u32 t = 1u << lt;
-      double w = 0, wh = 0;
-#pragma unroll
-      for (u32 p = 0; p < K / 2; p++) {
-        const u32 sb = p >> lt, kk = p & (t - 1), k = (sb << (lt + 1)) + kk;
-        if (kk == 0) {
-          const u32 idx = INV ? (N >> (G0 + l + 1)) + (blk << (S - l - 1)) + sb : (1u << (G0 + l)) + (blk << l) + sb;
-          w = __ldg((INV ? T.inv_d : T.fwd_d) + idx);
-          wh = __ldg((INV ? T.inv_h : T.fwd_h) + idx);
-        }
-        const double a = v[k], b = v[k + t];
-        if (!INV) {
-          const double m = fp_mulmod(b, w, wh, q2d);
-          v[k] = __dadd_rn(a, m);
-          v[k + t] = __dsub_rn(a, m);
-        } else {
-          v[k] = fp_reduce(__dadd_rn(a, b), qinv, qd);
-          v[k + t] = fp_mulmod(__dsub_rn(a, b), w, wh, q2d);
-        }
-      }
-      if (!INV && ((G0 + l) & 1)) {
-#pragma unroll
-        for (u32 i = 0; i < K; i++) v[i] = fp_reduce(v[i], qinv, qd);
-      }
-    }
-  }
+  for (u32 j = 0; j < MB; j++) nf_block<LOGN, P, INV>(x + j * (1u << S), (tu + j * TPU) >> LSTR, T);
 }
 
 // First-phase loads (as nr_load_global) converted to doubles; the OR of the
@@ -792,6 +796,144 @@ template <int LOGN, bool INC, bool INV>
 __global__ void __launch_bounds__(256) ntt_fp_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
   __shared__ double sm[NR_TILE + NR_TILE / 16];
   nf_tile<LOGN, INC, INV>(in, out, units, blockIdx.x, T, mag_or, sm);
+}
+
+// ---------------------------------------------------------------------------
+// Incomplete transforms of degree-128 ring elements (two 64-point halves)
+// with FP64 butterflies, one thread per (element, column r < 8) holding
+// both halves: 8 coefficients of each, e = r + 8k in the strided phase and
+// e = 8r + k in the contiguous one.  The same butterflies and exchange as
+// ntt_fp_kernel<6, true, INV> (identical words), with fewer L1 wavefronts
+// per coefficient, the limit of that kernel: the interleaved side moves one
+// 16-byte (half 0, half 1) pair per load or store, 8 lanes covering 128
+// contiguous bytes of an element; the slot-form side moves 32 bytes per
+// lane (256-bit loads and stores, rows 32-byte aligned); the exchange tile
+// holds (half 0, half 1) pairs with 16 bytes of padding per 8 pairs, so
+// both exchange patterns are free of bank conflicts.
+// ---------------------------------------------------------------------------
+constexpr u32 NP6_EL = 32;   // ring elements per CTA (4096 coefficients)
+constexpr u32 NP6_ROW = 72;  // pairs per element in the exchange tile (64 + 8 padding)
+__device__ __forceinline__ u32 np6_pos(u32 el, u32 e) { return el * NP6_ROW + e + (e >> 3); }
+
+__device__ __forceinline__ void st_v4_u64(u64* p, u64 a, u64 b, u64 c, u64 d) {
+  asm volatile("st.global.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(a), "l"(b), "l"(c), "l"(d) : "memory");
+}
+__device__ __forceinline__ void ld_v4_u64(const u64* p, u64& a, u64& b, u64& c, u64& d) {
+  asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
+}
+
+// Strided phase of the forward transform, exchange and contiguous phase;
+// x0 / x1 hold half 0 / 1 at e = r + 8k on entry and at e = 8r + k on exit.
+__device__ __forceinline__ void np6_forward(double (&x0)[8], double (&x1)[8], double2* sm, u32 el, u32 r,
+                                            bool active, const NttDev& T) {
+  if (active) {
+    nf_block<6, 0, false>(x0, 0, T);
+    nf_block<6, 0, false>(x1, 0, T);
+#pragma unroll
+    for (u32 k = 0; k < 8; k++) sm[np6_pos(el, r + 8 * k)] = make_double2(x0[k], x1[k]);
+  }
+  __syncthreads();
+  if (active) {
+#pragma unroll
+    for (u32 k = 0; k < 8; k++) {
+      const double2 v = sm[np6_pos(el, 8 * r + k)];
+      x0[k] = v.x;
+      x1[k] = v.y;
+    }
+    nf_block<6, 1, false>(x0, r, T);
+    nf_block<6, 1, false>(x1, r, T);
+  }
+}
+
+// Canonical words of the slot-form rows (2 e + h) of element e: 32 bytes per store.
+__device__ __forceinline__ void np6_store_slots(const double (&x0)[8], const double (&x1)[8], u64* out, u64 eg,
+                                                u32 r, const NttDev& T) {
+  const double qd = T.qd, qinv = T.qinv;
+  u64* d0 = out + 2 * eg * 64 + 8 * r;
+#pragma unroll
+  for (u32 h = 0; h < 2; h++) {
+    const double* x = h ? x1 : x0;
+#pragma unroll
+    for (u32 c = 0; c < 2; c++)
+      st_v4_u64(d0 + h * 64 + 4 * c, fp_to_word(x[4 * c], qinv, qd), fp_to_word(x[4 * c + 1], qinv, qd),
+                fp_to_word(x[4 * c + 2], qinv, qd), fp_to_word(x[4 * c + 3], qinv, qd));
+  }
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(256) ntt_fp6_kernel(const u64* in, u64* out, u64 count, NttDev T, u64* mag_or) {
+  __shared__ double2 sm[NP6_EL * NP6_ROW];
+  const u32 el = threadIdx.x >> 3, r = threadIdx.x & 7;
+  const u64 eg = (u64)blockIdx.x * NP6_EL + el;
+  const bool active = eg < count;
+  const double qd = T.qd, qinv = T.qinv;
+  double x0[8], x1[8];
+  u64 mag = 0;
+  if (!INV) {
+    if (active) {
+      const u64* src = in + eg * 128;
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) {
+        const ulonglong2 v = __ldg((const ulonglong2*)(src + 2 * (r + 8 * k)));
+        if (mag_or) mag |= nr_mag(v.x, T.q) | nr_mag(v.y, T.q);
+        x0[k] = fp_from_word(v.x);
+        x1[k] = fp_from_word(v.y);
+      }
+    }
+    np6_forward(x0, x1, sm, el, r, active, T);
+    if (active) np6_store_slots(x0, x1, out, eg, r, T);
+  } else {
+    if (active) {
+      const u64* s0 = in + 2 * eg * 64 + 8 * r;
+#pragma unroll
+      for (u32 h = 0; h < 2; h++) {
+        double* x = h ? x1 : x0;
+#pragma unroll
+        for (u32 c = 0; c < 2; c++) {
+          u64 a, b, cc, dd;
+          ld_v4_u64(s0 + h * 64 + 4 * c, a, b, cc, dd);
+          x[4 * c] = fp_from_word(a);
+          x[4 * c + 1] = fp_from_word(b);
+          x[4 * c + 2] = fp_from_word(cc);
+          x[4 * c + 3] = fp_from_word(dd);
+        }
+      }
+      nf_block<6, 0, true>(x0, r, T);
+      nf_block<6, 0, true>(x1, r, T);
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) sm[np6_pos(el, 8 * r + k)] = make_double2(x0[k], x1[k]);
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) {
+        const double2 v = sm[np6_pos(el, r + 8 * k)];
+        x0[k] = v.x;
+        x1[k] = v.y;
+      }
+      nf_block<6, 1, true>(x0, 0, T);
+      nf_block<6, 1, true>(x1, 0, T);
+      u64* dst = out + eg * 128;
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) {
+        const u64 a = fp_to_word(fp_mulmod(x0[k], T.ninv_d, T.ninv_h, T.q2d), qinv, qd);
+        const u64 b = fp_to_word(fp_mulmod(x1[k], T.ninv_d, T.ninv_h, T.q2d), qinv, qd);
+        *(ulonglong2*)(dst + 2 * (r + 8 * k)) = make_ulonglong2(a, b);
+        if (mag_or) mag |= nr_mag(a, T.q) | nr_mag(b, T.q);
+      }
+    }
+  }
+  if (mag_or) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
+    if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
+  }
+}
+
+// The paired kernel's alignment needs: 16-byte interleaved side, 32-byte slot side.
+bool np6_aligned(const u64* in, const u64* out, bool inverse) {
+  const uintptr_t il = (uintptr_t)(inverse ? out : in), sl = (uintptr_t)(inverse ? in : out);
+  return il % 16 == 0 && sl % 32 == 0;
 }
 
 // FP: FP64 butterflies (q < 2^50, the nf_* code), else the integer ones.
@@ -1028,6 +1170,61 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ntt_digits_kernel<6, true, true> in the paired layout of ntt_fp6_kernel:
+// one thread per (digit ring element, column r) with both halves, so each
+// source load and each coefficient-form digit store moves a (half 0,
+// half 1) pair and the transform's output leaves in 32-byte stores.
+__global__ void __launch_bounds__(256)
+    ntt_digits6_kernel(NttSrcRows src, u64 width, u32 parts, const u64* bw_or, u64* rlog_out, u64* radix_out,
+                       u64* dc, u64* ds, u64 count, NttDev T, bool narrow) {
+  __shared__ double2 sm[NP6_EL * NP6_ROW];
+  const u32 el = threadIdx.x >> 3, r = threadIdx.x & 7;
+  const u64 re = (u64)blockIdx.x * NP6_EL + el;  // ring element of the digit space
+  const bool active = re < count;
+  const u64 q = T.q;
+  const u64 orv = *bw_or;
+  const u32 bw = orv ? 64u - (u32)__clzll((long long)orv) : 0u;
+  const u32 rlog = (bw + parts - 1) / parts;
+  const u64 mask = rlog >= 64 ? ~0ULL : ((1ULL << rlog) - 1);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *rlog_out = rlog;
+    if (radix_out) *radix_out = 1ULL << rlog;
+  }
+  const u32 c = (u32)(re % parts);
+  const u64 se = re / parts;
+  const u32 k = active ? (u32)(se / width) : 0;
+  const u64 i = se % width;
+  const u64 dring = ((u64)k * parts + c) * width + i;  // output ring element
+  const u32 sh = rlog * c;
+  double x0[8], x1[8];
+  if (active) {
+    const u64* sp = src.p[k] + i * 128;
+#pragma unroll
+    for (u32 kk = 0; kk < 8; kk++) {
+      const u32 e = r + 8 * kk;
+      const ulonglong2 v2 = __ldg((const ulonglong2*)(sp + 2 * e));
+      u64 dv[2];
+      long long dn[2];
+#pragma unroll
+      for (u32 h = 0; h < 2; h++) {
+        const u64 v = h ? v2.y : v2.x;
+        const u64 pos = 2 * v > q ? 0 : v, neg = 2 * v > q ? q - v : 0;
+        const u64 pd = sh >= 64 ? 0 : ((pos >> sh) & mask), nd = sh >= 64 ? 0 : ((neg >> sh) & mask);
+        dv[h] = pd >= nd ? pd - nd : pd + q - nd;
+        dn[h] = (long long)pd - (long long)nd;
+      }
+      x0[kk] = fp_from_word(dv[0]);
+      x1[kk] = fp_from_word(dv[1]);
+      if (narrow)
+        *(int2*)((int*)dc + dring * 128 + 2 * e) = make_int2((int)dn[0], (int)dn[1]);
+      else
+        *(ulonglong2*)(dc + dring * 128 + 2 * e) = make_ulonglong2(dv[0], dv[1]);
+    }
+  }
+  np6_forward(x0, x1, sm, el, r, active, T);
+  if (active) np6_store_slots(x0, x1, ds, dring, r, T);
+}
+
 // Fused negacyclic product r = a * b mod (Y^n + 1) for a batch of polynomials:
 // forward transforms of a and b, the pointwise product and the inverse
 // transform in one pass over a tile, so HBM sees a and b read once and r
@@ -1191,6 +1388,12 @@ int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomple
       kern<<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T, mag_or);
       return 0;
     };
+    if (LOGN == 6 && incomplete && np6_aligned(in, out, inverse)) {
+      const u64 count = units / 2, g6 = (count + NP6_EL - 1) / NP6_EL;
+      if (inverse) ntt_fp6_kernel<true><<<(unsigned)g6, 256, 0, st>>>(in, out, count, T, mag_or);
+      else ntt_fp6_kernel<false><<<(unsigned)g6, 256, 0, st>>>(in, out, count, T, mag_or);
+      return 0;
+    }
     if (incomplete) {
       if constexpr (UPT >= 2)
         return inverse ? gof(ntt_fp_kernel<LOGN, true, true>) : gof(ntt_fp_kernel<LOGN, true, false>);
@@ -1376,7 +1579,13 @@ int nd_launch(const NttSrcRows& src, u32 rows, u64 width, u32 parts, const u64* 
   // the forward incomplete transform's schedule decides the arithmetic
   const bool relax = T.q < NR_RELAX_Q;
   const bool fp = relax && ntt_choice(LOGN, true, false, false, units * (1ULL << LOGN) >= NTT_LARGE_COEFFS).fp64();
-  if (fp)
+  bool src16 = true;
+  for (u32 k = 0; k < rows && k < 16; k++) src16 = src16 && (uintptr_t)src.p[k] % 16 == 0;
+  if (fp && LOGN == 6 && (uintptr_t)ds % 32 == 0 && src16) {
+    const u64 count = units / 2;
+    ntt_digits6_kernel<<<(unsigned)((count + NP6_EL - 1) / NP6_EL), 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
+                                                                                   radix_out, dc, ds, count, T, narrow);
+  } else if (fp)
     ntt_digits_kernel<LOGN, true, true><<<(unsigned)blocks, 256, 0, st>>>(src, width, parts, bw_or, rlog_out,
                                                                            radix_out, dc, ds, units, T, narrow);
   else if (relax)

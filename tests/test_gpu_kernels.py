@@ -68,6 +68,47 @@ def test_ntt_unaligned_and_out_of_place(api, oracle, incomplete):
     assert np.array_equal(api.to_host(view), x)
 
 
+@pytest.mark.parametrize("offset", [0, 1, 2, 4])
+def test_ntt_d128_paired_layouts(api, oracle, gpu_lib, offset):
+    """d = 128 incomplete transforms with FP64 butterflies: 32-byte aligned
+    buffers take the paired-half kernel, 16-byte aligned ones the one-half
+    kernel, 8-byte aligned ones the generic kernel; all give the oracle's
+    words, in place and out of place, with partial last tiles."""
+    import ctypes
+    import torch
+    L = gpu_lib
+    q, d = P.Q0, 128
+    keys = [(6, 1, inv, 0, large) for inv in (0, 1) for large in (0, 1)]
+    saved = []
+    for k in keys:
+        v, c = ctypes.c_int(), ctypes.c_int()
+        assert L.salsaa_ntt_tune_get(*k, ctypes.byref(v), ctypes.byref(c)) == 0
+        saved.append((v.value, c.value))
+    try:
+        for k in keys:
+            assert L.salsaa_ntt_tune_set(*k, 1, 0) == 0
+        rng = np.random.default_rng(40 + offset)
+        for count in (1, 31, 33, 100):
+            x = rand_mod(rng, (count, d), q)
+            want = oracle.ring_to_slot(x, q)
+            big = torch.zeros(count * d + 8, dtype=torch.int64, device="cuda")
+            big[offset:offset + count * d] = api.to_dev(x).view(-1)
+            view = big[offset:offset + count * d].view(count, d)
+            obig = torch.zeros(count * d + 8, dtype=torch.int64, device="cuda")
+            out = obig[offset:offset + count * d].view(count, d)
+            api.ntt(view, d, q, incomplete=True, out=out)
+            assert np.array_equal(api.to_host(out), want), count
+            api.ntt(out, d, q, inverse=True, incomplete=True, out=view)
+            assert np.array_equal(api.to_host(view), x), count
+            api.ntt(view, d, q, incomplete=True)  # in place
+            assert np.array_equal(api.to_host(view), want), count
+            api.ntt(view, d, q, inverse=True, incomplete=True)
+            assert np.array_equal(api.to_host(view), x), count
+    finally:
+        for k, (v, c) in zip(keys, saved):
+            L.salsaa_ntt_tune_set(*k, v, c)
+
+
 def test_ntt_ragged_tiles(api, oracle):
     """Batch sizes that leave the last tile of 4096 coefficients partly empty."""
     q = P.Q0
