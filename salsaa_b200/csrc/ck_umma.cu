@@ -82,20 +82,26 @@ __global__ void __launch_bounds__(128) umma_selftest_kernel(const uint8_t* A, co
 //   D[(k,p,y)][(r,c,x)] = sum_i byte_y(W_k,p(i)) byte_x(T_r,c(i)),
 // and value = sum_{x,y} 2^(8(x+y)) D mod q.  The key bytes are laid out once
 // per context in the operand's shared-memory image (ck_tk8), so each
-// 128-element chunk of both slots' key tiles is one bulk copy.
+// 64-element chunk of both slots' key tiles is one bulk copy.
 //
-// CTA = (slot pair s0, s0 + 1; block of Bw elements).  Per 128-element chunk:
-// thread 0 bulk-copies the two key tiles, all 256 threads load the witness
-// pairs (one 16-byte load covers both slots), split them into byte planes in
-// shared memory, and thread 0 issues 2 x 4 MMAs (K = 32) into two TMEM
-// accumulators.  Two stages: the witness of chunk c + 1 is staged while the
-// MMAs of chunk c run.  Epilogue: each thread reads its TMEM lane (one
+// CTA = (slot pair s0, s0 + 1; block of Bw elements), warp-specialised per
+// 64-element chunk, with no CTA-wide barrier inside the loop: warps 0..13
+// load the witness pairs (one 16-byte load covers both slots) and split them
+// into byte planes in shared memory, then arrive on the stage's a_full
+// mbarrier; one thread of warp 14 bulk-copies the two key tiles as soon as
+// the MMAs that read the stage's previous keys complete (key_full); one
+// thread of warp 15 issues 2 x 2 MMAs (K = 32) into two TMEM accumulators
+// once both are full, and commits them to the stage's done mbarrier, which
+// frees the stage for the next witness and key copies.  Two stages.  Every
+// wait is bounded; a role that gives up stops its loop, and the others then
+// give up on the arrivals it no longer makes.  Epilogue: each thread reads its TMEM lane (one
 // witness byte row), folds the key bytes x, the block's 7 y-rows are folded
 // through shared memory, and the result is multiplied by the block's high
 // key factor and added into the accumulator as in the CUDA-core path.
 // ---------------------------------------------------------------------------
-constexpr u32 CKU_CHUNK = 128;  // elements per pipeline step (K of 4 MMAs)
+constexpr u32 CKU_CHUNK = 64;  // elements per pipeline step (K of 2 MMAs per slot)
 constexpr u32 CKU_THREADS = 512;
+constexpr u32 CKU_CONV = 448;  // witness-converting threads (warps 0..13); warps 14, 15 copy keys and issue MMAs
 constexpr u32 CKU_ATILE = 128 * CKU_CHUNK;  // witness byte tile of one slot
 
 __global__ void ck_tk8_kernel(const u64* tlo, u32 nck, u32 n, u32 bt, u32 nkp, bool packed, uint8_t* tk8) {
@@ -105,8 +111,8 @@ __global__ void ck_tk8_kernel(const u64* tlo, u32 nck, u32 n, u32 bt, u32 nkp, b
     u64 rest = t / 16;
     const u32 row = (u32)(rest % nkp);
     rest /= nkp;
-    const u32 j = (u32)(rest % 8);
-    rest /= 8;
+    const u32 j = (u32)(rest % (CKU_CHUNK / 16));
+    rest /= CKU_CHUNK / 16;
     const u32 s = (u32)(rest % n), cc = (u32)(rest / n);
     uint8_t v = 0;
     if (row < nck * 14) {
@@ -139,8 +145,8 @@ __device__ __forceinline__ void ck_umma_body(const uint8_t* __restrict__ tk8, co
                                              const ModQ& M, const u64* zeta, u64* acc, u32 acc_rows, u32 koff,
                                              bool plain, u32 by) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ uint64_t full_bar[2], done_bar[2];
-  __shared__ uint32_t tslot;
+  __shared__ uint64_t key_full[2], a_full[2], done_bar[2];
+  __shared__ uint32_t tslot, last_commit;
   const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const u32 s0 = 2 * blockIdx.x, d = 2 * n;
   // element blocks g < G of this CTA start at i0 + g bt: the same offsets in
@@ -162,9 +168,11 @@ __device__ __forceinline__ void ck_umma_body(const uint8_t* __restrict__ tk8, co
   }
   if (tid == 0) {
     for (int i = 0; i < 2; i++) {
-      umma::mbar_init(&full_bar[i], 1);
+      umma::mbar_init(&key_full[i], 1);
+      umma::mbar_init(&a_full[i], CKU_CONV);
       umma::mbar_init(&done_bar[i], 1);
     }
+    last_commit = 0xffffffffu;
     umma::mbar_fence_init();
   }
   // two accumulators of nkp columns: 2 x 128 columns when they fit, so two
@@ -175,81 +183,93 @@ __device__ __forceinline__ void ck_umma_body(const uint8_t* __restrict__ tk8, co
   __syncthreads();
   umma::fence_after_sync();
   const u32 tmem = tslot;
+  bool ok = true;
 
-  // witness task t: (i4lo, kp within a group of 8, kp group, i4hi); kp = (virtual row, part).
-  // A thread's three tasks are the same in every chunk: their source (chunk 0)
-  // and shared-memory offsets are computed once.
-  const u32 nkpw = 2 * vrows, kpb = (nkpw + 7) / 8;
-  uint4 wv[3][4];
-  const u64* tsrc[3];
-  u32 toff[3];
-  bool tval[3];
-#pragma unroll
-  for (u32 x = 0; x < 3; x++) {
-    const u32 t = tid + x * CKU_THREADS;
+  if (warp < CKU_CONV / 32) {
+    // witness task t: (i4lo, kp within a group of 8, kp group, i4hi); kp = (virtual row, part).
+    // One task per thread (2 CKU_CHUNK kpb <= 384 tasks), the same in every
+    // chunk: its source (chunk 0) and shared-memory offset are computed once.
+    // Four register buffers hold the loads of chunks c .. c + 3, so each
+    // thread keeps four chunks of witness loads in flight.
+    const u32 nkpw = 2 * vrows, kpb = (nkpw + 7) / 8;
+    const u32 t = tid;
     const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
     const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
-    tval[x] = t < 256 * kpb && kp < nkpw;
-    const u32 v = kp >> 1, part = kp & 1, k = tval[x] ? v % rows : 0, g = tval[x] ? v / rows : 0;
+    const bool tval = t < 2 * CKU_CHUNK * kpb && kp < nkpw;
+    const u32 v = kp >> 1, part = kp & 1, k = tval ? v % rows : 0, g = tval ? v / rows : 0;
     const u32 i4 = i4hi * 4 + i4lo;  // elements 4 * i4 .. + 3 of the chunk
-    tsrc[x] = w.p[k] + (i0 + (u64)g * bt + i4 * 4) * d + part * n + s0;
-    toff[x] = (i4 >> 2) * (128 * 16) + (kp * 7) * 16 + (i4 & 3) * 4;
-  }
-  auto fetch = [&](u32 c) {
+    const u64* tsrc = w.p[k] + (i0 + (u64)g * bt + i4 * 4) * d + part * n + s0;
+    const u32 toff = (i4 >> 2) * (128 * 16) + (kp * 7) * 16 + (i4 & 3) * 4;
+    uint4 wb[4][4];
+    auto fetch = [&](u32 c, uint4 (&wv)[4]) {
+      if (tval) {
+        const u64* src = tsrc + (u64)c * CKU_CHUNK * d;
 #pragma unroll
-    for (u32 x = 0; x < 3; x++)
-      if (tval[x]) {
-        const u64* src = tsrc[x] + (u64)c * CKU_CHUNK * d;
-#pragma unroll
-        for (u32 e = 0; e < 4; e++) wv[x][e] = __ldg((const uint4*)(src + (u64)e * d));
+        for (u32 e = 0; e < 4; e++) wv[e] = __ldg((const uint4*)(src + (u64)e * d));
       }
-  };
-  auto stash = [&](u32 st) {
-    uint8_t* A = smem + st * stage_bytes;
+    };
+    auto stash = [&](u32 st, const uint4 (&wv)[4]) {
+      if (!tval) return;
+      uint8_t* A = smem + st * stage_bytes;
+      // byte plane b of the four elements: a 4 x 4 byte transpose of their
+      // low words (planes 0..3) and high words (planes 4..6)
 #pragma unroll
-    for (u32 x = 0; x < 3; x++)
-      if (tval[x]) {
-        const u32 off = toff[x];
-        // byte plane b of the four elements: a 4 x 4 byte transpose of their
-        // low words (planes 0..3) and high words (planes 4..6)
+      for (u32 sg = 0; sg < 2; sg++) {
+        u32 lo[4], hi[4], p[8];
 #pragma unroll
-        for (u32 sg = 0; sg < 2; sg++) {
-          u32 lo[4], hi[4], p[8];
-#pragma unroll
-          for (u32 e = 0; e < 4; e++) {
-            lo[e] = sg ? wv[x][e].z : wv[x][e].x;
-            hi[e] = sg ? wv[x][e].w : wv[x][e].y;
-          }
-          transpose4x4(lo[0], lo[1], lo[2], lo[3], p[0], p[1], p[2], p[3]);
-          transpose4x4(hi[0], hi[1], hi[2], hi[3], p[4], p[5], p[6], p[7]);
-#pragma unroll
-          for (u32 b = 0; b < 7; b++) *(u32*)(A + sg * CKU_ATILE + off + b * 16) = p[b];
+        for (u32 e = 0; e < 4; e++) {
+          lo[e] = sg ? wv[e].z : wv[e].x;
+          hi[e] = sg ? wv[e].w : wv[e].y;
         }
+        transpose4x4(lo[0], lo[1], lo[2], lo[3], p[0], p[1], p[2], p[3]);
+        transpose4x4(hi[0], hi[1], hi[2], hi[3], p[4], p[5], p[6], p[7]);
+#pragma unroll
+        for (u32 b = 0; b < 7; b++) *(u32*)(A + sg * CKU_ATILE + toff + b * 16) = p[b];
       }
-  };
-
-  const u32 idesc = umma::idesc_u8(128, nkp);
-  bool ok = true;
-  auto copy_keys = [&](u32 c) {  // thread 0: both slots' key tiles of chunk c into stage c & 1
-    const u32 sn = c & 1;
-    umma::mbar_expect_tx(&full_bar[sn], 2 * btile);
-    umma::bulk_g2s(smem + sn * stage_bytes + 2 * CKU_ATILE, tk8 + ((u64)(cc0 + c) * n + s0) * btile, 2 * btile,
-                   &full_bar[sn]);
-  };
-  if (tid == 0) copy_keys(0);
-  fetch(0);
-  for (u32 c = 0; c < nchunks; c++) {
-    const u32 st = c & 1;
-    uint8_t* stage = smem + st * stage_bytes;
-    if (c >= 2) ok &= umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1);
-    stash(st);
-    if (c + 1 < nchunks) fetch(c + 1);
-    umma::fence_proxy_async();
-    umma::fence_before_sync();
-    __syncthreads();
-    if (tid == 0) {
+    };
+    // chunk c: stage c & 1 (last read by the MMAs of chunk c - 2), loads in
+    // buffer c & 3, refilled with chunk c + 4 once stashed
+    auto step = [&](u32 c, uint4 (&wv)[4]) -> bool {
+      const u32 st = c & 1;
+      if (c >= 2 && !umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1)) return false;
+      stash(st, wv);
+      if (c + 4 < nchunks) fetch(c + 4, wv);
+      umma::fence_proxy_async();
+      umma::mbar_arrive(&a_full[st]);
+      return true;
+    };
+#pragma unroll
+    for (u32 b = 0; b < 4; b++)
+      if (b < nchunks) fetch(b, wb[b]);
+    for (u32 c = 0; c < nchunks; c += 4) {
+      if (!(ok = step(c, wb[0]))) break;
+      if (c + 1 < nchunks && !(ok = step(c + 1, wb[1]))) break;
+      if (c + 2 < nchunks && !(ok = step(c + 2, wb[2]))) break;
+      if (c + 3 < nchunks && !(ok = step(c + 3, wb[3]))) break;
+    }
+  } else if (warp == CKU_CONV / 32 && lane == 0) {
+    // key tiles of both slots, one bulk copy per chunk, into the stage freed
+    // by the MMAs of chunk c - 2
+    u32 issued = 0;
+    for (u32 c = 0; c < nchunks; c++) {
+      const u32 st = c & 1;
+      if (c >= 2 && !(ok = umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 4))) break;
+      umma::mbar_expect_tx(&key_full[st], 2 * btile);
+      umma::bulk_g2s(smem + st * stage_bytes + 2 * CKU_ATILE, tk8 + ((u64)(cc0 + c) * n + s0) * btile, 2 * btile,
+                     &key_full[st]);
+      issued = c + 1;
+    }
+    // the copies still in flight (the last one of each stage) land before the CTA moves on
+    for (u32 c = issued >= 2 ? issued - 2 : 0; c < issued; c++)
+      umma::mbar_wait(&key_full[c & 1], (c >> 1) & 1, err, 5);
+  } else if (warp == CKU_CONV / 32 + 1 && lane == 0) {
+    const u32 idesc = umma::idesc_u8(128, nkp);
+    for (u32 c = 0; c < nchunks; c++) {
+      const u32 st = c & 1;
+      uint8_t* stage = smem + st * stage_bytes;
+      if (!(ok = umma::mbar_wait(&a_full[st], (c >> 1) & 1, err, 2))) break;
+      if (!(ok = umma::mbar_wait(&key_full[st], (c >> 1) & 1, err, 2))) break;
       umma::fence_after_sync();
-      ok &= umma::mbar_wait(&full_bar[st], (c >> 1) & 1, err, 2);
 #pragma unroll
       for (u32 sg = 0; sg < 2; sg++)
 #pragma unroll
@@ -261,17 +281,14 @@ __device__ __forceinline__ void ck_umma_body(const uint8_t* __restrict__ tk8, co
           umma::mma_i8(tmem + sg * cs, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
         }
       umma::commit(&done_bar[st]);
-      // key tiles of the next chunk: its stage was last read by the MMAs of
-      // chunk c - 1, which complete before those just issued
-      if (c + 1 < nchunks) {
-        const u32 sn = (c + 1) & 1;
-        if (c >= 1) ok &= umma::mbar_wait(&done_bar[sn], ((c - 1) >> 1) & 1, err, 4);
-        copy_keys(c + 1);
-      }
+      last_commit = c;
     }
   }
-  // all MMAs done (the last commit covers every earlier MMA of thread 0)
-  ok &= umma::mbar_wait(&done_bar[(nchunks - 1) & 1], ((nchunks - 1) >> 1) & 1, err, 3);
+  // all MMAs done (the last commit covers every earlier MMA of its thread)
+  __syncthreads();
+  const u32 lc = last_commit;
+  if (lc != 0xffffffffu) ok &= umma::mbar_wait(&done_bar[lc & 1], (lc >> 1) & 1, err, 3);
+  ok &= lc == nchunks - 1;
   ok = __syncthreads_and(ok);
   umma::fence_after_sync();
 
@@ -382,6 +399,15 @@ int launch_ck_tk8(const u64* tlo, u32 nck, u32 n, u32 bt, bool packed, uint8_t* 
   return e == cudaSuccess ? 0 : salsaa_set_cuda_error(e, "ck_tk8");
 }
 
+// The smallest shared-memory carveout (percent of the SM's 228 KiB) that
+// holds one CTA's stages plus its static barriers: the rest stays L1, which
+// holds the witness loads in flight (one 16-byte load per 32-byte sector).
+static int ck_carveout(size_t smem) {
+  const size_t need = smem + 2048;
+  const size_t pct = (need * 100 + 228 * 1024 - 1) / (228 * 1024);
+  return pct > 100 ? 100 : (int)pct;
+}
+
 bool ck_umma_ok(const CommitArgs& a, u32 n) {
   if (!a.tk8 || a.rows == 0 || a.rows > CKU_MAX_WROWS || a.nck == 0 || a.nck > CKU_MAX_KEYS || (n & 1)) return false;
   if (a.width < CKU_CHUNK || a.ck_bt < CKU_CHUNK) return false;
@@ -442,6 +468,8 @@ int launch_ck_umma_multi(const CommitArgs* a, u32 ninst, u32 n, const ModQ& M, c
   const size_t smem = 2 * stage > epi ? 2 * stage : epi;
   cudaError_t e =
       cudaFuncSetAttribute(ck_umma_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ck_umma_multi_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, ck_carveout(smem));
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ck_umma_multi smem attribute");
   const int tr = salsaa_trace_begin("ck_umma_kernel", st, wit_bytes + out_bytes);
   salsaa_trace_alias(tr, "ck_umma_kernel:int8", ops);
@@ -464,6 +492,8 @@ int launch_ck_umma(const CommitArgs& a, u32 n, u32 Bw, u32 G, const ModQ& M, con
   const size_t epi = 2 * 128 * (size_t)(2 * a.nck) * sizeof(u64);
   const size_t smem = 2 * stage > epi ? 2 * stage : epi;
   cudaError_t e = cudaFuncSetAttribute(ck_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ck_umma_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, ck_carveout(smem));
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "ck_umma smem attribute");
   dim3 g(n / 2, (unsigned)(a.width / Bw / G));
   // Traced measures of one launch: algorithmic HBM bytes (the slot-form

@@ -109,6 +109,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// Plain arrival (release at CTA scope) on an mbarrier.
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
 // Bounded wait for the phase with the given parity; false (and *err set) on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t* err, uint32_t code) {
   for (uint32_t i = 0; i < SPIN_LIMIT; i++)
