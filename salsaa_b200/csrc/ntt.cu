@@ -370,47 +370,51 @@ struct NrCtx {
   u64 q, q2;
 };
 
+// Butterflies of phase P on one mini-block v[0 .. 2^S) with block index blk.
 template <int LOGN, int P, bool INV, bool RELAX>
-__device__ __forceinline__ void nr_compute(u64 (&x)[16], u32 tu, const NttDev& T, u64 q, u64 q2) {
+__device__ __forceinline__ void nr_block(u64* v, u32 blk, const NttDev& T, u64 q, u64 q2) {
   // inverse difference offset: 2q, or 2^LOGN q when sums are left unreduced
   const u64 cdiff = RELAX ? (q << LOGN) : q2;
   constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
-  constexpr u32 N = 1u << LOGN, TPU = N / 16, MB = 16 >> S, K = 1u << S;
-  constexpr u32 LSTR = INV ? G0 : LOGN - G0 - S;  // log2(stride)
+  constexpr u32 N = 1u << LOGN, K = 1u << S;
+  // pairs p < 2^(S-1) of level l: k = (sb << (l'+1)) + kk, one twiddle per sb
 #pragma unroll
-  for (u32 j = 0; j < MB; j++) {
-    const u32 mb = tu + j * TPU, blk = mb >> LSTR;
-    u64* v = x + j * (1u << S);
-    // pairs p < 2^(S-1) of level l: k = (sb << (l'+1)) + kk, one twiddle per sb
+  for (int l = 0; l < S; l++) {
+    const u32 lt = INV ? l : S - 1 - l;  // log2 of the pair distance in k
+    const u32 t = 1u << lt;
+    u64 w = 0, wp = 0;
 #pragma unroll
-    for (int l = 0; l < S; l++) {
-      const u32 lt = INV ? l : S - 1 - l;  // log2 of the pair distance in k
-      const u32 t = 1u << lt;
-      u64 w = 0, wp = 0;
-#pragma unroll
-      for (u32 p = 0; p < K / 2; p++) {
-        const u32 sb = p >> lt, kk = p & (t - 1), k = (sb << (lt + 1)) + kk;
-        if (kk == 0) {
-          const u32 idx = INV ? (N >> (G0 + l + 1)) + (blk << (S - l - 1)) + sb : (1u << (G0 + l)) + (blk << l) + sb;
-          w = __ldg((INV ? T.inv : T.fwd) + idx);
-          wp = __ldg((INV ? T.invp : T.fwdp) + idx);
-        }
-        if (!INV) {
-          u64 a = v[k];
-          if (!RELAX) a = a >= q2 ? a - q2 : a;
-          const u64 b = shoup_lazy(v[k + t], w, wp, q);
-          v[k] = a + b;
-          v[k + t] = a - b + q2;
-        } else {
-          const u64 a = v[k], b = v[k + t];
-          u64 s2 = a + b;
-          if (!RELAX) s2 = s2 >= q2 ? s2 - q2 : s2;
-          v[k] = s2;
-          v[k + t] = shoup_lazy(a - b + cdiff, w, wp, q);
-        }
+    for (u32 p = 0; p < K / 2; p++) {
+      const u32 sb = p >> lt, kk = p & (t - 1), k = (sb << (lt + 1)) + kk;
+      if (kk == 0) {
+        const u32 idx = INV ? (N >> (G0 + l + 1)) + (blk << (S - l - 1)) + sb : (1u << (G0 + l)) + (blk << l) + sb;
+        w = __ldg((INV ? T.inv : T.fwd) + idx);
+        wp = __ldg((INV ? T.invp : T.fwdp) + idx);
+      }
+      if (!INV) {
+        u64 a = v[k];
+        if (!RELAX) a = a >= q2 ? a - q2 : a;
+        const u64 b = shoup_lazy(v[k + t], w, wp, q);
+        v[k] = a + b;
+        v[k + t] = a - b + q2;
+      } else {
+        const u64 a = v[k], b = v[k + t];
+        u64 s2 = a + b;
+        if (!RELAX) s2 = s2 >= q2 ? s2 - q2 : s2;
+        v[k] = s2;
+        v[k + t] = shoup_lazy(a - b + cdiff, w, wp, q);
       }
     }
   }
+}
+
+template <int LOGN, int P, bool INV, bool RELAX>
+__device__ __forceinline__ void nr_compute(u64 (&x)[16], u32 tu, const NttDev& T, u64 q, u64 q2) {
+  constexpr int S = ph_size(LOGN, P), G0 = ph_start(LOGN, P);
+  constexpr u32 N = 1u << LOGN, TPU = N / 16, MB = 16 >> S;
+  constexpr u32 LSTR = INV ? G0 : LOGN - G0 - S;  // log2(stride)
+#pragma unroll
+  for (u32 j = 0; j < MB; j++) nr_block<LOGN, P, INV, RELAX>(x + j * (1u << S), (tu + j * TPU) >> LSTR, T, q, q2);
 }
 
 // element index (within its unit) of register (j, k) in phase P
@@ -930,6 +934,104 @@ __global__ void __launch_bounds__(256) ntt_fp6_kernel(const u64* in, u64* out, u
   }
 }
 
+// Full (not incomplete) 64-point transforms with integer butterflies in the
+// same paired layout: a thread holds column r of two neighbouring
+// polynomials (x0: polynomial 2 p, x1: 2 p + 1), the exchange tile holds
+// (x0, x1) pairs, and the contiguous side (forward output, inverse input)
+// moves 32 bytes per lane.  Same butterflies and words as
+// ntt_reg_kernel<6, false, INV, RELAX>.
+template <bool INV, bool RELAX>
+__global__ void __launch_bounds__(256) ntt_int6_kernel(const u64* in, u64* out, u64 units, NttDev T, u64* mag_or) {
+  __shared__ ulonglong2 sm[NP6_EL * NP6_ROW];
+  const u32 el = threadIdx.x >> 3, r = threadIdx.x & 7;
+  const u64 u0 = 2 * ((u64)blockIdx.x * NP6_EL + el);
+  const bool a0 = u0 < units, a1 = u0 + 1 < units;
+  const u64 q = T.q, q2 = 2 * T.q;
+  u64 x0[8], x1[8];
+  u64 mag = 0;
+#pragma unroll
+  for (u32 k = 0; k < 8; k++) x0[k] = x1[k] = 0;
+  if (!INV) {
+#pragma unroll
+    for (u32 k = 0; k < 8; k++) {
+      if (a0) x0[k] = __ldg(in + u0 * 64 + r + 8 * k);
+      if (a1) x1[k] = __ldg(in + (u0 + 1) * 64 + r + 8 * k);
+      if (mag_or) mag |= (a0 ? nr_mag(x0[k], q) : 0) | (a1 ? nr_mag(x1[k], q) : 0);
+    }
+    if (a0) {
+      nr_block<6, 0, false, RELAX>(x0, 0, T, q, q2);
+      nr_block<6, 0, false, RELAX>(x1, 0, T, q, q2);
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) sm[np6_pos(el, r + 8 * k)] = make_ulonglong2(x0[k], x1[k]);
+    }
+    __syncthreads();
+    if (a0) {
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) {
+        const ulonglong2 v = sm[np6_pos(el, 8 * r + k)];
+        x0[k] = v.x;
+        x1[k] = v.y;
+      }
+      nr_block<6, 1, false, RELAX>(x0, r, T, q, q2);
+      nr_block<6, 1, false, RELAX>(x1, r, T, q, q2);
+#pragma unroll
+      for (u32 h = 0; h < 2; h++) {
+        if (h && !a1) break;
+        const u64* x = h ? x1 : x0;
+        u64* dst = out + (u0 + h) * 64 + 8 * r;
+#pragma unroll
+        for (u32 c = 0; c < 2; c++)
+          st_v4_u64(dst + 4 * c, nr_canon<RELAX>(x[4 * c], q, q2, T.onep), nr_canon<RELAX>(x[4 * c + 1], q, q2, T.onep),
+                    nr_canon<RELAX>(x[4 * c + 2], q, q2, T.onep), nr_canon<RELAX>(x[4 * c + 3], q, q2, T.onep));
+      }
+    }
+  } else {
+    if (a0) {
+#pragma unroll
+      for (u32 h = 0; h < 2; h++) {
+        if (h && !a1) break;
+        u64* x = h ? x1 : x0;
+        const u64* src = in + (u0 + h) * 64 + 8 * r;
+#pragma unroll
+        for (u32 c = 0; c < 2; c++) ld_v4_u64(src + 4 * c, x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
+      }
+      nr_block<6, 0, true, RELAX>(x0, r, T, q, q2);
+      nr_block<6, 0, true, RELAX>(x1, r, T, q, q2);
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) sm[np6_pos(el, 8 * r + k)] = make_ulonglong2(x0[k], x1[k]);
+    }
+    __syncthreads();
+    if (a0) {
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) {
+        const ulonglong2 v = sm[np6_pos(el, r + 8 * k)];
+        x0[k] = v.x;
+        x1[k] = v.y;
+      }
+      nr_block<6, 1, true, RELAX>(x0, 0, T, q, q2);
+      nr_block<6, 1, true, RELAX>(x1, 0, T, q, q2);
+#pragma unroll
+      for (u32 k = 0; k < 8; k++) {
+        u64 v0 = shoup_lazy(x0[k], T.ninv, T.ninvp, q);
+        v0 = v0 >= q ? v0 - q : v0;
+        out[u0 * 64 + r + 8 * k] = v0;
+        if (mag_or) mag |= nr_mag(v0, q);
+        if (a1) {
+          u64 v1 = shoup_lazy(x1[k], T.ninv, T.ninvp, q);
+          v1 = v1 >= q ? v1 - q : v1;
+          out[(u0 + 1) * 64 + r + 8 * k] = v1;
+          if (mag_or) mag |= nr_mag(v1, q);
+        }
+      }
+    }
+  }
+  if (mag_or) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mag |= __shfl_xor_sync(0xffffffffu, mag, o);
+    if ((threadIdx.x & 31) == 0 && mag) atomicOr((unsigned long long*)mag_or, (unsigned long long)mag);
+  }
+}
+
 // The paired kernel's alignment needs: 16-byte interleaved side, 32-byte slot side.
 bool np6_aligned(const u64* in, const u64* out, bool inverse) {
   const uintptr_t il = (uintptr_t)(inverse ? out : in), sl = (uintptr_t)(inverse ? in : out);
@@ -1422,6 +1524,18 @@ int nr_launch(const u64* in, u64* out, u64 units, const NttDev& T, bool incomple
     kern<<<(unsigned)blocks, 256, 0, st>>>(in, out, units, T, mag_or);
     return 0;
   };
+  // full 64-point transforms: the paired layout when the contiguous side is 32-byte aligned
+  if (LOGN == 6 && !incomplete && (uintptr_t)(inverse ? in : out) % 32 == 0) {
+    const unsigned g6 = (unsigned)((units + 2 * NP6_EL - 1) / (2 * NP6_EL));
+    if (inverse) {
+      if (relax) ntt_int6_kernel<true, true><<<g6, 256, 0, st>>>(in, out, units, T, mag_or);
+      else ntt_int6_kernel<true, false><<<g6, 256, 0, st>>>(in, out, units, T, mag_or);
+    } else {
+      if (relax) ntt_int6_kernel<false, true><<<g6, 256, 0, st>>>(in, out, units, T, mag_or);
+      else ntt_int6_kernel<false, false><<<g6, 256, 0, st>>>(in, out, units, T, mag_or);
+    }
+    return 0;
+  }
   if (incomplete) {
     if constexpr (UPT >= 2) {
       if (inverse)

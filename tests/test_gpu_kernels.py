@@ -109,6 +109,33 @@ def test_ntt_d128_paired_layouts(api, oracle, gpu_lib, offset):
             L.salsaa_ntt_tune_set(*k, v, c)
 
 
+@pytest.mark.parametrize("offset", [0, 1, 2, 4])
+@pytest.mark.parametrize("q", [P.Q62, P.Q0])
+def test_ntt_n64_paired_layouts(api, oracle, offset, q):
+    """Full 64-point transforms: 32-byte aligned buffers take the paired
+    kernel (two polynomials per thread), others the one-polynomial kernel;
+    both give the oracle's words, with odd counts and partial last tiles."""
+    import torch
+    n = 64
+    rng = np.random.default_rng(60 + offset)
+    for count in (1, 63, 64, 65, 129):
+        x = rand_mod(rng, (count, n), q)
+        want = oracle.ntt_forward(x, q)
+        big = torch.zeros(count * n + 8, dtype=torch.int64, device="cuda")
+        big[offset:offset + count * n] = api.to_dev(x).view(-1)
+        view = big[offset:offset + count * n].view(count, n)
+        obig = torch.zeros(count * n + 8, dtype=torch.int64, device="cuda")
+        out = obig[offset:offset + count * n].view(count, n)
+        api.ntt(view, n, q, out=out)
+        assert np.array_equal(api.to_host(out), want), count
+        api.ntt(out, n, q, inverse=True, out=view)
+        assert np.array_equal(api.to_host(view), x), count
+        api.ntt(view, n, q)  # in place
+        assert np.array_equal(api.to_host(view), want), count
+        api.ntt(view, n, q, inverse=True)
+        assert np.array_equal(api.to_host(view), x), count
+
+
 def test_ntt_ragged_tiles(api, oracle):
     """Batch sizes that leave the last tile of 4096 coefficients partly empty."""
     q = P.Q0
