@@ -56,12 +56,15 @@ def test_mixed_stream_equals_alone(api, oracle, cuda, max_inflight):
         got = api.to_host(buf).view(np.uint8)
         assert np.array_equal(got, alone[nm].prove(seed)), (nm, seed)
         assert lat[t][0] >= lat[t][1] >= 0
-    # one of each verifies with the reference checks
+    # one of each verifies with the reference checks and equals the oracle's proof byte for byte
     for nm in names:
         nm_jobs = [(s, b) for (n2, s, b, _) in jobs if n2 == nm]
         if nm_jobs:
             s, b = nm_jobs[0]
-            assert oracle.verify(MIX[nm], 7, s, api.to_host(b).view(np.uint8)) == 0
+            got = api.to_host(b).view(np.uint8)
+            assert oracle.verify(MIX[nm], 7, s, got) == 0
+            rc, want, _ = oracle.prove(MIX[nm], 7, s)
+            assert rc == 0 and np.array_equal(got, want), nm
     srv.close()
 
 

@@ -2,7 +2,7 @@
 device memory on the call path (for example a serving loop that has already
 divided HBM among in-flight proofs).  Its output must equal the allocating
 entry point's, bit for bit, on consecutive calls that reuse the library's
-fixed scratch array.  Collected last so a run that stops at the first failure
+fixed scratch array, and the oracle's projection.  Collected last so a run that stops at the first failure
 has already run every other test."""
 import ctypes
 
@@ -19,7 +19,8 @@ def _call(fn, w, rows, width, d, q, seed, rnd, out, stream):
     return fn(ctypes.c_void_p(w.data_ptr()), rows, width, d, q, seed, rnd, ctypes.c_void_p(out.data_ptr()), stream)
 
 
-def test_noalloc_matches_allocating_entry(gpu_lib, cuda):
+def test_noalloc_matches_allocating_entry(gpu_lib, cuda, oracle):
+    from helpers import proj_challenge
     from salsaa_b200 import api
     torch = cuda
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -36,6 +37,9 @@ def test_noalloc_matches_allocating_entry(gpu_lib, cuda):
             gpu_lib.salsaa_last_error()
         torch.cuda.synchronize()
         assert torch.equal(ref, got)
+        iz, sg = proj_challenge(seed, rnd, rows * 256)  # and the oracle's projection, word for word
+        want = oracle.project(small_signed(np.random.default_rng(seed), (rows, width, d), bound, q), q, iz, sg)
+        assert np.array_equal(api.to_host(got), want)
 
 
 @pytest.mark.parametrize("rows,width,d,msg", [
