@@ -950,7 +950,7 @@ __device__ __forceinline__ u64 ng_challenge(const DevState* ds, u32 round, u32 r
 
 __global__ void __launch_bounds__(256, 2)
     nc_gram_kernel(RowSet w, u32 rows, u64 ng, u32 ntiles, ModQ M, const DevState* ds, u32 round, u64* out,
-                   u64 sout, u64* gram, u32* flag, bool plain) {
+                   u64 sout, u64* gram, u32* flag, bool plain, u64 w32p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ uint64_t done_bar[2];
   __shared__ uint32_t tslot;
@@ -1000,7 +1000,7 @@ __global__ void __launch_bounds__(256, 2)
                       ((128u >> 4) << 24);
   // s8 (limbs) x u8 (mu bytes), both K-major, M = 128, N = 16
   const u32 id_fold = (2u << 4) | (1u << 7) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
-  const u64 w32 = ((u64)1 << 32) % q, w32p = (u64)(((unsigned __int128)w32 << 64) / q);
+  const u64 w32 = ((u64)1 << 32) % q;  // its Shoup companion w32p comes from the host (a 128-bit division)
   bool bad = false, ok = true;
 
   // loads of this thread: 4 consecutive groups g0 .. g0 + 3 (g0 = 4 (tid % 64))
@@ -1235,8 +1235,9 @@ int launch_nc_gram(const RowSet& w, u32 rows, u64 nlen, const ModQ& M, const Dev
   u32* flag = (u32*)(gram + (u64)rows * 256);
   const bool gplain = plain && nb < (1u << 13);
   const int tr = salsaa_trace_begin("nc_gram_kernel", st, (double)rows * nlen * 8.0 * (1.0 + 2.0 / 16.0));
+  const u64 w32p = (u64)(((unsigned __int128)(((u64)1 << 32) % M.q) << 64) / M.q);
   nc_gram_kernel<<<dim3((unsigned)nb, rows), 256, NG_SMEM, st>>>(w, rows, ng, ntiles, M, ds, round, out, sout, gram,
-                                                                 flag, gplain);
+                                                                 flag, gplain, w32p);
   salsaa_trace_end(tr, st);
   salsaa_count_launch();
   e = cudaGetLastError();

@@ -204,7 +204,12 @@ int launch_pointwise_mul(u64* r, const u64* b, u64 n, u64 q, cudaStream_t st) {
 // sums[((rep * nr + j) * rows + k) * 3 + {0,1,2}] hold S00, S01, S11.
 // ---------------------------------------------------------------------------
 constexpr u32 SC_T = 4;          // rounds per streaming pass
-constexpr u32 SC_TAIL = 16384;   // vectors this short finish in one CTA
+constexpr u32 SC_TAIL = 16384;   // vectors this short finish in one CTA (batched sumchecks)
+// A single sumcheck streams four-round passes over many CTAs while the vector
+// is longer than this and the pass leaves at least d values (norm_check_3's
+// vector is captured at length d by the tail); the tail then finishes in one
+// CTA per (repetition, row).
+constexpr u32 SC_TAIL_ONE = 2048;
 
 // Lazy sums: with q < 2^50 each product is < 2^100 and a thread's sum of
 // far fewer than 2^27 products fits in 128 bits.
@@ -275,6 +280,26 @@ __device__ __forceinline__ u64 block_totals(const ModQ& M, ScAcc<LAZY> (&v)[NV],
   return r;
 }
 
+// Round challenges t < T (chal(t)) and their Shoup companions, computed by
+// threads 0 .. T-1 into shared memory sch[2T] and read by every thread: the
+// companion is a 128-bit division, far too costly to repeat in every thread.
+// Every thread of the CTA calls it; sch must not be read by a previous use
+// after this call starts (the callers' block reductions in between order it).
+template <u32 T, typename F>
+__device__ __forceinline__ void shared_challenges(u64* sch, F chal, u64 q, u64 (&c)[T], u64 (&cp)[T]) {
+  if (threadIdx.x < T) {
+    const u64 v = chal(threadIdx.x);
+    sch[threadIdx.x] = v;
+    sch[T + threadIdx.x] = (u64)((((unsigned __int128)v) << 64) / q);
+  }
+  __syncthreads();
+#pragma unroll
+  for (u32 t = 0; t < T; t++) {
+    c[t] = sch[t];
+    cp[t] = sch[T + t];
+  }
+}
+
 __device__ __forceinline__ u64 fold1(u64 a, u64 b, u64 c, u64 cp, u64 q) {
   return add_mod(a, mul_shoup(sub_mod(b, a, q), c, cp, q), q);
 }
@@ -316,12 +341,9 @@ __global__ void __launch_bounds__(256, 2) sc_first_kernel(RowSet w, u32 rows, u6
   const u64* x = w.p[k];
   const bool nar = (w.narrow >> k) & 1;
   const u64 q = M.q, ng = nlen / G;
+  __shared__ u64 sch[2 * T];
   u64 c[T], cp[T];
-#pragma unroll
-  for (u32 t = 0; t < T; t++) {
-    c[t] = nc_challenge(ds, round, rep, t, q);
-    cp[t] = shoup_dev(c[t], q);
-  }
+  shared_challenges<T>(sch, [&](u32 t) { return nc_challenge(ds, round, rep, t, q); }, q, c, cp);
   ScAcc<LAZY> acc[T][3];  // acc[0] = round 0, only kept by the rep-0 CTAs
 #pragma unroll
   for (u32 t = 0; t < T; t++)
@@ -358,12 +380,9 @@ __global__ void __launch_bounds__(256) sc_round_kernel(const u64* in, u64 sin, u
   const u64 q = M.q, ng = L / G;
   const u64* x = in + (u64)pair * sin;
   u64* y = out + (u64)pair * sout;
+  __shared__ u64 sch[2 * T];
   u64 c[T], cp[T];
-#pragma unroll
-  for (u32 t = 0; t < T; t++) {
-    c[t] = nc_challenge(ds, round, rep, j + t, q);
-    cp[t] = shoup_dev(c[t], q);
-  }
+  shared_challenges<T>(sch, [&](u32 t) { return nc_challenge(ds, round, rep, j + t, q); }, q, c, cp);
   ScAcc<LAZY> acc[T][3];
 #pragma unroll
   for (u32 t = 0; t < T; t++)
@@ -388,22 +407,19 @@ __global__ void __launch_bounds__(256) sc_round_kernel(const u64* in, u64 sin, u
   }
 }
 
-// One CTA per (rep,row) finishes rounds j0.. from v_{j0} (length L <= SC_TAIL),
+// One CTA per (rep,row) finishes rounds j0.. from v_{j0} (length L: at most
+// SC_TAIL_ONE, or 16 d when norm_check_3's vector is longer),
 // reading either a per-pair buffer or (j0 = 0) the witness row itself.
 // T rounds of the tail on the vector v (length cur, shared memory): groups of
 // 2^T values v[g + m ng] per thread, sums of all T rounds in one block
 // reduction, folded values back to v[g] (only thread g touches v[g]).
 template <bool LAZY, u32 T>
 __device__ __forceinline__ void tail_step(u64* v, u64 cur, const ModQ& M, const DevState* ds, u32 round, u32 rep,
-                                          u32 j, u64* sums, u32 nr, u32 rows, u32 k, Sum128* red) {
+                                          u32 j, u64* sums, u32 nr, u32 rows, u32 k, Sum128* red, u64* sch) {
   constexpr u32 G = 1u << T;
   const u64 q = M.q, ng = cur >> T;
   u64 c[T], cp[T];
-#pragma unroll
-  for (u32 t = 0; t < T; t++) {
-    c[t] = nc_challenge(ds, round, rep, j + t, q);
-    cp[t] = shoup_dev(c[t], q);
-  }
+  shared_challenges<T>(sch, [&](u32 t) { return nc_challenge(ds, round, rep, j + t, q); }, q, c, cp);
   ScAcc<LAZY> acc[T][3];
 #pragma unroll
   for (u32 t = 0; t < T; t++)
@@ -431,6 +447,7 @@ __global__ void __launch_bounds__(512) sc_tail_kernel(const u64* in, u64 sin, Ro
                                                        u32 d, u64* cap) {
   extern __shared__ u64 v[];
   __shared__ Sum128 red[SC_T * 3 * 32];
+  __shared__ u64 sch[2 * SC_T];
   const u32 pair = blockIdx.x, rep = pair / rows, k = pair % rows;
   const u64* x = (j0 == 0) ? w0.p[k] : in + (u64)pair * sin;
   const bool nar = j0 == 0 && ((w0.narrow >> k) & 1);
@@ -451,10 +468,10 @@ __global__ void __launch_bounds__(512) sc_tail_kernel(const u64* in, u64 sin, Ro
     }
     T = T < SC_T ? T : SC_T;
     switch (T) {
-      case 4: tail_step<LAZY, 4>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red); break;
-      case 3: tail_step<LAZY, 3>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red); break;
-      case 2: tail_step<LAZY, 2>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red); break;
-      default: tail_step<LAZY, 1>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red); break;
+      case 4: tail_step<LAZY, 4>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red, sch); break;
+      case 3: tail_step<LAZY, 3>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red, sch); break;
+      case 2: tail_step<LAZY, 2>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red, sch); break;
+      default: tail_step<LAZY, 1>(v, cur, M, ds, round, rep, j, sums, nr, rows, k, red, sch); break;
     }
     cur >>= T;
     j += T;
@@ -490,6 +507,7 @@ __global__ void __launch_bounds__(256, 2) sb_pass_kernel(const SbInst* inst, u32
   constexpr u32 T = SC_T, G = 1u << T;
   __shared__ Sum128 red[SC_T * 3 * 32];
   __shared__ u64 t0s[SB_MAX_INST + 1];
+  __shared__ u64 sch[2 * T];
   for (u32 i = threadIdx.x; i <= ninst; i += blockDim.x) t0s[i] = i < ninst ? inst[i].tile0 : ntiles;
   __syncthreads();
   const u64 q = M.q;
@@ -503,11 +521,7 @@ __global__ void __launch_bounds__(256, 2) sb_pass_kernel(const SbInst* inst, u32
     const SbInst I = inst[lo];
     const u64 ng = I.L / G, gbase = (tile - t0s[lo]) * SB_TILE_GROUPS;
     u64 c[T], cp[T];
-#pragma unroll
-    for (u32 t = 0; t < T; t++) {
-      c[t] = sb_challenge(seed, round, I.id, I.j + t, q);
-      cp[t] = shoup_dev(c[t], q);
-    }
+    shared_challenges<T>(sch, [&](u32 t) { return sb_challenge(seed, round, I.id, I.j + t, q); }, q, c, cp);
     ScAcc<LAZY> acc[T][3];
 #pragma unroll
     for (u32 t = 0; t < T; t++)
@@ -538,6 +552,7 @@ __global__ void __launch_bounds__(1024) sb_tail_kernel(const SbInst* inst, ModQ 
                                                        u32 nrmax) {
   extern __shared__ u64 v[];
   __shared__ Sum128 red[3 * 32];
+  __shared__ u64 sch[2];
   const u32 i = blockIdx.x;
   const SbInst I = inst[i];
   const u64 q = M.q;
@@ -560,8 +575,13 @@ __global__ void __launch_bounds__(1024) sb_tail_kernel(const SbInst* inst, ModQ 
     ScAcc<LAZY> tri[3] = {a0, a1, a2};
     const u64 r = block_totals<LAZY, 3>(M, tri, red);
     if (threadIdx.x < 3) sums[((u64)i * nrmax + j) * 3 + threadIdx.x] = r;
-    const u64 c = sb_challenge(seed, round, i, j, q), cp = shoup_dev(c, q);
+    if (threadIdx.x == 0) {
+      const u64 cv = sb_challenge(seed, round, i, j, q);
+      sch[0] = cv;
+      sch[1] = shoup_dev(cv, q);
+    }
     __syncthreads();
+    const u64 c = sch[0], cp = sch[1];
     for (u64 e = threadIdx.x; e < h; e += blockDim.x) v[e] = fold1(v[e], v[e + h], c, cp, q);
     __syncthreads();
     cur = h;
@@ -927,7 +947,8 @@ static int sumcheck_passes(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, c
     u64 g = (groups + 255) / 256;
     return (unsigned)(g < want ? (g ? g : 1) : want);
   };
-  if (L > SC_TAIL) {
+  auto pass_ok = [d](u64 len) { return len > SC_TAIL_ONE && (len >> SC_T) >= d; };
+  if (pass_ok(L)) {
     // rounds 0..3 on the tensor cores when the shapes allow; the CUDA-core
     // pass then runs only if a witness value did not fit the byte limbs
     const bool tc = B.gram && nc_gram_ok(w, rows, L, M.q);
@@ -944,7 +965,7 @@ static int sumcheck_passes(RowSet w, u32 rows, u64 nlen, u32 d, const ModQ& M, c
     to_a = false;
     L >>= SC_T;
     j = SC_T;
-    while (L > SC_TAIL) {
+    while (pass_ok(L)) {
       u64* out = to_a ? B.a : B.b;
       const u64 so = to_a ? sa : sb;
       dim3 gr(grid_for(L / (1u << SC_T), 2 * rows), 2 * rows);
