@@ -602,21 +602,25 @@ __global__ void __launch_bounds__(256, 2)
       u32 w4[4];
 #pragma unroll
       for (u32 g = 0; g < 4; g++) {
-        u32 packed = 0;
+        u32 tq[4];  // centred value + 128: below 256 iff it fits int8
 #pragma unroll
         for (u32 e = 0; e < 4; e++) {
           const ulonglong2 v2 = wv[4 * g + e];
-          long long cv;  // centred value
           if (nar) {
-            cv = (long long)(int)(u32)(p ? (v2.x >> 32) : v2.x);
+            const int cv = (int)(u32)(p ? (v2.x >> 32) : v2.x);
+            bad |= (cv > 127) | (cv < -128);
+            tq[e] = (u32)cv + 128u;
           } else {
             const u64 v = p ? v2.y : v2.x;
-            cv = v > half_q ? (long long)v - (long long)q : (long long)v;
+            const long long cv = v > half_q ? (long long)v - (long long)q : (long long)v;
+            const unsigned long long tb = (unsigned long long)(cv + 128);
+            bad |= tb > 255ULL;
+            tq[e] = (u32)tb;
           }
-          const unsigned long long tb = (unsigned long long)(cv + 128);  // below 256 iff it fits int8
-          bad |= tb > 255ULL;
-          packed |= ((u32)tb & 0xffu) << (8 * e);
         }
+        // low bytes of the four values, e in byte e
+        const u32 packed =
+            __byte_perm(__byte_perm(tq[0], tq[1], 0x0040), __byte_perm(tq[2], tq[3], 0x0040), 0x5410);
         w4[g] = packed ^ 0x80808080u;
       }
       *(uint4*)(B + nkq * (PU_POS * 16) + (2 * np2 + p) * 16) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
@@ -772,28 +776,29 @@ __global__ void __launch_bounds__(512, 1)
       u32 l0[4], l1[4], l2[4];
 #pragma unroll
       for (u32 g = 0; g < 4; g++) {
-        u32 a0 = 0, a1 = 0, a2 = 0;
+        u32 wq[4];
 #pragma unroll
         for (u32 e = 0; e < 4; e++) {
           const ulonglong2 v2 = wv[4 * g + e];
           // centred value + 0x808080: its bytes are the signed limbs + 128 when
           // the value lies in [-0x808080, 0x7f7f7f] (three balanced base-256 digits)
-          u64 tb;
           if (nar) {
-            tb = (u64)((long long)(int)(u32)(p ? (v2.x >> 32) : v2.x) + 0x808080LL);
+            const int v = (int)(u32)(p ? (v2.x >> 32) : v2.x);
+            bad |= (v > 0x7f7f7f) | (v < -0x808080);  // the value needs a fourth limb
+            wq[e] = ((u32)v + 0x808080u) ^ 0x808080u;
           } else {
             const u64 v = p ? v2.y : v2.x;
-            tb = v + 0x808080ULL - (v > half_q ? q : 0);
+            const u64 tb = v + 0x808080ULL - (v > half_q ? q : 0);
+            bad |= (tb >> 24) != 0;
+            wq[e] = (u32)tb ^ 0x808080u;
           }
-          bad |= (tb >> 24) != 0;  // the value needs a fourth limb
-          const u32 w = (u32)tb ^ 0x808080u;
-          a0 |= (w & 0xffu) << (8 * e);
-          a1 |= ((w >> 8) & 0xffu) << (8 * e);
-          a2 |= ((w >> 16) & 0xffu) << (8 * e);
         }
-        l0[g] = a0;
-        l1[g] = a1;
-        l2[g] = a2;
+        // limb planes of the four values: byte l of wq[0..3]
+        const u32 lo01 = __byte_perm(wq[0], wq[1], 0x5140), lo23 = __byte_perm(wq[2], wq[3], 0x5140);
+        const u32 hi01 = __byte_perm(wq[0], wq[1], 0x0062), hi23 = __byte_perm(wq[2], wq[3], 0x0062);
+        l0[g] = __byte_perm(lo01, lo23, 0x5410);
+        l1[g] = __byte_perm(lo01, lo23, 0x7632);
+        l2[g] = __byte_perm(hi01, hi23, 0x5410);
       }
       const u32 off = SU_A + nkq * (SU_POS * 16) + (2 * np2 + p) * 16;
       *(uint4*)(stage + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
