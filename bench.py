@@ -71,6 +71,8 @@ def parse():
                     help="log2 of the coefficients per NTT batch (28 = 2 GiB per buffer)")
     ap.add_argument("--no-tune-compare", action="store_true",
                     help="skip the runs with the untuned (default) kernel schedules")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch every proof's kernels directly (no CUDA-graph replay)")
     return ap.parse_args()
 
 
@@ -260,6 +262,11 @@ def run_ours(args):
     ctx = api.Context(params, crs_seed=1, device=local)
     S = args.slots
     slots = [api.Prover(ctx) for _ in range(S)]
+    # each slot replays a captured CUDA graph of its proof (the seed changed per
+    # proof) unless --no-graph; the graphs are captured again after a schedule
+    # change, so the default-vs-tuned comparison below compares like with like
+    for pr in slots:
+        pr.set_graph(not args.no_graph)
     words = ctx.proof_bytes // 8
     proofs = [torch.empty(words, dtype=torch.int64, device="cuda") for _ in range(S)]
     gen = torch.Generator(device="cuda")
@@ -333,7 +340,32 @@ def run_ours(args):
     elapsed_ms = max_over_ranks(elapsed_ms)
     total = S * args.steps * world
     value = total / (elapsed_ms / 1000.0)
+    # the same batches with direct launches, for the graph-replay comparison
+    direct_value = None
+    if not args.no_graph and args.steps > 0:
+        for pr in slots:
+            pr.set_graph(False)
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(main)
+        batch(-300, ev)  # warm
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(main)
+        nd = max(1, min(args.steps, 3))
+        for sidx in range(nd):
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(main)
+            batch(-400 - sidx, ev)
+        b.record(main)
+        b.synchronize()
+        direct_value = S * nd / (a.elapsed_time(b) / 1000.0)
+    # per-phase times come from a proof launched directly (replays keep none)
+    slots[0].set_graph(False)
+    slots[0].enqueue(seed=replicas.proof_seed(rank, 0, 0, S), d_proof=proofs[0], d_witness=witnesses[0])
+    slots[0].sync()
     timing = slots[0].timing()
+    for pr in slots:
+        pr.set_graph(not args.no_graph)
 
     # correctness spot checks after the timed region: the last batch's first
     # proof verifies on the CPU, and the committed oracle digest's statement
@@ -383,6 +415,12 @@ def run_ours(args):
     # then latency mode: each round's projection and each commitment's
     # statement rows run on a second stream beside the main chain
     plain = plain_run(True, False) if args.plain_proofs else []
+    plain_ms_graph = plain_ms_direct = None
+    if plain and not args.no_graph:
+        plain_ms_graph = statistics.mean(plain)
+        slots[0].set_graph(False)
+        plain_ms_direct = statistics.mean(plain_run(True, False))
+        slots[0].set_graph(True)
     slots[0].set_overlap(False)
     plain_value = 1000.0 / statistics.mean(plain) if plain else None
 
@@ -487,6 +525,13 @@ def run_ours(args):
             "roofline": roofline_ck(traced, sum(serial) if serial else None,
                                     args.preset == "A0" and not args.wit_log),
             "ntt_roofline": roofline_ntt(ntt, peak, kind),
+            "graphs": {"value_graph_replay": None if args.no_graph else value / world,
+                       "value_direct_launches": (value / world) if args.no_graph else direct_value,
+                       "graph_over_direct": (value / world) / direct_value if direct_value else None,
+                       "plain_ms_graph_replay": plain_ms_graph,
+                       "plain_ms_direct_launches": plain_ms_direct,
+                       "note": "each slot captures its proof's launch sequence once and replays it with "
+                               "the seed changed (salsaa_prover_set_graph); same proof bytes"},
             "tuning": {"table_entries": tuned_entries,
                        "value_default_schedules": default_value,
                        "value_tuned_schedules": value / world,

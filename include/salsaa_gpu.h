@@ -182,6 +182,14 @@ int salsaa_prover_enqueue_host_i8(salsaa_prover* pr, uint64_t seed, const int8_t
  * (results unchanged): lower latency for a proof alone on the GPU, slightly
  * lower throughput when many slots already fill it.  Off by default. */
 int salsaa_prover_set_overlap(salsaa_prover* pr, int on);
+/* No reference counterpart.  With on != 0 the slot captures a proof's launch
+ * sequence as a CUDA graph on its first enqueue for a (witness, proof) buffer
+ * pair and replays it for later proofs into the same buffers, changing only
+ * the seed (fewer launch gaps; results unchanged).  A new buffer pair is
+ * captured again; if a capture fails the slot launches directly.  Per-phase
+ * times (salsaa_prover_timing) are not kept for replayed proofs, and replay
+ * is skipped while salsaa_trace_enable is on.  Off by default. */
+int salsaa_prover_set_graph(salsaa_prover* pr, int on);
 /* 1 while the last enqueued proof runs, 0 when done, negative on error. */
 int salsaa_prover_query(salsaa_prover* pr);
 int salsaa_prover_sync(salsaa_prover* pr);

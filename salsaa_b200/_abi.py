@@ -69,6 +69,7 @@ DEVICE_SYMBOLS = {
     "salsaa_prove": (INT, [VP, U64, VP, VP, U64]),
     "salsaa_verify": (INT, [VP, U64, VP, U64, VP]),
     "salsaa_prover_set_overlap": (INT, [VP, INT]),
+    "salsaa_prover_set_graph": (INT, [VP, INT]),
     "salsaa_ntt": (INT, [VP, VP, U64, U64, U64, INT, INT, VP]),
     "salsaa_poly_mul": (INT, [VP, VP, VP, U64, U64, U64, VP]),
     "salsaa_ntt_multi": (INT, [ctypes.POINTER(VP), ctypes.POINTER(VP), ctypes.POINTER(U64), ctypes.c_uint32, U64,

@@ -187,6 +187,11 @@ class Prover:
         for a proof alone on the GPU; off by default)."""
         _check(lib().salsaa_prover_set_overlap(self.h, 1 if on else 0), "prover_set_overlap")
 
+    def set_graph(self, on=True):
+        """Replay a captured CUDA graph of the proof for later proofs into
+        the same buffers (fewer launch gaps; off by default)."""
+        _check(lib().salsaa_prover_set_graph(self.h, 1 if on else 0), "prover_set_graph")
+
     def query(self):
         rc = lib().salsaa_prover_query(self.h)
         if rc < 0:

@@ -5,6 +5,7 @@
 #include <cstdlib>
 #include <type_traits>
 #include <map>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -209,6 +210,12 @@ __global__ void __launch_bounds__(256) ntt_kernel(const u64* in, u64* out, u64 c
 // <ctas_per_sm>" per line, loaded from SALSAA_TUNE_FILE or from
 // tune_table.txt beside the library the first time a transform launches.
 // ---------------------------------------------------------------------------
+// Bumped by every change of the schedule table (loads, sets, resets), so a
+// captured CUDA graph of a proof, which holds the kernels chosen at capture
+// time, is captured again after a change.
+std::atomic<unsigned long long> g_sched_gen{0};
+unsigned long long schedule_generation() { return g_sched_gen.load(std::memory_order_acquire); }
+
 namespace {
 constexpr int TUNE_LOGN = 14;
 std::mutex g_tune_mu;
@@ -221,6 +228,7 @@ int tune_index_ok(u32 logn) { return logn < (u32)TUNE_LOGN; }
 int tune_load_locked(const char* path) {
   FILE* f = fopen(path, "r");
   if (!f) return -1;
+  g_sched_gen.fetch_add(1, std::memory_order_acq_rel);
   char line[256];
   int n = 0;
   while (fgets(line, sizeof line, f)) {
@@ -275,6 +283,7 @@ int ntt_tune_set(u32 logn, bool incomplete, bool inverse, bool wide, bool large,
   std::lock_guard<std::mutex> lk(g_tune_mu);
   tune_default_locked();
   g_tune[logn][incomplete][inverse][wide][large] = NttChoice{(uint8_t)variant, (uint8_t)ctas_per_sm};
+  g_sched_gen.fetch_add(1, std::memory_order_acq_rel);
   return 0;
 }
 
@@ -302,12 +311,14 @@ int fold_tune_set(int variant) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   tune_default_locked();
   g_fold_variant = variant;
+  g_sched_gen.fetch_add(1, std::memory_order_acq_rel);
   return 0;
 }
 
 void ntt_tune_reset() {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_loaded = true;  // defaults, and no automatic load afterwards
+  g_sched_gen.fetch_add(1, std::memory_order_acq_rel);
   g_fold_variant = 0;
   for (auto& a : g_tune)
     for (auto& b : a)

@@ -51,6 +51,8 @@ int ntt_tune_load(const char* path);  // number of entries read, or < 0
 void ntt_tune_reset();
 // Fold products (launch_fold): 0 = integer Shoup products, 1 = FP64 (q < 2^50).
 int fold_choice();
+// Changes whenever the schedule table changes (see g_sched_gen).
+unsigned long long schedule_generation();
 int fold_tune_set(int variant);
 int ntt_error_check();  // a bounded wait of the pipelined transform gave up
 

@@ -109,6 +109,8 @@ extern "C" int salsaa_trace_read(const char* name, double* total_ms, double* tot
   return 0;
 }
 
+static bool salsaa_trace_active() { return g_trace_on.load(std::memory_order_relaxed) != 0; }
+
 static std::atomic<uint64_t> g_launches{0};
 void salsaa_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 extern "C" uint64_t salsaa_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
@@ -422,10 +424,23 @@ struct salsaa_prover {
   int ev_phase[MAX_EVENTS];
   int nev = 0;
   int last_rc = 0;
+  // CUDA-graph replay (salsaa_prover_set_graph): the proof's launch sequence
+  // captured once for one (witness, proof) buffer pair; later proofs update
+  // the seed kernel's argument and relaunch the executable graph.
+  bool use_graph = false, capturing = false, graph_failed = false;
+  cudaGraph_t graph = nullptr;  // kept with its executable: the seed node belongs to it
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraphNode_t gseed = nullptr;
+  cudaKernelNodeParams gseed_p{};
+  const u64* g_witness = nullptr;
+  u64* g_proof = nullptr;
+  u64 g_kernels = 0;
+  unsigned long long g_sched = 0;  // schedule table generation at capture
+  bool g_overlap = false;          // overlap setting at capture
 };
 
 static int mark(salsaa_prover* pr, int phase) {
-  if (pr->nev >= MAX_EVENTS) return 0;
+  if (pr->capturing || pr->nev >= MAX_EVENTS) return 0;  // phase times are not kept for graph replays
   cudaError_t e = cudaEventRecord(pr->ev[pr->nev], pr->st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "event record");
   pr->ev_phase[pr->nev++] = phase;
@@ -570,10 +585,13 @@ extern "C" int salsaa_prover_create(salsaa_ctx* c, salsaa_prover** out) {
   return 0;
 }
 
+static void drop_graph(salsaa_prover* pr);
+
 extern "C" void salsaa_prover_destroy(salsaa_prover* pr) {
   if (!pr) return;
   cudaSetDevice(pr->ctx->device);
   if (pr->st) cudaStreamSynchronize(pr->st);
+  drop_graph(pr);
   pr->mem.release();
   if (pr->own_proof) cudaFree(pr->own_proof);
   if (pr->header_pinned) cudaFreeHost(pr->header_pinned);
@@ -924,13 +942,115 @@ static int enqueue_impl(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* 
   return 0;
 }
 
+extern "C" int salsaa_prover_set_graph(salsaa_prover* pr, int on) {
+  if (!pr) return salsaa_set_error(-1, "prover_set_graph: null argument");
+  pr->use_graph = on != 0;
+  return 0;
+}
+
+static void drop_graph(salsaa_prover* pr) {
+  if (pr->gexec) cudaGraphExecDestroy(pr->gexec);
+  if (pr->graph) cudaGraphDestroy(pr->graph);
+  pr->graph = nullptr;
+  pr->gexec = nullptr;
+  pr->gseed = nullptr;
+  pr->g_witness = nullptr;
+  pr->g_proof = nullptr;
+  pr->g_kernels = 0;
+}
+
+// Captures the proof's launch sequence on the slot's stream (relaxed mode:
+// the launchers' attribute calls are allowed), finds the seed kernel's node
+// and instantiates the graph.  Nothing runs while capturing.  Returns 0, or
+// nonzero when the capture could not be made (the caller then launches
+// directly; the CUDA error state is cleared).
+static int capture_graph(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* proof) {
+  drop_graph(pr);
+  const uint64_t counted = g_launches.load(std::memory_order_relaxed);  // capturing launches nothing
+  cudaError_t e = cudaStreamBeginCapture(pr->st, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  pr->capturing = true;
+  const int rc = enqueue_impl(pr, seed, d_witness, proof);
+  pr->capturing = false;
+  g_launches.fetch_sub(g_launches.load(std::memory_order_relaxed) - counted, std::memory_order_relaxed);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(pr->st, &g);
+  if (rc || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return -1;
+  }
+  size_t nn = 0;
+  int out = -1;
+  if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess) {
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess) {
+      u64 kernels = 0;
+      for (cudaGraphNode_t n : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(n, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+        kernels++;
+        cudaKernelNodeParams kp{};
+        if (cudaGraphKernelNodeGetParams(n, &kp) == cudaSuccess && kp.func == (void*)set_seed_kernel) {
+          pr->gseed = n;
+          pr->gseed_p = kp;
+        }
+      }
+      pr->g_kernels = kernels;
+      if (pr->gseed && cudaGraphInstantiate(&pr->gexec, g, 0) == cudaSuccess) out = 0;
+    }
+  }
+  pr->graph = g;
+  if (out) {
+    drop_graph(pr);
+    cudaGetLastError();
+    return -1;
+  }
+  pr->g_witness = d_witness;
+  pr->g_proof = proof;
+  pr->g_sched = schedule_generation();
+  pr->g_overlap = pr->overlap;
+  return 0;
+}
+
+// One proof, through the slot's graph when graph replay is on (captured on
+// the first call for these buffers), else by direct launches.
+static int enqueue_any(salsaa_prover* pr, u64 seed, const u64* d_witness, u64* proof) {
+  const bool graph = pr->use_graph && !pr->graph_failed && !salsaa_trace_active();
+  if (!graph) return enqueue_impl(pr, seed, d_witness, proof);
+  if (!pr->gexec || pr->g_witness != d_witness || pr->g_proof != proof || pr->g_overlap != pr->overlap ||
+      pr->g_sched != schedule_generation()) {
+    if (capture_graph(pr, seed, d_witness, proof)) {
+      pr->graph_failed = true;
+      return enqueue_impl(pr, seed, d_witness, proof);
+    }
+  } else {
+    DevState* ds = pr->ds;
+    u64 sd = seed;
+    void* args[2] = {&ds, &sd};
+    cudaKernelNodeParams kp = pr->gseed_p;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    cudaError_t e = cudaGraphExecKernelNodeSetParams(pr->gexec, pr->gseed, &kp);
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover graph: seed update");
+  }
+  pr->nev = 0;
+  cudaError_t e = cudaGraphLaunch(pr->gexec, pr->st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover graph: launch");
+  for (u64 i = 0; i < pr->g_kernels; i++) salsaa_count_launch();
+  return 0;
+}
+
 extern "C" int salsaa_prover_enqueue(salsaa_prover* pr, uint64_t seed, const uint64_t* d_witness,
                                      uint8_t* d_proof) {
   if (!pr || !d_proof) return salsaa_set_error(-1, "prover_enqueue: null argument");
   if (((uintptr_t)d_proof) & 7) return salsaa_set_error(-1, "prover_enqueue: proof buffer not 8-byte aligned");
   cudaError_t e = cudaSetDevice(pr->ctx->device);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue: cudaSetDevice");
-  pr->last_rc = enqueue_impl(pr, seed, d_witness, (u64*)d_proof);
+  pr->last_rc = enqueue_any(pr, seed, d_witness, (u64*)d_proof);
   return pr->last_rc;
 }
 
@@ -952,7 +1072,7 @@ extern "C" int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, cons
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host: witness upload");
     dw = pr->Dc;
   }
-  pr->last_rc = enqueue_impl(pr, seed, dw, (u64*)pr->own_proof);
+  pr->last_rc = enqueue_any(pr, seed, dw, (u64*)pr->own_proof);
   if (pr->last_rc) return pr->last_rc;
   e = cudaMemcpyAsync(h_proof, pr->own_proof, need, cudaMemcpyDeviceToHost, pr->st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host: proof download");
@@ -979,7 +1099,7 @@ extern "C" int salsaa_prover_enqueue_host_i8(salsaa_prover* pr, uint64_t seed, c
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: witness upload");
   pr->last_rc = launch_expand_i8(stage, n, c->P.q, pr->Dc, pr->st);
   if (pr->last_rc) return pr->last_rc;
-  pr->last_rc = enqueue_impl(pr, seed, pr->Dc, (u64*)pr->own_proof);
+  pr->last_rc = enqueue_any(pr, seed, pr->Dc, (u64*)pr->own_proof);
   if (pr->last_rc) return pr->last_rc;
   e = cudaMemcpyAsync(h_proof, pr->own_proof, need, cudaMemcpyDeviceToHost, pr->st);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: proof download");

@@ -141,3 +141,45 @@ def test_overlap_slot_matches_oracle(api, oracle, name):
         pr.sync()
         assert np.array_equal(api.to_host(buf).view(np.uint8), oracle.prove(p, 7, seed)[1])
     pr.close()
+
+
+@pytest.mark.parametrize("overlap", [False, True])
+def test_graph_replay_matches_oracle(api, oracle, cuda, overlap):
+    """A slot replaying its captured CUDA graph (the seed changed per proof,
+    queued back to back, the graph captured again for a new buffer pair and
+    for the int8 upload path) gives the oracle's proof bytes every time."""
+    torch = cuda
+    p = P.make_params(128, P.Q0, 4, 1 << 13, 2, False)
+    ctx = api.Context(p, crs_seed=7)
+    pr = api.Prover(ctx)
+    pr.set_overlap(overlap)
+    pr.set_graph(True)
+    bufs = [torch.empty(ctx.proof_bytes // 8, dtype=torch.int64, device="cuda") for _ in range(4)]
+    seeds = [21, 22, 23, 24]
+    plan = [(seeds[0], bufs[0]), (seeds[1], bufs[0]), (seeds[2], bufs[0]), (seeds[3], bufs[1])]
+    outs = []
+    for sd, b in plan:
+        pr.enqueue(sd, b)
+        pr.sync()
+        outs.append(api.to_host(b).view(np.uint8).copy())
+    for (sd, _), got in zip(plan, outs):
+        rc, want, _ = oracle.prove(p, 7, sd)
+        assert rc == 0 and np.array_equal(got, want), sd
+    # back to back without waiting: a replay queued behind a proof still running keeps its own seed
+    pr.enqueue(31, bufs[2])  # captures for bufs[2]
+    pr.enqueue(32, bufs[3])  # captures for bufs[3]
+    pr.enqueue(33, bufs[3])  # replays with a new seed while the previous proof may still run
+    pr.sync()
+    assert np.array_equal(api.to_host(bufs[2]).view(np.uint8), oracle.prove(p, 7, 31)[1])
+    assert np.array_equal(api.to_host(bufs[3]).view(np.uint8), oracle.prove(p, 7, 33)[1])
+    # the int8 upload path through the graph
+    rng = np.random.default_rng(8)
+    w8 = rng.integers(-1, 2, size=(p.init_wit_rep, p.wit_len, p.d)).astype(np.int8)
+    w = np.where(w8 < 0, p.q + w8.astype(np.int64), w8).astype(np.uint64)
+    for sd in (41, 42):
+        got = np.zeros(ctx.proof_bytes, dtype=np.uint8)
+        pr.enqueue_host_i8(sd, got, np.ascontiguousarray(w8.reshape(-1)))
+        pr.sync()
+        rc, want, _ = oracle.prove(p, 7, sd, witness=w)
+        assert rc == 0 and np.array_equal(got, want), sd
+    pr.close()
