@@ -340,6 +340,25 @@ def run_ours(args):
     elapsed_ms = max_over_ranks(elapsed_ms)
     total = S * args.steps * world
     value = total / (elapsed_ms / 1000.0)
+    # correctness spot checks after the timed region: the last batch's first
+    # proof verifies on the CPU, and the committed oracle digest's statement
+    # (witness sampled from its seed) gives the same proof bytes here
+    check = digest_check = None
+    if rank == 0 and args.steps > 0:
+        try:
+            O = _oracle()
+            pb = api.to_host(proofs[0]).view(np.uint8)
+            check = O.verify(params, 1, replicas.proof_seed(rank, args.steps - 1, 0, S), pb) == 0
+        except Exception as e:  # the checker is optional here; tests own parity
+            check = "not run: %s" % e
+        dg = committed_digest()
+        if dg and args.preset == PRESET and not args.wit_log:
+            import hashlib
+            slots[0].enqueue(seed=dg[1], d_proof=proofs[0])
+            slots[0].sync()
+            got = hashlib.sha256(api.to_host(proofs[0]).tobytes()).hexdigest()
+            digest_check = {"crs_seed": dg[0], "seed": dg[1], "sha256": got, "equals_committed": got == dg[2]}
+
     # the same batches with direct launches, for the graph-replay comparison
     direct_value = None
     if not args.no_graph and args.steps > 0:
@@ -367,24 +386,6 @@ def run_ours(args):
     for pr in slots:
         pr.set_graph(not args.no_graph)
 
-    # correctness spot checks after the timed region: the last batch's first
-    # proof verifies on the CPU, and the committed oracle digest's statement
-    # (witness sampled from its seed) gives the same proof bytes here
-    check = digest_check = None
-    if rank == 0 and args.steps > 0:
-        try:
-            O = _oracle()
-            pb = api.to_host(proofs[0]).view(np.uint8)
-            check = O.verify(params, 1, replicas.proof_seed(rank, args.steps - 1, 0, S), pb) == 0
-        except Exception as e:  # the checker is optional here; tests own parity
-            check = "not run: %s" % e
-        dg = committed_digest()
-        if dg and args.preset == PRESET and not args.wit_log:
-            import hashlib
-            slots[0].enqueue(seed=dg[1], d_proof=proofs[0])
-            slots[0].sync()
-            got = hashlib.sha256(api.to_host(proofs[0]).tobytes()).hexdigest()
-            digest_check = {"crs_seed": dg[0], "seed": dg[1], "sha256": got, "equals_committed": got == dg[2]}
 
     # plain path: one proof at a time on one slot.  First with every kernel on
     # the slot's stream: the per-kernel trace runs there, where nothing else
