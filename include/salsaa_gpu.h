@@ -175,7 +175,10 @@ int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, const uint64_t*
  * eighth of the bytes; the slot expands them on the device.  The witness of
  * the reference's relation is short (random_bounded, ternary in every
  * parameter set), so it always fits.  Proof bytes equal those of
- * salsaa_prover_enqueue_host for the same residues. */
+ * salsaa_prover_enqueue_host for the same residues.  The upload runs on the
+ * slot's own copy stream into one of two staging buffers (allocated on the
+ * first call), so it may start while the slot's previous proof still runs;
+ * the same buffer rules as salsaa_prover_enqueue_host apply. */
 int salsaa_prover_enqueue_host_i8(salsaa_prover* pr, uint64_t seed, const int8_t* h_witness, uint8_t* h_proof);
 /* No reference counterpart.  With on != 0 the slot's later proofs run each
  * round's projection on a second stream beside the norm-check sumcheck

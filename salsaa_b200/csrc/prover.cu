@@ -437,6 +437,12 @@ struct salsaa_prover {
   u64 g_kernels = 0;
   unsigned long long g_sched = 0;  // schedule table generation at capture
   bool g_overlap = false;          // overlap setting at capture
+  // int8 witness uploads, double-buffered: the next proof's witness crosses
+  // PCIe on cp_st into stage8[k % 2] while the current proof computes
+  cudaStream_t cp_st = nullptr;
+  int8_t* stage8[2] = {nullptr, nullptr};
+  cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  u64 n_i8 = 0;  // int8 uploads so far
 };
 
 static int mark(salsaa_prover* pr, int phase) {
@@ -591,7 +597,14 @@ extern "C" void salsaa_prover_destroy(salsaa_prover* pr) {
   if (!pr) return;
   cudaSetDevice(pr->ctx->device);
   if (pr->st) cudaStreamSynchronize(pr->st);
+  if (pr->cp_st) cudaStreamSynchronize(pr->cp_st);
   drop_graph(pr);
+  for (int i = 0; i < 2; i++) {
+    if (pr->stage8[i]) cudaFree(pr->stage8[i]);
+    if (pr->ev_copied[i]) cudaEventDestroy(pr->ev_copied[i]);
+    if (pr->ev_free[i]) cudaEventDestroy(pr->ev_free[i]);
+  }
+  if (pr->cp_st) cudaStreamDestroy(pr->cp_st);
   pr->mem.release();
   if (pr->own_proof) cudaFree(pr->own_proof);
   if (pr->header_pinned) cudaFreeHost(pr->header_pinned);
@@ -1079,9 +1092,11 @@ extern "C" int salsaa_prover_enqueue_host(salsaa_prover* pr, uint64_t seed, cons
   return 0;
 }
 
-// The signed bytes are staged in the slot-form witness buffer (an eighth of
-// its size), expanded into the coefficient-form buffer, and overwritten by
-// the proof's first forward transform, all in stream order.
+// The signed bytes cross PCIe on the slot's upload stream into one of two
+// staging buffers (an eighth of the u64 witness each), so the next proof's
+// witness uploads while the current proof runs; the slot's stream waits for
+// its upload, expands it into the coefficient-form buffer and releases the
+// staging buffer for the upload after next.
 extern "C" int salsaa_prover_enqueue_host_i8(salsaa_prover* pr, uint64_t seed, const int8_t* h_witness,
                                              uint8_t* h_proof) {
   if (!pr || !h_proof || !h_witness) return salsaa_set_error(-1, "prover_enqueue_host_i8: null argument");
@@ -1094,11 +1109,26 @@ extern "C" int salsaa_prover_enqueue_host_i8(salsaa_prover* pr, uint64_t seed, c
     if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: proof buffer");
   }
   const u64 n = c->P.init_wit_rep * c->L * c->d;
-  int8_t* stage = (int8_t*)pr->Ds;
-  e = cudaMemcpyAsync(stage, h_witness, n, cudaMemcpyHostToDevice, pr->st);
+  if (!pr->cp_st) {  // the upload stream, its two staging buffers and their events, on first use
+    e = cudaStreamCreateWithFlags(&pr->cp_st, cudaStreamNonBlocking);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+      e = cudaMalloc(&pr->stage8[i], (n + 15) & ~(u64)15);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pr->ev_copied[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&pr->ev_free[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: upload buffers");
+  }
+  // upload k into stage8[k % 2] once the expansion of upload k - 2 has read it
+  const int b = (int)(pr->n_i8++ & 1);
+  e = cudaStreamWaitEvent(pr->cp_st, pr->ev_free[b], 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(pr->stage8[b], h_witness, n, cudaMemcpyHostToDevice, pr->cp_st);
+  if (e == cudaSuccess) e = cudaEventRecord(pr->ev_copied[b], pr->cp_st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(pr->st, pr->ev_copied[b], 0);
   if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: witness upload");
-  pr->last_rc = launch_expand_i8(stage, n, c->P.q, pr->Dc, pr->st);
+  pr->last_rc = launch_expand_i8(pr->stage8[b], n, c->P.q, pr->Dc, pr->st);
   if (pr->last_rc) return pr->last_rc;
+  e = cudaEventRecord(pr->ev_free[b], pr->st);
+  if (e != cudaSuccess) return salsaa_set_cuda_error(e, "prover_enqueue_host_i8: stage release");
   pr->last_rc = enqueue_any(pr, seed, pr->Dc, (u64*)pr->own_proof);
   if (pr->last_rc) return pr->last_rc;
   e = cudaMemcpyAsync(h_proof, pr->own_proof, need, cudaMemcpyDeviceToHost, pr->st);
