@@ -166,10 +166,19 @@ __device__ __forceinline__ void ck_umma_body(const uint8_t* __restrict__ tk8, co
     const u32 st = v / (2 * CKU_ATILE / 16), o = v % (2 * CKU_ATILE / 16);
     *(uint4*)(smem + st * stage_bytes + o * 16) = make_uint4(0, 0, 0, 0);
   }
+  // converter tasks: TS task slots per chunk (kp in groups of 4, elements in
+  // quads).  When two groups of TS threads fit, group g takes the chunks
+  // c = g mod 2, so few witness rows still keep many loads in flight.  At
+  // most two groups: then each stage (c & 1) and its two barriers belong to
+  // one group, whose chunks pass them in order; with more groups a group
+  // could wait on a stage barrier more than one phase ahead, where a parity
+  // wait cannot tell the phases apart.
+  const u32 nkpw = 2 * vrows, kpb = (nkpw + 3) / 4, TS = 32 * kpb * (CKU_CHUNK / 32);
+  const u32 NG = CKU_CONV / TS >= 2 ? 2 : 1;
   if (tid == 0) {
     for (int i = 0; i < 2; i++) {
       umma::mbar_init(&key_full[i], 1);
-      umma::mbar_init(&a_full[i], CKU_CONV);
+      umma::mbar_init(&a_full[i], TS);
       umma::mbar_init(&done_bar[i], 1);
     }
     last_commit = 0xffffffffu;
@@ -185,19 +194,18 @@ __device__ __forceinline__ void ck_umma_body(const uint8_t* __restrict__ tk8, co
   const u32 tmem = tslot;
   bool ok = true;
 
-  if (warp < CKU_CONV / 32) {
-    // witness task t: (i4lo, kp within a group of 8, kp group, i4hi); kp = (virtual row, part).
-    // One task per thread (2 CKU_CHUNK kpb <= 384 tasks), the same in every
-    // chunk: its source (chunk 0) and shared-memory offset are computed once.
-    // Four register buffers hold the loads of chunks c .. c + 3, so each
-    // thread keeps four chunks of witness loads in flight.
-    const u32 nkpw = 2 * vrows, kpb = (nkpw + 7) / 8;
-    const u32 t = tid;
-    const u32 i4lo = t & 3, kpi = (t >> 2) & 7, rest = t >> 5;
-    const u32 kp = kpi + 8 * (rest % kpb), i4hi = rest / kpb;
-    const bool tval = t < 2 * CKU_CHUNK * kpb && kp < nkpw;
+  if (tid < NG * TS) {
+    // witness task t of group gi: (i4lo, kp within a group of 4, i4mid, kp
+    // group, i4hi); kp = (virtual row, part).  The same task in every chunk
+    // of the group: its source (chunk 0) and shared-memory offset are
+    // computed once.  Four register buffers hold the loads of the group's
+    // next four chunks.
+    const u32 gi = tid / TS, t = tid % TS;
+    const u32 i4lo = t & 3, kpi = (t >> 2) & 3, i4mid = (t >> 4) & 1, rest = t >> 5;
+    const u32 kp = kpi + 4 * (rest % kpb), i4hi = rest / kpb;
+    const bool tval = kp < nkpw;
     const u32 v = kp >> 1, part = kp & 1, k = tval ? v % rows : 0, g = tval ? v / rows : 0;
-    const u32 i4 = i4hi * 4 + i4lo;  // elements 4 * i4 .. + 3 of the chunk
+    const u32 i4 = (i4hi * 2 + i4mid) * 4 + i4lo;  // elements 4 * i4 .. + 3 of the chunk
     const u64* tsrc = w.p[k] + (i0 + (u64)g * bt + i4 * 4) * d + part * n + s0;
     const u32 toff = (i4 >> 2) * (128 * 16) + (kp * 7) * 16 + (i4 & 3) * 4;
     uint4 wb[4][4];
@@ -227,25 +235,25 @@ __device__ __forceinline__ void ck_umma_body(const uint8_t* __restrict__ tk8, co
         for (u32 b = 0; b < 7; b++) *(u32*)(A + sg * CKU_ATILE + toff + b * 16) = p[b];
       }
     };
-    // chunk c: stage c & 1 (last read by the MMAs of chunk c - 2), loads in
-    // buffer c & 3, refilled with chunk c + 4 once stashed
+    // chunk c = gi + NG m: stage c & 1 (last read by the MMAs of chunk c - 2),
+    // loads in buffer m & 3, refilled with chunk c + 4 NG once stashed
     auto step = [&](u32 c, uint4 (&wv)[4]) -> bool {
       const u32 st = c & 1;
       if (c >= 2 && !umma::mbar_wait(&done_bar[st], ((c - 2) >> 1) & 1, err, 1)) return false;
       stash(st, wv);
-      if (c + 4 < nchunks) fetch(c + 4, wv);
+      if (c + 4 * NG < nchunks) fetch(c + 4 * NG, wv);
       umma::fence_proxy_async();
       umma::mbar_arrive(&a_full[st]);
       return true;
     };
 #pragma unroll
     for (u32 b = 0; b < 4; b++)
-      if (b < nchunks) fetch(b, wb[b]);
-    for (u32 c = 0; c < nchunks; c += 4) {
+      if (gi + b * NG < nchunks) fetch(gi + b * NG, wb[b]);
+    for (u32 c = gi; c < nchunks; c += 4 * NG) {
       if (!(ok = step(c, wb[0]))) break;
-      if (c + 1 < nchunks && !(ok = step(c + 1, wb[1]))) break;
-      if (c + 2 < nchunks && !(ok = step(c + 2, wb[2]))) break;
-      if (c + 3 < nchunks && !(ok = step(c + 3, wb[3]))) break;
+      if (c + NG < nchunks && !(ok = step(c + NG, wb[1]))) break;
+      if (c + 2 * NG < nchunks && !(ok = step(c + 2 * NG, wb[2]))) break;
+      if (c + 3 * NG < nchunks && !(ok = step(c + 3 * NG, wb[3]))) break;
     }
   } else if (warp == CKU_CONV / 32 && lane == 0) {
     // key tiles of both slots, one bulk copy per chunk, into the stage freed
